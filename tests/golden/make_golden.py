@@ -1,0 +1,252 @@
+"""Generate golden vectors by running the UNMODIFIED reference on seeded synthetic inputs.
+
+Run in a container that has the reference checkout (default /root/reference):
+
+    python tests/golden/make_golden.py [--reference /root/reference]
+
+The reference's batched engine and stepper import ``cupy``; this script puts
+``oracle/cupy_standin`` first on ``sys.path`` so they run on NumPy, with the
+single CUDA kernel they launch restated by ``oracle.forces``.  The K1 arithmetic
+is pinned independently by ``DXGrid.batch_interpolate`` / ``batch_gradient``
+(reference code with the same +-h/2 central difference).
+
+Outputs (small .npz files next to this script) hold the inputs that are cheap
+to store, SHA-256 digests of the grids (rebuilt deterministically from
+``pystarc_b200.synth`` by the tests) and the reference's outputs.
+"""
+
+from __future__ import annotations
+
+import argparse
+import contextlib
+import hashlib
+import io
+import json
+import math
+import sys
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REPO = HERE.parents[1]
+
+
+def grid_digest(grids):
+    h = hashlib.sha256()
+    for g in grids:
+        h.update(np.ascontiguousarray(np.asarray(g.data, dtype=np.float32)).tobytes())
+        h.update(np.asarray(g.origin, dtype=np.float64).tobytes())
+        h.update(np.asarray(g.delta, dtype=np.float64).tobytes())
+    return h.hexdigest()
+
+
+def system_digest(s):
+    return grid_digest(list(s.elec_grids) + list(s.born_grids) + list(s.lig_born_grids))
+
+
+def quiet():
+    return contextlib.redirect_stdout(io.StringIO())
+
+
+def ref_grid(DXGrid, g):
+    return DXGrid(np.asarray(g.origin, dtype=float), np.asarray(g.delta, dtype=float),
+                  np.asarray(g.data, dtype=np.float64))
+
+
+def ref_molecules(mod, s):
+    Atom, Molecule = mod.Atom, mod.Molecule
+
+    def mk(name, pos, q, r):
+        return Molecule(name, [Atom(index=i + 1, name="A", x=float(p[0]), y=float(p[1]), z=float(p[2]),
+                                    charge=float(c), radius=float(rr)) for i, (p, c, rr) in enumerate(zip(pos, q, r))])
+
+    return mk("receptor", s.rec_pos, s.rec_q, s.rec_r), mk("ligand", s.lig_pos, s.lig_q, s.lig_r)
+
+
+def make_engine(ref, s, multipole=True):
+    from pystarc.forces.gpu_batch_engine import GPUBatchForceEngine
+    from pystarc.forces.multipole_farfield import MultipoleExpansion
+    from pystarc.forces.electrostatic.grid_force import DXGrid
+
+    mp = MultipoleExpansion(s.rec_pos, s.rec_q, debye_length=s.debye, sdie=s.sdie) if multipole else None
+    with quiet():
+        eng = GPUBatchForceEngine(
+            elec_grids=[ref_grid(DXGrid, g) for g in s.elec_grids],
+            born_grids=[ref_grid(DXGrid, g) for g in s.born_grids], alpha=s.alpha,
+            receptor_charge=float(np.sum(s.rec_q)), debye_length=s.debye, sdie=s.sdie,
+            lig_born_grids=[ref_grid(DXGrid, g) for g in s.lig_born_grids] or None,
+            rec_positions=s.rec_pos, rec_charges=s.rec_q, multipole_expansion=mp)
+    return eng
+
+
+def random_poses(n, rmin, rmax, rng):
+    v = rng.standard_normal((n, 3))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    c = v * rng.uniform(rmin, rmax, size=(n, 1))
+    u = rng.random((n, 3))
+    q = np.stack([np.sqrt(1 - u[:, 0]) * np.sin(2 * np.pi * u[:, 1]), np.sqrt(1 - u[:, 0]) * np.cos(2 * np.pi * u[:, 1]),
+                  np.sqrt(u[:, 0]) * np.sin(2 * np.pi * u[:, 2]), np.sqrt(u[:, 0]) * np.cos(2 * np.pi * u[:, 2])], 1)
+    return c, q
+
+
+def gen_k1(out):
+    from pystarc.forces.electrostatic.grid_force import DXGrid
+
+    rng = np.random.default_rng(7)
+    nx, ny, nz = 24, 20, 28
+    X, Y, Z = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    data = (np.sin(0.3 * X) * np.cos(0.2 * Y) + 0.05 * Z + 0.01 * rng.standard_normal((nx, ny, nz))).astype(np.float32)
+    origin = np.array([-3.0, 1.5, -7.25])
+    sp = np.array([0.5, 0.6, 0.4])
+    g = DXGrid(origin, np.diag(sp), data.astype(np.float64))
+    lo = origin + 0.6 * sp
+    hi = origin + (np.array([nx, ny, nz]) - 1.6) * sp
+    pts = lo + (hi - lo) * rng.random((400, 3))
+    edge = np.array([origin + 0.49 * sp, origin + (np.array([nx, ny, nz]) - 1.51) * sp, origin - 5.0,
+                     origin + (np.array([nx, ny, nz]) + 3) * sp, origin + np.array([2.0, 3.0, 4.0]) * sp])
+    pts = np.vstack([pts, edge])
+    out["k1"] = dict(data=data, origin=origin, sp=sp, points=pts, phi=g.batch_interpolate(pts),
+                     grad=g.batch_gradient(pts))
+
+
+def gen_engine(out, name, s, n_poses, rmin, rmax, seed):
+    import pystarc.forces.gpu_batch_engine as gbe
+    from pystarc.simulation.gpu_batch_simulator import GPUBatchSimulator
+
+    eng = make_engine(None, s)
+    rng = np.random.default_rng(seed)
+    c, q = random_poses(n_poses, rmin, rmax, rng)
+    sim = GPUBatchSimulator.__new__(GPUBatchSimulator)
+    R = sim._quats_to_rotmats(q)
+    body = s.lig_pos - s.lig_pos.mean(axis=0)
+    pos = np.einsum("nij,kj->nki", R, body) + c[:, None, :]
+    with quiet():
+        F, T, E = eng(pos, s.lig_q.astype(np.float64), R_matrices=R, centroids=c)
+    out[name] = dict(digest=system_digest(s), centroids=c, quats=q, R=R, positions=pos, F=F, T=T, E=E,
+                     V_factor=eng._V_factor, has_yukawa=eng._has_yukawa, n_elec=len(eng._elec_grids_gpu),
+                     n_born=len(eng._born_grids_gpu), n_lig_born=len(eng._lig_born_grids_gpu))
+
+
+def gen_physics(out):
+    from pystarc.hydrodynamics import rotne_prager as rp
+    from pystarc.simulation.gpu_batch_simulator import GPUBatchSimulator, GPUBatchResult
+    from pystarc.forces.multipole_farfield import MultipoleExpansion
+
+    rng = np.random.default_rng(11)
+    radii = np.array([1.0, 1.005, 5.0, 17.5, 20.0, 25.375])
+    out["stokes"] = dict(radii=radii, Dt=np.array([rp.stokes_translational_diffusion(r) for r in radii]),
+                         Dr=np.array([rp.stokes_rotational_diffusion(r) for r in radii]),
+                         Dt_089=np.array([rp.stokes_translational_diffusion(r, eta=0.89e-3) for r in radii]),
+                         Dr_089=np.array([rp.stokes_rotational_diffusion(r, eta=0.89e-3) for r in radii]))
+    rs = np.array([0.5, 2.0, 5.0, 20.0, 30.0, 33.9, 34.1, 50.0, 120.0])
+    rpy = []
+    for r in rs:
+        v = np.array([r, 0.3 * r, -0.2 * r]) / math.sqrt(1 + 0.09 + 0.04)
+        rpy.append(rp.rpy_offdiagonal(v, 17.5, 16.5, 0.0123, 0.0131))
+    out["rpy"] = dict(r=rs, M=np.array(rpy))
+    sim = GPUBatchSimulator.__new__(GPUBatchSimulator)
+    q = rng.standard_normal((50, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    om = rng.standard_normal((50, 3)) * np.array([[1.0]] * 25 + [[1e-12]] * 25)
+    out["quat"] = dict(q=q, omega=om, R=sim._quats_to_rotmats(q), q_new=sim._apply_rotation_gpu(q, om),
+                       shoemake=sim._random_quaternions_gpu(20, np.random.default_rng(5)),
+                       shoemake_u=np.random.default_rng(5).random((20, 3)))
+    cis = []
+    cases = [(500, 500), (50, 950), (2, 998), (0, 1000), (1000, 0), (4479, 5521), (1, 2)]
+    for nr, ne in cases:
+        res = GPUBatchResult(nr + ne, nr, ne, 0, {}, 50.0, 100.0, 0.2, 1.0, 1.0)
+        cis.append([res.reaction_probability, *res.reaction_probability_ci(0.95), *res.reaction_probability_ci(0.9),
+                    res.rate_constant(0.06, 57.449), res.rate_constant(0.06, 0.0), *res.rate_constant_ci(0.06, 57.449)])
+    out["wilson"] = dict(cases=np.array(cases), values=np.array(cis))
+    pos = rng.standard_normal((30, 3)) * 8
+    qq = rng.normal(0, 0.4, 30)
+    mp = MultipoleExpansion(pos, qq, debye_length=7.85, sdie=78.5)
+    pts = rng.standard_normal((12, 3)) * 40
+    out["multipole"] = dict(pos=pos, q=qq, Q=mp.Q, dipole=mp.dipole, quad=mp.quadrupole, fpe=mp.four_pi_eps,
+                            pts=pts, V=np.array([mp.potential(p) for p in pts]))
+
+
+def build_sim(s, n_traj, seed, max_steps, work):
+    from pystarc.simulation.gpu_batch_simulator import GPUBatchSimulator
+    from pystarc.simulation.nam_simulator import NAMParameters
+    from pystarc.hydrodynamics.rotne_prager import MobilityTensor
+    from pystarc.structures.molecules import ContactPair, ReactionCriteria
+    from pystarc.pathways.reaction_interface import ReactionInterface, PathwaySet
+    import pystarc.structures.molecules as mols
+
+    mol1, mol2 = ref_molecules(mols, s)
+    mob = MobilityTensor.from_radii(s.r_hydro_rec, s.r_hydro_lig, eta=s.eta, T=s.temperature)
+    pairs = [ContactPair(int(a), int(b), float(c)) for a, b, c in s.pairs]
+    ps = PathwaySet([ReactionInterface("stage_0", ReactionCriteria("stage_0", pairs, n_needed=s.n_needed))])
+    params = NAMParameters(n_trajectories=n_traj, max_steps=max_steps, r_start=s.r_start, r_escape=s.r_escape,
+                           seed=seed, hydrodynamic_interactions=s.hi)
+    params.max_dt = s.max_dt
+    params.checkpoint_interval = 0
+    params.convergence_interval = 0
+    params._work_dir = str(work)
+    params._kT_scale = s.temperature / 298.15
+    params._overlap_check = s.overlap
+    eng = make_engine(None, s, multipole=s.multipole)
+    with quiet():
+        sim = GPUBatchSimulator(mol1, mol2, mob, ps, params, eng)
+    return sim, mob
+
+
+def gen_run(out, name, s, n_traj, seed, max_steps):
+    with tempfile.TemporaryDirectory() as work:
+        sim, mob = build_sim(s, n_traj, seed, max_steps, work)
+        with quiet():
+            res = sim.run()
+    sd = res.sim_data
+    out[name] = dict(digest=system_digest(s), n_traj=n_traj, seed=seed, max_steps=max_steps,
+                     n_reacted=res.n_reacted, n_escaped=res.n_escaped, n_max_steps=res.n_max_steps,
+                     total_steps=int(round(res.steps_per_sec * res.elapsed_sec)), outcome=sd["outcome"],
+                     n_steps=sd["n_steps"], n_returns=sd["n_returns"], return_prob=sim._return_prob, k_b=sim._k_b,
+                     D_t=mob.relative_translational_diffusion(), D_r=mob.relative_rotational_diffusion(),
+                     ci=np.array(res.reaction_probability_ci(0.95)))
+
+
+def two_sphere_example():
+    """The reference's two-charged-spheres example (examples/two_charged_spheres) on a synthetic grid."""
+    from pystarc_b200.synth import BDSystem, sphere_dh_grid
+
+    rec_pos, lig_pos = np.zeros((2, 3)), np.zeros((2, 3))
+    q_r, q_l = np.array([1.0, 0.0]), np.array([-1.0, 0.0])
+    r_r = np.array([1.0, 0.0])
+    g = sphere_dh_grid(1.0, 1.0, (33, 33, 33), 1.0, 7.828, 78.0 * 0.000142)
+    return BDSystem("two_sphere_example", rec_pos, q_r, r_r, lig_pos, q_l, r_r.copy(), [g], [], [], [(0, 0, 2.5)], 1,
+                    r_start=10.0, r_escape=20.0, r_hydro_rec=1.005, r_hydro_lig=1.005, debye=7.828, sdie=78.0,
+                    eta=1.002e-3, alpha=0.0, hi=False, overlap=False)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default="/root/reference")
+    args = ap.parse_args()
+    sys.path.insert(0, str(REPO / "oracle" / "cupy_standin"))
+    sys.path.insert(0, str(REPO))
+    sys.path.insert(1, args.reference)
+    from pystarc_b200 import synth
+
+    out = {}
+    gen_k1(out)
+    gen_physics(out)
+    c2 = synth.config2(scale=0.3)
+    c3 = synth.config3(scale=0.25)
+    gen_engine(out, "engine_c2", c2, 96, 3.0, 40.0, 21)
+    gen_engine(out, "engine_c3", c3, 64, 4.0, 40.0, 22)
+    gen_run(out, "run_two_sphere", two_sphere_example(), 2000, 11111113, 1_000_000)
+    gen_run(out, "run_c2", c2, 160, 424242, 400)
+    gen_run(out, "run_c3", c3, 64, 515151, 150)
+    meta = {}
+    for k, v in out.items():
+        np.savez_compressed(HERE / f"{k}.npz", **{kk: np.asarray(vv) for kk, vv in v.items()})
+        meta[k] = sorted(v.keys())
+    (HERE / "MANIFEST.json").write_text(json.dumps(meta, indent=1, sort_keys=True) + "\n")
+    print("wrote", ", ".join(sorted(out)))
+
+
+if __name__ == "__main__":
+    main()

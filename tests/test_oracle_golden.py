@@ -1,0 +1,167 @@
+"""The oracle against golden vectors produced by the unmodified reference (CPU only)."""
+
+import math
+
+import numpy as np
+import pytest
+
+from oracle import physics as oph
+from oracle import stepper as ost
+from oracle.forces import OracleGrid, k1_batch_force, _interp, multipole_moments, yukawa_forces, FarField
+from oracle.philox import philox4x32_10, KeyedDraws
+from tests.helpers import golden, system, system_digest, oracle_engine, step_system, step_params
+
+
+def test_k1_matches_reference_dxgrid():
+    g = golden("k1")
+    data = g["data"].astype(np.float64)
+    pts = g["points"]
+    inv = 1.0 / g["sp"]
+    phi = _interp(data, g["origin"], inv, pts[:, 0], pts[:, 1], pts[:, 2])
+    np.testing.assert_allclose(phi, g["phi"], rtol=0, atol=1e-13)
+    # F = -q grad phi with q = -1 gives grad phi
+    f, e = k1_batch_force(pts, -np.ones(len(pts)), data, g["origin"], g["sp"], 0.0, False)
+    np.testing.assert_allclose(f, g["grad"], rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(e, -g["phi"], rtol=0, atol=1e-13)
+
+
+def test_k1_zero_charge_and_born_coefficients():
+    g = golden("k1")
+    data = g["data"].astype(np.float64)
+    pts = g["points"][:10]
+    f0, e0 = k1_batch_force(pts, np.full(10, 5e-10), data, g["origin"], g["sp"], 0.3, True)
+    assert np.all(f0 == 0) and np.all(e0 == 0)
+    fb, eb = k1_batch_force(pts, np.full(10, 0.5), data, g["origin"], g["sp"], 0.3, True)
+    fe, ee = k1_batch_force(pts, np.full(10, 1.0), data, g["origin"], g["sp"], 0.0, False)
+    np.testing.assert_allclose(fb, 0.3 * 0.25 * fe, rtol=1e-14)
+    np.testing.assert_allclose(eb, 0.3 * 0.25 * ee, rtol=1e-14)
+
+
+@pytest.mark.parametrize("name,sysname", [("engine_c2", "c2"), ("engine_c3", "c3")])
+def test_engine_matches_reference(name, sysname):
+    g = golden(name)
+    s = system(sysname)
+    assert system_digest(s) == str(g["digest"]), "synthetic system drifted from the golden fixture"
+    eng = oracle_engine(s)
+    assert len(eng.elec) == int(g["n_elec"]) and len(eng.born) == int(g["n_born"])
+    assert len(eng.lig_born) == int(g["n_lig_born"])
+    F, T, E = eng(g["positions"], s.lig_q, R_matrices=g["R"], centroids=g["centroids"])
+    scale = np.abs(g["F"]).max()
+    np.testing.assert_allclose(F, g["F"], rtol=1e-11, atol=1e-13 * scale)
+    np.testing.assert_allclose(E, g["E"], rtol=1e-11, atol=1e-12 * np.abs(g["E"]).max())
+    assert np.all(T == 0) and np.all(g["T"] == 0)
+    assert np.isclose(eng.ff.V_factor, float(g["V_factor"]), rtol=1e-15)
+
+
+def test_torque_centroid_is_consistent():
+    s = system("c2")
+    g = golden("engine_c2")
+    eng = oracle_engine(s)
+    F, T, E = eng(g["positions"], s.lig_q, g["R"], g["centroids"], torque_mode="centroid")
+    # a rigid translation of every atom by a about the same centre leaves the torque unchanged
+    assert np.all(np.isfinite(T)) and np.any(T != 0)
+    F2, T2, _ = eng(g["positions"], s.lig_q, g["R"], g["centroids"], torque_mode="zero")
+    np.testing.assert_array_equal(F, F2)
+    assert np.all(T2 == 0)
+
+
+def test_physics_constants():
+    g = golden("stokes")
+    for i, r in enumerate(g["radii"]):
+        assert math.isclose(oph.stokes_translational(r), g["Dt"][i], rel_tol=1e-15)
+        assert math.isclose(oph.stokes_rotational(r), g["Dr"][i], rel_tol=1e-15)
+        assert math.isclose(oph.stokes_translational(r, eta=0.89e-3), g["Dt_089"][i], rel_tol=1e-15)
+        assert math.isclose(oph.stokes_rotational(r, eta=0.89e-3), g["Dr_089"][i], rel_tol=1e-15)
+    g = golden("rpy")
+    for i, r in enumerate(g["r"]):
+        v = np.array([r, 0.3 * r, -0.2 * r]) / math.sqrt(1 + 0.09 + 0.04)
+        np.testing.assert_allclose(oph.rpy_offdiagonal(v, 17.5, 16.5, 0.0123, 0.0131), g["M"][i], rtol=1e-13,
+                                   atol=1e-18)
+
+
+def test_quaternion_conventions():
+    g = golden("quat")
+    np.testing.assert_array_equal(ost.rotmats(g["q"]), g["R"])
+    np.testing.assert_array_equal(ost.apply_rotation(g["q"], g["omega"]), g["q_new"])
+    np.testing.assert_array_equal(ost.shoemake(g["shoemake_u"]), g["shoemake"])
+
+
+def test_wilson_and_rate_constant():
+    g = golden("wilson")
+    for (nr, ne), v in zip(g["cases"], g["values"]):
+        n = nr + ne
+        P = nr / n if n else 0.0
+        assert P == v[0]
+        lo, hi = oph.wilson_ci(int(nr), int(ne), 0.95)
+        assert math.isclose(lo, v[1], rel_tol=1e-12, abs_tol=1e-15) and math.isclose(hi, v[2], rel_tol=1e-12)
+        lo, hi = oph.wilson_ci(int(nr), int(ne), 0.90)
+        assert math.isclose(lo, v[3], rel_tol=1e-12, abs_tol=1e-15) and math.isclose(hi, v[4], rel_tol=1e-12)
+        assert math.isclose(oph.rate_constant(P, 0.06, 57.449, 50.0, 100.0), v[5], rel_tol=1e-14)
+        assert math.isclose(oph.rate_constant(P, 0.06, 0.0, 50.0, 100.0), v[6], rel_tol=1e-14)
+
+
+def test_multipole_moments_and_farfield_potential():
+    g = golden("multipole")
+    dip, quad = multipole_moments(g["pos"], g["q"])
+    np.testing.assert_allclose(dip, g["dipole"], rtol=1e-13, atol=1e-13)
+    np.testing.assert_allclose(quad, g["quad"], rtol=1e-13, atol=1e-12)
+    ff = FarField(float(g["Q"]), 7.85, 78.5, dip, quad, float(g["fpe"]))
+    _, e = yukawa_forces(g["pts"], np.ones(len(g["pts"])), ff)
+    # the reference potential() uses r itself; the far-field uses max(r, 1): same for these points
+    np.testing.assert_allclose(e, g["V"], rtol=1e-12)
+
+
+def test_reference_known_answers():
+    """Known-answer values from the reference's own test suite (tests/test_pystarc.py)."""
+    eps = 78.0 * 0.000142
+    V = 1.0 * -1.0 / (4 * math.pi * eps)
+    assert abs(V - (-7.1847)) < 0.01  # :4027-4029
+    assert abs(V * math.exp(-10.0 / 7.828) / 10.0 - (-0.200268)) < 0.001  # :4031-4034
+    D = 1.0 / (6 * math.pi * 0.243 * 1.0)
+    assert abs(D - 0.21803) < 0.001  # :3988-3990
+    rp, kb = oph.return_prob_and_kb(10.0, 20.1, 1.0, -1.0, 7.828, 0.43371)
+    assert abs(kb - 57.5) < 1.0 and abs(rp - 0.52) < 0.03  # :4246-4263
+    assert abs(oph.CONV - 6.022e8) / 6.022e8 < 1e-3  # :4322-4325
+    assert abs(math.sqrt(2 * 0.43371 * 0.2) - 0.4169) < 0.001  # :4147-4151
+    lo, hi = oph.wilson_ci(50, 950)
+    assert 0 <= lo < 0.05 < hi <= 1
+
+
+def test_philox_known_answers():
+    """Random123 known-answer vectors for philox4x32-10."""
+    out = philox4x32_10(0, 0, 0, 0, 0, 0)
+    assert [int(x) for x in out] == [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]
+    out = philox4x32_10(0xFFFFFFFF, 0xFFFFFFFF, 0xFFFFFFFF, 0xFFFFFFFF, 0xFFFFFFFF, 0xFFFFFFFF)
+    assert [int(x) for x in out] == [0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD]
+    out = philox4x32_10(0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344, 0xA4093822, 0x299F31D0)
+    assert [int(x) for x in out] == [0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1]
+
+
+def test_keyed_draw_statistics():
+    d = KeyedDraws(99)
+    ids = np.arange(200000)
+    xi_t, xi_r = d.step_normals(np.full(ids.shape, 3), ids)
+    for x in (xi_t, xi_r):
+        assert abs(x.mean()) < 0.01 and abs(x.std() - 1) < 0.01
+    u = d.u_escape(np.zeros_like(ids), ids)
+    assert 0 <= u.min() and u.max() < 1 and abs(u.mean() - 0.5) < 0.005
+
+
+@pytest.mark.parametrize("name,sysname", [("run_two_sphere", "two_sphere"), ("run_c2", "c2"), ("run_c3", "c3")])
+def test_stepper_reproduces_reference_run_exactly(name, sysname):
+    g = golden(name)
+    s = system(sysname)
+    assert system_digest(s) == str(g["digest"])
+    ss = step_system(s)
+    assert math.isclose(ss.D_t, float(g["D_t"]), rel_tol=1e-15)
+    assert math.isclose(ss.D_r, float(g["D_r"]), rel_tol=1e-15)
+    res = ost.run(ss, step_params(s, int(g["n_traj"]), int(g["seed"]), int(g["max_steps"])), noise="pcg64")
+    assert res.return_prob == float(g["return_prob"]) and res.k_b == float(g["k_b"])
+    assert (res.n_reacted, res.n_escaped, res.n_max_steps) == (int(g["n_reacted"]), int(g["n_escaped"]),
+                                                              int(g["n_max_steps"]))
+    assert abs(res.total_steps - int(g["total_steps"])) <= 1  # reference reports steps/s x elapsed
+    np.testing.assert_array_equal(res.n_steps, g["n_steps"])
+    np.testing.assert_array_equal(res.n_returns, g["n_returns"])
+    ref_outcome = g["outcome"].copy()
+    ref_outcome[ref_outcome == 0] = 3
+    np.testing.assert_array_equal(res.status, ref_outcome)
