@@ -1,0 +1,377 @@
+"""BD steps/s of the batched rigid-body BD step on B200 (protein + small ligand workload).
+
+Workload: the synthetic protein + small-ligand system (3200-atom receptor in a
+22 A ball, +8 e; 18-atom ligand, +1 e; nested 193^3 @ 0.5 A and 129^3 @ 2 A
+FP32 electrostatic grids, matching Born grids, a 65^3 ligand Born grid), b = 60 A,
+max_dt 20 ps, 1e6 trajectories seeded on the b-sphere.  Data are synthetic
+(seeded; no structure files).
+
+One bench "step" = one launch of the persistent stepper: every live
+trajectory advances ``--inner`` BD steps (finished ones are replaced from the
+pending pool inside the launch), then finished slots are compacted.  The
+metric is the reference's BD steps/s: trajectory-steps completed / time.
+L2 is flushed (a 256 MiB write) between timed launches, outside the timed
+region.
+
+Arms:
+  default            the B200 engine (mixed precision, the headline) plus a plain
+                     FP64 measurement in the same run
+  --impl reference   the reference's batched stepper restated in NumPy (the same
+                     algorithm, its own PCG64 draw order) on all host cores
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "BD steps/sec on 1 B200, surrogate vs plain at k_on within Wilson 95% CI"
+UNIT = "BD steps/s"
+WORKLOAD = "protein+small-ligand (3200/18 atoms, 193^3+129^3 grids, 1e6 trajectories)"
+ALGO_BYTES_PER_GATHER = 224  # 7 trilinear interpolations x 8 corners x 4 B per (atom, grid)
+STATE_BYTES_PER_STEP = 128  # FP64 pose read + write and status/counters per trajectory-step
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.index), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def build_system(device):
+    from pystarc_b200 import synth
+
+    return synth.config2(n_traj=1_000_000, scale=1.0, device=device)
+
+
+class _MP:
+    def __init__(self, s):
+        self.dipole, self.quadrupole, self.four_pi_eps = s.multipole_moments()
+
+
+def make_sim(s, precision, n_traj, K, id_offset=0, torque="zero"):
+    from pystarc_b200.engine import B200ForceEngine
+    from pystarc_b200.simulator import B200BatchSimulator
+
+    eng = B200ForceEngine(**s.engine_kwargs(), multipole_expansion=_MP(s), precision=precision, torque_mode=torque,
+                          device=int(os.environ.get("LOCAL_RANK", 0)))
+    mol1, mol2 = s.molecules()
+    sim = B200BatchSimulator(mol1, mol2, s.mobility(), s.pathway_set(), s.params(n_traj=n_traj), eng,
+                             termination="complete", steps_per_launch=K, id_offset=id_offset)
+    return sim
+
+
+def time_device_arm(s, precision, steps, warmup, K, n_traj, id_offset, dist):
+    """Per-launch CUDA-event times (graph launches) with L2 flushes in between."""
+    import torch
+
+    sim = make_sim(s, precision, n_traj, K, id_offset)
+    sim._setup()
+    h = sim.engine.handle
+    h.call("bd_sim_reset", None)
+    stream = torch.cuda.current_stream()
+    sp = sim.engine.handle  # noqa: F841
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    from pystarc_b200 import _lib
+
+    sptr = _lib.P(stream.cuda_stream)
+    for _ in range(warmup):
+        h.call("bd_sim_run", 1, K, sptr)
+    c0 = sim.read_counters()
+    times = []
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    for i in range(steps):
+        flush.zero_()
+        ev[i][0].record(stream)
+        h.call("bd_sim_run", 1, K, sptr)
+        ev[i][1].record(stream)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    times = [a.elapsed_time(b) / 1e3 for a, b in ev]
+    c1 = sim.read_counters()
+    d = {k: c1[k] - c0[k] for k in c1}
+    d["started_total"] = c1["started"]
+    g = np.zeros(3, dtype=np.int32)
+    h.call("bd_get_launch", _lib.ptr(g[0:1], _lib.C.c_int32), _lib.ptr(g[1:2], _lib.C.c_int32),
+           _lib.ptr(g[2:3], _lib.C.c_int32))
+    sim.engine.close()
+    return sum(times), times, d, g.tolist()
+
+
+def e2e_arm(s, precision, steps, K, n_traj, id_offset):
+    """Through the public API from host arrays: engine construction (grid uploads), run(), outcomes."""
+    import torch
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sim = make_sim(s, precision, n_traj, K, id_offset)
+    sim.M = 1
+    res = sim.run(max_launches=steps)
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    h2d = sum(np.asarray(g.data).nbytes for g in s.elec_grids[:1] + s.born_grids[:1] + s.lig_born_grids)
+    h2d += np.asarray(s.elec_grids[0].data).nbytes * 2  # interleaved elec+Born copy of the shared lattice
+    h2d += (len(s.rec_q) + len(s.lig_q)) * 32
+    d2h = n_traj * 9 + steps * 12 * 8 * 2
+    launches = max(1, steps)
+    sim.engine.close()
+    return res.total_steps / el, h2d / launches, d2h / launches, res
+
+
+# --------------------------------------------------------------------------- CPU baseline
+def _cpu_worker(args):
+    grid_file, n_traj, seed, n_steps = args
+    from oracle import stepper as ost
+    from oracle.forces import FarField, OracleForceEngine, OracleGrid
+
+    d = np.load(grid_file, allow_pickle=False)
+    grids = lambda k: [OracleGrid(d[f"{k}{i}_data"].astype(np.float64), d[f"{k}{i}_origin"], d[f"{k}{i}_sp"])
+                       for i in range(int(d[f"n_{k}"]))]
+    ff = FarField(float(d["Q"]), float(d["debye"]), float(d["sdie"]), d["dip"], d["quad"], float(d["fpe"]))
+    eng = OracleForceEngine(grids("elec"), grids("born"), float(d["alpha"]), ff, grids("lig_born"), d["rec_pos"],
+                            d["rec_q"])
+    P = len(d["pair_cut"])
+    ss = ost.StepSystem(lig_body=d["lig_body"], lig_q=d["lig_q"], rec_pos=d["rec_pos"], engine=eng,
+                        rxn_rec_pos=d["pair_rec"].reshape(P, 3), rxn_lig_idx=d["pair_lig"], rxn_cutoff=d["pair_cut"],
+                        n_needed=int(d["n_needed"]), D_t=float(d["D_t"]), D_r=float(d["D_r"]),
+                        r_h_rec=float(d["r_h_rec"]), r_h_lig=float(d["r_h_lig"]), q_rec_total=float(d["Q"]),
+                        q_lig_total=float(d["q_lig"]), debye=float(d["debye"]))
+    prm = ost.StepParams(n_traj=n_traj, seed=seed, r_b=float(d["r_b"]), r_esc=float(d["r_esc"]), max_steps=n_steps,
+                         max_dt=float(d["max_dt"]), use_hi=bool(d["hi"]), overlap=bool(d["overlap"]))
+    t0 = time.perf_counter()
+    res = ost.run(ss, prm, noise="pcg64", termination="reference")
+    return res.total_steps, time.perf_counter() - t0
+
+
+def save_cpu_inputs(s, path):
+    mob = s.mobility()
+    dip, quad, fpe = s.multipole_moments()
+    arr = dict(Q=float(np.sum(s.rec_q)), q_lig=float(np.sum(s.lig_q)), debye=s.debye, sdie=s.sdie, dip=dip, quad=quad,
+               fpe=fpe, alpha=s.alpha, rec_pos=s.rec_pos, rec_q=s.rec_q, lig_body=s.lig_pos - s.lig_pos.mean(0),
+               lig_q=s.lig_q, pair_rec=np.array([s.rec_pos[a] for a, _, _ in s.pairs]),
+               pair_lig=np.array([b for _, b, _ in s.pairs]), pair_cut=np.array([c for _, _, c in s.pairs]),
+               n_needed=s.n_needed, D_t=mob.relative_translational_diffusion(),
+               D_r=mob.relative_rotational_diffusion(), r_h_rec=s.r_hydro_rec, r_h_lig=s.r_hydro_lig,
+               r_b=s.r_start, r_esc=s.r_escape, max_dt=s.max_dt, hi=s.hi, overlap=s.overlap)
+    for k, gl in (("elec", s.elec_grids), ("born", s.born_grids), ("lig_born", s.lig_born_grids)):
+        arr[f"n_{k}"] = len(gl)
+        for i, g in enumerate(gl):
+            arr[f"{k}{i}_data"] = np.asarray(g.data, dtype=np.float32)
+            arr[f"{k}{i}_origin"] = np.asarray(g.origin)
+            arr[f"{k}{i}_sp"] = np.asarray([g.delta[j, j] for j in range(3)])
+    np.savez(path, **arr)
+
+
+def cpu_baseline(s, cores, traj_per_proc=256, n_steps=40):
+    """The reference's step loop restated in NumPy on `cores` processes, each a bounded sample."""
+    with tempfile.TemporaryDirectory() as td:
+        f = os.path.join(td, "inputs.npz")
+        save_cpu_inputs(s, f)
+        ctx = mp.get_context("spawn")
+        t0 = time.perf_counter()
+        with ctx.Pool(cores) as pool:
+            out = pool.map(_cpu_worker, [(f, traj_per_proc, 1000 + i, n_steps) for i in range(cores)])
+        wall = time.perf_counter() - t0
+    steps = sum(o[0] for o in out)
+    busy = max(o[1] for o in out)
+    return steps / busy, {"value": steps / busy, "unit": UNIT, "cores": cores, "kind": "port",
+                          "sample": f"{cores} processes x {traj_per_proc} trajectories x <= {n_steps} steps of the "
+                                    f"same system from the b-sphere ({steps} trajectory-steps, {busy:.1f} s)",
+                          "wall_s": round(wall, 1)}
+
+
+# --------------------------------------------------------------------------- main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--inner", type=int, default=64, help="BD steps per trajectory per launch")
+    ap.add_argument("--n-traj", type=int, default=1_000_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=40)
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        s = build_system(None if not _has_cuda() else "cuda")
+        cores = os.cpu_count() or 1
+        vals = []
+        for i in range(args.warmup + args.steps):
+            v, info = cpu_baseline(s, cores, n_steps=max(4, args.cpu_steps // 4))
+            if i >= args.warmup:
+                vals.append(v)
+        val = float(np.mean(vals))
+        info["value"] = val
+        print(json.dumps({"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
+                          "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                          "config": {"workload": WORKLOAD, "arm": "reference batched stepper restated in NumPy "
+                                     "(PCG64 order), CPU"},
+                          "cpu_baseline": info, "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0,
+                                                        "d2h_bytes_per_step": 0}}))
+        return
+
+    import torch
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as td
+
+        torch.cuda.set_device(local)
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = td
+    s = build_system("cuda")
+    n_traj = args.n_traj
+    id_offset = rank * n_traj
+    clocks = Clocks(local)
+    clocks.start()
+    t_mixed, tl_mixed, d_mixed, launch = time_device_arm(s, "mixed", args.steps, args.warmup, args.inner, n_traj,
+                                                         id_offset, dist)
+    ck = clocks.stop()
+    t_fp64, tl_fp64, d_fp64, _ = time_device_arm(s, "fp64", args.steps, args.warmup, args.inner, n_traj, id_offset,
+                                                 dist)
+    e2e_val, h2d, d2h, e2e_res = e2e_arm(s, "mixed", args.steps, args.inner, n_traj, id_offset)
+    t_max = t_mixed
+    steps_all = d_mixed["steps"]
+    if dist is not None:
+        tt = torch.tensor([t_mixed], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+        st = torch.tensor([steps_all], device="cuda", dtype=torch.int64)
+        dist.all_reduce(st)
+        steps_all = int(st.item())
+    value = steps_all / t_max
+    peak, peak_kind = peaks()
+    gathers = d_mixed["grid_evals"] + d_mixed["rev_evals"]
+    algo_bytes = gathers * ALGO_BYTES_PER_GATHER + d_mixed["steps"] * STATE_BYTES_PER_STEP
+    achieved = algo_bytes / t_mixed / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "step_kernel_traffic.json"
+    if tf.exists():
+        tj = json.loads(tf.read_text())
+        traffic = tj.get("dram_bytes_per_launch")
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 forces / f64 poses", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "trajectories_per_gpu": n_traj, "bd_steps_per_launch": args.inner,
+                   "parallelism": f"trajectory shards x{world}", "l2": "flushed (256 MiB write) between launches",
+                   "launch": {"group": launch[0], "block": launch[1], "grid": launch[2]}},
+        "variants": {
+            "mixed": {"bd_steps_per_s": d_mixed["steps"] / t_mixed, "steps": d_mixed["steps"]},
+            "fp64": {"bd_steps_per_s": d_fp64["steps"] / t_fp64, "steps": d_fp64["steps"]},
+            "mixed_over_fp64": (d_mixed["steps"] / t_mixed) / (d_fp64["steps"] / t_fp64),
+        },
+        "counters": {k: int(v) for k, v in d_mixed.items()},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_kind": peak_kind,
+                     "algorithmic_bytes": "224 B per (atom, grid) stencil + 128 B per trajectory-step"},
+        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "note": "B200ForceEngine + B200BatchSimulator.run() from host arrays, incl. grid upload"},
+        "gpu_launches": 3 * args.steps,
+        "clocks": ck,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        _, info = cpu_baseline(s, os.cpu_count() or 1, n_steps=args.cpu_steps)
+        line["cpu_baseline"] = info
+    print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def _has_cuda():
+    try:
+        import torch
+
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+if __name__ == "__main__":
+    main()

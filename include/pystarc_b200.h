@@ -1,0 +1,149 @@
+/*
+ * pystarc_b200 -- C ABI of the B200-native batched rigid-body Brownian-dynamics engine.
+ *
+ * Every entry point returns an int status (BD_OK = 0, negative on error) and
+ * never exits or aborts; bd_last_error() gives the message.  One handle is used
+ * by one host thread at a time; handles are independent.  Array arguments are
+ * plain pointers; which side (device or host) each pointer lives on is stated
+ * per function.  Units are the reference's: Angstrom, ps, kBT, e.
+ *
+ * Reference interfaces replaced (paths inside anandojha/PySTARC):
+ *   GPUBatchForceEngine.__init__ / _upload_grids   pystarc/forces/gpu_batch_engine.py:139-287
+ *   GPUBatchForceEngine.__call__                  pystarc/forces/gpu_batch_engine.py:531-605
+ *   GPUBatchSimulator.__init__                    pystarc/simulation/gpu_batch_simulator.py:159-318
+ *   GPUBatchSimulator.run (step loop)             pystarc/simulation/gpu_batch_simulator.py:462-1594
+ */
+#ifndef PYSTARC_B200_H
+#define PYSTARC_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct BdHandle BdHandle;
+
+enum {
+  BD_OK = 0,
+  BD_ERR_ARG = -1,      /* invalid argument or unsupported size */
+  BD_ERR_CUDA = -2,     /* CUDA runtime error */
+  BD_ERR_OOM = -3,      /* device allocation failed */
+  BD_ERR_NAN = -4,      /* non-finite input or result */
+  BD_ERR_STALL = -5,    /* watchdog: a bounded device loop gave up */
+  BD_ERR_STATE = -6     /* call out of order (e.g. run before configure) */
+};
+
+enum { BD_GRID_ELEC = 0, BD_GRID_BORN = 1, BD_GRID_LIG_BORN = 2 };
+enum { BD_PREC_FP64 = 0, BD_PREC_MIXED = 1 };         /* force/torque/mobility arithmetic */
+enum { BD_TORQUE_ZERO = 0, BD_TORQUE_CENTROID = 1 };  /* zero = reference GPU path */
+
+/* Far-field and Born parameters (gpu_batch_engine.py:139-175). */
+typedef struct {
+  double receptor_charge; /* Q_rec, e */
+  double debye_length;    /* A */
+  double sdie;            /* solvent dielectric of the far-field */
+  double alpha;           /* Born desolvation alpha */
+  int use_multipole;      /* 1: dipole + quadrupole terms (MultipoleExpansion) */
+  double dipole[3];
+  double quadrupole[9];   /* row-major, 1/2 sum q (3 r r - r^2 I) */
+  double four_pi_eps;     /* 4 pi sdie eps0 of the multipole terms */
+} BdForceParams;
+
+/* Stepper parameters (GPUBatchSimulator.run, gpu_batch_simulator.py:462-1254). */
+typedef struct {
+  int64_t n_traj;
+  uint64_t seed;
+  double r_start, r_escape;  /* b-sphere, escape sphere */
+  double return_prob;        /* host-computed (Romberg), applied at r_escape */
+  int32_t max_steps;         /* per-trajectory cap; reached -> max-steps outcome */
+  double max_dt, min_core_dt;
+  int32_t use_hi, overlap;
+  double D_t, D_r;           /* relative translational / rotational diffusion */
+  double q_rec_total, q_lig_total, adt_debye;  /* adaptive-dt force criterion */
+  double r_hydro_rec, r_hydro_lig;
+  int32_t precision, torque_mode;
+  int32_t slots;             /* live-slot capacity; 0 = automatic */
+  int64_t id_offset;         /* global id of local trajectory 0 (keys the noise; shards across GPUs) */
+} BdSimParams;
+
+/* Counter indices of bd_sim_counters(). */
+enum {
+  BD_CTR_STARTED = 0, BD_CTR_REACTED, BD_CTR_ESCAPED, BD_CTR_MAXSTEPS, BD_CTR_STEPS, BD_CTR_RETURNS,
+  BD_CTR_OVERLAP, BD_CTR_BRIDGE, BD_CTR_GRID_EVALS, BD_CTR_REV_EVALS, BD_CTR_FF_EVALS, BD_CTR_NONFINITE,
+  BD_CTR_NUM = 12
+};
+
+/* Library version string. */
+const char* bd_version(void);
+
+/* Create a handle bound to CUDA device `device`.  Replaces the engine's device setup. */
+int bd_create(int device, BdHandle** out);
+int bd_destroy(BdHandle* h);
+/* Copy the last error message of `h` (or of the last failed bd_create when h is NULL). */
+int bd_last_error(const BdHandle* h, char* buf, int len);
+
+/* Ligand atoms in the body frame (about the centroid), host arrays: xyz (n*3), charges (n).
+ * Replaces GPUBatchSimulator._mol2_pos0 / _charges (gpu_batch_simulator.py:171-176). */
+int bd_set_ligand(BdHandle* h, int n, const double* body_xyz, const double* charges);
+/* Receptor atoms (receptor at the origin), host arrays.  Replaces the engine's
+ * rec_positions / rec_charges and the stepper's overlap table (gpu_batch_engine.py:207-217,
+ * gpu_batch_simulator.py:771-781). */
+int bd_set_receptor(BdHandle* h, int n, const double* xyz, const double* charges);
+/* Add a FP32 grid (host array, C order, z fastest).  kind = BD_GRID_*.  Grids are sorted
+ * finest-first and dropped as the reference does (gpu_batch_engine.py:179-211, :248-287). */
+int bd_add_grid(BdHandle* h, int kind, const float* data, int nx, int ny, int nz, const double* origin,
+                const double* spacing);
+int bd_clear_grids(BdHandle* h);
+int bd_set_force_params(BdHandle* h, const BdForceParams* p);
+/* Flattened reaction pairs (gpu_batch_simulator.py:186-215, :643-660): receptor atom
+ * positions (n*3), ligand atom body positions (n*3), cutoffs, bridge D_eff per pair,
+ * n_needed (already resolved: -1 handled by the caller).  Host arrays. */
+int bd_set_reactions(BdHandle* h, int n_pairs, const double* rec_xyz, const double* lig_body_xyz,
+                     const double* cutoffs, const double* d_eff, int n_needed);
+
+/* Net force, torque and energy for n poses.  DEVICE arrays: centroids (n*3), rotations
+ * (n*4 quaternions w,x,y,z or n*9 row-major matrices), outputs F (n*3), T (n*3), E (n).
+ * Same result as GPUBatchForceEngine.__call__ (gpu_batch_engine.py:531-605) with the
+ * ligand placed as R b + c; torque_mode BD_TORQUE_ZERO reproduces its zero torque. */
+int bd_eval_forces(BdHandle* h, int64_t n, const double* centroids, const double* rotations, int rot_is_matrix,
+                   double* F, double* T, double* E, int precision, int torque_mode, void* stream);
+/* Same with explicit lab-frame ligand atom positions (n * n_lig * 3), rotation matrices
+ * (n*9) and centroids (n*3): the reference __call__ argument list.  DEVICE arrays. */
+int bd_eval_forces_atoms(BdHandle* h, int64_t n, const double* lig_positions, const double* R,
+                         const double* centroids, double* F, double* T, double* E, int precision, int torque_mode,
+                         void* stream);
+
+/* Stepper.  configure allocates the live-slot pool and per-trajectory outputs; reset
+ * starts the first `slots` trajectories; run enqueues n_launch launches of
+ * steps_per_launch BD steps each (refill from the pending pool inside, compaction
+ * between launches).  run is asynchronous on `stream`. */
+int bd_sim_configure(BdHandle* h, const BdSimParams* p);
+int bd_sim_reset(BdHandle* h, void* stream);
+int bd_sim_run(BdHandle* h, int n_launch, int steps_per_launch, void* stream);
+/* Synchronise `stream` and copy the BD_CTR_NUM counters to a host array. */
+int bd_sim_counters(BdHandle* h, uint64_t* out, int n, void* stream);
+/* Host copies of the per-trajectory outcome (0 running/unstarted, 1 reacted, 2 escaped,
+ * 3 max-steps, 5 non-finite pose), step counts and return counts (n_traj each). */
+int bd_sim_outcomes(BdHandle* h, int8_t* status, int32_t* steps, int32_t* returns);
+/* Live-slot count after the last compaction (synchronises the handle's work). */
+int bd_sim_live(BdHandle* h, int32_t* n_live);
+/* Checkpoint: host copies of the live slots (cap entries each; c: 3*cap, q: 4*cap, SoA)
+ * plus counters and outcomes are enough to resume exactly (bd_sim_restore). */
+int bd_sim_capacity(BdHandle* h, int32_t* cap);
+int bd_sim_snapshot(BdHandle* h, double* c, double* q, int32_t* traj, int32_t* steps, int32_t* rets,
+                    int8_t* status, int32_t* n_live, uint64_t* counters);
+int bd_sim_restore(BdHandle* h, const double* c, const double* q, const int32_t* traj, const int32_t* steps,
+                   const int32_t* rets, const int8_t* status, int32_t n_live, const uint64_t* counters,
+                   const int8_t* out_status, const int32_t* out_steps, const int32_t* out_returns);
+
+/* Launch shape: lanes per trajectory (1, 4, 8, 16 or 32) and threads per block (multiple
+ * of 32, <= 256).  Set by the autotuner; 0 keeps the current value. */
+int bd_set_launch(BdHandle* h, int group, int block_threads);
+int bd_get_launch(BdHandle* h, int* group, int* block_threads, int* grid_blocks);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PYSTARC_B200_H */

@@ -1,0 +1,115 @@
+"""ctypes binding of ``libpystarc_b200.so`` (declared in include/pystarc_b200.h).
+
+The library is built in-tree by ``pystarc_b200.build``.  There is no fallback:
+if the shared object is missing or cannot be loaded, every entry point raises.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libpystarc_b200.so"
+
+BD_OK, BD_ERR_ARG, BD_ERR_CUDA, BD_ERR_OOM, BD_ERR_NAN, BD_ERR_STALL, BD_ERR_STATE = 0, -1, -2, -3, -4, -5, -6
+GRID_ELEC, GRID_BORN, GRID_LIG_BORN = 0, 1, 2
+PREC_FP64, PREC_MIXED = 0, 1
+TORQUE_ZERO, TORQUE_CENTROID = 0, 1
+CTR_NAMES = ("started", "reacted", "escaped", "max_steps", "steps", "returns", "overlap", "bridge", "grid_evals",
+             "rev_evals", "ff_evals", "nonfinite")
+N_CTR = len(CTR_NAMES)
+
+_ERR_NAMES = {BD_ERR_ARG: "bad argument", BD_ERR_CUDA: "CUDA error", BD_ERR_OOM: "out of device memory",
+              BD_ERR_NAN: "non-finite value", BD_ERR_STALL: "device watchdog", BD_ERR_STATE: "call out of order"}
+
+
+class BdForceParams(C.Structure):
+    _fields_ = [("receptor_charge", C.c_double), ("debye_length", C.c_double), ("sdie", C.c_double),
+                ("alpha", C.c_double), ("use_multipole", C.c_int), ("dipole", C.c_double * 3),
+                ("quadrupole", C.c_double * 9), ("four_pi_eps", C.c_double)]
+
+
+class BdSimParams(C.Structure):
+    _fields_ = [("n_traj", C.c_int64), ("seed", C.c_uint64), ("r_start", C.c_double), ("r_escape", C.c_double),
+                ("return_prob", C.c_double), ("max_steps", C.c_int32), ("max_dt", C.c_double),
+                ("min_core_dt", C.c_double), ("use_hi", C.c_int32), ("overlap", C.c_int32), ("D_t", C.c_double),
+                ("D_r", C.c_double), ("q_rec_total", C.c_double), ("q_lig_total", C.c_double),
+                ("adt_debye", C.c_double), ("r_hydro_rec", C.c_double), ("r_hydro_lig", C.c_double),
+                ("precision", C.c_int32), ("torque_mode", C.c_int32), ("slots", C.c_int32),
+                ("id_offset", C.c_int64)]
+
+
+P = C.c_void_p
+dp = C.POINTER(C.c_double)
+fp = C.POINTER(C.c_float)
+i32p = C.POINTER(C.c_int32)
+i8p = C.POINTER(C.c_int8)
+u64p = C.POINTER(C.c_uint64)
+
+# name -> (restype, argtypes); mirrors include/pystarc_b200.h
+SIGNATURES = {
+    "bd_version": (C.c_char_p, []),
+    "bd_create": (C.c_int, [C.c_int, C.POINTER(P)]),
+    "bd_destroy": (C.c_int, [P]),
+    "bd_last_error": (C.c_int, [P, C.c_char_p, C.c_int]),
+    "bd_set_ligand": (C.c_int, [P, C.c_int, dp, dp]),
+    "bd_set_receptor": (C.c_int, [P, C.c_int, dp, dp]),
+    "bd_add_grid": (C.c_int, [P, C.c_int, fp, C.c_int, C.c_int, C.c_int, dp, dp]),
+    "bd_clear_grids": (C.c_int, [P]),
+    "bd_set_force_params": (C.c_int, [P, C.POINTER(BdForceParams)]),
+    "bd_set_reactions": (C.c_int, [P, C.c_int, dp, dp, dp, dp, C.c_int]),
+    "bd_eval_forces": (C.c_int, [P, C.c_int64, P, P, C.c_int, P, P, P, C.c_int, C.c_int, P]),
+    "bd_eval_forces_atoms": (C.c_int, [P, C.c_int64, P, P, P, P, P, P, C.c_int, C.c_int, P]),
+    "bd_sim_configure": (C.c_int, [P, C.POINTER(BdSimParams)]),
+    "bd_sim_reset": (C.c_int, [P, P]),
+    "bd_sim_run": (C.c_int, [P, C.c_int, C.c_int, P]),
+    "bd_sim_counters": (C.c_int, [P, u64p, C.c_int, P]),
+    "bd_sim_outcomes": (C.c_int, [P, i8p, i32p, i32p]),
+    "bd_sim_live": (C.c_int, [P, i32p]),
+    "bd_sim_capacity": (C.c_int, [P, i32p]),
+    "bd_sim_snapshot": (C.c_int, [P, dp, dp, i32p, i32p, i32p, i8p, i32p, u64p]),
+    "bd_sim_restore": (C.c_int, [P, dp, dp, i32p, i32p, i32p, i8p, C.c_int32, u64p, i8p, i32p, i32p]),
+    "bd_set_launch": (C.c_int, [P, C.c_int, C.c_int]),
+    "bd_get_launch": (C.c_int, [P, i32p, i32p, i32p]),
+}
+
+_LIB = None
+
+
+class BdError(RuntimeError):
+    """An engine entry point returned an error status."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"{_ERR_NAMES.get(code, 'error')} ({code}): {msg}")
+        self.code = code
+
+
+def load(path: Path | None = None):
+    """Load the shared library once and bind every declared entry point."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    p = Path(path or os.environ.get("PYSTARC_B200_LIB", LIB_PATH))
+    if not p.exists():
+        raise RuntimeError(f"{p} not found: build it with `python -c 'import pystarc_b200.build as b; b.build()'`")
+    lib = C.CDLL(str(p))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = lib
+    return lib
+
+
+def check(rc, handle=None):
+    if rc != BD_OK:
+        buf = C.create_string_buffer(1024)
+        load().bd_last_error(handle, buf, 1024)
+        raise BdError(rc, buf.value.decode(errors="replace"))
+    return rc
+
+
+def ptr(a, ctype=C.c_double):
+    """ctypes pointer to a contiguous NumPy array."""
+    return a.ctypes.data_as(C.POINTER(ctype))

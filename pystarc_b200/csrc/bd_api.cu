@@ -1,0 +1,826 @@
+// C ABI of the batched BD engine: handle, uploads, force evaluation and the stepper.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "bd_kernels.cuh"
+#include "pystarc_b200.h"
+
+using namespace bd;
+
+namespace {
+
+const double kEps0 = 0.000142;
+const double kPi = 3.14159265358979323846;
+
+struct GridHost {
+  std::vector<float> data;
+  int n[3];
+  double o[3], sp[3];
+};
+
+std::string g_create_error;
+
+}  // namespace
+
+struct BdHandle {
+  int device = 0;
+  int n_sm = 148;
+  std::string err;
+  cudaStream_t own = nullptr;
+  // host-side inputs
+  std::vector<double> lig;  // x,y,z,q
+  std::vector<double> rec;  // x,y,z,q
+  std::vector<GridHost> grids[3];
+  BdForceParams fp{};
+  bool fp_set = false;
+  int n_pairs = 0, n_needed = 1;
+  double rx_rec[BD_MAX_PAIRS][3], rx_body[BD_MAX_PAIRS][3], rx_cut[BD_MAX_PAIRS], rx_deff[BD_MAX_PAIRS];
+  bool dirty = true;
+  // device system
+  DevSystem S{};
+  std::vector<void*> sys_allocs;
+  // stepper
+  bool sim_ready = false;
+  BdSimParams sp{};
+  DevSim P{};
+  SlotBuf buf[2]{};
+  int* d_live = nullptr;  // [2]
+  int cur = 0;
+  unsigned long long* d_ctr = nullptr;
+  std::vector<void*> sim_allocs;
+  int group = 8, block = 128;
+  bool launch_user = false;
+  // graphs: [cur][steps] cache
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  int graph_K = -1, graph_G = -1, graph_B = -1, graph_prec = -1, graph_torque = -1;
+};
+
+namespace {
+
+int fail(BdHandle* h, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (h) h->err = buf;
+  else g_create_error = buf;
+  return code;
+}
+
+#define CK(h, x)                                                                                   \
+  do {                                                                                             \
+    cudaError_t e_ = (x);                                                                          \
+    if (e_ != cudaSuccess)                                                                         \
+      return fail(h, e_ == cudaErrorMemoryAllocation ? BD_ERR_OOM : BD_ERR_CUDA, "%s: %s (%s:%d)", #x, \
+                  cudaGetErrorString(e_), __FILE__, __LINE__);                                      \
+  } while (0)
+
+int dev_alloc(BdHandle* h, std::vector<void*>& list, void** p, size_t bytes) {
+  CK(h, cudaMalloc(p, bytes ? bytes : 16));
+  list.push_back(*p);
+  return BD_OK;
+}
+
+void free_list(std::vector<void*>& list) {
+  for (void* p : list) cudaFree(p);
+  list.clear();
+}
+
+uint32_t spread3(uint32_t v) {
+  v &= 0x3ff;
+  v = (v | (v << 16)) & 0x030000FF;
+  v = (v | (v << 8)) & 0x0300F00F;
+  v = (v | (v << 4)) & 0x030C30C3;
+  v = (v | (v << 2)) & 0x09249249;
+  return v;
+}
+
+void grid_to_dev(const GridHost& g, const float* dptr, int ch, DevGrid& d) {
+  d.data = dptr;
+  d.nx = g.n[0];
+  d.ny = g.n[1];
+  d.nz = g.n[2];
+  d.ch = ch;
+  d.ox = g.o[0];
+  d.oy = g.o[1];
+  d.oz = g.o[2];
+  d.isx = 1.0 / g.sp[0];
+  d.isy = 1.0 / g.sp[1];
+  d.isz = 1.0 / g.sp[2];
+  const double m = 3.0;
+  d.lox = g.o[0] + m * g.sp[0];
+  d.loy = g.o[1] + m * g.sp[1];
+  d.loz = g.o[2] + m * g.sp[2];
+  d.hix = g.o[0] + ((double)g.n[0] - 1 - m) * g.sp[0];
+  d.hiy = g.o[1] + ((double)g.n[1] - 1 - m) * g.sp[1];
+  d.hiz = g.o[2] + ((double)g.n[2] - 1 - m) * g.sp[2];
+}
+
+int upload_floats(BdHandle* h, const float* src, size_t n, const float** out) {
+  void* p = nullptr;
+  int rc = dev_alloc(h, h->sys_allocs, &p, n * sizeof(float));
+  if (rc) return rc;
+  CK(h, cudaMemcpy(p, src, n * sizeof(float), cudaMemcpyHostToDevice));
+  *out = (const float*)p;
+  return BD_OK;
+}
+
+bool same_lattice(const GridHost& a, const GridHost& b) {
+  for (int i = 0; i < 3; ++i)
+    if (a.n[i] != b.n[i] || a.o[i] != b.o[i] || a.sp[i] != b.sp[i]) return false;
+  return true;
+}
+
+// Build the device-side system: grid selection rules, uploads, receptor chunks.
+int finalize(BdHandle* h) {
+  if (!h->dirty) return BD_OK;
+  CK(h, cudaSetDevice(h->device));
+  CK(h, cudaDeviceSynchronize());
+  free_list(h->sys_allocs);
+  DevSystem S{};
+  if (h->lig.empty()) return fail(h, BD_ERR_STATE, "ligand not set");
+  const BdForceParams& fp = h->fp;
+  // far field (gpu_batch_engine.py:162-175)
+  const double eps_s = fp.sdie * kEps0;
+  S.V_factor = eps_s > 0 ? fp.receptor_charge / (4.0 * kPi * eps_s) : 0.0;
+  S.has_yukawa = std::fabs(fp.receptor_charge) > 1e-9 && fp.debye_length > 0;
+  S.inv_debye = fp.debye_length > 0 ? 1.0 / fp.debye_length : 0.0;
+  S.alpha = fp.alpha;
+  if (fp.use_multipole) {
+    double pn = 0, qn = 0;
+    for (int i = 0; i < 3; ++i) pn += fp.dipole[i] * fp.dipole[i];
+    for (int i = 0; i < 9; ++i) qn += fp.quadrupole[i] * fp.quadrupole[i];
+    S.use_dip = std::sqrt(pn) > 1e-9;
+    S.use_quad = std::sqrt(qn) > 1e-9;
+    for (int i = 0; i < 3; ++i) S.dip[i] = fp.dipole[i];
+    for (int i = 0; i < 9; ++i) S.quad[i] = fp.quadrupole[i];
+    S.inv_fpe = 1.0 / fp.four_pi_eps;
+  }
+  // grids: finest first (stable on the x spacing), reference dropping rules
+  std::vector<GridHost> el = h->grids[BD_GRID_ELEC], bo = h->grids[BD_GRID_BORN], lb = h->grids[BD_GRID_LIG_BORN];
+  auto finer = [](const GridHost& a, const GridHost& b) { return a.sp[0] < b.sp[0]; };
+  std::stable_sort(el.begin(), el.end(), finer);
+  std::stable_sort(bo.begin(), bo.end(), finer);
+  std::stable_sort(lb.begin(), lb.end(), finer);
+  if (S.has_yukawa && el.size() > 1) el.resize(1);
+  if (bo.size() > 1) bo.resize(1);
+  if (lb.size() > 1) lb.resize(1);
+  if (el.size() > BD_MAX_ELEC) return fail(h, BD_ERR_ARG, "at most %d electrostatic grids", BD_MAX_ELEC);
+  S.n_elec = (int)el.size();
+  for (int k = 0; k < S.n_elec; ++k) {
+    const float* p;
+    int rc = upload_floats(h, el[k].data.data(), el[k].data.size(), &p);
+    if (rc) return rc;
+    grid_to_dev(el[k], p, 1, S.elec[k]);
+  }
+  S.has_born = !bo.empty();
+  if (S.has_born) {
+    const float* p;
+    int rc = upload_floats(h, bo[0].data.data(), bo[0].data.size(), &p);
+    if (rc) return rc;
+    grid_to_dev(bo[0], p, 1, S.born);
+    if (S.n_elec > 0 && same_lattice(el[0], bo[0])) {
+      std::vector<float> il(2 * el[0].data.size());
+      for (size_t i = 0; i < el[0].data.size(); ++i) {
+        il[2 * i] = el[0].data[i];
+        il[2 * i + 1] = bo[0].data[i];
+      }
+      rc = upload_floats(h, il.data(), il.size(), &p);
+      if (rc) return rc;
+      grid_to_dev(el[0], p, 2, S.pair);
+      S.paired = 1;
+    }
+  }
+  // ligand
+  const int nl = (int)(h->lig.size() / 4);
+  S.n_lig = nl;
+  {
+    void* p;
+    int rc = dev_alloc(h, h->sys_allocs, &p, h->lig.size() * sizeof(double));
+    if (rc) return rc;
+    CK(h, cudaMemcpy(p, h->lig.data(), h->lig.size() * sizeof(double), cudaMemcpyHostToDevice));
+    S.lig = (const double4*)p;
+  }
+  // receptor: spatial (Morton) order, chunks of BD_CHUNK with bounding spheres
+  const int nr = (int)(h->rec.size() / 4);
+  if (nr > 0) {
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    double rmax = 0;
+    for (int i = 0; i < nr; ++i) {
+      for (int k = 0; k < 3; ++k) {
+        lo[k] = std::min(lo[k], h->rec[4 * i + k]);
+        hi[k] = std::max(hi[k], h->rec[4 * i + k]);
+      }
+      rmax = std::max(rmax, std::sqrt(h->rec[4 * i] * h->rec[4 * i] + h->rec[4 * i + 1] * h->rec[4 * i + 1] +
+                                      h->rec[4 * i + 2] * h->rec[4 * i + 2]));
+    }
+    std::vector<uint32_t> code(nr);
+    for (int i = 0; i < nr; ++i) {
+      uint32_t c = 0;
+      for (int k = 0; k < 3; ++k) {
+        const double w = hi[k] - lo[k];
+        const uint32_t v = w > 0 ? (uint32_t)std::min(1023.0, (h->rec[4 * i + k] - lo[k]) / w * 1023.0) : 0u;
+        c |= spread3(v) << k;
+      }
+      code[i] = c;
+    }
+    std::vector<int> order(nr);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return code[a] < code[b]; });
+    const int nc = (nr + BD_CHUNK - 1) / BD_CHUNK;
+    std::vector<double> ra(4 * (size_t)nc * BD_CHUNK), cs(4 * (size_t)nc);
+    for (int j = 0; j < nc * BD_CHUNK; ++j) {
+      const int src = order[std::min(j, nr - 1)];
+      for (int k = 0; k < 3; ++k) ra[4 * j + k] = h->rec[4 * src + k];
+      ra[4 * j + 3] = j < nr ? h->rec[4 * src + 3] : 0.0;
+    }
+    for (int c = 0; c < nc; ++c) {
+      double m[3] = {0, 0, 0};
+      for (int a = 0; a < BD_CHUNK; ++a)
+        for (int k = 0; k < 3; ++k) m[k] += ra[4 * (c * BD_CHUNK + a) + k] / BD_CHUNK;
+      double r = 0;
+      for (int a = 0; a < BD_CHUNK; ++a) {
+        double d2 = 0;
+        for (int k = 0; k < 3; ++k) {
+          const double d = ra[4 * (c * BD_CHUNK + a) + k] - m[k];
+          d2 += d * d;
+        }
+        r = std::max(r, std::sqrt(d2));
+      }
+      for (int k = 0; k < 3; ++k) cs[4 * c + k] = m[k];
+      cs[4 * c + 3] = r * (1 + 1e-12) + 1e-9;  // conservative against rounding
+    }
+    void* p;
+    int rc = dev_alloc(h, h->sys_allocs, &p, ra.size() * sizeof(double));
+    if (rc) return rc;
+    CK(h, cudaMemcpy(p, ra.data(), ra.size() * sizeof(double), cudaMemcpyHostToDevice));
+    S.rec = (const double4*)p;
+    rc = dev_alloc(h, h->sys_allocs, &p, cs.size() * sizeof(double));
+    if (rc) return rc;
+    CK(h, cudaMemcpy(p, cs.data(), cs.size() * sizeof(double), cudaMemcpyHostToDevice));
+    S.chunks = (const double4*)p;
+    S.n_chunks = nc;
+    S.n_rec_pad = nc * BD_CHUNK;
+    S.rec_max_r = rmax * (1 + 1e-12) + 1e-9;
+  }
+  // Born direction 2 needs the ligand Born grid, receptor atoms and alpha > 1e-12 (gpu_batch_engine.py:583-590)
+  if (!lb.empty() && nr > 0 && fp.alpha > 1e-12) {
+    const float* p;
+    int rc = upload_floats(h, lb[0].data.data(), lb[0].data.size(), &p);
+    if (rc) return rc;
+    grid_to_dev(lb[0], p, 1, S.lig_born);
+    S.born_rev = 1;
+    const DevGrid& g = S.lig_born;
+    const double mx = std::max(std::fabs(g.lox), std::fabs(g.hix)), my = std::max(std::fabs(g.loy), std::fabs(g.hiy)),
+                 mz = std::max(std::fabs(g.loz), std::fabs(g.hiz));
+    S.lig_born_rho = std::sqrt(mx * mx + my * my + mz * mz) * (1 + 1e-12) + 1e-9;
+  }
+  // reactions
+  S.n_pairs = h->n_pairs;
+  S.n_needed = h->n_needed;
+  for (int p = 0; p < h->n_pairs; ++p) {
+    for (int k = 0; k < 3; ++k) {
+      S.rx_rec[p][k] = h->rx_rec[p][k];
+      S.rx_body[p][k] = h->rx_body[p][k];
+    }
+    S.rx_cut[p] = h->rx_cut[p];
+    S.rx_deff[p] = h->rx_deff[p];
+  }
+  h->S = S;
+  h->dirty = false;
+  h->graph_K = -1;  // system changed: rebuild graphs
+  return BD_OK;
+}
+
+cudaStream_t pick(BdHandle* h, void* s) { return s ? (cudaStream_t)s : h->own; }
+
+// ---------------------------------------------------------------------------
+// Kernel dispatch over (precision, group size, torque)
+// ---------------------------------------------------------------------------
+template <typename FT, int G, bool TQ>
+struct K {
+  static void* pose() { return (void*)&eval_pose_kernel<FT, G, TQ>; }
+  static void* atoms() { return (void*)&eval_atoms_kernel<FT, G, TQ>; }
+  static void* step() { return (void*)&step_kernel<FT, G, TQ>; }
+};
+
+template <typename FT, bool TQ>
+void* pick_g(int G, int which) {
+  switch (G) {
+#define BD_CASE(g)                                                  \
+  case g:                                                           \
+    return which == 0 ? K<FT, g, TQ>::pose() : which == 1 ? K<FT, g, TQ>::atoms() : K<FT, g, TQ>::step();
+    BD_CASE(1)
+    BD_CASE(4)
+    BD_CASE(8)
+    BD_CASE(16)
+    BD_CASE(32)
+#undef BD_CASE
+  }
+  return nullptr;
+}
+
+void* kernel_for(int prec, int G, int torque, int which) {
+  const bool tq = torque == BD_TORQUE_CENTROID;
+  if (prec == BD_PREC_FP64) return tq ? pick_g<double, true>(G, which) : pick_g<double, false>(G, which);
+  return tq ? pick_g<float, true>(G, which) : pick_g<float, false>(G, which);
+}
+
+bool valid_group(int g) { return g == 1 || g == 4 || g == 8 || g == 16 || g == 32; }
+
+int default_group(int n_lig_charged, bool born_rev) {
+  if (born_rev) return n_lig_charged > 64 ? 32 : 8;
+  if (n_lig_charged <= 2) return 1;
+  if (n_lig_charged <= 12) return 4;
+  if (n_lig_charged <= 48) return 8;
+  if (n_lig_charged <= 200) return 16;
+  return 32;
+}
+
+int n_charged(const BdHandle* h) {
+  int n = 0;
+  for (size_t i = 0; i < h->lig.size() / 4; ++i) n += std::fabs(h->lig[4 * i + 3]) >= 1e-9;
+  return n;
+}
+
+int eval_grid_blocks(BdHandle* h, long long n, int G, int block) {
+  const long long groups = (n + 0);
+  const long long per_block = block / G;
+  long long blocks = (groups + per_block - 1) / per_block;
+  blocks = std::min<long long>(blocks, (long long)h->n_sm * 64);
+  return (int)std::max<long long>(blocks, 1);
+}
+
+int persistent_blocks(BdHandle* h, void* fn, int block) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, 0) != cudaSuccess || per_sm < 1) per_sm = 1;
+  return per_sm * h->n_sm;
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+const char* bd_version(void) { return "pystarc_b200 0.1.0 (sm_100a)"; }
+
+int bd_create(int device, BdHandle** out) {
+  if (!out) return fail(nullptr, BD_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0)
+    return fail(nullptr, BD_ERR_CUDA, "no CUDA device: %s", e != cudaSuccess ? cudaGetErrorString(e) : "count 0");
+  if (device < 0 || device >= n) return fail(nullptr, BD_ERR_ARG, "device %d out of range (%d devices)", device, n);
+  BdHandle* h = new BdHandle();
+  h->device = device;
+  e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->n_sm, cudaDevAttrMultiProcessorCount, device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    fail(nullptr, BD_ERR_CUDA, "device setup: %s", cudaGetErrorString(e));
+    delete h;
+    return BD_ERR_CUDA;
+  }
+  *out = h;
+  return BD_OK;
+}
+
+int bd_destroy(BdHandle* h) {
+  if (!h) return BD_OK;
+  cudaSetDevice(h->device);
+  cudaDeviceSynchronize();
+  for (auto& g : h->graph)
+    if (g) cudaGraphExecDestroy(g);
+  free_list(h->sys_allocs);
+  free_list(h->sim_allocs);
+  if (h->own) cudaStreamDestroy(h->own);
+  delete h;
+  return BD_OK;
+}
+
+int bd_last_error(const BdHandle* h, char* buf, int len) {
+  if (!buf || len <= 0) return BD_ERR_ARG;
+  const std::string& s = h ? h->err : g_create_error;
+  snprintf(buf, (size_t)len, "%s", s.c_str());
+  return BD_OK;
+}
+
+int bd_set_ligand(BdHandle* h, int n, const double* xyz, const double* q) {
+  if (!h || n <= 0 || !xyz || !q) return fail(h, BD_ERR_ARG, "bd_set_ligand: bad arguments");
+  h->lig.assign(4 * (size_t)n, 0.0);
+  for (int i = 0; i < n; ++i) {
+    for (int k = 0; k < 3; ++k) h->lig[4 * i + k] = xyz[3 * i + k];
+    h->lig[4 * i + 3] = q[i];
+    for (int k = 0; k < 4; ++k)
+      if (!std::isfinite(h->lig[4 * i + k])) return fail(h, BD_ERR_NAN, "ligand atom %d is not finite", i);
+  }
+  h->dirty = true;
+  return BD_OK;
+}
+
+int bd_set_receptor(BdHandle* h, int n, const double* xyz, const double* q) {
+  if (!h || n < 0 || (n > 0 && (!xyz || !q))) return fail(h, BD_ERR_ARG, "bd_set_receptor: bad arguments");
+  h->rec.assign(4 * (size_t)n, 0.0);
+  for (int i = 0; i < n; ++i) {
+    for (int k = 0; k < 3; ++k) h->rec[4 * i + k] = xyz[3 * i + k];
+    h->rec[4 * i + 3] = q[i];
+    for (int k = 0; k < 4; ++k)
+      if (!std::isfinite(h->rec[4 * i + k])) return fail(h, BD_ERR_NAN, "receptor atom %d is not finite", i);
+  }
+  h->dirty = true;
+  return BD_OK;
+}
+
+int bd_add_grid(BdHandle* h, int kind, const float* data, int nx, int ny, int nz, const double* origin,
+                const double* spacing) {
+  if (!h) return BD_ERR_ARG;
+  if (kind < 0 || kind > 2 || !data || !origin || !spacing) return fail(h, BD_ERR_ARG, "bd_add_grid: bad arguments");
+  if (nx < 8 || ny < 8 || nz < 8) return fail(h, BD_ERR_ARG, "grid %dx%dx%d: each axis needs >= 8 nodes", nx, ny, nz);
+  if ((long long)nx * ny * nz > (1ll << 31) / 2) return fail(h, BD_ERR_ARG, "grid too large");
+  GridHost g;
+  g.n[0] = nx;
+  g.n[1] = ny;
+  g.n[2] = nz;
+  for (int k = 0; k < 3; ++k) {
+    g.o[k] = origin[k];
+    g.sp[k] = spacing[k];
+    if (!(spacing[k] > 0) || !std::isfinite(origin[k])) return fail(h, BD_ERR_ARG, "bad grid origin/spacing");
+  }
+  const size_t n = (size_t)nx * ny * nz;
+  g.data.assign(data, data + n);
+  for (size_t i = 0; i < n; ++i)
+    if (!std::isfinite(g.data[i])) return fail(h, BD_ERR_NAN, "grid value %zu is not finite", i);
+  h->grids[kind].push_back(std::move(g));
+  h->dirty = true;
+  return BD_OK;
+}
+
+int bd_clear_grids(BdHandle* h) {
+  if (!h) return BD_ERR_ARG;
+  for (auto& v : h->grids) v.clear();
+  h->dirty = true;
+  return BD_OK;
+}
+
+int bd_set_force_params(BdHandle* h, const BdForceParams* p) {
+  if (!h || !p) return fail(h, BD_ERR_ARG, "bd_set_force_params: NULL");
+  if (p->use_multipole && !(p->four_pi_eps > 0)) return fail(h, BD_ERR_ARG, "four_pi_eps must be > 0");
+  h->fp = *p;
+  h->fp_set = true;
+  h->dirty = true;
+  return BD_OK;
+}
+
+int bd_set_reactions(BdHandle* h, int n_pairs, const double* rec_xyz, const double* lig_xyz, const double* cut,
+                     const double* d_eff, int n_needed) {
+  if (!h) return BD_ERR_ARG;
+  if (n_pairs < 0 || n_pairs > BD_MAX_PAIRS) return fail(h, BD_ERR_ARG, "n_pairs must be in [0, %d]", BD_MAX_PAIRS);
+  if (n_pairs > 0 && (!rec_xyz || !lig_xyz || !cut || !d_eff)) return fail(h, BD_ERR_ARG, "bd_set_reactions: NULL");
+  h->n_pairs = n_pairs;
+  h->n_needed = n_needed;
+  for (int p = 0; p < n_pairs; ++p) {
+    for (int k = 0; k < 3; ++k) {
+      h->rx_rec[p][k] = rec_xyz[3 * p + k];
+      h->rx_body[p][k] = lig_xyz[3 * p + k];
+    }
+    h->rx_cut[p] = cut[p];
+    h->rx_deff[p] = d_eff[p];
+  }
+  h->dirty = true;
+  return BD_OK;
+}
+
+int bd_eval_forces(BdHandle* h, int64_t n, const double* cen, const double* rot, int rot_is_matrix, double* F,
+                   double* T, double* E, int prec, int torque, void* stream) {
+  if (!h) return BD_ERR_ARG;
+  if (n < 0 || (n > 0 && (!cen || !rot || !F || !T || !E))) return fail(h, BD_ERR_ARG, "bd_eval_forces: bad arguments");
+  if (prec != BD_PREC_FP64 && prec != BD_PREC_MIXED) return fail(h, BD_ERR_ARG, "bad precision %d", prec);
+  if (torque != BD_TORQUE_ZERO && torque != BD_TORQUE_CENTROID) return fail(h, BD_ERR_ARG, "bad torque mode %d", torque);
+  int rc = finalize(h);
+  if (rc) return rc;
+  if (n == 0) return BD_OK;
+  const int G = h->launch_user ? h->group : default_group(n_charged(h), h->S.born_rev);
+  const int block = 128;
+  void* fn = kernel_for(prec, G, torque, 0);
+  unsigned long long* ctr = nullptr;
+  long long nn = n;
+  int rim = rot_is_matrix;
+  void* args[] = {&h->S, &nn, &cen, &rot, &rim, &F, &T, &E, &ctr};
+  CK(h, cudaLaunchKernel(fn, dim3(eval_grid_blocks(h, n, G, block)), dim3(block), args, 0, pick(h, stream)));
+  return BD_OK;
+}
+
+int bd_eval_forces_atoms(BdHandle* h, int64_t n, const double* pos, const double* R, const double* cen, double* F,
+                         double* T, double* E, int prec, int torque, void* stream) {
+  if (!h) return BD_ERR_ARG;
+  if (n < 0 || (n > 0 && (!pos || !R || !cen || !F || !T || !E)))
+    return fail(h, BD_ERR_ARG, "bd_eval_forces_atoms: bad arguments");
+  if (prec != BD_PREC_FP64 && prec != BD_PREC_MIXED) return fail(h, BD_ERR_ARG, "bad precision %d", prec);
+  if (torque != BD_TORQUE_ZERO && torque != BD_TORQUE_CENTROID) return fail(h, BD_ERR_ARG, "bad torque mode %d", torque);
+  int rc = finalize(h);
+  if (rc) return rc;
+  if (n == 0) return BD_OK;
+  const int G = h->launch_user ? h->group : default_group(n_charged(h), h->S.born_rev);
+  const int block = 128;
+  void* fn = kernel_for(prec, G, torque, 1);
+  long long nn = n;
+  void* args[] = {&h->S, &nn, &pos, &R, &cen, &F, &T, &E};
+  CK(h, cudaLaunchKernel(fn, dim3(eval_grid_blocks(h, n, G, block)), dim3(block), args, 0, pick(h, stream)));
+  return BD_OK;
+}
+
+int bd_set_launch(BdHandle* h, int group, int block) {
+  if (!h) return BD_ERR_ARG;
+  if (group && !valid_group(group)) return fail(h, BD_ERR_ARG, "group must be 1, 4, 8, 16 or 32");
+  if (block && (block % 32 || block < 32 || block > 256)) return fail(h, BD_ERR_ARG, "block must be 32..256, x32");
+  if (group) h->group = group;
+  if (block) h->block = block;
+  h->launch_user = group != 0 || h->launch_user;
+  h->graph_K = -1;
+  return BD_OK;
+}
+
+int bd_get_launch(BdHandle* h, int* group, int* block, int* grid) {
+  if (!h) return BD_ERR_ARG;
+  const int G = h->launch_user ? h->group : default_group(n_charged(h), h->S.born_rev);
+  if (group) *group = G;
+  if (block) *block = h->block;
+  if (grid) {
+    void* fn = kernel_for(h->sp.precision, G, h->sp.torque_mode, 2);
+    *grid = fn ? persistent_blocks(h, fn, h->block) : 0;
+  }
+  return BD_OK;
+}
+
+int bd_sim_configure(BdHandle* h, const BdSimParams* p) {
+  if (!h || !p) return fail(h, BD_ERR_ARG, "bd_sim_configure: NULL");
+  if (p->n_traj <= 0 || p->n_traj > 0x7ffffff0ll) return fail(h, BD_ERR_ARG, "n_traj out of range");
+  if (p->id_offset < 0) return fail(h, BD_ERR_ARG, "id_offset must be >= 0");
+  if (!(p->r_escape > p->r_start) || !(p->r_start > 0)) return fail(h, BD_ERR_ARG, "need 0 < r_start < r_escape");
+  if (!(p->D_t > 0) || !(p->D_r >= 0)) return fail(h, BD_ERR_ARG, "diffusion coefficients must be positive");
+  if (p->max_steps <= 0) return fail(h, BD_ERR_ARG, "max_steps must be positive");
+  if (p->precision != BD_PREC_FP64 && p->precision != BD_PREC_MIXED) return fail(h, BD_ERR_ARG, "bad precision");
+  if (p->torque_mode != BD_TORQUE_ZERO && p->torque_mode != BD_TORQUE_CENTROID) return fail(h, BD_ERR_ARG, "bad torque");
+  if (p->use_hi && !(p->r_hydro_rec > 0 && p->r_hydro_lig > 0)) return fail(h, BD_ERR_ARG, "HI needs hydro radii");
+  int rc = finalize(h);
+  if (rc) return rc;
+  CK(h, cudaSetDevice(h->device));
+  CK(h, cudaDeviceSynchronize());
+  free_list(h->sim_allocs);
+  h->sim_ready = false;
+  h->sp = *p;
+  // live-slot capacity
+  const int G = h->launch_user ? h->group : default_group(n_charged(h), h->S.born_rev);
+  void* fn = kernel_for(p->precision, G, p->torque_mode, 2);
+  const long long resident = (long long)persistent_blocks(h, fn, h->block) * (h->block / G);
+  long long cap = p->slots > 0 ? p->slots : std::max<long long>(65536, 8 * resident);
+  cap = std::min<long long>(cap, p->n_traj);
+  const int C = (int)cap;
+  for (int b = 0; b < 2; ++b) {
+    SlotBuf& B = h->buf[b];
+    void* q;
+    if ((rc = dev_alloc(h, h->sim_allocs, &q, 3 * (size_t)C * sizeof(double)))) return rc;
+    B.c = (double*)q;
+    if ((rc = dev_alloc(h, h->sim_allocs, &q, 4 * (size_t)C * sizeof(double)))) return rc;
+    B.q = (double*)q;
+    if ((rc = dev_alloc(h, h->sim_allocs, &q, (size_t)C * sizeof(int)))) return rc;
+    B.traj = (int*)q;
+    if ((rc = dev_alloc(h, h->sim_allocs, &q, (size_t)C * sizeof(int)))) return rc;
+    B.steps = (int*)q;
+    if ((rc = dev_alloc(h, h->sim_allocs, &q, (size_t)C * sizeof(int)))) return rc;
+    B.rets = (int*)q;
+    if ((rc = dev_alloc(h, h->sim_allocs, &q, (size_t)C))) return rc;
+    B.status = (int8_t*)q;
+    B.cap = C;
+  }
+  void* q;
+  if ((rc = dev_alloc(h, h->sim_allocs, &q, 2 * sizeof(int)))) return rc;
+  h->d_live = (int*)q;
+  if ((rc = dev_alloc(h, h->sim_allocs, &q, C_NUM * sizeof(unsigned long long)))) return rc;
+  h->d_ctr = (unsigned long long*)q;
+  DevSim& P = h->P;
+  P = DevSim{};
+  P.n_traj = p->n_traj;
+  P.id_offset = p->id_offset;
+  P.k0 = (uint32_t)(p->seed & 0xffffffffull);
+  P.k1 = (uint32_t)(p->seed >> 32);
+  P.r_b = p->r_start;
+  P.r_esc = p->r_escape;
+  P.return_prob = p->return_prob;
+  P.max_steps = p->max_steps;
+  P.max_dt = p->max_dt;
+  P.min_core_dt = p->min_core_dt;
+  P.use_hi = p->use_hi;
+  P.overlap = p->overlap && h->S.n_chunks > 0;
+  P.D_t = p->D_t;
+  P.D_r = p->D_r;
+  // adaptive dt force criterion: dielectric hard-coded to 78 (gpu_batch_simulator.py:622-629)
+  P.adt_V0 = p->q_rec_total * p->q_lig_total / (4.0 * kPi * (78.0 * kEps0));
+  P.adt_has_force = std::fabs(P.adt_V0) > 1e-9;
+  P.adt_debye = p->adt_debye;
+  P.adt_inv_debye = 1.0 / p->adt_debye;
+  // HI constants, mu = 0.243 hard-coded (gpu_batch_simulator.py:741-751)
+  P.hi_Df = 1.0 / 0.243;
+  if (p->use_hi) {
+    const double a0 = p->r_hydro_rec, a1 = p->r_hydro_lig;
+    P.hi_a2 = 0.5 * (a0 * a0 + a1 * a1);
+    P.hi_ainv = (P.hi_Df / (6.0 * kPi * a0) + P.hi_Df / (6.0 * kPi * a1)) / P.hi_Df;
+  }
+  P.ctr = h->d_ctr;
+  if ((rc = dev_alloc(h, h->sim_allocs, &q, (size_t)p->n_traj))) return rc;
+  P.out_status = (int8_t*)q;
+  if ((rc = dev_alloc(h, h->sim_allocs, &q, (size_t)p->n_traj * sizeof(int)))) return rc;
+  P.out_steps = (int*)q;
+  if ((rc = dev_alloc(h, h->sim_allocs, &q, (size_t)p->n_traj * sizeof(int)))) return rc;
+  P.out_returns = (int*)q;
+  h->sim_ready = true;
+  h->graph_K = -1;
+  return BD_OK;
+}
+
+int bd_sim_reset(BdHandle* h, void* stream) {
+  if (!h) return BD_ERR_ARG;
+  if (!h->sim_ready) return fail(h, BD_ERR_STATE, "bd_sim_reset before bd_sim_configure");
+  int rc = finalize(h);
+  if (rc) return rc;
+  cudaStream_t s = pick(h, stream);
+  const int C = h->buf[0].cap;
+  CK(h, cudaMemsetAsync(h->d_ctr, 0, C_NUM * sizeof(unsigned long long), s));
+  CK(h, cudaMemsetAsync(h->P.out_status, 0, (size_t)h->P.n_traj, s));
+  CK(h, cudaMemsetAsync(h->P.out_steps, 0, (size_t)h->P.n_traj * sizeof(int), s));
+  CK(h, cudaMemsetAsync(h->P.out_returns, 0, (size_t)h->P.n_traj * sizeof(int), s));
+  init_slots_kernel<<<(C + 255) / 256, 256, 0, s>>>(h->P, h->buf[0], C);
+  CK(h, cudaGetLastError());
+  const unsigned long long started = (unsigned long long)C;
+  CK(h, cudaMemcpyAsync(h->d_ctr + C_PENDING, &started, sizeof started, cudaMemcpyHostToDevice, s));
+  CK(h, cudaMemcpyAsync(h->d_live, &C, sizeof C, cudaMemcpyHostToDevice, s));
+  CK(h, cudaStreamSynchronize(s));
+  h->cur = 0;
+  return BD_OK;
+}
+
+namespace {
+
+int enqueue_launch(BdHandle* h, int K, cudaStream_t s, int cur) {
+  const int G = h->launch_user ? h->group : default_group(n_charged(h), h->S.born_rev);
+  void* fn = kernel_for(h->sp.precision, G, h->sp.torque_mode, 2);
+  const int blocks = persistent_blocks(h, fn, h->block);
+  SlotBuf src = h->buf[cur], dst = h->buf[1 - cur];
+  const int* live = h->d_live + cur;
+  int* live_dst = h->d_live + (1 - cur);
+  void* args[] = {&h->S, &h->P, &src, &live, &K};
+  CK(h, cudaLaunchKernel(fn, dim3(blocks), dim3(h->block), args, 0, s));
+  compact_kernel<<<h->n_sm * 4, 256, 0, s>>>(src, dst, live, h->d_ctr);
+  CK(h, cudaGetLastError());
+  finish_compact_kernel<<<1, 1, 0, s>>>(live_dst, h->d_ctr);
+  CK(h, cudaGetLastError());
+  return BD_OK;
+}
+
+int build_graphs(BdHandle* h, int K) {
+  const int G = h->launch_user ? h->group : default_group(n_charged(h), h->S.born_rev);
+  if (h->graph_K == K && h->graph_G == G && h->graph_B == h->block && h->graph_prec == h->sp.precision &&
+      h->graph_torque == h->sp.torque_mode)
+    return BD_OK;
+  for (auto& g : h->graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+  for (int c = 0; c < 2; ++c) {
+    cudaGraph_t graph;
+    CK(h, cudaStreamBeginCapture(h->own, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_launch(h, K, h->own, c);
+    cudaError_t e = cudaStreamEndCapture(h->own, &graph);
+    if (rc) return rc;
+    CK(h, e);
+    e = cudaGraphInstantiate(&h->graph[c], graph, 0);
+    cudaGraphDestroy(graph);
+    CK(h, e);
+  }
+  h->graph_K = K;
+  h->graph_G = G;
+  h->graph_B = h->block;
+  h->graph_prec = h->sp.precision;
+  h->graph_torque = h->sp.torque_mode;
+  return BD_OK;
+}
+
+}  // namespace
+
+int bd_sim_run(BdHandle* h, int n_launch, int K, void* stream) {
+  if (!h) return BD_ERR_ARG;
+  if (!h->sim_ready) return fail(h, BD_ERR_STATE, "bd_sim_run before bd_sim_configure");
+  if (n_launch < 0 || K <= 0) return fail(h, BD_ERR_ARG, "bd_sim_run: n_launch >= 0 and steps > 0 needed");
+  if (h->dirty) return fail(h, BD_ERR_STATE, "system changed after bd_sim_reset; reset again");
+  int rc = build_graphs(h, K);
+  if (rc) return rc;
+  cudaStream_t s = pick(h, stream);
+  for (int i = 0; i < n_launch; ++i) {
+    CK(h, cudaGraphLaunch(h->graph[h->cur], s));
+    h->cur = 1 - h->cur;
+  }
+  return BD_OK;
+}
+
+int bd_sim_counters(BdHandle* h, uint64_t* out, int n, void* stream) {
+  if (!h || !out) return BD_ERR_ARG;
+  if (!h->sim_ready) return fail(h, BD_ERR_STATE, "no simulation configured");
+  unsigned long long c[C_NUM];
+  cudaStream_t s = pick(h, stream);
+  CK(h, cudaMemcpyAsync(c, h->d_ctr, sizeof c, cudaMemcpyDeviceToHost, s));
+  CK(h, cudaStreamSynchronize(s));
+  const int m = std::min(n, (int)BD_CTR_NUM);
+  for (int i = 0; i < m; ++i) out[i] = c[i];
+  if (m > 0) out[0] = std::min<unsigned long long>(c[C_PENDING], (unsigned long long)h->P.n_traj);
+  return BD_OK;
+}
+
+int bd_sim_outcomes(BdHandle* h, int8_t* status, int32_t* steps, int32_t* rets) {
+  if (!h) return BD_ERR_ARG;
+  if (!h->sim_ready) return fail(h, BD_ERR_STATE, "no simulation configured");
+  CK(h, cudaDeviceSynchronize());
+  const size_t n = (size_t)h->P.n_traj;
+  if (status) CK(h, cudaMemcpy(status, h->P.out_status, n, cudaMemcpyDeviceToHost));
+  if (steps) CK(h, cudaMemcpy(steps, h->P.out_steps, n * sizeof(int), cudaMemcpyDeviceToHost));
+  if (rets) CK(h, cudaMemcpy(rets, h->P.out_returns, n * sizeof(int), cudaMemcpyDeviceToHost));
+  return BD_OK;
+}
+
+int bd_sim_live(BdHandle* h, int32_t* n_live) {
+  if (!h || !n_live) return BD_ERR_ARG;
+  if (!h->sim_ready) return fail(h, BD_ERR_STATE, "no simulation configured");
+  CK(h, cudaDeviceSynchronize());
+  CK(h, cudaMemcpy(n_live, h->d_live + h->cur, sizeof(int), cudaMemcpyDeviceToHost));
+  return BD_OK;
+}
+
+int bd_sim_capacity(BdHandle* h, int32_t* cap) {
+  if (!h || !cap) return BD_ERR_ARG;
+  if (!h->sim_ready) return fail(h, BD_ERR_STATE, "no simulation configured");
+  *cap = h->buf[0].cap;
+  return BD_OK;
+}
+
+int bd_sim_snapshot(BdHandle* h, double* c, double* q, int32_t* traj, int32_t* steps, int32_t* rets, int8_t* status,
+                    int32_t* n_live, uint64_t* counters) {
+  if (!h || !c || !q || !traj || !steps || !rets || !status || !n_live || !counters)
+    return fail(h, BD_ERR_ARG, "bd_sim_snapshot: NULL");
+  if (!h->sim_ready) return fail(h, BD_ERR_STATE, "no simulation configured");
+  CK(h, cudaDeviceSynchronize());
+  const SlotBuf& B = h->buf[h->cur];
+  const size_t C = (size_t)B.cap;
+  CK(h, cudaMemcpy(c, B.c, 3 * C * sizeof(double), cudaMemcpyDeviceToHost));
+  CK(h, cudaMemcpy(q, B.q, 4 * C * sizeof(double), cudaMemcpyDeviceToHost));
+  CK(h, cudaMemcpy(traj, B.traj, C * sizeof(int), cudaMemcpyDeviceToHost));
+  CK(h, cudaMemcpy(steps, B.steps, C * sizeof(int), cudaMemcpyDeviceToHost));
+  CK(h, cudaMemcpy(rets, B.rets, C * sizeof(int), cudaMemcpyDeviceToHost));
+  CK(h, cudaMemcpy(status, B.status, C, cudaMemcpyDeviceToHost));
+  CK(h, cudaMemcpy(n_live, h->d_live + h->cur, sizeof(int), cudaMemcpyDeviceToHost));
+  unsigned long long ctr[C_NUM];
+  CK(h, cudaMemcpy(ctr, h->d_ctr, sizeof ctr, cudaMemcpyDeviceToHost));
+  for (int i = 0; i < BD_CTR_NUM; ++i) counters[i] = ctr[i];
+  return BD_OK;
+}
+
+int bd_sim_restore(BdHandle* h, const double* c, const double* q, const int32_t* traj, const int32_t* steps,
+                   const int32_t* rets, const int8_t* status, int32_t n_live, const uint64_t* counters,
+                   const int8_t* out_status, const int32_t* out_steps, const int32_t* out_returns) {
+  if (!h || !c || !q || !traj || !steps || !rets || !status || !counters || !out_status || !out_steps || !out_returns)
+    return fail(h, BD_ERR_ARG, "bd_sim_restore: NULL");
+  if (!h->sim_ready) return fail(h, BD_ERR_STATE, "no simulation configured");
+  int rc = finalize(h);
+  if (rc) return rc;
+  const SlotBuf& B = h->buf[0];
+  const size_t C = (size_t)B.cap;
+  if (n_live < 0 || (size_t)n_live > C) return fail(h, BD_ERR_ARG, "n_live out of range");
+  CK(h, cudaDeviceSynchronize());
+  CK(h, cudaMemcpy(B.c, c, 3 * C * sizeof(double), cudaMemcpyHostToDevice));
+  CK(h, cudaMemcpy(B.q, q, 4 * C * sizeof(double), cudaMemcpyHostToDevice));
+  CK(h, cudaMemcpy(B.traj, traj, C * sizeof(int), cudaMemcpyHostToDevice));
+  CK(h, cudaMemcpy(B.steps, steps, C * sizeof(int), cudaMemcpyHostToDevice));
+  CK(h, cudaMemcpy(B.rets, rets, C * sizeof(int), cudaMemcpyHostToDevice));
+  CK(h, cudaMemcpy(B.status, status, C, cudaMemcpyHostToDevice));
+  unsigned long long ctr[C_NUM] = {0};
+  for (int i = 0; i < BD_CTR_NUM; ++i) ctr[i] = counters[i];
+  ctr[C_SLOT_CURSOR] = 0;
+  ctr[C_LIVE_NEXT] = 0;
+  CK(h, cudaMemcpy(h->d_ctr, ctr, sizeof ctr, cudaMemcpyHostToDevice));
+  CK(h, cudaMemcpy(h->d_live, &n_live, sizeof(int), cudaMemcpyHostToDevice));
+  const size_t n = (size_t)h->P.n_traj;
+  CK(h, cudaMemcpy(h->P.out_status, out_status, n, cudaMemcpyHostToDevice));
+  CK(h, cudaMemcpy(h->P.out_steps, out_steps, n * sizeof(int), cudaMemcpyHostToDevice));
+  CK(h, cudaMemcpy(h->P.out_returns, out_returns, n * sizeof(int), cudaMemcpyHostToDevice));
+  h->cur = 0;
+  return BD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,377 @@
+// Device-side building blocks of the batched rigid-body BD engine (sm_100a).
+//
+// Conventions follow the reference's batched stepper and force engine:
+//   quaternions (w,x,y,z), R(q) as pystarc/simulation/gpu_batch_simulator.py:1611-1629,
+//   q <- normalize(q (x) dq(omega)) as :1631-1660,
+//   grids C-ordered (nx,ny,nz), z fastest, index i*ny*nz + j*nz + k
+//   (pystarc/forces/electrostatic/grid_force.py:144), strict in-grid box
+//   [origin + 3 sp, origin + (n-4) sp] (pystarc/forces/gpu_batch_engine.py:268-273).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define BD_MAX_ELEC 4
+#define BD_MAX_PAIRS 16
+#define BD_CHUNK 32
+
+namespace bd {
+
+enum : int { ST_RUNNING = 0, ST_REACTED = 1, ST_ESCAPED = 2, ST_MAXSTEPS = 3, ST_EMPTY = 4, ST_ERROR = 5 };
+
+// Tally slots (unsigned long long counters on the device).
+enum : int {
+  C_PENDING = 0,    // next trajectory id to start (the pending pool cursor)
+  C_REACTED,
+  C_ESCAPED,
+  C_MAXSTEPS,
+  C_STEPS,          // trajectory-steps (reference total_steps)
+  C_RETURNS,        // escape -> return events
+  C_OVERLAP,        // overlap rejections
+  C_BRIDGE,         // reactions found by the Brownian bridge
+  C_GRID_EVALS,     // (atom, grid) stencil evaluations, forward direction
+  C_REV_EVALS,      // receptor-atom stencil evaluations, reverse Born
+  C_FF_EVALS,       // far-field atom evaluations
+  C_NONFINITE,      // steps that produced a non-finite pose (trajectory stopped)
+  C_SLOT_CURSOR,    // dynamic slot cursor of the current launch
+  C_LIVE_NEXT,      // live-slot count being built by the compaction
+  C_NUM
+};
+
+struct DevGrid {
+  const float* data;  // FP32 values; `ch` interleaved channels per node
+  int nx, ny, nz, ch;
+  double ox, oy, oz;
+  double isx, isy, isz;  // 1/spacing
+  double lox, loy, loz, hix, hiy, hiz;  // strict margin box
+};
+
+struct DevSystem {
+  // ligand (body frame = about the ligand centroid)
+  int n_lig;
+  const double4* lig;  // x,y,z,q (FP64)
+  // receptor atoms in spatial chunks of BD_CHUNK (padded with copies of the last atom, q = 0)
+  int n_rec_pad, n_chunks;
+  const double4* rec;     // x,y,z,q
+  const double4* chunks;  // centre xyz, radius
+  double rec_max_r;
+  // grids
+  int n_elec;
+  DevGrid elec[BD_MAX_ELEC];
+  int has_born;
+  DevGrid born;
+  int paired;        // elec[0] and born share a lattice; `pair` holds both (ch = 2)
+  DevGrid pair;
+  int born_rev;      // reverse Born active
+  DevGrid lig_born;
+  double lig_born_rho;  // circumradius of the ligand Born box about the ligand origin
+  // far field (receptor at the origin)
+  int has_yukawa, use_dip, use_quad;
+  double V_factor, inv_debye, inv_fpe;
+  double dip[3], quad[9];
+  double alpha;
+  // reaction pairs (flattened)
+  int n_pairs, n_needed;
+  double rx_rec[BD_MAX_PAIRS][3];
+  double rx_body[BD_MAX_PAIRS][3];
+  double rx_cut[BD_MAX_PAIRS];
+  double rx_deff[BD_MAX_PAIRS];
+};
+
+struct DevSim {
+  long long n_traj;
+  long long id_offset;  // global id of local trajectory 0
+  uint32_t k0, k1;  // seed words
+  double r_b, r_esc, return_prob;
+  int max_steps;
+  double max_dt, min_core_dt;
+  int use_hi, overlap;
+  double D_t, D_r;
+  double adt_V0, adt_inv_debye, adt_debye;
+  int adt_has_force;
+  double hi_Df, hi_ainv, hi_a2;
+  unsigned long long* ctr;
+  int8_t* out_status;
+  int* out_steps;
+  int* out_returns;
+};
+
+struct SlotBuf {
+  double* c;    // 3 * cap (x block, y block, z block)
+  double* q;    // 4 * cap
+  int* traj;
+  int* steps;
+  int* rets;
+  int8_t* status;
+  int cap;
+};
+
+// ----------------------------------------------------------------------------
+// Philox4x32-10 (Salmon et al., SC'11) and the draws built from it
+// ----------------------------------------------------------------------------
+struct W4 { uint32_t a, b, c, d; };
+
+__device__ __forceinline__ W4 philox10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0,
+                                       uint32_t k1) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    if (r > 0) {
+      k0 += 0x9E3779B9u;
+      k1 += 0xBB67AE85u;
+    }
+    const uint32_t hi0 = __umulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
+    const uint32_t hi1 = __umulhi(0xCD9E8D57u, c2), lo1 = 0xCD9E8D57u * c2;
+    const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+    c0 = n0;
+    c1 = lo1;
+    c2 = n2;
+    c3 = lo0;
+  }
+  return {c0, c1, c2, c3};
+}
+
+__device__ __forceinline__ double u53(uint32_t a, uint32_t b) {
+  return ((double)(a >> 5) * 67108864.0 + (double)(b >> 6)) * (1.0 / 9007199254740992.0);
+}
+
+__device__ __forceinline__ void box_muller(double u1, double u2, double& n0, double& n1) {
+  const double rad = sqrt(-2.0 * log(1.0 - u1));
+  double s, c;
+  sincospi(2.0 * u2, &s, &c);
+  n0 = rad * c;
+  n1 = rad * s;
+}
+
+enum : uint32_t { SUB_ESCAPE = 0, SUB_NORMALS = 1, SUB_RETURN_Q = 4, SUB_BRIDGE = 6 };
+enum : uint32_t { INIT_STEP = 0xFFFFFFFFu, SUB_INIT_DIR = 0, SUB_INIT_Q = 2 };
+
+struct Keyed {
+  uint32_t k0, k1, t0, t1;
+  __device__ __forceinline__ W4 w(uint32_t step, uint32_t sub) const { return philox10(step, sub, t0, t1, k0, k1); }
+};
+
+// ----------------------------------------------------------------------------
+// Small vector helpers
+// ----------------------------------------------------------------------------
+__device__ __forceinline__ double norm3(double x, double y, double z) { return sqrt(x * x + y * y + z * z); }
+
+__device__ __forceinline__ void quat_to_rot(const double q[4], double R[9]) {
+  const double w = q[0], x = q[1], y = q[2], z = q[3];
+  R[0] = 1 - 2 * (y * y + z * z);
+  R[1] = 2 * (x * y - w * z);
+  R[2] = 2 * (x * z + w * y);
+  R[3] = 2 * (x * y + w * z);
+  R[4] = 1 - 2 * (x * x + z * z);
+  R[5] = 2 * (y * z - w * x);
+  R[6] = 2 * (x * z - w * y);
+  R[7] = 2 * (y * z + w * x);
+  R[8] = 1 - 2 * (x * x + y * y);
+}
+
+__device__ __forceinline__ void shoemake(double u0, double u1, double u2, double q[4]) {
+  const double a = sqrt(1 - u0), b = sqrt(u0);
+  double s1, c1, s2, c2;
+  sincospi(2.0 * u1, &s1, &c1);
+  sincospi(2.0 * u2, &s2, &c2);
+  q[0] = a * s1;
+  q[1] = a * c1;
+  q[2] = b * s2;
+  q[3] = b * c2;
+}
+
+// q <- normalize(q (x) dq(omega)); omega applied in the body frame.
+__device__ __forceinline__ void rotate_quat(double q[4], double o0, double o1, double o2) {
+  const double angle = norm3(o0, o1, o2);
+  double a0 = 0, a1 = 0, a2 = 0;
+  if (angle > 1e-10) {
+    a0 = o0 / angle;
+    a1 = o1 / angle;
+    a2 = o2 / angle;
+  }
+  double sh, ch;
+  sincos(angle * 0.5, &sh, &ch);
+  const double w2 = ch, x2 = a0 * sh, y2 = a1 * sh, z2 = a2 * sh;
+  const double w1 = q[0], x1 = q[1], y1 = q[2], z1 = q[3];
+  double n0 = w1 * w2 - x1 * x2 - y1 * y2 - z1 * z2;
+  double n1 = w1 * x2 + x1 * w2 + y1 * z2 - z1 * y2;
+  double n2 = w1 * y2 - x1 * z2 + y1 * w2 + z1 * x2;
+  double n3 = w1 * z2 + x1 * y2 - y1 * x2 + z1 * w2;
+  const double nn = sqrt(n0 * n0 + n1 * n1 + n2 * n2 + n3 * n3);
+  q[0] = n0 / nn;
+  q[1] = n1 / nn;
+  q[2] = n2 / nn;
+  q[3] = n3 / nn;
+}
+
+// ----------------------------------------------------------------------------
+// Grid stencil.
+//
+// The reference's gradient is (I(x+h) - I(x-h)) / (2h), h = sp/2, with I the
+// trilinear interpolant, per axis and at the centre point's other two
+// coordinates (gpu_batch_engine.py:111-114).  Because I is linear in the node
+// values, each axis term equals a weighted sum of ADJACENT-node differences:
+// with c = floor(u), s = u - c, the two probes share the fraction |s - 1/2|
+// and straddle one extra node e = c-1 (s < 1/2) or c+2 (s >= 1/2), so
+//     D = (1 - a) (v[c+1] - v[c]) + a * De,   a = |s - 1/2|,
+// De = v[c] - v[c-1] or v[c+2] - v[c+1], summed with the centre's bilinear
+// weights on the other axes.  This reads 20 distinct nodes (centre cube + one
+// extra node per cube edge line) instead of the reference's 7 x 8 = 56, and
+// the differences avoid cancelling the large common offset in FP32.
+// ----------------------------------------------------------------------------
+template <typename FT, int CH>
+struct StencilOut {
+  FT phi[CH], gx[CH], gy[CH], gz[CH];
+};
+
+__device__ __forceinline__ bool in_box(const DevGrid& g, double x, double y, double z) {
+  return x > g.lox && x < g.hix && y > g.loy && y < g.hiy && z > g.loz && z < g.hiz;
+}
+
+template <int CH>
+__device__ __forceinline__ void ld(const float* p, float v[CH]) {
+  if constexpr (CH == 1) {
+    v[0] = __ldg(p);
+  } else {
+    const float2 t = __ldg(reinterpret_cast<const float2*>(p));
+    v[0] = t.x;
+    v[1] = t.y;
+  }
+}
+
+template <typename FT, int CH>
+__device__ __forceinline__ StencilOut<FT, CH> stencil(const DevGrid& g, double x, double y, double z) {
+  const double ux = (x - g.ox) * g.isx, uy = (y - g.oy) * g.isy, uz = (z - g.oz) * g.isz;
+  const double fx = floor(ux), fy = floor(uy), fz = floor(uz);
+  const int cx = (int)fx, cy = (int)fy, cz = (int)fz;
+  const double sxd = ux - fx, syd = uy - fy, szd = uz - fz;
+  const bool lx = sxd < 0.5, ly = syd < 0.5, lz = szd < 0.5;
+  const int ex = lx ? cx - 1 : cx + 2, ey = ly ? cy - 1 : cy + 2;
+  const FT sx = (FT)sxd, sy = (FT)syd, sz = (FT)szd;
+  const FT ax = (FT)(lx ? 0.5 - sxd : sxd - 0.5);
+  const FT ay = (FT)(ly ? 0.5 - syd : syd - 0.5);
+  const FT az = (FT)(lz ? 0.5 - szd : szd - 0.5);
+  const long nz = g.nz, syz = (long)g.ny * g.nz;
+  const float* d = g.data;
+  // centre rows (cx+i, cy+j): three z nodes starting at zb
+  const int zb = lz ? cz - 1 : cz;
+  const int zc = lz ? 1 : 0;  // position of node cz inside the three-node run
+  const int ze = lz ? 0 : 2;  // position of the extra z node
+  float r[2][2][3][CH];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const long base = ((long)(cx + i) * syz + (long)(cy + j) * nz + zb) * CH;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) ld<CH>(d + base + k * CH, r[i][j][k]);
+    }
+  float xe[2][2][CH], ye[2][2][CH];
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const long base = ((long)ex * syz + (long)(cy + j) * nz + cz) * CH;
+    ld<CH>(d + base, xe[j][0]);
+    ld<CH>(d + base + CH, xe[j][1]);
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const long base = ((long)(cx + i) * syz + (long)ey * nz + cz) * CH;
+    ld<CH>(d + base, ye[i][0]);
+    ld<CH>(d + base + CH, ye[i][1]);
+  }
+  const FT wx[2] = {(FT)1 - sx, sx}, wy[2] = {(FT)1 - sy, sy}, wz[2] = {(FT)1 - sz, sz};
+  StencilOut<FT, CH> o;
+#pragma unroll
+  for (int c = 0; c < CH; ++c) {
+    FT v[2][2][2], zx[2][2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        v[i][j][0] = (FT)r[i][j][zc][c];
+        v[i][j][1] = (FT)r[i][j][zc + 1][c];
+        zx[i][j] = (FT)r[i][j][ze][c];
+      }
+    FT phi = 0, Dx = 0, Dy = 0, Dz = 0;
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int k = 0; k < 2; ++k) phi += wx[i] * wy[j] * wz[k] * v[i][j][k];
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const FT d0 = v[1][j][k] - v[0][j][k];
+        const FT e = (FT)xe[j][k][c];
+        const FT de = lx ? (v[0][j][k] - e) : (e - v[1][j][k]);
+        Dx += wy[j] * wz[k] * (((FT)1 - ax) * d0 + ax * de);
+      }
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const FT d0 = v[i][1][k] - v[i][0][k];
+        const FT e = (FT)ye[i][k][c];
+        const FT de = ly ? (v[i][0][k] - e) : (e - v[i][1][k]);
+        Dy += wx[i] * wz[k] * (((FT)1 - ay) * d0 + ay * de);
+      }
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const FT d0 = v[i][j][1] - v[i][j][0];
+        const FT e = zx[i][j];
+        const FT de = lz ? (v[i][j][0] - e) : (e - v[i][j][1]);
+        Dz += wx[i] * wy[j] * (((FT)1 - az) * d0 + az * de);
+      }
+    o.phi[c] = phi;
+    o.gx[c] = Dx * (FT)g.isx;
+    o.gy[c] = Dy * (FT)g.isy;
+    o.gz[c] = Dz * (FT)g.isz;
+  }
+  return o;
+}
+
+// ----------------------------------------------------------------------------
+// Yukawa multipole far-field for one ligand atom (gpu_batch_engine.py:393-472):
+// monopole + dipole + quadrupole, radial derivative only, r clamped at 1 A.
+// ----------------------------------------------------------------------------
+template <typename FT>
+__device__ __forceinline__ void farfield(const DevSystem& S, double xd, double yd, double zd, FT q, FT f[3],
+                                         FT& e) {
+  const FT x = (FT)xd, y = (FT)yd, z = (FT)zd;
+  const FT r = sqrt(x * x + y * y + z * z);
+  const FT sr = r > (FT)1 ? r : (FT)1;
+  const FT inv = (FT)1 / sr;
+  const FT il = (FT)S.inv_debye;
+  const FT ex = exp(-sr * il);
+  const FT rx = x * inv, ry = y * inv, rz = z * inv;
+  const FT Vf = (FT)S.V_factor;
+  FT phi = Vf * ex * inv;
+  FT dphi = Vf * ex * (-inv * inv - inv * il);
+  if (S.use_dip) {
+    const FT pr = rx * (FT)S.dip[0] + ry * (FT)S.dip[1] + rz * (FT)S.dip[2];
+    const FT ifpe = (FT)S.inv_fpe;
+    phi += pr * ifpe * inv * inv * ((FT)1 + sr * il) * ex;
+    dphi += pr * ifpe * ex * ((FT)-2 * inv * inv * inv - (FT)2 * inv * inv * il - inv * il * il);
+  }
+  if (S.use_quad) {
+    const FT qx = (FT)S.quad[0] * rx + (FT)S.quad[1] * ry + (FT)S.quad[2] * rz;
+    const FT qy = (FT)S.quad[3] * rx + (FT)S.quad[4] * ry + (FT)S.quad[5] * rz;
+    const FT qz = (FT)S.quad[6] * rx + (FT)S.quad[7] * ry + (FT)S.quad[8] * rz;
+    const FT rQr = rx * qx + ry * qy + rz * qz;
+    const FT ifpe = (FT)S.inv_fpe;
+    const FT i2 = inv * inv, i3 = i2 * inv;
+    phi += rQr * ifpe * i3 * ((FT)1 + sr * il + sr * sr * il * il * ((FT)1 / (FT)3)) * ex;
+    dphi += rQr * ifpe * ex *
+            ((FT)-3 * i3 * inv - (FT)3 * i3 * il - i2 * il * il - inv * il * il * il * ((FT)1 / (FT)3));
+  }
+  const FT c = -q * dphi;
+  f[0] = c * rx;
+  f[1] = c * ry;
+  f[2] = c * rz;
+  e = q * phi;
+}
+
+}  // namespace bd

@@ -1,0 +1,614 @@
+// Kernels of the batched BD engine: fused per-trajectory forces, the persistent
+// K-step stepper with refill from the pending pool, and slot compaction.
+#pragma once
+
+#include "bd_device.cuh"
+
+namespace bd {
+
+template <int G>
+__device__ __forceinline__ double gsum(double v, unsigned m) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(m, v, o, G);
+  return v;
+}
+
+template <int G>
+__device__ __forceinline__ unsigned gsumu(unsigned v, unsigned m) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(m, v, o, G);
+  return v;
+}
+
+template <int G>
+__device__ __forceinline__ unsigned group_mask() {
+  if constexpr (G == 32) {
+    return 0xffffffffu;
+  } else {
+    const unsigned lane = threadIdx.x & 31u;
+    return ((1u << G) - 1u) << (lane & ~(unsigned)(G - 1));
+  }
+}
+
+struct Counts {
+  unsigned grid, rev, ff;
+};
+
+// Lab-frame offset ro = x - c and lab position x of ligand atom i.
+struct PosFromPose {
+  const double* R;
+  const double* c;
+  __device__ __forceinline__ void operator()(int, const double4& a, double ro[3], double x[3]) const {
+    ro[0] = R[0] * a.x + R[1] * a.y + R[2] * a.z;
+    ro[1] = R[3] * a.x + R[4] * a.y + R[5] * a.z;
+    ro[2] = R[6] * a.x + R[7] * a.y + R[8] * a.z;
+    x[0] = c[0] + ro[0];
+    x[1] = c[1] + ro[1];
+    x[2] = c[2] + ro[2];
+  }
+};
+
+struct PosFromAtoms {
+  const double* p;  // this trajectory's (n_lig, 3) lab positions
+  const double* c;
+  __device__ __forceinline__ void operator()(int i, const double4&, double ro[3], double x[3]) const {
+    x[0] = p[3 * i];
+    x[1] = p[3 * i + 1];
+    x[2] = p[3 * i + 2];
+    ro[0] = x[0] - c[0];
+    ro[1] = x[1] - c[1];
+    ro[2] = x[2] - c[2];
+  }
+};
+
+// Net force, torque (about c) and energy on the ligand of one trajectory,
+// computed cooperatively by the G lanes of a group.  Follows
+// GPUBatchForceEngine.__call__ (pystarc/forces/gpu_batch_engine.py:531-605):
+// elec grid (finest containing grid) or Yukawa multipole far-field, Born
+// direction 1 on the receptor Born grid, Born direction 2 on the ligand Born
+// grid at the receptor atoms with the force negated.  Every lane returns the
+// same totals.
+template <typename FT, int G, bool TORQUE, bool ENERGY, class PosFn>
+__device__ void group_forces(const DevSystem& S, const double c[3], const double R[9], int lane, unsigned gm,
+                             const PosFn& pos, double F[3], double T[3], double& E, Counts& cnt) {
+  double f0 = 0, f1 = 0, f2 = 0, t0 = 0, t1 = 0, t2 = 0, e = 0;
+  unsigned ng = 0, nf = 0, nr = 0;
+  const int nl = S.n_lig;
+  for (int i = lane; i < nl; i += G) {
+    const double4 a = S.lig[i];
+    if (fabs(a.w) < 1e-9) continue;
+    double ro[3], x[3];
+    pos(i, a, ro, x);
+    const FT q = (FT)a.w;
+    FT fa0 = 0, fa1 = 0, fa2 = 0, ea = 0;
+    int gi = -1;
+    for (int k = 0; k < S.n_elec; ++k)
+      if (in_box(S.elec[k], x[0], x[1], x[2])) {
+        gi = k;
+        break;
+      }
+    const bool bin = S.has_born && in_box(S.born, x[0], x[1], x[2]);
+    const FT cb = (FT)S.alpha * q * q;
+    if (gi == 0 && bin && S.paired) {
+      const StencilOut<FT, 2> s = stencil<FT, 2>(S.pair, x[0], x[1], x[2]);
+      fa0 = -q * s.gx[0] - cb * s.gx[1];
+      fa1 = -q * s.gy[0] - cb * s.gy[1];
+      fa2 = -q * s.gz[0] - cb * s.gz[1];
+      if (ENERGY) ea = q * s.phi[0] + cb * s.phi[1];
+      ng += 2;
+    } else {
+      if (gi >= 0) {
+        const StencilOut<FT, 1> s = stencil<FT, 1>(S.elec[gi], x[0], x[1], x[2]);
+        fa0 = -q * s.gx[0];
+        fa1 = -q * s.gy[0];
+        fa2 = -q * s.gz[0];
+        if (ENERGY) ea = q * s.phi[0];
+        ng += 1;
+      } else if (S.has_yukawa) {
+        FT ff[3], ef;
+        farfield<FT>(S, x[0], x[1], x[2], q, ff, ef);
+        fa0 = ff[0];
+        fa1 = ff[1];
+        fa2 = ff[2];
+        if (ENERGY) ea = ef;
+        nf += 1;
+      }
+      if (bin) {
+        const StencilOut<FT, 1> s = stencil<FT, 1>(S.born, x[0], x[1], x[2]);
+        fa0 -= cb * s.gx[0];
+        fa1 -= cb * s.gy[0];
+        fa2 -= cb * s.gz[0];
+        if (ENERGY) ea += cb * s.phi[0];
+        ng += 1;
+      }
+    }
+    f0 += (double)fa0;
+    f1 += (double)fa1;
+    f2 += (double)fa2;
+    if (ENERGY) e += (double)ea;
+    if (TORQUE) {
+      t0 += ro[1] * (double)fa2 - ro[2] * (double)fa1;
+      t1 += ro[2] * (double)fa0 - ro[0] * (double)fa2;
+      t2 += ro[0] * (double)fa1 - ro[1] * (double)fa0;
+    }
+  }
+  // Born direction 2: ligand Born grid at the receptor atoms, in the ligand frame.
+  double r0 = 0, r1 = 0, r2 = 0, u0 = 0, u1 = 0, u2 = 0;
+  if (S.born_rev) {
+    const double rho = S.lig_born_rho;
+    if (norm3(c[0], c[1], c[2]) - S.rec_max_r < rho) {
+      const double rho2 = rho * rho;
+      for (int k = 0; k < S.n_chunks; ++k) {
+        const double4 sp = S.chunks[k];
+        const double dx = sp.x - c[0], dy = sp.y - c[1], dz = sp.z - c[2];
+        const double lim = rho + sp.w;
+        if (dx * dx + dy * dy + dz * dz >= lim * lim) continue;
+        for (int a = lane; a < BD_CHUNK; a += G) {
+          const double4 at = S.rec[k * BD_CHUNK + a];
+          if (fabs(at.w) < 1e-9) continue;
+          const double d0 = at.x - c[0], d1 = at.y - c[1], d2 = at.z - c[2];
+          if (d0 * d0 + d1 * d1 + d2 * d2 >= rho2) continue;
+          const double l0 = R[0] * d0 + R[3] * d1 + R[6] * d2;
+          const double l1 = R[1] * d0 + R[4] * d1 + R[7] * d2;
+          const double l2 = R[2] * d0 + R[5] * d1 + R[8] * d2;
+          if (!in_box(S.lig_born, l0, l1, l2)) continue;
+          const StencilOut<FT, 1> s = stencil<FT, 1>(S.lig_born, l0, l1, l2);
+          const FT qr = (FT)at.w;
+          const FT cf = -(FT)S.alpha * qr * qr;
+          const FT g0 = cf * s.gx[0], g1 = cf * s.gy[0], g2 = cf * s.gz[0];
+          r0 += (double)g0;
+          r1 += (double)g1;
+          r2 += (double)g2;
+          if (TORQUE) {
+            u0 += l1 * (double)g2 - l2 * (double)g1;
+            u1 += l2 * (double)g0 - l0 * (double)g2;
+            u2 += l0 * (double)g1 - l1 * (double)g0;
+          }
+          nr += 1;
+        }
+      }
+    }
+  }
+  if (G > 1) {
+    f0 = gsum<G>(f0, gm);
+    f1 = gsum<G>(f1, gm);
+    f2 = gsum<G>(f2, gm);
+    if (ENERGY) e = gsum<G>(e, gm);
+    if (TORQUE) {
+      t0 = gsum<G>(t0, gm);
+      t1 = gsum<G>(t1, gm);
+      t2 = gsum<G>(t2, gm);
+    }
+    if (S.born_rev) {
+      r0 = gsum<G>(r0, gm);
+      r1 = gsum<G>(r1, gm);
+      r2 = gsum<G>(r2, gm);
+      if (TORQUE) {
+        u0 = gsum<G>(u0, gm);
+        u1 = gsum<G>(u1, gm);
+        u2 = gsum<G>(u2, gm);
+      }
+    }
+  }
+  // Reverse-Born force on the receptor, rotated to the lab frame, acts on the ligand with the opposite sign.
+  F[0] = f0 - (R[0] * r0 + R[1] * r1 + R[2] * r2);
+  F[1] = f1 - (R[3] * r0 + R[4] * r1 + R[5] * r2);
+  F[2] = f2 - (R[6] * r0 + R[7] * r1 + R[8] * r2);
+  if (TORQUE) {
+    T[0] = t0 - (R[0] * u0 + R[1] * u1 + R[2] * u2);
+    T[1] = t1 - (R[3] * u0 + R[4] * u1 + R[5] * u2);
+    T[2] = t2 - (R[6] * u0 + R[7] * u1 + R[8] * u2);
+  } else {
+    T[0] = T[1] = T[2] = 0.0;
+  }
+  E = e;
+  cnt.grid += ng;
+  cnt.rev += nr;
+  cnt.ff += nf;
+}
+
+// Parity kernel: one group per pose.  pose = centroid + quaternion (w,x,y,z) or rotation matrix.
+template <typename FT, int G, bool TORQUE>
+__global__ void __launch_bounds__(256) eval_pose_kernel(DevSystem S, long long n, const double* __restrict__ cen,
+                                                        const double* __restrict__ rot, int rot_is_matrix,
+                                                        double* __restrict__ F, double* __restrict__ T,
+                                                        double* __restrict__ E, unsigned long long* ctr) {
+  const int lane = threadIdx.x & (G - 1);
+  const unsigned gm = group_mask<G>();
+  const long long groups = (long long)gridDim.x * (blockDim.x / G);
+  Counts cnt{0, 0, 0};
+  for (long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / G; t < n; t += groups) {
+    double c[3] = {cen[3 * t], cen[3 * t + 1], cen[3 * t + 2]};
+    double R[9];
+    if (rot_is_matrix) {
+#pragma unroll
+      for (int k = 0; k < 9; ++k) R[k] = rot[9 * t + k];
+    } else {
+      double q[4] = {rot[4 * t], rot[4 * t + 1], rot[4 * t + 2], rot[4 * t + 3]};
+      quat_to_rot(q, R);
+    }
+    double f[3], tq[3], e;
+    group_forces<FT, G, TORQUE, true>(S, c, R, lane, gm, PosFromPose{R, c}, f, tq, e, cnt);
+    if (lane == 0) {
+      F[3 * t] = f[0];
+      F[3 * t + 1] = f[1];
+      F[3 * t + 2] = f[2];
+      T[3 * t] = tq[0];
+      T[3 * t + 1] = tq[1];
+      T[3 * t + 2] = tq[2];
+      E[t] = e;
+    }
+  }
+  if (ctr) {
+    const unsigned g = gsumu<32>(cnt.grid, 0xffffffffu), r = gsumu<32>(cnt.rev, 0xffffffffu),
+                   f = gsumu<32>(cnt.ff, 0xffffffffu);
+    if ((threadIdx.x & 31) == 0) {
+      atomicAdd(ctr + C_GRID_EVALS, (unsigned long long)g);
+      atomicAdd(ctr + C_REV_EVALS, (unsigned long long)r);
+      atomicAdd(ctr + C_FF_EVALS, (unsigned long long)f);
+    }
+  }
+}
+
+// Parity kernel with explicit lab atom positions (the reference __call__ signature).
+template <typename FT, int G, bool TORQUE>
+__global__ void __launch_bounds__(256) eval_atoms_kernel(DevSystem S, long long n, const double* __restrict__ pos,
+                                                         const double* __restrict__ Rm,
+                                                         const double* __restrict__ cen, double* __restrict__ F,
+                                                         double* __restrict__ T, double* __restrict__ E) {
+  const int lane = threadIdx.x & (G - 1);
+  const unsigned gm = group_mask<G>();
+  const long long groups = (long long)gridDim.x * (blockDim.x / G);
+  Counts cnt{0, 0, 0};
+  for (long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / G; t < n; t += groups) {
+    double c[3] = {cen[3 * t], cen[3 * t + 1], cen[3 * t + 2]};
+    double R[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) R[k] = Rm[9 * t + k];
+    double f[3], tq[3], e;
+    group_forces<FT, G, TORQUE, true>(S, c, R, lane, gm, PosFromAtoms{pos + (long long)t * S.n_lig * 3, c}, f,
+                                      tq, e, cnt);
+    if (lane == 0) {
+      F[3 * t] = f[0];
+      F[3 * t + 1] = f[1];
+      F[3 * t + 2] = f[2];
+      T[3 * t] = tq[0];
+      T[3 * t + 1] = tq[1];
+      T[3 * t + 2] = tq[2];
+      E[t] = e;
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------
+// Stepper
+// ----------------------------------------------------------------------------
+struct Traj {
+  double c[3], q[4];
+  int id, steps, rets, status;
+};
+
+struct Tally {
+  unsigned long long steps;
+  unsigned reacted, escaped, maxsteps, returns, overlap, bridge, nonfinite;
+  Counts cnt;
+};
+
+__device__ __forceinline__ Keyed traj_key(const DevSim& P, int id) {
+  const unsigned long long g = (unsigned long long)(P.id_offset + id);
+  return Keyed{P.k0, P.k1, (uint32_t)(g & 0xffffffffull), (uint32_t)(g >> 32)};
+}
+
+__device__ __forceinline__ void start_trajectory(const DevSim& P, int id, Traj& tr) {
+  const Keyed key = traj_key(P, id);
+  const W4 a = key.w(INIT_STEP, SUB_INIT_DIR), b = key.w(INIT_STEP, SUB_INIT_DIR + 1);
+  double v0, v1, v2, spare;
+  box_muller(u53(a.a, a.b), u53(a.c, a.d), v0, v1);
+  box_muller(u53(b.a, b.b), u53(b.c, b.d), v2, spare);
+  const double n = norm3(v0, v1, v2);
+  tr.c[0] = v0 / n * P.r_b;
+  tr.c[1] = v1 / n * P.r_b;
+  tr.c[2] = v2 / n * P.r_b;
+  const W4 qa = key.w(INIT_STEP, SUB_INIT_Q), qb = key.w(INIT_STEP, SUB_INIT_Q + 1);
+  shoemake(u53(qa.a, qa.b), u53(qa.c, qa.d), u53(qb.a, qb.b), tr.q);
+  tr.id = id;
+  tr.steps = 0;
+  tr.rets = 0;
+  tr.status = ST_RUNNING;
+}
+
+__device__ __forceinline__ void pair_distances(const DevSystem& S, const double c[3], const double R[9],
+                                               double d[BD_MAX_PAIRS]) {
+  for (int p = 0; p < S.n_pairs; ++p) {
+    const double* b = S.rx_body[p];
+    const double lx = R[0] * b[0] + R[1] * b[1] + R[2] * b[2] + c[0] - S.rx_rec[p][0];
+    const double ly = R[3] * b[0] + R[4] * b[1] + R[5] * b[2] + c[1] - S.rx_rec[p][1];
+    const double lz = R[6] * b[0] + R[7] * b[1] + R[8] * b[2] + c[2] - S.rx_rec[p][2];
+    d[p] = norm3(lx, ly, lz);
+  }
+}
+
+// Adaptive dt (pystarc/simulation/gpu_batch_simulator.py:961-1067, flattened-pairs mode).
+__device__ __forceinline__ double adaptive_dt(const DevSim& P, double r) {
+  const double D_t = P.D_t;
+  const double dt_pair = (0.1 * 0.1 / 2.0) * r * r / D_t;
+  double dt_force = dt_pair;
+  if (P.adt_has_force) {
+    const double lam = P.adt_debye;
+    const double expf_ = exp(-r / lam);
+    const double Fr0 = P.adt_V0 * expf_ * (1.0 / (r * r) + 1.0 / (r * lam));
+    const double Fr1 = -P.adt_V0 * expf_ / (lam * lam) - 2.0 * Fr0 / r;
+    const double DFr1 = fabs(D_t * Fr1);
+    if (DFr1 > 1e-15 && r < 3.0 * lam) dt_force = 0.01 / DFr1;
+  }
+  const double dist_b = fmax(r - P.r_b, 1e-3), dist_esc = fmax(P.r_esc - r, 1e-3);
+  const double de = fmin(dist_b, dist_esc);
+  const double dt_edge = de * de / (18.0 * D_t);
+  double dt = (r > 1.1 * P.r_b) ? fmin(fmin(dt_force, dt_edge), dt_pair) : fmin(dt_force, dt_pair);
+  if (P.max_dt > 0) dt = fmin(dt, P.max_dt);
+  if (P.min_core_dt > 0) dt = fmax(dt, P.min_core_dt);
+  return dt;
+}
+
+// Relative translational diffusion with HI (far-field RPY along the line of
+// centres, mu = 0.243, clamp 1e-6; gpu_batch_simulator.py:741-751, :1074-1084).
+template <typename FT>
+__device__ __forceinline__ double hi_diffusion(const DevSim& P, double r) {
+  if (!P.use_hi) return P.D_t;
+  const FT rm1 = (FT)1 / (FT)fmax(r, 0.01);
+  const FT rm3 = rm1 * rm1 * rm1;
+  const FT Df = (FT)P.hi_Df;
+  const FT Di = (FT)-2 * Df * ((FT)2 * rm1 - ((FT)4 / (FT)3) * (FT)P.hi_a2 * rm3) / (FT)(8.0 * 3.14159265358979323846);
+  const FT D = Df * (FT)P.hi_ainv + Di;
+  return (double)(D > (FT)1e-6 ? D : (FT)1e-6);
+}
+
+template <int G>
+__device__ __forceinline__ bool overlap_any(const DevSystem& S, const double c[3], int lane, unsigned gm) {
+  bool hit = false;
+  if (norm3(c[0], c[1], c[2]) < S.rec_max_r + 1.5) {
+    for (int k = 0; k < S.n_chunks && !hit; ++k) {
+      const double4 sp = S.chunks[k];
+      const double dx = sp.x - c[0], dy = sp.y - c[1], dz = sp.z - c[2];
+      const double lim = sp.w + 1.5;
+      if (dx * dx + dy * dy + dz * dz >= lim * lim) continue;
+      for (int a = lane; a < BD_CHUNK; a += G) {
+        const double4 at = S.rec[k * BD_CHUNK + a];
+        if (norm3(c[0] - at.x, c[1] - at.y, c[2] - at.z) < 1.5) hit = true;
+      }
+    }
+  }
+  if (G > 1) hit = __any_sync(gm, hit);
+  return hit;
+}
+
+// One BD step of one trajectory, in the reference's order
+// (gpu_batch_simulator.py:783-1254): discrete reaction test, escape/return,
+// forces, old pair distances, adaptive dt, D(r), translation, rotation,
+// overlap rejection, Brownian bridge, step count.  Returns the new status.
+template <typename FT, int G, bool TORQUE>
+__device__ __forceinline__ int bd_step(const DevSystem& S, const DevSim& P, Traj& tr, int lane, unsigned gm,
+                                       Tally& tl) {
+  const Keyed key = traj_key(P, tr.id);
+  const uint32_t s = (uint32_t)tr.steps;
+  double R[9];
+  quat_to_rot(tr.q, R);
+  double d[BD_MAX_PAIRS];
+  if (S.n_pairs > 0) {
+    pair_distances(S, tr.c, R, d);
+    int nsat = 0;
+    for (int p = 0; p < S.n_pairs; ++p) nsat += d[p] < S.rx_cut[p];
+    if (nsat >= S.n_needed) return ST_REACTED;
+  }
+  double r = norm3(tr.c[0], tr.c[1], tr.c[2]);
+  if (r >= P.r_esc) {
+    const W4 w = key.w(s, SUB_ESCAPE);
+    if (u53(w.a, w.b) < P.return_prob) {
+      tr.c[0] = tr.c[0] / r * P.r_b;
+      tr.c[1] = tr.c[1] / r * P.r_b;
+      tr.c[2] = tr.c[2] / r * P.r_b;
+      const W4 qa = key.w(s, SUB_RETURN_Q), qb = key.w(s, SUB_RETURN_Q + 1);
+      shoemake(u53(qa.a, qa.b), u53(qa.c, qa.d), u53(qb.a, qb.b), tr.q);
+      quat_to_rot(tr.q, R);
+      tr.rets += 1;
+      tl.returns += 1;
+      r = norm3(tr.c[0], tr.c[1], tr.c[2]);
+    } else {
+      return ST_ESCAPED;
+    }
+  }
+  double F[3], T[3], E;
+  group_forces<FT, G, TORQUE, false>(S, tr.c, R, lane, gm, PosFromPose{R, tr.c}, F, T, E, tl.cnt);
+  if (S.n_pairs > 0) pair_distances(S, tr.c, R, d);
+  const double dt = adaptive_dt(P, r);
+  const double D = hi_diffusion<FT>(P, r);
+  double xt[3], xr[3];
+  {
+    const W4 a = key.w(s, SUB_NORMALS), b = key.w(s, SUB_NORMALS + 1), c = key.w(s, SUB_NORMALS + 2);
+    box_muller(u53(a.a, a.b), u53(a.c, a.d), xt[0], xt[1]);
+    box_muller(u53(b.a, b.b), u53(b.c, b.d), xt[2], xr[0]);
+    box_muller(u53(c.a, c.b), u53(c.c, c.d), xr[1], xr[2]);
+  }
+  const double sig_t = sqrt(2.0 * D * dt), ddt = D * dt;
+  double cn[3], qn[4] = {tr.q[0], tr.q[1], tr.q[2], tr.q[3]};
+#pragma unroll
+  for (int k = 0; k < 3; ++k) cn[k] = tr.c[k] + (ddt * F[k] + sig_t * xt[k]);
+  const double sig_r = sqrt(2.0 * P.D_r * dt), rdt = P.D_r * dt;
+  rotate_quat(qn, rdt * T[0] + sig_r * xr[0], rdt * T[1] + sig_r * xr[1], rdt * T[2] + sig_r * xr[2]);
+  if (!(isfinite(cn[0]) && isfinite(cn[1]) && isfinite(cn[2]) && isfinite(qn[0]))) {
+    tl.nonfinite += 1;
+    return ST_ERROR;
+  }
+  if (P.overlap && overlap_any<G>(S, cn, lane, gm)) {
+    tl.overlap += 1;
+  } else {
+    tr.c[0] = cn[0];
+    tr.c[1] = cn[1];
+    tr.c[2] = cn[2];
+    tr.q[0] = qn[0];
+    tr.q[1] = qn[1];
+    tr.q[2] = qn[2];
+    tr.q[3] = qn[3];
+  }
+  int st = ST_RUNNING;
+  if (S.n_pairs > 0) {
+    double Rn[9], d1[BD_MAX_PAIRS];
+    quat_to_rot(tr.q, Rn);
+    pair_distances(S, tr.c, Rn, d1);
+    int fired = 0;
+    for (int p = 0; p < S.n_pairs; ++p) {
+      const double x0 = d[p] - S.rx_cut[p], x1 = d1[p] - S.rx_cut[p];
+      double pc = 0.0;
+      if (x0 > 0 && x1 > 0) pc = exp(-x0 * x1 / fmax(S.rx_deff[p] * dt, 1e-30));
+      const W4 w = key.w(s, SUB_BRIDGE + (uint32_t)(p >> 1));
+      const double u = (p & 1) ? u53(w.c, w.d) : u53(w.a, w.b);
+      fired += (u < pc) || (d1[p] < S.rx_cut[p]);
+    }
+    if (fired >= S.n_needed) {
+      st = ST_REACTED;
+      tl.bridge += 1;
+    }
+  }
+  tr.steps += 1;
+  tl.steps += 1;
+  if (st == ST_RUNNING && tr.steps >= P.max_steps) st = ST_MAXSTEPS;
+  return st;
+}
+
+__device__ __forceinline__ void load_slot(const SlotBuf& B, int s, Traj& tr) {
+  tr.c[0] = B.c[s];
+  tr.c[1] = B.c[B.cap + s];
+  tr.c[2] = B.c[2 * B.cap + s];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) tr.q[k] = B.q[k * B.cap + s];
+  tr.id = B.traj[s];
+  tr.steps = B.steps[s];
+  tr.rets = B.rets[s];
+  tr.status = B.status[s];
+}
+
+__device__ __forceinline__ void store_slot(const SlotBuf& B, int s, const Traj& tr) {
+  B.c[s] = tr.c[0];
+  B.c[B.cap + s] = tr.c[1];
+  B.c[2 * B.cap + s] = tr.c[2];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) B.q[k * B.cap + s] = tr.q[k];
+  B.traj[s] = tr.id;
+  B.steps[s] = tr.steps;
+  B.rets[s] = tr.rets;
+  B.status[s] = (int8_t)tr.status;
+}
+
+template <int G>
+__device__ __forceinline__ int group_fetch(unsigned long long* p, int lane, unsigned gm) {
+  unsigned long long v = 0;
+  if (lane == 0) v = atomicAdd(p, 1ull);
+  v = __shfl_sync(gm, v, 0, G);
+  return v > 0x7fffffffull ? 0x7fffffff : (int)v;
+}
+
+// Fill `n_slots` slots with the first trajectories of the pending pool.
+__global__ void init_slots_kernel(DevSim P, SlotBuf B, int n_slots) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n_slots) return;
+  Traj tr;
+  start_trajectory(P, s, tr);
+  store_slot(B, s, tr);
+}
+
+// Persistent stepper: groups take live slots from a dynamic cursor, advance
+// each by K steps with its state in registers, start a pending trajectory
+// whenever theirs ends, and write the slot back.  Slots whose trajectory ended
+// with the pool empty are left EMPTY for the compaction.
+template <typename FT, int G, bool TORQUE>
+__global__ void __launch_bounds__(256) step_kernel(DevSystem S, DevSim P, SlotBuf B, const int* __restrict__ n_live,
+                                                   int K) {
+  const int lane = threadIdx.x & (G - 1);
+  const unsigned gm = group_mask<G>();
+  const int live = *n_live;
+  Tally tl{};
+  for (;;) {
+    const int slot = group_fetch<G>(P.ctr + C_SLOT_CURSOR, lane, gm);
+    if (slot >= live) break;
+    Traj tr;
+    load_slot(B, slot, tr);
+    for (int k = 0; k < K; ++k) {
+      if (tr.status != ST_RUNNING) {
+        const int id = group_fetch<G>(P.ctr + C_PENDING, lane, gm);
+        if (id >= P.n_traj) {
+          tr.status = ST_EMPTY;
+          break;
+        }
+        start_trajectory(P, id, tr);
+      }
+      const int st = bd_step<FT, G, TORQUE>(S, P, tr, lane, gm, tl);
+      if (st != ST_RUNNING) {
+        tr.status = st;
+        if (lane == 0) {
+          P.out_status[tr.id] = (int8_t)st;
+          P.out_steps[tr.id] = tr.steps;
+          P.out_returns[tr.id] = tr.rets;
+        }
+        tl.reacted += st == ST_REACTED;
+        tl.escaped += st == ST_ESCAPED;
+        tl.maxsteps += st == ST_MAXSTEPS;
+      }
+    }
+    if (lane == 0) store_slot(B, slot, tr);
+  }
+  // Flush tallies: only lane 0 of each group counts scalar events.
+  if (lane != 0) {
+    tl.steps = 0;
+    tl.reacted = tl.escaped = tl.maxsteps = tl.returns = tl.overlap = tl.bridge = tl.nonfinite = 0;
+  }
+  __syncwarp();
+  const unsigned long long st64 = [&] {
+    unsigned long long v = tl.steps;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+  }();
+  const unsigned vals[10] = {tl.reacted, tl.escaped, tl.maxsteps, tl.returns, tl.overlap, tl.bridge,
+                             tl.nonfinite, tl.cnt.grid, tl.cnt.rev, tl.cnt.ff};
+  unsigned red[10];
+#pragma unroll
+  for (int i = 0; i < 10; ++i) red[i] = gsumu<32>(vals[i], 0xffffffffu);
+  if ((threadIdx.x & 31) == 0) {
+    const int idx[10] = {C_REACTED, C_ESCAPED, C_MAXSTEPS, C_RETURNS, C_OVERLAP, C_BRIDGE, C_NONFINITE,
+                         C_GRID_EVALS, C_REV_EVALS, C_FF_EVALS};
+    if (st64) atomicAdd(P.ctr + C_STEPS, st64);
+#pragma unroll
+    for (int i = 0; i < 10; ++i)
+      if (red[i]) atomicAdd(P.ctr + idx[i], (unsigned long long)red[i]);
+  }
+}
+
+// Move live slots of `src` (status RUNNING) densely into `dst`; the order is
+// irrelevant because every draw is keyed by trajectory id and step.
+__global__ void compact_kernel(SlotBuf src, SlotBuf dst, const int* __restrict__ n_live_src,
+                               unsigned long long* ctr) {
+  const int n = *n_live_src;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    const bool alive = src.status[s] == ST_RUNNING;
+    const unsigned m = __ballot_sync(__activemask(), alive);
+    if (!alive) continue;
+    const int leader = __ffs(m) - 1;
+    const int lane = threadIdx.x & 31;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(ctr + C_LIVE_NEXT, (unsigned long long)__popc(m));
+    base = __shfl_sync(m, base, leader);
+    const int d = (int)base + __popc(m & ((1u << lane) - 1u));
+    Traj tr;
+    load_slot(src, s, tr);
+    store_slot(dst, d, tr);
+  }
+}
+
+// Publish the compacted count and reset the cursors for the next launch.
+__global__ void finish_compact_kernel(int* n_live_dst, unsigned long long* ctr) {
+  *n_live_dst = (int)ctr[C_LIVE_NEXT];
+  ctr[C_LIVE_NEXT] = 0;
+  ctr[C_SLOT_CURSOR] = 0;
+}
+
+}  // namespace bd

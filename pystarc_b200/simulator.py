@@ -1,0 +1,320 @@
+"""``B200BatchSimulator``: drop-in for the reference's ``GPUBatchSimulator``.
+
+Constructor and ``run()`` follow pystarc/simulation/gpu_batch_simulator.py:159-318 and
+:462-1594; the result has ``GPUBatchResult``'s fields and methods (:45-140), and
+``_k_b`` / ``_return_prob`` are set by ``run()`` as the pipeline expects
+(pystarc/pipeline/pipeline.py:343-385).
+
+The step loop runs on the GPU: a persistent kernel advances every live
+trajectory ``steps_per_launch`` steps per launch with its state in registers,
+starts pending trajectories as others finish, and a compaction drops finished
+slots between launches; both are replayed from a CUDA graph.  The host only
+polls a dozen counters between batches of launches.  Noise is Philox4x32-10
+keyed by (seed, trajectory, step), so a run replays exactly and a trajectory's
+fate does not depend on the launch shape.
+
+Reaction criteria use the flattened-pairs mode of the reference (all pairs of
+all reactions, ``n_needed`` of the first reaction, -1 meaning all pairs).
+"""
+
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+from pathlib import Path
+from typing import Dict
+
+import numpy as np
+
+from . import _lib
+from .hostphys import CONV, bridge_d_eff, rate_constant, return_prob_and_kb, wilson_ci
+
+
+@dataclass
+class B200BatchResult:
+    """Same fields and methods as the reference's GPUBatchResult (gpu_batch_simulator.py:45-140)."""
+
+    n_trajectories: int
+    n_reacted: int
+    n_escaped: int
+    n_max_steps: int
+    reaction_counts: Dict[str, int]
+    r_start: float
+    r_escape: float
+    dt: float
+    elapsed_sec: float
+    steps_per_sec: float
+    sim_data: Dict = None
+    total_steps: int = 0
+    counters: Dict = field(default_factory=dict)
+
+    @property
+    def n_completed(self) -> int:
+        return self.n_reacted + self.n_escaped
+
+    @property
+    def reaction_probability(self) -> float:
+        n = self.n_completed
+        return self.n_reacted / n if n > 0 else 0.0
+
+    def reaction_probability_ci(self, confidence: float = 0.95):
+        return wilson_ci(self.n_reacted, self.n_escaped, confidence)
+
+    def rate_constant(self, D_rel: float, k_b: float = 0.0) -> float:
+        P = self.reaction_probability
+        if P == 0.0:
+            return 0.0
+        return rate_constant(P, D_rel, k_b, self.r_start, self.r_escape)
+
+    def rate_constant_ci(self, D_rel: float, k_b: float = 0.0, confidence: float = 0.95):
+        lo, hi = self.reaction_probability_ci(confidence)
+        return (rate_constant(lo, D_rel, k_b, self.r_start, self.r_escape),
+                rate_constant(hi, D_rel, k_b, self.r_start, self.r_escape))
+
+    def summary(self, D_rel: float, k_b: float = 0.0, confidence: float = 0.95) -> str:
+        k = self.rate_constant(D_rel, k_b)
+        k_lo, k_hi = self.rate_constant_ci(D_rel, k_b, confidence)
+        p = self.reaction_probability
+        p_lo, p_hi = self.reaction_probability_ci(confidence)
+        pct = int(confidence * 100)
+        lines = [f"  Trajectories : {self.n_trajectories:,}",
+                 f"  Completed    : {self.n_completed:,}  ({self.n_reacted:,} reacted + {self.n_escaped:,} escaped)"]
+        if self.n_max_steps:
+            lines.append(f"  Max-steps    : {self.n_max_steps:,}  (excluded)")
+        lines += [f"  P_rxn        : {p:.6f}  ({pct}% CI: [{p_lo:.6f}, {p_hi:.6f}])",
+                  f"  k_on         : {k:.4e} M-1 s-1", f"  {pct}% CI     : [{k_lo:.4e}, {k_hi:.4e}] M-1 s-1"]
+        if k > 0:
+            lines.append(f"  log10(k_on)  : {math.log10(k):.3f}")
+        lines += [f"  Wall time    : {self.elapsed_sec:.1f} s", f"  BD steps/sec : {self.steps_per_sec:,.0f}",
+                  "  Backend      : B200 (sm_100a persistent kernel)"]
+        return "\n".join(lines)
+
+
+def flatten_pairs(pathway_set):
+    """All pairs of all reactions; n_needed of the first reaction (gpu_batch_simulator.py:186-205)."""
+    rec_idx, lig_idx, cut = [], [], []
+    for rxn in pathway_set.reactions:
+        for pair in rxn.criteria.pairs:
+            rec_idx.append(int(pair.mol1_atom_index))
+            lig_idx.append(int(pair.mol2_atom_index))
+            cut.append(float(pair.distance_cutoff))
+    if pathway_set.reactions:
+        nn = pathway_set.reactions[0].criteria.n_needed
+        n_needed = len(cut) if (nn < 0 or nn > len(cut)) else nn
+    else:
+        n_needed = 1
+    return rec_idx, lig_idx, np.asarray(cut, dtype=float), n_needed
+
+
+class B200BatchSimulator:
+    """Batched BD of all trajectories on one GPU.
+
+    Extra keyword options (not in the reference): ``precision`` ("fp64" or
+    "mixed"), ``torque_mode`` ("zero" or "centroid"), ``termination``
+    ("reference": stop once 99.5 % are done, as the reference loop does;
+    "complete": run every trajectory to an outcome or to ``max_steps``),
+    ``steps_per_launch`` (K) and ``launches_per_poll``.
+    """
+
+    def __init__(self, mol1, mol2, mob, pathway_set, params, batch_engine, *, precision=None, torque_mode=None,
+                 termination="reference", steps_per_launch=64, launches_per_poll=8, slots=0, id_offset=0,
+                 verbose=False):
+        if not hasattr(batch_engine, "handle"):
+            raise TypeError("batch_engine must be a B200ForceEngine")
+        if any(getattr(r, "state_before", None) is not None for r in pathway_set.reactions):
+            raise NotImplementedError("state-machine reactions are not implemented by this engine")
+        self.mol1, self.mol2, self.mob = mol1, mol2, mob
+        self.pathway_set = pathway_set
+        self.params = params
+        self.engine = batch_engine
+        self.precision = precision or batch_engine.precision
+        self.torque_mode = torque_mode or batch_engine.torque_mode
+        self.termination = termination
+        self.K = int(steps_per_launch)
+        self.M = int(launches_per_poll)
+        self.slots = int(slots)
+        self.id_offset = int(id_offset)
+        self.verbose = verbose
+        c0 = np.asarray(mol2.centroid(), dtype=float)
+        self._mol2_pos0 = np.asarray(mol2.positions_array(), dtype=float) - c0
+        self._charges = np.asarray(mol2.charges_array(), dtype=float)
+        self._N_lig = len(self._charges)
+        self._use_hi = bool(getattr(params, "hydrodynamic_interactions", False))
+        rec_idx, lig_idx, cut, n_needed = flatten_pairs(pathway_set)
+        rec_pos = np.asarray(mol1.positions_array(), dtype=float)
+        self._rxn_rec = rec_pos[rec_idx].reshape(-1, 3) if rec_idx else np.zeros((0, 3))
+        self._rxn_lig_body = self._mol2_pos0[lig_idx].reshape(-1, 3) if lig_idx else np.zeros((0, 3))
+        self._rxn_cutoffs = cut
+        self._rxn_n_needed = n_needed
+        self._return_prob = 0.0
+        self._k_b = 0.0
+        self._qb_factor = 1.1
+        self.counters = {}
+
+    # ------------------------------------------------------------------
+    def _setup(self):
+        p = self.params
+        D_t = float(self.mob.relative_translational_diffusion())
+        D_r = float(self.mob.relative_rotational_diffusion())
+        q_rec = float(self.mol1.total_charge())
+        q_lig = float(self.mol2.total_charge())
+        r_h_rec = float(getattr(self.mob, "radius1", 0.0))
+        r_h_lig = float(getattr(self.mob, "radius2", 0.0))
+        debye = float(getattr(self.engine, "_debye", 7.858))
+        kT = float(getattr(p, "_kT_scale", 1.0))
+        self._return_prob, self._k_b = return_prob_and_kb(p.r_start, p.r_escape, q_rec, q_lig, debye, D_t,
+                                                          self._use_hi, r_h_rec, r_h_lig, kT)
+        h = self.engine.handle
+        self.engine.set_ligand(self._mol2_pos0, self._charges)
+        P = len(self._rxn_cutoffs)
+        if P:
+            # lever-arm radii default to 1 A when the mobility has none (gpu_batch_simulator.py:644-645)
+            d_eff = np.ascontiguousarray(bridge_d_eff(D_t, float(getattr(self.mob, "radius1", 1.0)),
+                                                      float(getattr(self.mob, "radius2", 1.0)), self._rxn_rec,
+                                                      self._rxn_lig_body), dtype=np.float64)
+            rr = np.ascontiguousarray(self._rxn_rec, dtype=np.float64)
+            lb = np.ascontiguousarray(self._rxn_lig_body, dtype=np.float64)
+            cc = np.ascontiguousarray(self._rxn_cutoffs, dtype=np.float64)
+            h.call("bd_set_reactions", P, _lib.ptr(rr), _lib.ptr(lb), _lib.ptr(cc), _lib.ptr(d_eff),
+                   int(self._rxn_n_needed))
+        else:
+            h.call("bd_set_reactions", 0, None, None, None, None, 1)
+        sp = _lib.BdSimParams()
+        sp.n_traj = int(p.n_trajectories)
+        sp.seed = int(p.seed if p.seed is not None else 0) & 0xFFFFFFFFFFFFFFFF
+        sp.r_start = float(p.r_start)
+        sp.r_escape = float(p.r_escape)
+        sp.return_prob = float(self._return_prob)
+        sp.max_steps = int(min(p.max_steps, 2 ** 31 - 1))
+        sp.max_dt = float(getattr(p, "max_dt", 0.0) or 0.0)
+        sp.min_core_dt = float(getattr(p, "minimum_core_dt", 0.0) or 0.0)
+        sp.use_hi = int(self._use_hi)
+        sp.overlap = int(bool(getattr(p, "_overlap_check", True)))
+        sp.D_t = D_t
+        sp.D_r = D_r
+        sp.q_rec_total = q_rec
+        sp.q_lig_total = q_lig
+        sp.adt_debye = debye
+        sp.r_hydro_rec = r_h_rec
+        sp.r_hydro_lig = r_h_lig
+        sp.precision = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}[self.precision]
+        sp.torque_mode = {"zero": _lib.TORQUE_ZERO, "centroid": _lib.TORQUE_CENTROID}[self.torque_mode]
+        sp.slots = self.slots
+        sp.id_offset = self.id_offset
+        h.call("bd_sim_configure", _lib.C.byref(sp))
+        return D_t
+
+    def read_counters(self):
+        out = np.zeros(_lib.N_CTR, dtype=np.uint64)
+        self.engine.handle.call("bd_sim_counters", _lib.ptr(out, _lib.C.c_uint64), _lib.N_CTR, None)
+        return dict(zip(_lib.CTR_NAMES, (int(v) for v in out)))
+
+    def outcomes(self):
+        N = int(self.params.n_trajectories)
+        st = np.zeros(N, dtype=np.int8)
+        steps = np.zeros(N, dtype=np.int32)
+        rets = np.zeros(N, dtype=np.int32)
+        self.engine.handle.call("bd_sim_outcomes", _lib.ptr(st, _lib.C.c_int8), _lib.ptr(steps, _lib.C.c_int32),
+                                _lib.ptr(rets, _lib.C.c_int32))
+        return st, steps, rets
+
+    def _checkpoint_path(self):
+        return Path(getattr(self.params, "_work_dir", "bd_sims")) / "checkpoint_b200.npz"
+
+    def save_checkpoint(self, path=None):
+        """Slots, counters and outcomes: enough to resume the same trajectories exactly."""
+        h = self.engine.handle
+        cap = _lib.C.c_int32()
+        h.call("bd_sim_capacity", _lib.C.byref(cap))
+        C = cap.value
+        c = np.zeros(3 * C)
+        q = np.zeros(4 * C)
+        traj, steps, rets = (np.zeros(C, dtype=np.int32) for _ in range(3))
+        status = np.zeros(C, dtype=np.int8)
+        live = _lib.C.c_int32()
+        ctr = np.zeros(_lib.N_CTR, dtype=np.uint64)
+        h.call("bd_sim_snapshot", _lib.ptr(c), _lib.ptr(q), _lib.ptr(traj, _lib.C.c_int32),
+               _lib.ptr(steps, _lib.C.c_int32), _lib.ptr(rets, _lib.C.c_int32), _lib.ptr(status, _lib.C.c_int8),
+               _lib.C.byref(live), _lib.ptr(ctr, _lib.C.c_uint64))
+        o_st, o_steps, o_rets = self.outcomes()
+        path = Path(path or self._checkpoint_path())
+        path.parent.mkdir(parents=True, exist_ok=True)
+        np.savez_compressed(path, c=c, q=q, traj=traj, steps=steps, rets=rets, status=status, n_live=live.value,
+                            counters=ctr, out_status=o_st, out_steps=o_steps, out_returns=o_rets,
+                            n_traj=int(self.params.n_trajectories), seed=int(self.params.seed or 0), cap=C)
+        return path
+
+    def load_checkpoint(self, path):
+        """Restore a checkpoint written by ``save_checkpoint`` (same system, seed and n_trajectories)."""
+        d = np.load(path)
+        if int(d["n_traj"]) != int(self.params.n_trajectories) or int(d["seed"]) != int(self.params.seed or 0):
+            raise ValueError(f"{path}: checkpoint is for another run (n_trajectories/seed differ)")
+        h = self.engine.handle
+        cap = _lib.C.c_int32()
+        h.call("bd_sim_capacity", _lib.C.byref(cap))
+        if int(d["cap"]) != cap.value:
+            raise ValueError(f"{path}: slot capacity {int(d['cap'])} != {cap.value}")
+        arr = {k: np.ascontiguousarray(d[k]) for k in d.files}
+        h.call("bd_sim_restore", _lib.ptr(arr["c"]), _lib.ptr(arr["q"]), _lib.ptr(arr["traj"], _lib.C.c_int32),
+               _lib.ptr(arr["steps"], _lib.C.c_int32), _lib.ptr(arr["rets"], _lib.C.c_int32),
+               _lib.ptr(arr["status"], _lib.C.c_int8), int(arr["n_live"]), _lib.ptr(arr["counters"], _lib.C.c_uint64),
+               _lib.ptr(arr["out_status"], _lib.C.c_int8), _lib.ptr(arr["out_steps"], _lib.C.c_int32),
+               _lib.ptr(arr["out_returns"], _lib.C.c_int32))
+
+    # ------------------------------------------------------------------
+    def run(self, max_launches=None) -> B200BatchResult:
+        t0 = time.perf_counter()
+        N = int(self.params.n_trajectories)
+        self._setup()
+        h = self.engine.handle
+        h.call("bd_sim_reset", None)
+        ckpt_interval = int(getattr(self.params, "checkpoint_interval", 0) or 0)
+        ckpt = self._checkpoint_path()
+        if ckpt_interval > 0 and ckpt.exists():
+            try:
+                self.load_checkpoint(ckpt)
+            except (ValueError, OSError, KeyError) as e:
+                print(f" Checkpoint load failed: {e}. Starting fresh.")
+                h.call("bd_sim_reset", None)
+        last_ckpt_done = 0
+        launches = 0
+        stop_at = int(N * 0.995) if self.termination == "reference" else N
+        while True:
+            h.call("bd_sim_run", self.M, self.K, None)
+            launches += self.M
+            c = self.read_counters()
+            if c["nonfinite"]:
+                raise _lib.BdError(_lib.BD_ERR_NAN, f"{c['nonfinite']} trajectories produced a non-finite pose")
+            done = c["reacted"] + c["escaped"] + c["max_steps"]
+            if self.verbose:
+                print(f"  [b200] launches={launches} done={done}/{N} steps={c['steps']:,}")
+            if ckpt_interval > 0 and done - last_ckpt_done >= ckpt_interval:
+                last_ckpt_done = done
+                self.save_checkpoint(ckpt)
+            if done >= stop_at:
+                break
+            live = _lib.C.c_int32()
+            h.call("bd_sim_live", _lib.C.byref(live))
+            if live.value == 0 and c["started"] >= N:
+                break
+            if max_launches is not None and launches >= max_launches:
+                break
+        c = self.read_counters()
+        status, steps, rets = self.outcomes()
+        elapsed = time.perf_counter() - t0
+        n_reacted = int(np.sum(status == 1))
+        n_escaped = int(np.sum(status == 2))
+        n_max = N - n_reacted - n_escaped
+        if ckpt_interval > 0 and ckpt.exists():
+            ckpt.unlink()
+        self.counters = c
+        outcome = status.astype(np.int32)
+        outcome[(outcome != 1) & (outcome != 2)] = 0
+        sim_data = {"outcome": outcome, "n_steps": steps.astype(np.int64), "n_returns": rets.astype(np.int64)}
+        total = int(c["steps"])
+        return B200BatchResult(n_trajectories=N, n_reacted=n_reacted, n_escaped=n_escaped, n_max_steps=n_max,
+                               reaction_counts={"stage_0": n_reacted}, r_start=float(self.params.r_start),
+                               r_escape=float(self.params.r_escape), dt=float(getattr(self.params, "dt", 0.2)),
+                               elapsed_sec=elapsed, steps_per_sec=total / elapsed if elapsed > 0 else 0.0,
+                               sim_data=sim_data, total_steps=total, counters=c)

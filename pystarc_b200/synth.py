@@ -195,7 +195,7 @@ class BDSystem:
         dip = np.sum(q[:, None] * pos, axis=0)
         r2 = np.sum(pos ** 2, axis=1)
         quad = 0.5 * (3.0 * np.einsum("i,ia,ib->ab", q, pos, pos) - np.sum(q * r2) * np.eye(3))
-        return dip, quad, 4.0 * math.pi * self.sdie * EPS0
+        return dip, quad, 4.0 * math.pi * (self.sdie * EPS0)
 
     def engine_kwargs(self):
         return dict(elec_grids=self.elec_grids, born_grids=self.born_grids, alpha=self.alpha,

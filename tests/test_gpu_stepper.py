@@ -1,0 +1,124 @@
+"""CUDA stepper against the oracle stepper (same keyed Philox draws) and the reference's statistics."""
+
+import numpy as np
+import pytest
+
+from oracle import stepper as ost
+from tests.helpers import golden, oracle_engine, step_params, step_system, system
+
+pytestmark = pytest.mark.gpu
+
+
+class _MP:
+    def __init__(self, s):
+        self.dipole, self.quadrupole, self.four_pi_eps = s.multipole_moments()
+
+
+def make_sim(s, n_traj, max_steps, precision="fp64", torque="zero", seed=None, **kw):
+    from pystarc_b200.engine import B200ForceEngine
+    from pystarc_b200.simulator import B200BatchSimulator
+
+    eng = B200ForceEngine(**s.engine_kwargs(), multipole_expansion=_MP(s) if s.multipole else None,
+                          precision=precision, torque_mode=torque)
+    mol1, mol2 = s.molecules()
+    kw.setdefault("termination", "complete")
+    return B200BatchSimulator(mol1, mol2, s.mobility(), s.pathway_set(),
+                              s.params(n_traj=n_traj, max_steps=max_steps, seed=seed), eng, **kw)
+
+
+def oracle_keyed(s, n_traj, max_steps, torque="zero", seed=None):
+    eng = oracle_engine(s, born_chunk_skip=False)
+    fn = (lambda *a, **k: eng(*a, torque_mode="centroid", **k)) if torque == "centroid" else eng
+    return ost.run(step_system(s, fn), step_params(s, n_traj, seed or s.seed, max_steps), noise="philox",
+                   termination="complete")
+
+
+CASES = [("two_sphere", 400, 100000, "zero"), ("c2", 96, 300, "zero"), ("c3", 32, 80, "centroid")]
+
+
+@pytest.mark.parametrize("sysname,n,max_steps,torque", CASES)
+def test_fp64_trajectories_match_oracle_exactly(sysname, n, max_steps, torque):
+    s = system(sysname)
+    sim = make_sim(s, n, max_steps, "fp64", torque, steps_per_launch=16, launches_per_poll=4)
+    res = sim.run()
+    st, steps, rets = sim.outcomes()
+    o = oracle_keyed(s, n, max_steps, torque)
+    np.testing.assert_array_equal(st, o.status)
+    np.testing.assert_array_equal(steps, o.n_steps)
+    np.testing.assert_array_equal(rets, o.n_returns)
+    assert res.total_steps == o.total_steps
+    assert sim._return_prob == o.return_prob and sim._k_b == o.k_b
+    assert res.n_reacted == o.n_reacted and res.n_escaped == o.n_escaped
+
+
+@pytest.mark.parametrize("sysname,n,max_steps,torque", CASES[1:])
+def test_mixed_precision_trajectories_mostly_identical(sysname, n, max_steps, torque):
+    s = system(sysname)
+    sim = make_sim(s, n, max_steps, "mixed", torque, steps_per_launch=16, launches_per_poll=4)
+    sim.run()
+    st, steps, _ = sim.outcomes()
+    o = oracle_keyed(s, n, max_steps, torque)
+    same = (st == o.status) & (steps == o.n_steps)
+    assert same.mean() >= 0.9, same.mean()
+
+
+def test_two_sphere_k_on_within_reference_ci():
+    """Reference run (2000 trajectories through its own stepper) vs 200k GPU trajectories: Wilson CIs overlap."""
+    g = golden("run_two_sphere")
+    s = system("two_sphere")
+    sim = make_sim(s, 200_000, 1_000_000, "fp64", termination="reference", seed=int(g["seed"]))
+    res = sim.run()
+    lo, hi = res.reaction_probability_ci()
+    rlo, rhi = g["ci"]
+    assert lo <= rhi and rlo <= hi, ((lo, hi), (rlo, rhi))
+    assert abs(sim._k_b - float(g["k_b"])) < 1e-12
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_every_trajectory_gets_one_outcome(precision):
+    s = system("c2")
+    N = 5000
+    sim = make_sim(s, N, 200, precision, slots=1024, steps_per_launch=8, launches_per_poll=2)
+    res = sim.run()
+    st, steps, _ = sim.outcomes()
+    assert set(np.unique(st)) <= {1, 2, 3}
+    assert res.counters["started"] == N
+    assert int(steps.sum()) == res.total_steps
+    assert res.n_reacted + res.n_escaped + res.n_max_steps == N
+    assert res.counters["reacted"] == res.n_reacted and res.counters["escaped"] == res.n_escaped
+    assert np.all(steps[st == 3] == 200)
+
+
+def test_checkpoint_resume_replays_exactly(tmp_path):
+    from pystarc_b200 import _lib
+
+    s = system("c2")
+    sim = make_sim(s, 3000, 400, "mixed", slots=512, steps_per_launch=8, launches_per_poll=1)
+    sim._setup()
+    h = sim.engine.handle
+    h.call("bd_sim_reset", None)
+    h.call("bd_sim_run", 5, 8, None)
+    path = sim.save_checkpoint(tmp_path / "ck.npz")
+    h.call("bd_sim_run", 400, 8, None)
+    a = sim.outcomes()
+    sim2 = make_sim(s, 3000, 400, "mixed", slots=512, steps_per_launch=8, launches_per_poll=1)
+    sim2._setup()
+    sim2.engine.handle.call("bd_sim_reset", None)
+    sim2.load_checkpoint(path)
+    sim2.engine.handle.call("bd_sim_run", 400, 8, None)
+    b = sim2.outcomes()
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+    assert (a[0] > 0).all()
+
+
+def test_launch_shape_does_not_change_fates():
+    s = system("c2")
+    outs = []
+    for group, slots in [(4, 300), (16, 2000)]:
+        sim = make_sim(s, 600, 250, "fp64", slots=slots, steps_per_launch=4 if group == 4 else 32)
+        sim.engine.handle.call("bd_set_launch", group, 128)
+        sim.run()
+        outs.append(sim.outcomes())
+    for x, y in zip(*outs):
+        np.testing.assert_array_equal(x, y)
