@@ -311,7 +311,7 @@ def main():
     ck = clocks.stop()
     t_fp64, tl_fp64, d_fp64, _ = time_device_arm(s, "fp64", args.steps, args.warmup, args.inner, n_traj, id_offset,
                                                  dist)
-    e2e_val, h2d, d2h, e2e_res = e2e_arm(s, "mixed", args.steps, args.inner, n_traj, id_offset)
+    e2e_val, h2d, d2h, e2e_res = e2e_arm(s, "mixed", max(args.steps, 20), args.inner, n_traj, id_offset)
     t_max = t_mixed
     steps_all = d_mixed["steps"]
     if dist is not None:

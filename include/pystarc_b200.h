@@ -3,7 +3,8 @@
  *
  * Every entry point returns an int status (BD_OK = 0, negative on error) and
  * never exits or aborts; bd_last_error() gives the message.  One handle is used
- * by one host thread at a time; handles are independent.  Array arguments are
+ * by one host thread at a time; handles are independent.  `stream` arguments are
+ * cudaStream_t values (NULL = the legacy default stream).  Array arguments are
  * plain pointers; which side (device or host) each pointer lives on is stated
  * per function.  Units are the reference's: Angstrom, ps, kBT, e.
  *

@@ -299,7 +299,9 @@ int finalize(BdHandle* h) {
   return BD_OK;
 }
 
-cudaStream_t pick(BdHandle* h, void* s) { return s ? (cudaStream_t)s : h->own; }
+// Stream arguments follow CUDA: NULL is the legacy default stream.  The handle's own
+// stream is only used to capture the stepper's CUDA graphs.
+cudaStream_t pick(BdHandle*, void* s) { return (cudaStream_t)s; }
 
 // ---------------------------------------------------------------------------
 // Kernel dispatch over (precision, group size, torque)
