@@ -34,6 +34,28 @@ struct Counts {
   unsigned grid, rev, ff;
 };
 
+// Bit j set: receptor chunk k0 + j has a bounding sphere within `reach` of c.
+// Lane j of the group tests chunk k0 + j; the mask is the same on every lane.
+template <int G>
+__device__ __forceinline__ unsigned chunk_hits(const DevSystem& S, const double c[3], double reach, int k0, int lane,
+                                               unsigned gm) {
+  const int k = k0 + lane;
+  bool hit = false;
+  if (k < S.n_chunks) {
+    const double4 sp = S.chunks[k];
+    const double dx = sp.x - c[0], dy = sp.y - c[1], dz = sp.z - c[2];
+    const double lim = reach + sp.w;
+    hit = dx * dx + dy * dy + dz * dz < lim * lim;
+  }
+  if constexpr (G == 1) {
+    return hit ? 1u : 0u;
+  } else {
+    unsigned m = __ballot_sync(gm, hit);
+    if constexpr (G < 32) m = (m >> ((threadIdx.x & 31u) & ~(unsigned)(G - 1))) & ((1u << G) - 1u);
+    return m;
+  }
+}
+
 // Lab-frame offset ro = x - c and lab position x of ligand atom i.
 struct PosFromPose {
   const double* R;
@@ -133,16 +155,18 @@ __device__ void group_forces(const DevSystem& S, const double c[3], const double
     }
   }
   // Born direction 2: ligand Born grid at the receptor atoms, in the ligand frame.
+  // Lanes test G receptor chunks at a time against the box's circumsphere, then
+  // sweep the hit chunks' atoms together.
   double r0 = 0, r1 = 0, r2 = 0, u0 = 0, u1 = 0, u2 = 0;
   if (S.born_rev) {
     const double rho = S.lig_born_rho;
     if (norm3(c[0], c[1], c[2]) - S.rec_max_r < rho) {
       const double rho2 = rho * rho;
-      for (int k = 0; k < S.n_chunks; ++k) {
-        const double4 sp = S.chunks[k];
-        const double dx = sp.x - c[0], dy = sp.y - c[1], dz = sp.z - c[2];
-        const double lim = rho + sp.w;
-        if (dx * dx + dy * dy + dz * dz >= lim * lim) continue;
+      for (int k0 = 0; k0 < S.n_chunks; k0 += G) {
+       unsigned hits = chunk_hits<G>(S, c, rho, k0, lane, gm);
+       while (hits) {
+        const int k = k0 + __ffs(hits) - 1;
+        hits &= hits - 1;
         for (int a = lane; a < BD_CHUNK; a += G) {
           const double4 at = S.rec[k * BD_CHUNK + a];
           if (fabs(at.w) < 1e-9) continue;
@@ -166,6 +190,7 @@ __device__ void group_forces(const DevSystem& S, const double c[3], const double
           }
           nr += 1;
         }
+       }
       }
     }
   }
@@ -317,17 +342,6 @@ __device__ __forceinline__ void start_trajectory(const DevSim& P, int id, Traj& 
   tr.status = ST_RUNNING;
 }
 
-__device__ __forceinline__ void pair_distances(const DevSystem& S, const double c[3], const double R[9],
-                                               double d[BD_MAX_PAIRS]) {
-  for (int p = 0; p < S.n_pairs; ++p) {
-    const double* b = S.rx_body[p];
-    const double lx = R[0] * b[0] + R[1] * b[1] + R[2] * b[2] + c[0] - S.rx_rec[p][0];
-    const double ly = R[3] * b[0] + R[4] * b[1] + R[5] * b[2] + c[1] - S.rx_rec[p][1];
-    const double lz = R[6] * b[0] + R[7] * b[1] + R[8] * b[2] + c[2] - S.rx_rec[p][2];
-    d[p] = norm3(lx, ly, lz);
-  }
-}
-
 // Adaptive dt (pystarc/simulation/gpu_batch_simulator.py:961-1067, flattened-pairs mode).
 __device__ __forceinline__ double adaptive_dt(const DevSim& P, double r) {
   const double D_t = P.D_t;
@@ -363,23 +377,36 @@ __device__ __forceinline__ double hi_diffusion(const DevSim& P, double r) {
   return (double)(D > (FT)1e-6 ? D : (FT)1e-6);
 }
 
+// Overlap rejection test: is the new centroid within 1.5 A of any receptor atom
+// (gpu_batch_simulator.py:1106-1128)?  Chunks whose bounding sphere is farther
+// than 1.5 A are skipped; the answer is exact.
 template <int G>
 __device__ __forceinline__ bool overlap_any(const DevSystem& S, const double c[3], int lane, unsigned gm) {
-  bool hit = false;
+  bool any = false;
   if (norm3(c[0], c[1], c[2]) < S.rec_max_r + 1.5) {
-    for (int k = 0; k < S.n_chunks && !hit; ++k) {
-      const double4 sp = S.chunks[k];
-      const double dx = sp.x - c[0], dy = sp.y - c[1], dz = sp.z - c[2];
-      const double lim = sp.w + 1.5;
-      if (dx * dx + dy * dy + dz * dz >= lim * lim) continue;
-      for (int a = lane; a < BD_CHUNK; a += G) {
-        const double4 at = S.rec[k * BD_CHUNK + a];
-        if (norm3(c[0] - at.x, c[1] - at.y, c[2] - at.z) < 1.5) hit = true;
+    for (int k0 = 0; k0 < S.n_chunks && !any; k0 += G) {
+      unsigned hits = chunk_hits<G>(S, c, 1.5, k0, lane, gm);
+      bool hit = false;
+      while (hits) {
+        const int k = k0 + __ffs(hits) - 1;
+        hits &= hits - 1;
+        for (int a = lane; a < BD_CHUNK; a += G) {
+          const double4 at = S.rec[k * BD_CHUNK + a];
+          if (norm3(c[0] - at.x, c[1] - at.y, c[2] - at.z) < 1.5) hit = true;
+        }
       }
+      any = G > 1 ? __any_sync(gm, hit) : hit;
     }
   }
-  if (G > 1) hit = __any_sync(gm, hit);
-  return hit;
+  return any;
+}
+
+__device__ __forceinline__ double pair_distance(const DevSystem& S, const double c[3], const double R[9], int p) {
+  const double* b = S.rx_body[p];
+  const double lx = R[0] * b[0] + R[1] * b[1] + R[2] * b[2] + c[0] - S.rx_rec[p][0];
+  const double ly = R[3] * b[0] + R[4] * b[1] + R[5] * b[2] + c[1] - S.rx_rec[p][1];
+  const double lz = R[6] * b[0] + R[7] * b[1] + R[8] * b[2] + c[2] - S.rx_rec[p][2];
+  return norm3(lx, ly, lz);
 }
 
 // One BD step of one trajectory, in the reference's order
@@ -393,11 +420,9 @@ __device__ __forceinline__ int bd_step(const DevSystem& S, const DevSim& P, Traj
   const uint32_t s = (uint32_t)tr.steps;
   double R[9];
   quat_to_rot(tr.q, R);
-  double d[BD_MAX_PAIRS];
   if (S.n_pairs > 0) {
-    pair_distances(S, tr.c, R, d);
     int nsat = 0;
-    for (int p = 0; p < S.n_pairs; ++p) nsat += d[p] < S.rx_cut[p];
+    for (int p = 0; p < S.n_pairs; ++p) nsat += pair_distance(S, tr.c, R, p) < S.rx_cut[p];
     if (nsat >= S.n_needed) return ST_REACTED;
   }
   double r = norm3(tr.c[0], tr.c[1], tr.c[2]);
@@ -419,7 +444,7 @@ __device__ __forceinline__ int bd_step(const DevSystem& S, const DevSim& P, Traj
   }
   double F[3], T[3], E;
   group_forces<FT, G, TORQUE, false>(S, tr.c, R, lane, gm, PosFromPose{R, tr.c}, F, T, E, tl.cnt);
-  if (S.n_pairs > 0) pair_distances(S, tr.c, R, d);
+  const double c0[3] = {tr.c[0], tr.c[1], tr.c[2]};  // pose of the old pair distances
   const double dt = adaptive_dt(P, r);
   const double D = hi_diffusion<FT>(P, r);
   double xt[3], xr[3];
@@ -439,9 +464,8 @@ __device__ __forceinline__ int bd_step(const DevSystem& S, const DevSim& P, Traj
     tl.nonfinite += 1;
     return ST_ERROR;
   }
-  if (P.overlap && overlap_any<G>(S, cn, lane, gm)) {
-    tl.overlap += 1;
-  } else {
+  const bool moved = !(P.overlap && overlap_any<G>(S, cn, lane, gm));
+  if (moved) {
     tr.c[0] = cn[0];
     tr.c[1] = cn[1];
     tr.c[2] = cn[2];
@@ -449,20 +473,27 @@ __device__ __forceinline__ int bd_step(const DevSystem& S, const DevSim& P, Traj
     tr.q[1] = qn[1];
     tr.q[2] = qn[2];
     tr.q[3] = qn[3];
+  } else {
+    tl.overlap += 1;
   }
   int st = ST_RUNNING;
   if (S.n_pairs > 0) {
-    double Rn[9], d1[BD_MAX_PAIRS];
-    quat_to_rot(tr.q, Rn);
-    pair_distances(S, tr.c, Rn, d1);
+    double Rn[9];
+    if (moved) {
+      quat_to_rot(tr.q, Rn);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 9; ++k) Rn[k] = R[k];
+    }
     int fired = 0;
     for (int p = 0; p < S.n_pairs; ++p) {
-      const double x0 = d[p] - S.rx_cut[p], x1 = d1[p] - S.rx_cut[p];
+      const double d0 = pair_distance(S, c0, R, p), d1 = pair_distance(S, tr.c, Rn, p);
+      const double x0 = d0 - S.rx_cut[p], x1 = d1 - S.rx_cut[p];
       double pc = 0.0;
       if (x0 > 0 && x1 > 0) pc = exp(-x0 * x1 / fmax(S.rx_deff[p] * dt, 1e-30));
       const W4 w = key.w(s, SUB_BRIDGE + (uint32_t)(p >> 1));
       const double u = (p & 1) ? u53(w.c, w.d) : u53(w.a, w.b);
-      fired += (u < pc) || (d1[p] < S.rx_cut[p]);
+      fired += (u < pc) || (d1 < S.rx_cut[p]);
     }
     if (fired >= S.n_needed) {
       st = ST_REACTED;

@@ -255,7 +255,7 @@ class B200BatchSimulator:
         h.call("bd_sim_capacity", _lib.C.byref(cap))
         if int(d["cap"]) != cap.value:
             raise ValueError(f"{path}: slot capacity {int(d['cap'])} != {cap.value}")
-        arr = {k: np.ascontiguousarray(d[k]) for k in d.files}
+        arr = {k: (np.ascontiguousarray(d[k]) if d[k].ndim else d[k][()]) for k in d.files}
         h.call("bd_sim_restore", _lib.ptr(arr["c"]), _lib.ptr(arr["q"]), _lib.ptr(arr["traj"], _lib.C.c_int32),
                _lib.ptr(arr["steps"], _lib.C.c_int32), _lib.ptr(arr["rets"], _lib.C.c_int32),
                _lib.ptr(arr["status"], _lib.C.c_int8), int(arr["n_live"]), _lib.ptr(arr["counters"], _lib.C.c_uint64),

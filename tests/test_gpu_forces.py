@@ -95,7 +95,9 @@ def test_no_yukawa_uses_every_grid_finest_first():
     import copy
 
     s = copy.copy(system("c2"))
-    s.rec_q = s.rec_q - s.rec_q.sum() / len(s.rec_q) * (np.abs(s.rec_q) > 0)
+    charged = np.abs(s.rec_q) > 0
+    s.rec_q = s.rec_q - s.rec_q.sum() / charged.sum() * charged
+    assert abs(s.rec_q.sum()) < 1e-9
     eng = make_engine(s, "fp64")
     assert len(eng._elec_grids_gpu) == 2 and not eng._has_yukawa
     c, q = random_poses(800, 5.0, 75.0, 9)

@@ -89,9 +89,21 @@ def test_every_trajectory_gets_one_outcome(precision):
     assert np.all(steps[st == 3] == 200)
 
 
-def test_checkpoint_resume_replays_exactly(tmp_path):
+def _run_to_completion(sim, K):
     from pystarc_b200 import _lib
 
+    h = sim.engine.handle
+    for _ in range(10000):
+        h.call("bd_sim_run", 4, K, None)
+        live = _lib.C.c_int32()
+        h.call("bd_sim_live", _lib.C.byref(live))
+        if live.value == 0 and sim.read_counters()["started"] >= int(sim.params.n_trajectories):
+            return
+    raise AssertionError("did not complete")
+
+
+def test_checkpoint_resume_replays_exactly(tmp_path):
+    """Resume from a mid-run checkpoint gives every trajectory the same outcome as the uninterrupted run."""
     s = system("c2")
     sim = make_sim(s, 3000, 400, "mixed", slots=512, steps_per_launch=8, launches_per_poll=1)
     sim._setup()
@@ -99,17 +111,17 @@ def test_checkpoint_resume_replays_exactly(tmp_path):
     h.call("bd_sim_reset", None)
     h.call("bd_sim_run", 5, 8, None)
     path = sim.save_checkpoint(tmp_path / "ck.npz")
-    h.call("bd_sim_run", 400, 8, None)
+    _run_to_completion(sim, 8)
     a = sim.outcomes()
     sim2 = make_sim(s, 3000, 400, "mixed", slots=512, steps_per_launch=8, launches_per_poll=1)
     sim2._setup()
     sim2.engine.handle.call("bd_sim_reset", None)
     sim2.load_checkpoint(path)
-    sim2.engine.handle.call("bd_sim_run", 400, 8, None)
+    _run_to_completion(sim2, 8)
     b = sim2.outcomes()
     for x, y in zip(a, b):
         np.testing.assert_array_equal(x, y)
-    assert (a[0] > 0).all()
+    assert set(np.unique(a[0])) <= {1, 2, 3}
 
 
 def test_launch_shape_does_not_change_fates():
