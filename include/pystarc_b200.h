@@ -138,8 +138,12 @@ int bd_sim_restore(BdHandle* h, const double* c, const double* q, const int32_t*
                    const int32_t* rets, const int8_t* status, int32_t n_live, const uint64_t* counters,
                    const int8_t* out_status, const int32_t* out_steps, const int32_t* out_returns);
 
-/* Launch shape: lanes per trajectory (1, 4, 8, 16 or 32) and threads per block (multiple
- * of 32, <= 256).  Set by the autotuner; 0 keeps the current value. */
+/* Launch shape: lanes per trajectory (1, 4, 8, 16 or 32: the lanes of a group share one
+ * trajectory's whole step) or BD_GROUP_WARP (each lane owns one trajectory's step logic and
+ * the warp sweeps each trajectory's atoms together; BD_GROUP_WARP_CAPPED is the same with
+ * registers capped at 128 per thread), and threads per block (multiple of 32, <= 256).
+ * Set by the autotuner; 0 keeps the current value. */
+enum { BD_GROUP_WARP = 64, BD_GROUP_WARP_CAPPED = 65 };
 int bd_set_launch(BdHandle* h, int group, int block_threads);
 int bd_get_launch(BdHandle* h, int* group, int* block_threads, int* grid_blocks);
 

@@ -315,6 +315,12 @@ struct K {
 
 template <typename FT, bool TQ>
 void* pick_g(int G, int which) {
+  if (G == BD_GROUP_WARP || G == BD_GROUP_WARP_CAPPED) {
+    // warp-cooperative stepper; the parity kernels use a full-warp group (same sweep code)
+    if (which == 2)
+      return G == BD_GROUP_WARP ? (void*)&step_kernel_warp<FT, TQ, 1> : (void*)&step_kernel_warp<FT, TQ, 2>;
+    G = 32;
+  }
   switch (G) {
 #define BD_CASE(g)                                                  \
   case g:                                                           \
@@ -335,21 +341,30 @@ void* kernel_for(int prec, int G, int torque, int which) {
   return tq ? pick_g<float, true>(G, which) : pick_g<float, false>(G, which);
 }
 
-bool valid_group(int g) { return g == 1 || g == 4 || g == 8 || g == 16 || g == 32; }
+bool valid_group(int g) {
+  return g == 1 || g == 4 || g == 8 || g == 16 || g == 32 || g == BD_GROUP_WARP || g == BD_GROUP_WARP_CAPPED;
+}
 
-int default_group(int n_lig_charged, bool born_rev) {
-  if (born_rev) return n_lig_charged > 64 ? 32 : 8;
-  if (n_lig_charged <= 2) return 1;
-  if (n_lig_charged <= 12) return 4;
-  if (n_lig_charged <= 48) return 8;
-  if (n_lig_charged <= 200) return 16;
-  return 32;
+// Lanes that hold one trajectory's state (the warp-cooperative modes keep one per lane).
+int lanes_per_traj(int g) { return (g == BD_GROUP_WARP || g == BD_GROUP_WARP_CAPPED) ? 1 : g; }
+
+// Tiny ligands with nothing to sweep: one lane per trajectory does everything.
+// Otherwise the warp-cooperative mode.  The autotuner can override either.
+int default_group(int n_lig_charged, bool sweeps_receptor) {
+  if (!sweeps_receptor && n_lig_charged <= 2) return 1;
+  return BD_GROUP_WARP;
 }
 
 int n_charged(const BdHandle* h) {
   int n = 0;
   for (size_t i = 0; i < h->lig.size() / 4; ++i) n += std::fabs(h->lig[4 * i + 3]) >= 1e-9;
   return n;
+}
+
+int launch_group(const BdHandle* h) {
+  if (h->launch_user) return h->group;
+  const bool sweeps = h->S.born_rev || (h->sp.overlap && !h->rec.empty());
+  return default_group(n_charged(h), sweeps);
 }
 
 int eval_grid_blocks(BdHandle* h, long long n, int G, int block) {
@@ -509,7 +524,7 @@ int bd_eval_forces(BdHandle* h, int64_t n, const double* cen, const double* rot,
   int rc = finalize(h);
   if (rc) return rc;
   if (n == 0) return BD_OK;
-  const int G = h->launch_user ? h->group : default_group(n_charged(h), h->S.born_rev);
+  const int G = launch_group(h);
   const int block = 128;
   void* fn = kernel_for(prec, G, torque, 0);
   unsigned long long* ctr = nullptr;
@@ -530,7 +545,7 @@ int bd_eval_forces_atoms(BdHandle* h, int64_t n, const double* pos, const double
   int rc = finalize(h);
   if (rc) return rc;
   if (n == 0) return BD_OK;
-  const int G = h->launch_user ? h->group : default_group(n_charged(h), h->S.born_rev);
+  const int G = launch_group(h);
   const int block = 128;
   void* fn = kernel_for(prec, G, torque, 1);
   long long nn = n;
@@ -541,7 +556,7 @@ int bd_eval_forces_atoms(BdHandle* h, int64_t n, const double* pos, const double
 
 int bd_set_launch(BdHandle* h, int group, int block) {
   if (!h) return BD_ERR_ARG;
-  if (group && !valid_group(group)) return fail(h, BD_ERR_ARG, "group must be 1, 4, 8, 16 or 32");
+  if (group && !valid_group(group)) return fail(h, BD_ERR_ARG, "group must be 1, 4, 8, 16, 32, 64 or 65 (warp-cooperative)");
   if (block && (block % 32 || block < 32 || block > 256)) return fail(h, BD_ERR_ARG, "block must be 32..256, x32");
   if (group) h->group = group;
   if (block) h->block = block;
@@ -552,7 +567,7 @@ int bd_set_launch(BdHandle* h, int group, int block) {
 
 int bd_get_launch(BdHandle* h, int* group, int* block, int* grid) {
   if (!h) return BD_ERR_ARG;
-  const int G = h->launch_user ? h->group : default_group(n_charged(h), h->S.born_rev);
+  const int G = launch_group(h);
   if (group) *group = G;
   if (block) *block = h->block;
   if (grid) {
@@ -580,9 +595,9 @@ int bd_sim_configure(BdHandle* h, const BdSimParams* p) {
   h->sim_ready = false;
   h->sp = *p;
   // live-slot capacity
-  const int G = h->launch_user ? h->group : default_group(n_charged(h), h->S.born_rev);
+  const int G = launch_group(h);
   void* fn = kernel_for(p->precision, G, p->torque_mode, 2);
-  const long long resident = (long long)persistent_blocks(h, fn, h->block) * (h->block / G);
+  const long long resident = (long long)persistent_blocks(h, fn, h->block) * (h->block / lanes_per_traj(G));
   long long cap = p->slots > 0 ? p->slots : std::max<long long>(65536, 8 * resident);
   cap = std::min<long long>(cap, p->n_traj);
   const int C = (int)cap;
@@ -672,7 +687,7 @@ int bd_sim_reset(BdHandle* h, void* stream) {
 namespace {
 
 int enqueue_launch(BdHandle* h, int K, cudaStream_t s, int cur) {
-  const int G = h->launch_user ? h->group : default_group(n_charged(h), h->S.born_rev);
+  const int G = launch_group(h);
   void* fn = kernel_for(h->sp.precision, G, h->sp.torque_mode, 2);
   const int blocks = persistent_blocks(h, fn, h->block);
   SlotBuf src = h->buf[cur], dst = h->buf[1 - cur];
@@ -688,7 +703,7 @@ int enqueue_launch(BdHandle* h, int K, cudaStream_t s, int cur) {
 }
 
 int build_graphs(BdHandle* h, int K) {
-  const int G = h->launch_user ? h->group : default_group(n_charged(h), h->S.born_rev);
+  const int G = launch_group(h);
   if (h->graph_K == K && h->graph_G == G && h->graph_B == h->block && h->graph_prec == h->sp.precision &&
       h->graph_torque == h->sp.torque_mode)
     return BD_OK;

@@ -319,6 +319,8 @@ struct Tally {
   Counts cnt;
 };
 
+__device__ __forceinline__ void flush_tally(const DevSim& P, Tally tl, bool owner);
+
 __device__ __forceinline__ Keyed traj_key(const DevSim& P, int id) {
   const unsigned long long g = (unsigned long long)(P.id_offset + id);
   return Keyed{P.k0, P.k1, (uint32_t)(g & 0xffffffffull), (uint32_t)(g >> 32)};
@@ -409,23 +411,18 @@ __device__ __forceinline__ double pair_distance(const DevSystem& S, const double
   return norm3(lx, ly, lz);
 }
 
-// One BD step of one trajectory, in the reference's order
-// (gpu_batch_simulator.py:783-1254): discrete reaction test, escape/return,
-// forces, old pair distances, adaptive dt, D(r), translation, rotation,
-// overlap rejection, Brownian bridge, step count.  Returns the new status.
-template <typename FT, int G, bool TORQUE>
-__device__ __forceinline__ int bd_step(const DevSystem& S, const DevSim& P, Traj& tr, int lane, unsigned gm,
-                                       Tally& tl) {
-  const Keyed key = traj_key(P, tr.id);
-  const uint32_t s = (uint32_t)tr.steps;
-  double R[9];
+// Discrete reaction test and escape/return at the start of a step
+// (gpu_batch_simulator.py:856-911).  Returns ST_RUNNING if the trajectory
+// goes on to the force evaluation; sets R = R(q) and r = |c| of that pose.
+__device__ __forceinline__ int step_begin(const DevSystem& S, const DevSim& P, const Keyed& key, uint32_t s, Traj& tr,
+                                          double R[9], double& r, Tally& tl) {
   quat_to_rot(tr.q, R);
   if (S.n_pairs > 0) {
     int nsat = 0;
     for (int p = 0; p < S.n_pairs; ++p) nsat += pair_distance(S, tr.c, R, p) < S.rx_cut[p];
     if (nsat >= S.n_needed) return ST_REACTED;
   }
-  double r = norm3(tr.c[0], tr.c[1], tr.c[2]);
+  r = norm3(tr.c[0], tr.c[1], tr.c[2]);
   if (r >= P.r_esc) {
     const W4 w = key.w(s, SUB_ESCAPE);
     if (u53(w.a, w.b) < P.return_prob) {
@@ -442,10 +439,16 @@ __device__ __forceinline__ int bd_step(const DevSystem& S, const DevSim& P, Traj
       return ST_ESCAPED;
     }
   }
-  double F[3], T[3], E;
-  group_forces<FT, G, TORQUE, false>(S, tr.c, R, lane, gm, PosFromPose{R, tr.c}, F, T, E, tl.cnt);
-  const double c0[3] = {tr.c[0], tr.c[1], tr.c[2]};  // pose of the old pair distances
-  const double dt = adaptive_dt(P, r);
+  return ST_RUNNING;
+}
+
+// Adaptive dt, D(r), Ermak-McCammon translation and the body-frame rotation
+// (gpu_batch_simulator.py:961-1101).  Writes the proposed pose; false if it is not finite.
+template <typename FT>
+__device__ __forceinline__ bool step_move(const DevSim& P, const Keyed& key, uint32_t s, const Traj& tr, double r,
+                                          const double F[3], const double T[3], double cn[3], double qn[4],
+                                          double& dt) {
+  dt = adaptive_dt(P, r);
   const double D = hi_diffusion<FT>(P, r);
   double xt[3], xr[3];
   {
@@ -455,16 +458,21 @@ __device__ __forceinline__ int bd_step(const DevSystem& S, const DevSim& P, Traj
     box_muller(u53(c.a, c.b), u53(c.c, c.d), xr[1], xr[2]);
   }
   const double sig_t = sqrt(2.0 * D * dt), ddt = D * dt;
-  double cn[3], qn[4] = {tr.q[0], tr.q[1], tr.q[2], tr.q[3]};
 #pragma unroll
   for (int k = 0; k < 3; ++k) cn[k] = tr.c[k] + (ddt * F[k] + sig_t * xt[k]);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) qn[k] = tr.q[k];
   const double sig_r = sqrt(2.0 * P.D_r * dt), rdt = P.D_r * dt;
   rotate_quat(qn, rdt * T[0] + sig_r * xr[0], rdt * T[1] + sig_r * xr[1], rdt * T[2] + sig_r * xr[2]);
-  if (!(isfinite(cn[0]) && isfinite(cn[1]) && isfinite(cn[2]) && isfinite(qn[0]))) {
-    tl.nonfinite += 1;
-    return ST_ERROR;
-  }
-  const bool moved = !(P.overlap && overlap_any<G>(S, cn, lane, gm));
+  return isfinite(cn[0]) && isfinite(cn[1]) && isfinite(cn[2]) && isfinite(qn[0]);
+}
+
+// Overlap outcome, Brownian bridge, step count (gpu_batch_simulator.py:1102-1254).
+// R is the rotation at the old pose tr.c; the pose moves to (cn, qn) if `moved`.
+__device__ __forceinline__ int step_end(const DevSystem& S, const DevSim& P, const Keyed& key, uint32_t s, Traj& tr,
+                                        const double R[9], const double cn[3], const double qn[4], bool moved,
+                                        double dt, Tally& tl) {
+  const double c0[3] = {tr.c[0], tr.c[1], tr.c[2]};
   if (moved) {
     tr.c[0] = cn[0];
     tr.c[1] = cn[1];
@@ -504,6 +512,29 @@ __device__ __forceinline__ int bd_step(const DevSystem& S, const DevSim& P, Traj
   tl.steps += 1;
   if (st == ST_RUNNING && tr.steps >= P.max_steps) st = ST_MAXSTEPS;
   return st;
+}
+
+// One BD step of one trajectory by the G lanes of its group, in the
+// reference's order (gpu_batch_simulator.py:783-1254): discrete reaction test,
+// escape/return, forces, adaptive dt, D(r), translation, rotation, overlap
+// rejection, Brownian bridge, step count.  Returns the new status.
+template <typename FT, int G, bool TORQUE>
+__device__ __forceinline__ int bd_step(const DevSystem& S, const DevSim& P, Traj& tr, int lane, unsigned gm,
+                                       Tally& tl) {
+  const Keyed key = traj_key(P, tr.id);
+  const uint32_t s = (uint32_t)tr.steps;
+  double R[9], r;
+  const int st0 = step_begin(S, P, key, s, tr, R, r, tl);
+  if (st0 != ST_RUNNING) return st0;
+  double F[3], T[3], E;
+  group_forces<FT, G, TORQUE, false>(S, tr.c, R, lane, gm, PosFromPose{R, tr.c}, F, T, E, tl.cnt);
+  double cn[3], qn[4], dt;
+  if (!step_move<FT>(P, key, s, tr, r, F, T, cn, qn, dt)) {
+    tl.nonfinite += 1;
+    return ST_ERROR;
+  }
+  const bool moved = !(P.overlap && overlap_any<G>(S, cn, lane, gm));
+  return step_end(S, P, key, s, tr, R, cn, qn, moved, dt, tl);
 }
 
 __device__ __forceinline__ void load_slot(const SlotBuf& B, int s, Traj& tr) {
@@ -587,8 +618,135 @@ __global__ void __launch_bounds__(256) step_kernel(DevSystem S, DevSim P, SlotBu
     }
     if (lane == 0) store_slot(B, slot, tr);
   }
-  // Flush tallies: only lane 0 of each group counts scalar events.
-  if (lane != 0) {
+  // Only lane 0 of each group counts scalar events.
+  flush_tally(P, tl, lane == 0);
+}
+
+// All forces of the lanes with `need`, one trajectory at a time, the whole warp
+// sweeping that trajectory's ligand atoms and receptor chunks.
+template <typename FT, bool TORQUE>
+__device__ __forceinline__ void warp_forces(const DevSystem& S, const double c[3], const double R[9], bool need,
+                                            double F[3], double T[3], int lane, Counts& cnt) {
+  const unsigned FULL = 0xffffffffu;
+  unsigned m = __ballot_sync(FULL, need);
+  while (m) {
+    const int j = __ffs(m) - 1;
+    m &= m - 1;
+    double cj[3], Rj[9];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) cj[k] = __shfl_sync(FULL, c[k], j);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Rj[k] = __shfl_sync(FULL, R[k], j);
+    double f[3], t[3], e;
+    group_forces<FT, 32, TORQUE, false>(S, cj, Rj, lane, FULL, PosFromPose{Rj, cj}, f, t, e, cnt);
+    if (lane == j) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        F[k] = f[k];
+        T[k] = t[k];
+      }
+    }
+  }
+}
+
+// Overlap test of every lane with `need`, the warp sweeping the receptor chunks together.
+__device__ __forceinline__ bool warp_overlap(const DevSystem& S, const double cn[3], bool need, int lane) {
+  const unsigned FULL = 0xffffffffu;
+  unsigned m = __ballot_sync(FULL, need);
+  bool mine = false;
+  while (m) {
+    const int j = __ffs(m) - 1;
+    m &= m - 1;
+    double cj[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) cj[k] = __shfl_sync(FULL, cn[k], j);
+    const bool hit = overlap_any<32>(S, cj, lane, FULL);
+    if (lane == j) mine = hit;
+  }
+  return mine;
+}
+
+// Warp-cooperative persistent stepper.  Each lane owns one live slot and does
+// that trajectory's per-step scalar work (reaction test, escape/return, dt,
+// noise, pose update, bridge) with no redundancy; the warp then sweeps the
+// force and overlap loops one trajectory at a time, so those loops run with
+// all 32 lanes on the same trajectory instead of diverging groups.
+// MINB = minimum resident 256-thread blocks per SM requested from the register
+// allocator (1: no cap; 2: at most 128 registers per thread).
+template <typename FT, bool TORQUE, int MINB>
+__global__ void __launch_bounds__(256, MINB) step_kernel_warp(DevSystem S, DevSim P, SlotBuf B,
+                                                              const int* __restrict__ n_live, int K) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int live = *n_live;
+  Tally tl{};
+  for (;;) {
+    unsigned long long b = 0;
+    if (lane == 0) b = atomicAdd(P.ctr + C_SLOT_CURSOR, 32ull);
+    b = __shfl_sync(FULL, b, 0);
+    if (b >= (unsigned long long)live) break;
+    const int slot = (int)b + lane;
+    const bool own = slot < live;
+    Traj tr{};
+    tr.status = ST_EMPTY;
+    if (own) load_slot(B, slot, tr);
+    bool dead = !own;
+    for (int k = 0; k < K; ++k) {
+      // lanes whose trajectory ended take the next pending ids (one atomic per warp)
+      const bool want = !dead && tr.status != ST_RUNNING;
+      const unsigned wm = __ballot_sync(FULL, want);
+      if (wm) {
+        const int leader = __ffs(wm) - 1;
+        unsigned long long base = 0;
+        if (lane == leader) base = atomicAdd(P.ctr + C_PENDING, (unsigned long long)__popc(wm));
+        base = __shfl_sync(FULL, base, leader);
+        if (want) {
+          const unsigned long long id = base + __popc(wm & ((1u << lane) - 1u));
+          if (id >= (unsigned long long)P.n_traj) {
+            tr.status = ST_EMPTY;
+            dead = true;
+          } else {
+            start_trajectory(P, (int)id, tr);
+          }
+        }
+      }
+      if (__all_sync(FULL, dead)) break;
+      const Keyed key = traj_key(P, tr.id);
+      const uint32_t s = (uint32_t)tr.steps;
+      double R[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, r = 0;
+      int st = ST_EMPTY;
+      if (!dead) st = step_begin(S, P, key, s, tr, R, r, tl);
+      const bool need_f = !dead && st == ST_RUNNING;
+      double F[3] = {0, 0, 0}, T[3] = {0, 0, 0};
+      warp_forces<FT, TORQUE>(S, tr.c, R, need_f, F, T, lane, tl.cnt);
+      double cn[3] = {0, 0, 0}, qn[4] = {1, 0, 0, 0}, dt = 0;
+      bool ok = true;
+      if (need_f) ok = step_move<FT>(P, key, s, tr, r, F, T, cn, qn, dt);
+      if (need_f && !ok) {
+        tl.nonfinite += 1;
+        st = ST_ERROR;
+      }
+      const bool ovl = warp_overlap(S, cn, need_f && ok && P.overlap, lane);
+      if (need_f && ok) st = step_end(S, P, key, s, tr, R, cn, qn, !ovl, dt, tl);
+      if (!dead && st != ST_RUNNING) {
+        tr.status = st;
+        P.out_status[tr.id] = (int8_t)st;
+        P.out_steps[tr.id] = tr.steps;
+        P.out_returns[tr.id] = tr.rets;
+        tl.reacted += st == ST_REACTED;
+        tl.escaped += st == ST_ESCAPED;
+        tl.maxsteps += st == ST_MAXSTEPS;
+      }
+    }
+    if (own) store_slot(B, slot, tr);
+  }
+  flush_tally(P, tl, true);
+}
+
+// Sum the per-thread tallies of a warp and add them to the device counters.
+// Threads that do not own scalar events pass owner = false.
+__device__ __forceinline__ void flush_tally(const DevSim& P, Tally tl, bool owner) {
+  if (!owner) {
     tl.steps = 0;
     tl.reacted = tl.escaped = tl.maxsteps = tl.returns = tl.overlap = tl.bridge = tl.nonfinite = 0;
   }

@@ -77,7 +77,7 @@ def test_random_poses_against_oracle(sysname, precision, tol):
     eng.close()
 
 
-@pytest.mark.parametrize("group", [1, 4, 8, 16, 32])
+@pytest.mark.parametrize("group", [1, 4, 8, 16, 32, 64, 65])
 def test_launch_shape_does_not_change_results(group):
     s = system("c2")
     eng = make_engine(s, "fp64", "centroid")

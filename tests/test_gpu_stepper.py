@@ -127,8 +127,8 @@ def test_checkpoint_resume_replays_exactly(tmp_path):
 def test_launch_shape_does_not_change_fates():
     s = system("c2")
     outs = []
-    for group, slots in [(4, 300), (16, 2000)]:
-        sim = make_sim(s, 600, 250, "fp64", slots=slots, steps_per_launch=4 if group == 4 else 32)
+    for group, slots in [(4, 300), (16, 2000), (64, 500), (65, 150)]:
+        sim = make_sim(s, 600, 250, "fp64", slots=slots, steps_per_launch=4 if group in (4, 65) else 32)
         sim.engine.handle.call("bd_set_launch", group, 128)
         sim.run()
         outs.append(sim.outcomes())
