@@ -42,7 +42,6 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "BD steps/sec on 1 B200, surrogate vs plain at k_on within Wilson 95% CI"
 UNIT = "BD steps/s"
-WORKLOAD = "protein+small-ligand (3200/18 atoms, 193^3+129^3 grids, 1e6 trajectories)"
 ALGO_BYTES_PER_GATHER = 224  # 7 trilinear interpolations x 8 corners x 4 B per (atom, grid)
 STATE_BYTES_PER_STEP = 128  # FP64 pose read + write and status/counters per trajectory-step
 
@@ -107,9 +106,20 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def build_system(device):
+WORKLOADS = {
+    "protein-ligand": ("protein+small-ligand (3200/18 atoms, 193^3+129^3 grids, 1e6 trajectories)", 1_000_000),
+    "two-spheres": ("two charged spheres (+5/-5 e, 129^3 grid, 1e5 trajectories, FP64 physics)", 100_000),
+    "protein-protein": ("protein-protein (1700/1400 atoms, 3 x 161^3 grids, HI, 1e7 trajectories)", 10_000_000),
+}
+
+
+def build_system(device, workload="protein-ligand"):
     from pystarc_b200 import synth
 
+    if workload == "two-spheres":
+        return synth.config1()
+    if workload == "protein-protein":
+        return synth.config3(scale=1.0, device=device)
     return synth.config2(n_traj=1_000_000, scale=1.0, device=device)
 
 
@@ -130,7 +140,7 @@ def make_sim(s, precision, n_traj, K, id_offset=0, torque="zero"):
     return sim
 
 
-def time_device_arm(s, precision, steps, warmup, K, n_traj, id_offset, dist):
+def time_device_arm(s, precision, steps, warmup, K, n_traj, id_offset, dist, fixed_launch=None):
     """Per-launch CUDA-event times (graph launches) with L2 flushes in between."""
     import torch
 
@@ -138,7 +148,11 @@ def time_device_arm(s, precision, steps, warmup, K, n_traj, id_offset, dist):
     from pystarc_b200.autotune import autotune
 
     sim = make_sim(s, precision, n_traj, K, id_offset)
-    best, table = autotune(sim)  # untimed; the run below starts from a fresh reset
+    if fixed_launch:
+        table = {}
+        sim.engine.handle.call("bd_set_launch", fixed_launch[0], fixed_launch[1])
+    else:
+        best, table = autotune(sim)  # untimed; the run below starts from a fresh reset
     sim._setup()
     h = sim.engine.handle
     h.call("bd_sim_reset", None)
@@ -266,7 +280,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--inner", type=int, default=64, help="BD steps per trajectory per launch")
-    ap.add_argument("--n-traj", type=int, default=1_000_000)
+    ap.add_argument("--n-traj", type=int, default=0, help="trajectories per GPU (0: the workload's own count)")
+    ap.add_argument("--workload", default="protein-ligand", choices=sorted(WORKLOADS))
+    ap.add_argument("--launch", default="", help="fixed launch shape GROUPxBLOCK (default: autotune)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=40)
     args = ap.parse_args()
@@ -277,7 +293,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        s = build_system(None if not _has_cuda() else "cuda")
+        s = build_system(None if not _has_cuda() else "cuda", args.workload)
         cores = os.cpu_count() or 1
         vals = []
         for i in range(args.warmup + args.steps):
@@ -289,7 +305,8 @@ def main():
         print(json.dumps({"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
                           "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
                           "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                          "config": {"workload": WORKLOAD, "arm": "reference batched stepper restated in NumPy "
+                          "config": {"workload": WORKLOADS[args.workload][0],
+                                     "arm": "reference batched stepper restated in NumPy "
                                      "(PCG64 order), CPU"},
                           "cpu_baseline": info, "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0,
                                                         "d2h_bytes_per_step": 0}}))
@@ -306,16 +323,17 @@ def main():
         torch.cuda.set_device(local)
         td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         dist = td
-    s = build_system("cuda")
-    n_traj = args.n_traj
+    s = build_system("cuda", args.workload)
+    n_traj = args.n_traj or WORKLOADS[args.workload][1]
     id_offset = rank * n_traj
     clocks = Clocks(local)
     clocks.start()
+    fixed = tuple(int(v) for v in args.launch.split("x")) if args.launch else None
     t_mixed, tl_mixed, d_mixed, launch = time_device_arm(s, "mixed", args.steps, args.warmup, args.inner, n_traj,
-                                                         id_offset, dist)
+                                                         id_offset, dist, fixed)
     ck = clocks.stop()
     t_fp64, tl_fp64, d_fp64, launch64 = time_device_arm(s, "fp64", args.steps, args.warmup, args.inner, n_traj,
-                                                        id_offset, dist)
+                                                        id_offset, dist, fixed)
     e2e_val, h2d, d2h, e2e_res = e2e_arm(s, "mixed", max(args.steps, 20), args.inner, n_traj, id_offset,
                                          (launch["group"], launch["block"]))
     t_max = t_mixed
@@ -345,7 +363,8 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 forces / f64 poses", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "trajectories_per_gpu": n_traj, "bd_steps_per_launch": args.inner,
+        "config": {"workload": WORKLOADS[args.workload][0], "trajectories_per_gpu": n_traj,
+                   "bd_steps_per_launch": args.inner,
                    "parallelism": f"trajectory shards x{world}", "l2": "flushed (256 MiB write) between launches",
                    "launch": launch},
         "variants": {

@@ -147,6 +147,7 @@ enum { BD_GROUP_WARP = 64, BD_GROUP_WARP_CAPPED = 65 };
 int bd_set_launch(BdHandle* h, int group, int block_threads);
 int bd_get_launch(BdHandle* h, int* group, int* block_threads, int* grid_blocks);
 
+
 #ifdef __cplusplus
 }
 #endif

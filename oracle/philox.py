@@ -71,13 +71,14 @@ def box_muller(u1, u2):
 class KeyedDraws:
     """Per-(trajectory, step) draws with the layout in the module docstring."""
 
-    def __init__(self, seed: int):
+    def __init__(self, seed: int, id_offset: int = 0):
         seed = int(seed) & 0xFFFFFFFFFFFFFFFF
         self.k0 = np.uint64(seed & 0xFFFFFFFF)
         self.k1 = np.uint64(seed >> 32)
+        self.offset = np.uint64(id_offset)
 
     def words(self, step, sub, traj):
-        traj = np.asarray(traj, dtype=np.uint64)
+        traj = np.asarray(traj, dtype=np.uint64) + self.offset
         return philox4x32_10(step, sub, traj & MASK32, traj >> np.uint64(32), self.k0, self.k1)
 
     def uniform_pair(self, step, sub, traj):

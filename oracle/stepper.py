@@ -233,17 +233,18 @@ def _forces(sys, R_sr, cen_sr, force_batch=None):
 
 
 def run(sys: StepSystem, prm: StepParams, noise: str = "pcg64", termination: str = "reference",
-        force_batch=None) -> StepResult:
+        force_batch=None, id_offset: int = 0) -> StepResult:
     """Run ``prm.n_traj`` trajectories; see the module docstring for the two noise modes.
 
     ``termination="reference"`` stops the loop when 99.5 % are done or on a stall
     (gpu_batch_simulator.py:1347-1356); ``"complete"`` runs until every
-    trajectory has reacted, escaped or used ``max_steps`` steps.
+    trajectory has reacted, escaped or used ``max_steps`` steps.  With keyed
+    noise, local trajectory i draws as global trajectory ``id_offset + i``.
     """
     N = prm.n_traj
     keyed = noise == "philox"
     if keyed:
-        draws = KeyedDraws(prm.seed)
+        draws = KeyedDraws(prm.seed, id_offset)
     else:
         rng = np.random.default_rng(prm.seed)
     if prm.return_prob is None or prm.k_b is None:

@@ -594,7 +594,10 @@ __global__ void __launch_bounds__(256) step_kernel(DevSystem S, DevSim P, SlotBu
     if (slot >= live) break;
     Traj tr;
     load_slot(B, slot, tr);
-    for (int k = 0; k < K; ++k) {
+    // A slot always leaves a launch RUNNING or EMPTY: an ended trajectory is
+    // replaced right away, even after the launch's last step, so the compaction
+    // only ever drops slots whose replacement found the pool empty.
+    for (int k = 0; k < K && tr.status != ST_EMPTY; ++k) {
       if (tr.status != ST_RUNNING) {
         const int id = group_fetch<G>(P.ctr + C_PENDING, lane, gm);
         if (id >= P.n_traj) {
@@ -614,6 +617,12 @@ __global__ void __launch_bounds__(256) step_kernel(DevSystem S, DevSim P, SlotBu
         tl.reacted += st == ST_REACTED;
         tl.escaped += st == ST_ESCAPED;
         tl.maxsteps += st == ST_MAXSTEPS;
+        const int id = group_fetch<G>(P.ctr + C_PENDING, lane, gm);
+        if (id >= P.n_traj) {
+          tr.status = ST_EMPTY;
+        } else {
+          start_trajectory(P, id, tr);
+        }
       }
     }
     if (lane == 0) store_slot(B, slot, tr);
@@ -666,6 +675,28 @@ __device__ __forceinline__ bool warp_overlap(const DevSystem& S, const double cn
   return mine;
 }
 
+// Lanes whose trajectory ended (and that are not out of work) take the next
+// pending ids, one atomic per warp; a lane that finds the pool empty goes EMPTY.
+__device__ __forceinline__ void warp_refill(const DevSim& P, Traj& tr, bool& dead, int lane) {
+  const unsigned FULL = 0xffffffffu;
+  const bool want = !dead && tr.status != ST_RUNNING;
+  const unsigned wm = __ballot_sync(FULL, want);
+  if (!wm) return;
+  const int leader = __ffs(wm) - 1;
+  unsigned long long base = 0;
+  if (lane == leader) base = atomicAdd(P.ctr + C_PENDING, (unsigned long long)__popc(wm));
+  base = __shfl_sync(FULL, base, leader);
+  if (want) {
+    const unsigned long long id = base + __popc(wm & ((1u << lane) - 1u));
+    if (id >= (unsigned long long)P.n_traj) {
+      tr.status = ST_EMPTY;
+      dead = true;
+    } else {
+      start_trajectory(P, (int)id, tr);
+    }
+  }
+}
+
 // Warp-cooperative persistent stepper.  Each lane owns one live slot and does
 // that trajectory's per-step scalar work (reaction test, escape/return, dt,
 // noise, pose update, bridge) with no redundancy; the warp then sweeps the
@@ -692,24 +723,7 @@ __global__ void __launch_bounds__(256, MINB) step_kernel_warp(DevSystem S, DevSi
     if (own) load_slot(B, slot, tr);
     bool dead = !own;
     for (int k = 0; k < K; ++k) {
-      // lanes whose trajectory ended take the next pending ids (one atomic per warp)
-      const bool want = !dead && tr.status != ST_RUNNING;
-      const unsigned wm = __ballot_sync(FULL, want);
-      if (wm) {
-        const int leader = __ffs(wm) - 1;
-        unsigned long long base = 0;
-        if (lane == leader) base = atomicAdd(P.ctr + C_PENDING, (unsigned long long)__popc(wm));
-        base = __shfl_sync(FULL, base, leader);
-        if (want) {
-          const unsigned long long id = base + __popc(wm & ((1u << lane) - 1u));
-          if (id >= (unsigned long long)P.n_traj) {
-            tr.status = ST_EMPTY;
-            dead = true;
-          } else {
-            start_trajectory(P, (int)id, tr);
-          }
-        }
-      }
+      warp_refill(P, tr, dead, lane);
       if (__all_sync(FULL, dead)) break;
       const Keyed key = traj_key(P, tr.id);
       const uint32_t s = (uint32_t)tr.steps;
@@ -738,6 +752,8 @@ __global__ void __launch_bounds__(256, MINB) step_kernel_warp(DevSystem S, DevSi
         tl.maxsteps += st == ST_MAXSTEPS;
       }
     }
+    // a slot leaves the launch RUNNING or EMPTY (ended trajectories are replaced now)
+    warp_refill(P, tr, dead, lane);
     if (own) store_slot(B, slot, tr);
   }
   flush_tally(P, tl, true);

@@ -279,6 +279,7 @@ class B200BatchSimulator:
                 h.call("bd_sim_reset", None)
         last_ckpt_done = 0
         launches = 0
+        stalled, last_steps = 0, -1
         stop_at = int(N * 0.995) if self.termination == "reference" else N
         while True:
             h.call("bd_sim_run", self.M, self.K, None)
@@ -298,6 +299,14 @@ class B200BatchSimulator:
             h.call("bd_sim_live", _lib.C.byref(live))
             if live.value == 0 and c["started"] >= N:
                 break
+            # watchdog: live slots but no step taken for many polls means the device work stopped
+            if c["steps"] == last_steps:
+                stalled += 1
+                if stalled >= 50:
+                    raise _lib.BdError(_lib.BD_ERR_STALL, f"no BD step in {stalled} polls with {live.value} live "
+                                                          f"slots, {done}/{N} trajectories done")
+            else:
+                stalled, last_steps = 0, c["steps"]
             if max_launches is not None and launches >= max_launches:
                 break
         c = self.read_counters()
