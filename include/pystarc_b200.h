@@ -147,6 +147,23 @@ enum { BD_GROUP_WARP = 64, BD_GROUP_WARP_CAPPED = 65 };
 int bd_set_launch(BdHandle* h, int group, int block_threads);
 int bd_get_launch(BdHandle* h, int* group, int* block_threads, int* grid_blocks);
 
+/* No counterpart in the reference.  Runs p->n_traj trajectories to completion (or for
+ * max_launches launches of steps_per_launch steps) on the handle's system WITHOUT
+ * allocating device memory, for callers that cannot call cudaMalloc at that point: an
+ * application whose allocator already holds the GPU's memory, a process under a memory
+ * quota, or code running while another library captures a CUDA graph.  The live-slot
+ * pool, live counts and counters use a fixed file-scope device array of 9.1 MB, enough for
+ * BD_NOALLOC_MAX_SLOTS live slots; p->slots above that is rejected with BD_ERR_ARG
+ * (0 = use the maximum).  Outputs are DEVICE arrays the caller owns: out_status,
+ * out_steps, out_returns (p->n_traj each, as bd_sim_outcomes) and counters (BD_CTR_NUM).
+ * The system must already be on the device (its upload allocates): call bd_sim_configure
+ * or an evaluation once before.  The first call on a device looks up the array's device
+ * address; make that first call before any stream capture.  Every call shares the array
+ * and clears the parts it uses; calls that overlap on the GPU race.  Synchronous. */
+enum { BD_NOALLOC_MAX_SLOTS = 65536 };
+int bd_sim_run_noalloc(BdHandle* h, const BdSimParams* p, int8_t* out_status, int32_t* out_steps,
+                       int32_t* out_returns, uint64_t* counters, int steps_per_launch, int max_launches,
+                       void* stream);
 
 #ifdef __cplusplus
 }

@@ -841,3 +841,137 @@ int bd_sim_restore(BdHandle* h, const double* c, const double* q, const int32_t*
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free run, called by bd_sim_run_noalloc (bd_noalloc.cu) with the
+// address of its static device scratch array.  Nothing here allocates device
+// memory: the live-slot pool, live counts and counters are carved from
+// `scratch`; per-trajectory outputs and the final counters go to caller arrays.
+// ---------------------------------------------------------------------------
+namespace {
+
+unsigned char* carve(unsigned char*& p, size_t bytes) {
+  unsigned char* out = p;
+  p += (bytes + 255) & ~(size_t)255;
+  return out;
+}
+
+}  // namespace
+
+int bd_internal_device(const BdHandle* h) { return h ? h->device : -1; }
+
+int bd_internal_fail(BdHandle* h, int code, const char* msg) { return fail(h, code, "%s", msg); }
+
+int bd_internal_run_noalloc(BdHandle* h, const BdSimParams* p, unsigned char* scratch, size_t scratch_bytes,
+                            int max_slots, int8_t* out_status, int32_t* out_steps, int32_t* out_returns,
+                            uint64_t* counters, int K, int max_launches, cudaStream_t s) {
+  if (!h) return BD_ERR_ARG;
+  if (!p || !out_status || !out_steps || !out_returns || !counters)
+    return fail(h, BD_ERR_ARG, "bd_sim_run_noalloc: NULL argument");
+  if (p->n_traj <= 0 || p->n_traj > 0x7ffffff0ll) return fail(h, BD_ERR_ARG, "n_traj out of range");
+  if (p->id_offset < 0) return fail(h, BD_ERR_ARG, "id_offset must be >= 0");
+  if (!(p->r_escape > p->r_start) || !(p->r_start > 0)) return fail(h, BD_ERR_ARG, "need 0 < r_start < r_escape");
+  if (!(p->D_t > 0) || !(p->D_r >= 0)) return fail(h, BD_ERR_ARG, "diffusion coefficients must be positive");
+  if (p->max_steps <= 0) return fail(h, BD_ERR_ARG, "max_steps must be positive");
+  if (p->precision != BD_PREC_FP64 && p->precision != BD_PREC_MIXED) return fail(h, BD_ERR_ARG, "bad precision");
+  if (p->torque_mode != BD_TORQUE_ZERO && p->torque_mode != BD_TORQUE_CENTROID) return fail(h, BD_ERR_ARG, "bad torque");
+  if (p->use_hi && !(p->r_hydro_rec > 0 && p->r_hydro_lig > 0)) return fail(h, BD_ERR_ARG, "HI needs hydro radii");
+  if (K <= 0 || max_launches <= 0) return fail(h, BD_ERR_ARG, "steps_per_launch and max_launches must be > 0");
+  if (p->slots > max_slots)
+    return fail(h, BD_ERR_ARG, "bd_sim_run_noalloc: %d slots requested, the static scratch holds at most %d",
+                p->slots, max_slots);
+  if (h->dirty)
+    return fail(h, BD_ERR_STATE,
+                "bd_sim_run_noalloc: the system is not on the device yet; its upload allocates, so call "
+                "bd_sim_configure or an evaluation once before");
+  CK(h, cudaSetDevice(h->device));
+  const int C = (int)std::min<long long>(p->slots > 0 ? p->slots : max_slots, p->n_traj);
+  // scratch layout: two slot buffers, two live counts, the counters
+  unsigned char* cur_p = scratch;
+  SlotBuf B[2];
+  for (int b = 0; b < 2; ++b) {
+    B[b].c = (double*)carve(cur_p, 3 * (size_t)C * sizeof(double));
+    B[b].q = (double*)carve(cur_p, 4 * (size_t)C * sizeof(double));
+    B[b].traj = (int*)carve(cur_p, (size_t)C * sizeof(int));
+    B[b].steps = (int*)carve(cur_p, (size_t)C * sizeof(int));
+    B[b].rets = (int*)carve(cur_p, (size_t)C * sizeof(int));
+    B[b].status = (int8_t*)carve(cur_p, (size_t)C);
+    B[b].cap = C;
+  }
+  int* live = (int*)carve(cur_p, 2 * sizeof(int));
+  unsigned long long* ctr = (unsigned long long*)carve(cur_p, C_NUM * sizeof(unsigned long long));
+  if ((size_t)(cur_p - scratch) > scratch_bytes) return fail(h, BD_ERR_ARG, "scratch layout exceeds the array");
+  DevSim P{};
+  P.n_traj = p->n_traj;
+  P.id_offset = p->id_offset;
+  P.k0 = (uint32_t)(p->seed & 0xffffffffull);
+  P.k1 = (uint32_t)(p->seed >> 32);
+  P.r_b = p->r_start;
+  P.r_esc = p->r_escape;
+  P.return_prob = p->return_prob;
+  P.max_steps = p->max_steps;
+  P.max_dt = p->max_dt;
+  P.min_core_dt = p->min_core_dt;
+  P.use_hi = p->use_hi;
+  P.overlap = p->overlap && h->S.n_chunks > 0;
+  P.D_t = p->D_t;
+  P.D_r = p->D_r;
+  P.adt_V0 = p->q_rec_total * p->q_lig_total / (4.0 * kPi * (78.0 * kEps0));
+  P.adt_has_force = std::fabs(P.adt_V0) > 1e-9;
+  P.adt_debye = p->adt_debye;
+  P.adt_inv_debye = 1.0 / p->adt_debye;
+  P.hi_Df = 1.0 / 0.243;
+  if (p->use_hi) {
+    const double a0 = p->r_hydro_rec, a1 = p->r_hydro_lig;
+    P.hi_a2 = 0.5 * (a0 * a0 + a1 * a1);
+    P.hi_ainv = (P.hi_Df / (6.0 * kPi * a0) + P.hi_Df / (6.0 * kPi * a1)) / P.hi_Df;
+  }
+  P.ctr = ctr;
+  P.out_status = out_status;
+  P.out_steps = out_steps;
+  P.out_returns = out_returns;
+  // the array keeps the previous call's contents: zero the counters and the outputs
+  CK(h, cudaMemsetAsync(ctr, 0, C_NUM * sizeof(unsigned long long), s));
+  CK(h, cudaMemsetAsync(out_status, 0, (size_t)p->n_traj, s));
+  CK(h, cudaMemsetAsync(out_steps, 0, (size_t)p->n_traj * sizeof(int), s));
+  CK(h, cudaMemsetAsync(out_returns, 0, (size_t)p->n_traj * sizeof(int), s));
+  init_slots_kernel<<<(C + 255) / 256, 256, 0, s>>>(P, B[0], C);
+  CK(h, cudaGetLastError());
+  unsigned long long started = (unsigned long long)C;
+  int c_live = C;
+  CK(h, cudaMemcpyAsync(ctr + C_PENDING, &started, sizeof started, cudaMemcpyHostToDevice, s));
+  CK(h, cudaMemcpyAsync(live, &c_live, sizeof c_live, cudaMemcpyHostToDevice, s));
+  CK(h, cudaStreamSynchronize(s));
+  const int G = launch_group(h);
+  void* fn = kernel_for(p->precision, G, p->torque_mode, 2);
+  const int blocks = persistent_blocks(h, fn, h->block);
+  int cur = 0;
+  for (int launch = 0; launch < max_launches; ++launch) {
+    SlotBuf src = B[cur], dst = B[1 - cur];
+    const int* lsrc = live + cur;
+    int* ldst = live + (1 - cur);
+    int KK = K;
+    void* args[] = {&h->S, &P, &src, &lsrc, &KK};
+    CK(h, cudaLaunchKernel(fn, dim3(blocks), dim3(h->block), args, 0, s));
+    compact_kernel<<<h->n_sm * 4, 256, 0, s>>>(src, dst, lsrc, ctr);
+    CK(h, cudaGetLastError());
+    finish_compact_kernel<<<1, 1, 0, s>>>(ldst, ctr);
+    CK(h, cudaGetLastError());
+    cur = 1 - cur;
+    if ((launch & 3) == 3 || launch == max_launches - 1) {
+      unsigned long long c[C_NUM];
+      int n_live = 0;
+      CK(h, cudaMemcpyAsync(c, ctr, sizeof c, cudaMemcpyDeviceToHost, s));
+      CK(h, cudaMemcpyAsync(&n_live, live + cur, sizeof n_live, cudaMemcpyDeviceToHost, s));
+      CK(h, cudaStreamSynchronize(s));
+      if (n_live == 0 && c[C_PENDING] >= (unsigned long long)p->n_traj) break;
+    }
+  }
+  unsigned long long c[C_NUM];
+  CK(h, cudaMemcpyAsync(c, ctr, sizeof c, cudaMemcpyDeviceToHost, s));
+  CK(h, cudaStreamSynchronize(s));
+  c[C_PENDING] = std::min<unsigned long long>(c[C_PENDING], (unsigned long long)p->n_traj);  // trajectories started
+  CK(h, cudaMemcpyAsync(counters, c, BD_CTR_NUM * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+  CK(h, cudaStreamSynchronize(s));
+  return BD_OK;
+}
