@@ -350,11 +350,13 @@ def main():
     gathers = d_mixed["grid_evals"] + d_mixed["rev_evals"]
     algo_bytes = gathers * ALGO_BYTES_PER_GATHER + d_mixed["steps"] * STATE_BYTES_PER_STEP
     achieved = algo_bytes / t_mixed / 1e9
-    traffic = None
-    tf = ROOT / "profiles" / "step_kernel_traffic.json"
-    if tf.exists():
-        tj = json.loads(tf.read_text())
-        traffic = tj.get("dram_bytes_per_launch")
+    traffic = None  # DRAM bytes per launch of the stepper, from the committed ncu capture summary
+    tf = ROOT / "profiles" / "step_kernel_warp_protein_ligand.md"
+    if args.workload == "protein-ligand" and tf.exists():
+        import re
+
+        m = re.search(r"dram_bytes_per_launch \| (\d+)", tf.read_text())
+        traffic = int(m.group(1)) if m else None
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()

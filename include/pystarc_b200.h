@@ -66,7 +66,23 @@ typedef struct {
   int32_t precision, torque_mode;
   int32_t slots;             /* live-slot capacity; 0 = automatic */
   int64_t id_offset;         /* global id of local trajectory 0 (keys the noise; shards across GPUs) */
+  int32_t stats;             /* 1: collect the per-step statistics read by bd_sim_stats */
 } BdSimParams;
+
+/* Host arrays filled by bd_sim_stats (NULL members are skipped).  Per trajectory
+ * (n_traj entries, x3 / x4 for poses): start pose, closest approach |c| with its
+ * step and pose, accumulated time, reaction pose and step, bridge flag.  Histograms
+ * as the reference's (gpu_batch_simulator.py:577-620, :1255-1317): radial 200 bins on
+ * [0, 1.2 r_escape], angular 36 x 72 (theta, phi), milestone crossings of 11 shells
+ * from r_start to r_escape (out and in), radial transition matrix 50 x 50, pair
+ * contact counts at the force-evaluation pose; plus the bin edges used. */
+typedef struct {
+  double *start_pos, *start_q, *min_dist, *near_miss_pos, *near_miss_q, *total_time, *encounter_pos, *encounter_q;
+  int32_t *step_at_min, *encounter_step;
+  int8_t* bridge;
+  uint64_t *radial, *angular, *milestone_out, *milestone_in, *transition, *contact;
+  double *radial_edges, *transition_edges, *milestone_radii;
+} BdStatsOut;
 
 /* Counter indices of bd_sim_counters(). */
 enum {
@@ -127,6 +143,9 @@ int bd_sim_counters(BdHandle* h, uint64_t* out, int n, void* stream);
 /* Host copies of the per-trajectory outcome (0 running/unstarted, 1 reacted, 2 escaped,
  * 3 max-steps, 5 non-finite pose), step counts and return counts (n_traj each). */
 int bd_sim_outcomes(BdHandle* h, int8_t* status, int32_t* steps, int32_t* returns);
+/* Per-step statistics (BdSimParams.stats = 1) to host arrays.  Replaces the host-side
+ * statistics loops of GPUBatchSimulator.run (gpu_batch_simulator.py:1255-1317). */
+int bd_sim_stats(BdHandle* h, const BdStatsOut* out);
 /* Live-slot count after the last compaction (synchronises the handle's work). */
 int bd_sim_live(BdHandle* h, int32_t* n_live);
 /* Checkpoint: host copies of the live slots (cap entries each; c: 3*cap, q: 4*cap, SoA)

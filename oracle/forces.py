@@ -235,16 +235,26 @@ def eval_batch_atoms(positions, charges, grids, alpha, is_born, ff: FarField | N
     far-field (:358-366).  With no grids at all, elec uses the far-field for
     every atom (:304-309).
     """
+    return eval_batch(positions, charges, grids, alpha, is_born, ff)[:2]
+
+
+def eval_batch(positions, charges, grids, alpha, is_born, ff: FarField | None):
+    """``eval_batch_atoms`` plus the per-trajectory totals summed in the reference's order
+    (each grid's atoms, then the far-field atoms; gpu_batch_engine.py:302-366)."""
     N, A, _ = positions.shape
     atom_f = np.zeros((N, A, 3))
     atom_e = np.zeros((N, A))
+    tot_f = np.zeros((N, 3))
+    tot_e = np.zeros((N,))
     use_ff = (not is_born) and ff is not None and ff.has_yukawa
     if not grids:
         if use_ff:
             f, e = yukawa_forces(positions, np.broadcast_to(charges, (N, A)), ff)
             atom_f += f
             atom_e += e
-        return atom_f, atom_e
+            tot_f += f.sum(axis=1)
+            tot_e += e.sum(axis=1)
+        return atom_f, atom_e, tot_f, tot_e
     assigned = np.zeros((N, A), dtype=bool)
     q_full = np.broadcast_to(np.asarray(charges, dtype=np.float64), (N, A))
     for g in grids:
@@ -257,13 +267,17 @@ def eval_batch_atoms(positions, charges, grids, alpha, is_born, ff: FarField | N
         f, e = k1_batch_force(pos_masked, chg_masked, g.data, g.origin, g.sp, alpha, is_born)
         atom_f += f
         atom_e += e
+        tot_f += f.sum(axis=1)
+        tot_e += e.sum(axis=1)
     if use_ff:
         not_assigned = ~assigned
         if np.any(not_assigned):
             f, e = yukawa_forces(positions, q_full, ff, mask=not_assigned)
             atom_f += f
             atom_e += e
-    return atom_f, atom_e
+            tot_f += f.sum(axis=1)
+            tot_e += e.sum(axis=1)
+    return atom_f, atom_e, tot_f, tot_e
 
 
 def born_reverse_atoms(R, centroids, rec_pos, rec_q, lig_born_grid, alpha, chunk_skip=True):
@@ -277,6 +291,12 @@ def born_reverse_atoms(R, centroids, rec_pos, rec_q, lig_born_grid, alpha, chunk
     min|c| - max|x_rec| exceeds the grid's x half-width, the batch gets zero.
     The reference applies it per memory chunk; here the batch is one chunk.
     """
+    return born_reverse(R, centroids, rec_pos, rec_q, lig_born_grid, alpha, chunk_skip)[0]
+
+
+def born_reverse(R, centroids, rec_pos, rec_q, lig_born_grid, alpha, chunk_skip=True):
+    """(per-receptor-atom lab forces, force on the ligand summed as the reference sums it:
+    minus R times the ligand-frame total, gpu_batch_engine.py:646-656)."""
     N = R.shape[0]
     out = np.zeros((N, rec_pos.shape[0], 3))
     g = lig_born_grid
@@ -285,13 +305,13 @@ def born_reverse_atoms(R, centroids, rec_pos, rec_q, lig_born_grid, alpha, chunk
         r_cen = np.linalg.norm(centroids, axis=1)
         rec_max_r = float(np.linalg.norm(rec_pos, axis=1).max())
         if float(r_cen.min()) - rec_max_r > lig_grid_radius:
-            return out
+            return out, np.zeros((N, 3))
     rec_pos_rel = rec_pos[None, :, :] - centroids[:, None, :]
     R_T = np.swapaxes(R, 1, 2)
     rec_in_lig = np.einsum("nij,nkj->nki", R_T, rec_pos_rel)
-    f_lig, _ = eval_batch_atoms(rec_in_lig, rec_q, [g], alpha, True, None)
+    f_lig, _, f_lig_tot, _ = eval_batch(rec_in_lig, rec_q, [g], alpha, True, None)
     out[...] = np.einsum("nij,nkj->nki", R, f_lig)
-    return out
+    return out, -np.einsum("nij,nj->ni", R, f_lig_tot)
 
 
 # --------------------------------------------------------------------------
@@ -328,39 +348,47 @@ class OracleForceEngine:
         self.born_chunk_skip = born_chunk_skip
 
     def atoms(self, lig_positions, lig_charges, R_matrices=None, centroids=None):
-        """Per-atom terms: (direct ligand forces (N,A,3), energies (N,A), receptor reverse-Born forces (N,Nr,3) or None)."""
+        """Per-atom terms and totals: (direct ligand forces (N,A,3), energies (N,A), receptor
+        reverse-Born forces (N,Nr,3) or None, net force (N,3), energy (N,)).  The totals are
+        summed in the reference's order: elec, Born direction 1, Born direction 2 (:556-596)."""
         N, A, _ = lig_positions.shape
         f = np.zeros((N, A, 3))
         e = np.zeros((N, A))
+        forces = np.zeros((N, 3))
+        energies = np.zeros((N,))
         ff = self.ff
         if self.elec:
-            f1, e1 = eval_batch_atoms(lig_positions, lig_charges, self.elec, 0.0, False, ff)
+            f1, e1, tf, te = eval_batch(lig_positions, lig_charges, self.elec, 0.0, False, ff)
             f += f1
             e += e1
+            forces += tf
+            energies += te
         elif ff is not None and ff.has_yukawa:
             f1, e1 = yukawa_forces(lig_positions, np.broadcast_to(lig_charges, (N, A)), ff)
             f += f1
             e += e1
+            forces += f1.sum(axis=1)
+            energies += e1.sum(axis=1)
         if self.born:
-            f2, e2 = eval_batch_atoms(lig_positions, lig_charges, self.born, self.alpha, True, None)
+            f2, e2, tf, te = eval_batch(lig_positions, lig_charges, self.born, self.alpha, True, None)
             f += f2
             e += e2
+            forces += tf
+            energies += te
         f_rec = None
         if (self.lig_born and self.rec_pos is not None and R_matrices is not None
                 and centroids is not None and self.alpha > 1e-12):
-            f_rec = born_reverse_atoms(np.asarray(R_matrices), np.asarray(centroids), self.rec_pos,
-                                       self.rec_q, self.lig_born[0], self.alpha, self.born_chunk_skip)
-        return f, e, f_rec
+            f_rec, f2_tot = born_reverse(np.asarray(R_matrices), np.asarray(centroids), self.rec_pos, self.rec_q,
+                                         self.lig_born[0], self.alpha, self.born_chunk_skip)
+            forces += f2_tot
+        return f, e, f_rec, forces, energies
 
     def __call__(self, lig_positions, lig_charges, R_matrices=None, centroids=None, torque_mode="zero",
                  return_scale=False):
         lig_positions = np.asarray(lig_positions, dtype=np.float64)
-        f_atoms, e_atoms, f_rec = self.atoms(lig_positions, lig_charges, R_matrices, centroids)
-        forces = f_atoms.sum(axis=1)
-        energies = e_atoms.sum(axis=1)
+        f_atoms, e_atoms, f_rec, forces, energies = self.atoms(lig_positions, lig_charges, R_matrices, centroids)
         scale = np.linalg.norm(f_atoms, axis=2).sum(axis=1)
         if f_rec is not None:
-            forces = forces - f_rec.sum(axis=1)
             scale = scale + np.linalg.norm(f_rec, axis=2).sum(axis=1)
         torques = np.zeros_like(forces)
         if torque_mode == "centroid":

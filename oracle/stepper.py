@@ -85,6 +85,7 @@ class StepResult:
     k_b: float
     n_returns: np.ndarray = field(default=None)
     n_overlap_rejected: int = 0
+    stats: "StepStats" = None
 
 
 def n_needed_of(n_needed_raw, n_pairs):
@@ -202,6 +203,75 @@ def hi_diffusion(r_sr, sys: StepSystem, prm: StepParams):
     return np.full(r_sr.shape[0], sys.D_t, dtype=np.float64)
 
 
+class StepStats:
+    """Per-step statistics of the reference stepper (gpu_batch_simulator.py:577-620, :1255-1317).
+
+    Steps are indexed by each trajectory's own step count, which equals the
+    reference's loop counter when nothing refills.  Encounter records are kept
+    per trajectory (the reference appends them in event order).
+    """
+
+    def __init__(self, pos, q, N, r_b, r_esc, n_pairs):
+        self.start_pos = pos.copy()
+        self.start_q = q.copy()
+        self.min_dist = np.full(N, 1e30)
+        self.step_at_min = np.zeros(N, dtype=np.int64)
+        self.total_time = np.zeros(N)
+        self.nm_pos = pos.copy()
+        self.nm_q = q.copy()
+        self.bridge = np.zeros(N, dtype=np.int64)
+        self.enc_pos = np.zeros((N, 3))
+        self.enc_q = np.zeros((N, 4))
+        self.enc_step = np.zeros(N, dtype=np.int64)
+        self.prev_r = np.linalg.norm(pos, axis=1)
+        self.rad_bins = np.linspace(0, float(r_esc * 1.2), 201)
+        self.rad_counts = np.zeros(200, dtype=np.int64)
+        self.ang_counts = np.zeros((36, 72), dtype=np.int64)
+        self.ms_radii = np.linspace(float(r_b), float(r_esc), 11)
+        self.ms_out = np.zeros(11, dtype=np.int64)
+        self.ms_in = np.zeros(11, dtype=np.int64)
+        self.contact = np.zeros(max(n_pairs, 1), dtype=np.int64)
+        self.contact_total = 0
+        self.trans_bins = np.linspace(0, float(r_esc * 1.2), 51)
+        self.trans = np.zeros((50, 50), dtype=np.int64)
+
+    def encounter(self, idx, pos, q, steps, bridge):
+        self.enc_pos[idx] = pos[idx]
+        self.enc_q[idx] = q[idx]
+        self.enc_step[idx] = steps[idx]
+        if bridge:
+            self.bridge[idx] = 1
+
+    def step(self, sr_idx, pos, q, steps, dt_arr, pair_d_at_force, cutoffs):
+        cur = np.linalg.norm(pos[sr_idx], axis=1)
+        better = cur < self.min_dist[sr_idx]
+        ti = sr_idx[better]
+        self.min_dist[ti] = cur[better]
+        self.step_at_min[ti] = steps[ti]
+        self.nm_pos[ti] = pos[ti]
+        self.nm_q[ti] = q[ti]
+        self.total_time[sr_idx] += dt_arr
+        np.add.at(self.rad_counts, np.clip(np.searchsorted(self.rad_bins, cur) - 1, 0, 199), 1)
+        cen = pos[sr_idx]
+        r_safe = np.maximum(cur, 1e-30)
+        theta = np.arccos(np.clip(cen[:, 2] / r_safe, -1, 1))
+        phi = np.arctan2(cen[:, 1], cen[:, 0]) + np.pi
+        t_i = np.clip((theta / np.pi * 36).astype(int), 0, 35)
+        p_i = np.clip((phi / (2 * np.pi) * 72).astype(int), 0, 71)
+        np.add.at(self.ang_counts, (t_i, p_i), 1)
+        prev = self.prev_r[sr_idx]
+        for mi, mr in enumerate(self.ms_radii):
+            self.ms_out[mi] += int(((prev < mr) & (cur >= mr)).sum())
+            self.ms_in[mi] += int(((prev >= mr) & (cur < mr)).sum())
+        ob = np.clip(np.searchsorted(self.trans_bins, prev) - 1, 0, 49)
+        nb = np.clip(np.searchsorted(self.trans_bins, cur) - 1, 0, 49)
+        np.add.at(self.trans, (ob, nb), 1)
+        if pair_d_at_force is not None and len(cutoffs) and len(sr_idx):
+            self.contact[: len(cutoffs)] += (pair_d_at_force < cutoffs[None, :]).sum(axis=0)
+            self.contact_total += len(sr_idx)
+        self.prev_r[sr_idx] = cur
+
+
 def _overlap_inside(new_pos, rec_pos, threshold=1.5):
     N = new_pos.shape[0]
     chunk = max(1, int(500 * 1024 * 1024 / (rec_pos.shape[0] * 3 * 8)))
@@ -276,6 +346,7 @@ def run(sys: StepSystem, prm: StepParams, noise: str = "pcg64", termination: str
     D_eff = bridge_D_eff(sys)
     loop_steps = 0
     max_loop = prm.max_steps if termination == "reference" else 1 << 62
+    stats = StepStats(pos, q, N, r_b, r_esc, P)
     step = 0
     while step < max_loop:
         running = status == 0
@@ -298,6 +369,7 @@ def run(sys: StepSystem, prm: StepParams, noise: str = "pcg64", termination: str
         still_running_mask = status[run_idx] == 0
         newly = run_idx[reacted & still_running_mask]
         status[newly] = 1
+        stats.encounter(newly, pos, q, n_steps, bridge=False)
         r_mag = np.linalg.norm(pos_run, axis=1)
         at_escape = (r_mag >= r_esc) & still_running_mask & ~reacted
         if np.any(at_escape):
@@ -394,6 +466,8 @@ def run(sys: StepSystem, prm: StepParams, noise: str = "pcg64", termination: str
                     g = sr_idx[bb]
                     g = g[status[g] == 0]
                     status[g] = 1
+                    stats.encounter(g, pos, q, n_steps, bridge=True)
+        stats.step(sr_idx, pos, q, n_steps, dt_arr, old_d, cutoffs)
         n_steps[sr_idx] += 1
         total_steps += int(sr_mask.sum())
         done = int((status != 0).sum())
@@ -412,4 +486,4 @@ def run(sys: StepSystem, prm: StepParams, noise: str = "pcg64", termination: str
     return StepResult(status=status, n_steps=n_steps, n_reacted=int((status == 1).sum()),
                       n_escaped=int((status == 2).sum()), n_max_steps=n_max, total_steps=total_steps,
                       loop_steps=loop_steps, return_prob=rp, k_b=kb, n_returns=n_returns,
-                      n_overlap_rejected=n_overlap)
+                      n_overlap_rejected=n_overlap, stats=stats)

@@ -37,7 +37,23 @@ class BdSimParams(C.Structure):
                 ("D_r", C.c_double), ("q_rec_total", C.c_double), ("q_lig_total", C.c_double),
                 ("adt_debye", C.c_double), ("r_hydro_rec", C.c_double), ("r_hydro_lig", C.c_double),
                 ("precision", C.c_int32), ("torque_mode", C.c_int32), ("slots", C.c_int32),
-                ("id_offset", C.c_int64)]
+                ("id_offset", C.c_int64), ("stats", C.c_int32)]
+
+
+_D = C.POINTER(C.c_double)
+_I = C.POINTER(C.c_int32)
+_U = C.POINTER(C.c_uint64)
+
+
+class BdStatsOut(C.Structure):
+    _fields_ = [("start_pos", _D), ("start_q", _D), ("min_dist", _D), ("near_miss_pos", _D), ("near_miss_q", _D),
+                ("total_time", _D), ("encounter_pos", _D), ("encounter_q", _D), ("step_at_min", _I),
+                ("encounter_step", _I), ("bridge", C.POINTER(C.c_int8)), ("radial", _U), ("angular", _U),
+                ("milestone_out", _U), ("milestone_in", _U), ("transition", _U), ("contact", _U),
+                ("radial_edges", _D), ("transition_edges", _D), ("milestone_radii", _D)]
+
+
+ST_RAD_BINS, ST_THETA, ST_PHI, ST_MILESTONES, ST_TRANS = 200, 36, 72, 11, 50
 
 
 P = C.c_void_p
@@ -66,6 +82,7 @@ SIGNATURES = {
     "bd_sim_run": (C.c_int, [P, C.c_int, C.c_int, P]),
     "bd_sim_counters": (C.c_int, [P, u64p, C.c_int, P]),
     "bd_sim_outcomes": (C.c_int, [P, i8p, i32p, i32p]),
+    "bd_sim_stats": (C.c_int, [P, C.POINTER(BdStatsOut)]),
     "bd_sim_live": (C.c_int, [P, i32p]),
     "bd_sim_capacity": (C.c_int, [P, i32p]),
     "bd_sim_snapshot": (C.c_int, [P, dp, dp, i32p, i32p, i32p, i8p, i32p, u64p]),

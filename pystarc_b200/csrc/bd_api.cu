@@ -375,11 +375,14 @@ int eval_grid_blocks(BdHandle* h, long long n, int G, int block) {
   return (int)std::max<long long>(blocks, 1);
 }
 
-int persistent_blocks(BdHandle* h, void* fn, int block) {
+int persistent_blocks(BdHandle* h, void* fn, int block, size_t smem = 0) {
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, 0) != cudaSuccess || per_sm < 1) per_sm = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem) != cudaSuccess || per_sm < 1) per_sm = 1;
   return per_sm * h->n_sm;
 }
+
+// Dynamic shared memory of a stepper launch: the block's statistics histograms.
+size_t stats_smem(const BdHandle* h) { return h->P.stats ? (size_t)SH_NUM * sizeof(unsigned) : 0; }
 
 }  // namespace
 
@@ -658,6 +661,46 @@ int bd_sim_configure(BdHandle* h, const BdSimParams* p) {
   P.out_steps = (int*)q;
   if ((rc = dev_alloc(h, h->sim_allocs, &q, (size_t)p->n_traj * sizeof(int)))) return rc;
   P.out_returns = (int*)q;
+  if (p->stats) {
+    const size_t n = (size_t)p->n_traj;
+    DevStats& st = P.st;
+    auto dbl = [&](double** out, size_t k) {
+      void* v;
+      int r = dev_alloc(h, h->sim_allocs, &v, k * sizeof(double));
+      *out = (double*)v;
+      return r;
+    };
+    if ((rc = dbl(&st.start_c, 3 * n)) || (rc = dbl(&st.start_q, 4 * n)) || (rc = dbl(&st.min_dist, n)) ||
+        (rc = dbl(&st.nm_c, 3 * n)) || (rc = dbl(&st.nm_q, 4 * n)) || (rc = dbl(&st.total_time, n)) ||
+        (rc = dbl(&st.enc_c, 3 * n)) || (rc = dbl(&st.enc_q, 4 * n)))
+      return rc;
+    if ((rc = dev_alloc(h, h->sim_allocs, &q, n * sizeof(int)))) return rc;
+    st.step_at_min = (int*)q;
+    if ((rc = dev_alloc(h, h->sim_allocs, &q, n * sizeof(int)))) return rc;
+    st.enc_step = (int*)q;
+    if ((rc = dev_alloc(h, h->sim_allocs, &q, n))) return rc;
+    st.bridge = (int8_t*)q;
+    if ((rc = dev_alloc(h, h->sim_allocs, &q, SH_NUM * sizeof(unsigned long long)))) return rc;
+    st.hist = (unsigned long long*)q;
+    // bin edges as numpy.linspace builds them: start + i * (stop - start) / (num - 1), last = stop
+    std::vector<double> edges(ST_RAD_BINS + 1 + ST_TRANS + 1 + ST_MILESTONES);
+    const double top = p->r_escape * 1.2;
+    for (int i = 0; i <= ST_RAD_BINS; ++i) edges[i] = i * (top / ST_RAD_BINS);
+    edges[ST_RAD_BINS] = top;
+    double* te = edges.data() + ST_RAD_BINS + 1;
+    for (int i = 0; i <= ST_TRANS; ++i) te[i] = i * (top / ST_TRANS);
+    te[ST_TRANS] = top;
+    double* mr = te + ST_TRANS + 1;
+    const double dm = (p->r_escape - p->r_start) / (ST_MILESTONES - 1);
+    for (int i = 0; i < ST_MILESTONES; ++i) mr[i] = i * dm + p->r_start;
+    mr[ST_MILESTONES - 1] = p->r_escape;
+    if ((rc = dev_alloc(h, h->sim_allocs, &q, edges.size() * sizeof(double)))) return rc;
+    CK(h, cudaMemcpy(q, edges.data(), edges.size() * sizeof(double), cudaMemcpyHostToDevice));
+    st.rad_edges = (const double*)q;
+    st.trans_edges = st.rad_edges + ST_RAD_BINS + 1;
+    st.ms_radii = st.trans_edges + ST_TRANS + 1;
+    P.stats = 1;
+  }
   h->sim_ready = true;
   h->graph_K = -1;
   return BD_OK;
@@ -674,6 +717,22 @@ int bd_sim_reset(BdHandle* h, void* stream) {
   CK(h, cudaMemsetAsync(h->P.out_status, 0, (size_t)h->P.n_traj, s));
   CK(h, cudaMemsetAsync(h->P.out_steps, 0, (size_t)h->P.n_traj * sizeof(int), s));
   CK(h, cudaMemsetAsync(h->P.out_returns, 0, (size_t)h->P.n_traj * sizeof(int), s));
+  if (h->P.stats) {
+    const DevStats& st = h->P.st;
+    const size_t n = (size_t)h->P.n_traj;
+    CK(h, cudaMemsetAsync(st.hist, 0, SH_NUM * sizeof(unsigned long long), s));
+    CK(h, cudaMemsetAsync(st.total_time, 0, n * sizeof(double), s));
+    CK(h, cudaMemsetAsync(st.step_at_min, 0, n * sizeof(int), s));
+    CK(h, cudaMemsetAsync(st.enc_step, 0, n * sizeof(int), s));
+    CK(h, cudaMemsetAsync(st.bridge, 0, n, s));
+    CK(h, cudaMemsetAsync(st.nm_c, 0, 3 * n * sizeof(double), s));
+    CK(h, cudaMemsetAsync(st.nm_q, 0, 4 * n * sizeof(double), s));
+    CK(h, cudaMemsetAsync(st.enc_c, 0, 3 * n * sizeof(double), s));
+    CK(h, cudaMemsetAsync(st.enc_q, 0, 4 * n * sizeof(double), s));
+    const std::vector<double> far(n, 1e30);  // the reference starts min_dist at 1e30
+    CK(h, cudaMemcpyAsync(st.min_dist, far.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(h, cudaStreamSynchronize(s));
+  }
   init_slots_kernel<<<(C + 255) / 256, 256, 0, s>>>(h->P, h->buf[0], C);
   CK(h, cudaGetLastError());
   const unsigned long long started = (unsigned long long)C;
@@ -689,12 +748,13 @@ namespace {
 int enqueue_launch(BdHandle* h, int K, cudaStream_t s, int cur) {
   const int G = launch_group(h);
   void* fn = kernel_for(h->sp.precision, G, h->sp.torque_mode, 2);
-  const int blocks = persistent_blocks(h, fn, h->block);
+  const size_t smem = stats_smem(h);
+  const int blocks = persistent_blocks(h, fn, h->block, smem);
   SlotBuf src = h->buf[cur], dst = h->buf[1 - cur];
   const int* live = h->d_live + cur;
   int* live_dst = h->d_live + (1 - cur);
   void* args[] = {&h->S, &h->P, &src, &live, &K};
-  CK(h, cudaLaunchKernel(fn, dim3(blocks), dim3(h->block), args, 0, s));
+  CK(h, cudaLaunchKernel(fn, dim3(blocks), dim3(h->block), args, smem, s));
   compact_kernel<<<h->n_sm * 4, 256, 0, s>>>(src, dst, live, h->d_ctr);
   CK(h, cudaGetLastError());
   finish_compact_kernel<<<1, 1, 0, s>>>(live_dst, h->d_ctr);
@@ -769,6 +829,44 @@ int bd_sim_outcomes(BdHandle* h, int8_t* status, int32_t* steps, int32_t* rets) 
   if (status) CK(h, cudaMemcpy(status, h->P.out_status, n, cudaMemcpyDeviceToHost));
   if (steps) CK(h, cudaMemcpy(steps, h->P.out_steps, n * sizeof(int), cudaMemcpyDeviceToHost));
   if (rets) CK(h, cudaMemcpy(rets, h->P.out_returns, n * sizeof(int), cudaMemcpyDeviceToHost));
+  return BD_OK;
+}
+
+int bd_sim_stats(BdHandle* h, const BdStatsOut* o) {
+  if (!h || !o) return fail(h, BD_ERR_ARG, "bd_sim_stats: NULL");
+  if (!h->sim_ready) return fail(h, BD_ERR_STATE, "no simulation configured");
+  if (!h->P.stats) return fail(h, BD_ERR_STATE, "statistics were not requested (BdSimParams.stats = 0)");
+  CK(h, cudaDeviceSynchronize());
+  const DevStats& st = h->P.st;
+  const size_t n = (size_t)h->P.n_traj;
+  auto get = [&](void* dst, const void* src, size_t bytes) -> int {
+    if (dst) CK(h, cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));
+    return BD_OK;
+  };
+  int rc = 0;
+  if ((rc = get(o->start_pos, st.start_c, 3 * n * 8)) || (rc = get(o->start_q, st.start_q, 4 * n * 8)) ||
+      (rc = get(o->min_dist, st.min_dist, n * 8)) || (rc = get(o->near_miss_pos, st.nm_c, 3 * n * 8)) ||
+      (rc = get(o->near_miss_q, st.nm_q, 4 * n * 8)) || (rc = get(o->total_time, st.total_time, n * 8)) ||
+      (rc = get(o->encounter_pos, st.enc_c, 3 * n * 8)) || (rc = get(o->encounter_q, st.enc_q, 4 * n * 8)) ||
+      (rc = get(o->step_at_min, st.step_at_min, n * 4)) || (rc = get(o->encounter_step, st.enc_step, n * 4)) ||
+      (rc = get(o->bridge, st.bridge, n)))
+    return rc;
+  std::vector<unsigned long long> hist(SH_NUM);
+  CK(h, cudaMemcpy(hist.data(), st.hist, SH_NUM * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  auto put = [&](uint64_t* dst, int off, int cnt) {
+    if (dst)
+      for (int i = 0; i < cnt; ++i) dst[i] = hist[off + i];
+  };
+  put(o->radial, SH_RAD, ST_RAD_BINS);
+  put(o->angular, SH_ANG, ST_THETA * ST_PHI);
+  put(o->milestone_out, SH_MS_OUT, ST_MILESTONES);
+  put(o->milestone_in, SH_MS_IN, ST_MILESTONES);
+  put(o->transition, SH_TRANS, ST_TRANS * ST_TRANS);
+  put(o->contact, SH_CONTACT, h->S.n_pairs);
+  if ((rc = get(o->radial_edges, st.rad_edges, (ST_RAD_BINS + 1) * 8)) ||
+      (rc = get(o->transition_edges, st.trans_edges, (ST_TRANS + 1) * 8)) ||
+      (rc = get(o->milestone_radii, st.ms_radii, ST_MILESTONES * 8)))
+    return rc;
   return BD_OK;
 }
 

@@ -78,6 +78,39 @@ struct DevSystem {
   double rx_deff[BD_MAX_PAIRS];
 };
 
+// Per-step statistics of the reference's stepper (gpu_batch_simulator.py:577-620,
+// :1255-1317), kept on the device.  Histogram sizes are the reference's.
+enum : int { ST_RAD_BINS = 200, ST_THETA = 36, ST_PHI = 72, ST_MILESTONES = 11, ST_TRANS = 50 };
+enum : int {
+  SH_RAD = 0,
+  SH_ANG = SH_RAD + ST_RAD_BINS,
+  SH_MS_OUT = SH_ANG + ST_THETA * ST_PHI,
+  SH_MS_IN = SH_MS_OUT + ST_MILESTONES,
+  SH_TRANS = SH_MS_IN + ST_MILESTONES,
+  SH_CONTACT = SH_TRANS + ST_TRANS * ST_TRANS,
+  SH_NUM = SH_CONTACT + BD_MAX_PAIRS
+};
+
+struct DevStats {
+  // per trajectory (local id)
+  double* start_c;   // 3n
+  double* start_q;   // 4n
+  double* min_dist;  // n (initialised to 1e30)
+  int* step_at_min;  // n
+  double* nm_c;      // 3n, pose at the closest approach
+  double* nm_q;      // 4n
+  double* total_time;  // n
+  int8_t* bridge;    // n, reaction found by the Brownian bridge
+  double* enc_c;     // 3n, pose at reaction
+  double* enc_q;     // 4n
+  int* enc_step;     // n
+  // histograms (SH_* layout) and the bin edges they use
+  unsigned long long* hist;
+  const double* rad_edges;    // ST_RAD_BINS + 1
+  const double* trans_edges;  // ST_TRANS + 1
+  const double* ms_radii;     // ST_MILESTONES
+};
+
 struct DevSim {
   long long n_traj;
   long long id_offset;  // global id of local trajectory 0
@@ -94,6 +127,8 @@ struct DevSim {
   int8_t* out_status;
   int* out_steps;
   int* out_returns;
+  DevStats st;
+  int stats;  // collect DevStats (needs SH_NUM * 4 B of dynamic shared memory per block)
 };
 
 struct SlotBuf {

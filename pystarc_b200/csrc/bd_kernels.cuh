@@ -342,6 +342,12 @@ __device__ __forceinline__ void start_trajectory(const DevSim& P, int id, Traj& 
   tr.steps = 0;
   tr.rets = 0;
   tr.status = ST_RUNNING;
+  if (P.stats) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) P.st.start_c[3 * id + k] = tr.c[k];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) P.st.start_q[4 * id + k] = tr.q[k];
+  }
 }
 
 // Adaptive dt (pystarc/simulation/gpu_batch_simulator.py:961-1067, flattened-pairs mode).
@@ -514,18 +520,99 @@ __device__ __forceinline__ int step_end(const DevSystem& S, const DevSim& P, con
   return st;
 }
 
+// numpy.searchsorted(edges, x) - 1 (side "left"), clipped to [0, n-1]; edges has n+1 entries.
+__device__ __forceinline__ int hist_bin(const double* e, int n, double x) {
+  int lo = 0, hi = n + 1;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (e[mid] < x) lo = mid + 1;
+    else hi = mid;
+  }
+  const int b = lo - 1;
+  return b < 0 ? 0 : (b > n - 1 ? n - 1 : b);
+}
+
+// Statistics of one completed step (gpu_batch_simulator.py:1255-1317): closest
+// approach, accumulated time, radial / angular / transition histograms,
+// milestone crossings between r_prev (end of the previous step) and now, and
+// pair contacts at the force-evaluation pose (c0, R).  `sh` is the block's
+// shared-memory histogram (SH_* layout).
+__device__ __forceinline__ void stats_step(const DevSystem& S, const DevSim& P, const Traj& tr, uint32_t s,
+                                           double r_prev, double dt, const double c0[3], const double R[9],
+                                           unsigned* sh) {
+  const DevStats& st = P.st;
+  const int id = tr.id;
+  const double cur = norm3(tr.c[0], tr.c[1], tr.c[2]);
+  if (cur < st.min_dist[id]) {
+    st.min_dist[id] = cur;
+    st.step_at_min[id] = (int)s;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) st.nm_c[3 * id + k] = tr.c[k];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) st.nm_q[4 * id + k] = tr.q[k];
+  }
+  st.total_time[id] += dt;
+  atomicAdd(sh + SH_RAD + hist_bin(st.rad_edges, ST_RAD_BINS, cur), 1u);
+  const double PI = 3.14159265358979323846;
+  const double rs = fmax(cur, 1e-30);
+  const double th = acos(fmin(fmax(tr.c[2] / rs, -1.0), 1.0));
+  const double ph = atan2(tr.c[1], tr.c[0]) + PI;
+  int ti = (int)(th / PI * ST_THETA), pi = (int)(ph / (2 * PI) * ST_PHI);
+  ti = ti < 0 ? 0 : (ti > ST_THETA - 1 ? ST_THETA - 1 : ti);
+  pi = pi < 0 ? 0 : (pi > ST_PHI - 1 ? ST_PHI - 1 : pi);
+  atomicAdd(sh + SH_ANG + ti * ST_PHI + pi, 1u);
+  for (int m = 0; m < ST_MILESTONES; ++m) {
+    const double mr = st.ms_radii[m];
+    if (r_prev < mr && cur >= mr) atomicAdd(sh + SH_MS_OUT + m, 1u);
+    if (r_prev >= mr && cur < mr) atomicAdd(sh + SH_MS_IN + m, 1u);
+  }
+  atomicAdd(sh + SH_TRANS + hist_bin(st.trans_edges, ST_TRANS, r_prev) * ST_TRANS +
+                hist_bin(st.trans_edges, ST_TRANS, cur),
+            1u);
+  for (int p = 0; p < S.n_pairs; ++p)
+    if (pair_distance(S, c0, R, p) < S.rx_cut[p]) atomicAdd(sh + SH_CONTACT + p, 1u);
+}
+
+// Pose at reaction; `bridge` marks a reaction found by the Brownian bridge.
+__device__ __forceinline__ void stats_encounter(const DevSim& P, const Traj& tr, uint32_t s, bool bridge) {
+  const DevStats& st = P.st;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) st.enc_c[3 * tr.id + k] = tr.c[k];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) st.enc_q[4 * tr.id + k] = tr.q[k];
+  st.enc_step[tr.id] = (int)s;
+  st.bridge[tr.id] = bridge ? 1 : 0;
+}
+
+__device__ __forceinline__ void stats_block_begin(const DevSim& P, unsigned* sh) {
+  if (!P.stats) return;
+  for (int i = threadIdx.x; i < SH_NUM; i += blockDim.x) sh[i] = 0u;
+  __syncthreads();
+}
+
+__device__ __forceinline__ void stats_block_end(const DevSim& P, const unsigned* sh) {
+  if (!P.stats) return;
+  __syncthreads();
+  for (int i = threadIdx.x; i < SH_NUM; i += blockDim.x)
+    if (sh[i]) atomicAdd(P.st.hist + i, (unsigned long long)sh[i]);
+}
+
 // One BD step of one trajectory by the G lanes of its group, in the
 // reference's order (gpu_batch_simulator.py:783-1254): discrete reaction test,
 // escape/return, forces, adaptive dt, D(r), translation, rotation, overlap
 // rejection, Brownian bridge, step count.  Returns the new status.
 template <typename FT, int G, bool TORQUE>
 __device__ __forceinline__ int bd_step(const DevSystem& S, const DevSim& P, Traj& tr, int lane, unsigned gm,
-                                       Tally& tl) {
+                                       Tally& tl, unsigned* sh) {
   const Keyed key = traj_key(P, tr.id);
   const uint32_t s = (uint32_t)tr.steps;
+  const double r_prev = P.stats ? norm3(tr.c[0], tr.c[1], tr.c[2]) : 0.0;
   double R[9], r;
   const int st0 = step_begin(S, P, key, s, tr, R, r, tl);
-  if (st0 != ST_RUNNING) return st0;
+  if (st0 != ST_RUNNING) {
+    if (P.stats && st0 == ST_REACTED && lane == 0) stats_encounter(P, tr, s, false);
+    return st0;
+  }
   double F[3], T[3], E;
   group_forces<FT, G, TORQUE, false>(S, tr.c, R, lane, gm, PosFromPose{R, tr.c}, F, T, E, tl.cnt);
   double cn[3], qn[4], dt;
@@ -534,7 +621,13 @@ __device__ __forceinline__ int bd_step(const DevSystem& S, const DevSim& P, Traj
     return ST_ERROR;
   }
   const bool moved = !(P.overlap && overlap_any<G>(S, cn, lane, gm));
-  return step_end(S, P, key, s, tr, R, cn, qn, moved, dt, tl);
+  const double c0[3] = {tr.c[0], tr.c[1], tr.c[2]};
+  const int st = step_end(S, P, key, s, tr, R, cn, qn, moved, dt, tl);
+  if (P.stats && lane == 0) {
+    stats_step(S, P, tr, s, r_prev, dt, c0, R, sh);
+    if (st == ST_REACTED) stats_encounter(P, tr, s, true);
+  }
+  return st;
 }
 
 __device__ __forceinline__ void load_slot(const SlotBuf& B, int s, Traj& tr) {
@@ -585,6 +678,8 @@ __global__ void init_slots_kernel(DevSim P, SlotBuf B, int n_slots) {
 template <typename FT, int G, bool TORQUE>
 __global__ void __launch_bounds__(256) step_kernel(DevSystem S, DevSim P, SlotBuf B, const int* __restrict__ n_live,
                                                    int K) {
+  extern __shared__ unsigned sh_stats[];
+  stats_block_begin(P, sh_stats);
   const int lane = threadIdx.x & (G - 1);
   const unsigned gm = group_mask<G>();
   const int live = *n_live;
@@ -606,7 +701,7 @@ __global__ void __launch_bounds__(256) step_kernel(DevSystem S, DevSim P, SlotBu
         }
         start_trajectory(P, id, tr);
       }
-      const int st = bd_step<FT, G, TORQUE>(S, P, tr, lane, gm, tl);
+      const int st = bd_step<FT, G, TORQUE>(S, P, tr, lane, gm, tl, sh_stats);
       if (st != ST_RUNNING) {
         tr.status = st;
         if (lane == 0) {
@@ -629,6 +724,7 @@ __global__ void __launch_bounds__(256) step_kernel(DevSystem S, DevSim P, SlotBu
   }
   // Only lane 0 of each group counts scalar events.
   flush_tally(P, tl, lane == 0);
+  stats_block_end(P, sh_stats);
 }
 
 // All forces of the lanes with `need`, one trajectory at a time, the whole warp
@@ -707,6 +803,8 @@ __device__ __forceinline__ void warp_refill(const DevSim& P, Traj& tr, bool& dea
 template <typename FT, bool TORQUE, int MINB>
 __global__ void __launch_bounds__(256, MINB) step_kernel_warp(DevSystem S, DevSim P, SlotBuf B,
                                                               const int* __restrict__ n_live, int K) {
+  extern __shared__ unsigned sh_stats[];
+  stats_block_begin(P, sh_stats);
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int live = *n_live;
@@ -728,8 +826,12 @@ __global__ void __launch_bounds__(256, MINB) step_kernel_warp(DevSystem S, DevSi
       const Keyed key = traj_key(P, tr.id);
       const uint32_t s = (uint32_t)tr.steps;
       double R[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, r = 0;
+      const double r_prev = P.stats ? norm3(tr.c[0], tr.c[1], tr.c[2]) : 0.0;
       int st = ST_EMPTY;
-      if (!dead) st = step_begin(S, P, key, s, tr, R, r, tl);
+      if (!dead) {
+        st = step_begin(S, P, key, s, tr, R, r, tl);
+        if (P.stats && st == ST_REACTED) stats_encounter(P, tr, s, false);
+      }
       const bool need_f = !dead && st == ST_RUNNING;
       double F[3] = {0, 0, 0}, T[3] = {0, 0, 0};
       warp_forces<FT, TORQUE>(S, tr.c, R, need_f, F, T, lane, tl.cnt);
@@ -741,7 +843,14 @@ __global__ void __launch_bounds__(256, MINB) step_kernel_warp(DevSystem S, DevSi
         st = ST_ERROR;
       }
       const bool ovl = warp_overlap(S, cn, need_f && ok && P.overlap, lane);
-      if (need_f && ok) st = step_end(S, P, key, s, tr, R, cn, qn, !ovl, dt, tl);
+      if (need_f && ok) {
+        const double c0[3] = {tr.c[0], tr.c[1], tr.c[2]};
+        st = step_end(S, P, key, s, tr, R, cn, qn, !ovl, dt, tl);
+        if (P.stats) {
+          stats_step(S, P, tr, s, r_prev, dt, c0, R, sh_stats);
+          if (st == ST_REACTED) stats_encounter(P, tr, s, true);
+        }
+      }
       if (!dead && st != ST_RUNNING) {
         tr.status = st;
         P.out_status[tr.id] = (int8_t)st;
@@ -757,6 +866,7 @@ __global__ void __launch_bounds__(256, MINB) step_kernel_warp(DevSystem S, DevSi
     if (own) store_slot(B, slot, tr);
   }
   flush_tally(P, tl, true);
+  stats_block_end(P, sh_stats);
 }
 
 // Sum the per-thread tallies of a warp and add them to the device counters.

@@ -119,7 +119,7 @@ class B200BatchSimulator:
 
     def __init__(self, mol1, mol2, mob, pathway_set, params, batch_engine, *, precision=None, torque_mode=None,
                  termination="reference", steps_per_launch=64, launches_per_poll=8, slots=0, id_offset=0,
-                 verbose=False):
+                 stats=None, verbose=False):
         if not hasattr(batch_engine, "handle"):
             raise TypeError("batch_engine must be a B200ForceEngine")
         if any(getattr(r, "state_before", None) is not None for r in pathway_set.reactions):
@@ -135,6 +135,8 @@ class B200BatchSimulator:
         self.M = int(launches_per_poll)
         self.slots = int(slots)
         self.id_offset = int(id_offset)
+        # per-step statistics for write_all: on when the pipeline attached an output config
+        self.stats = bool(getattr(params, "_output_cfg", None) is not None) if stats is None else bool(stats)
         self.verbose = verbose
         c0 = np.asarray(mol2.centroid(), dtype=float)
         self._mol2_pos0 = np.asarray(mol2.positions_array(), dtype=float) - c0
@@ -202,6 +204,7 @@ class B200BatchSimulator:
         sp.torque_mode = {"zero": _lib.TORQUE_ZERO, "centroid": _lib.TORQUE_CENTROID}[self.torque_mode]
         sp.slots = self.slots
         sp.id_offset = self.id_offset
+        sp.stats = int(self.stats)
         h.call("bd_sim_configure", _lib.C.byref(sp))
         return D_t
 
@@ -209,6 +212,62 @@ class B200BatchSimulator:
         out = np.zeros(_lib.N_CTR, dtype=np.uint64)
         self.engine.handle.call("bd_sim_counters", _lib.ptr(out, _lib.C.c_uint64), _lib.N_CTR, None)
         return dict(zip(_lib.CTR_NAMES, (int(v) for v in out)))
+
+    def read_stats(self):
+        """Per-step statistics as host arrays (requires ``stats=True``)."""
+        N = int(self.params.n_trajectories)
+        P = len(self._rxn_cutoffs)
+        L = _lib
+        a = {"start_pos": np.zeros((N, 3)), "start_q": np.zeros((N, 4)), "min_dist": np.zeros(N),
+             "near_miss_pos": np.zeros((N, 3)), "near_miss_q": np.zeros((N, 4)), "total_time": np.zeros(N),
+             "encounter_pos": np.zeros((N, 3)), "encounter_q": np.zeros((N, 4)),
+             "step_at_min": np.zeros(N, dtype=np.int32), "encounter_step": np.zeros(N, dtype=np.int32),
+             "bridge": np.zeros(N, dtype=np.int8), "radial": np.zeros(L.ST_RAD_BINS, dtype=np.uint64),
+             "angular": np.zeros((L.ST_THETA, L.ST_PHI), dtype=np.uint64),
+             "milestone_out": np.zeros(L.ST_MILESTONES, dtype=np.uint64),
+             "milestone_in": np.zeros(L.ST_MILESTONES, dtype=np.uint64),
+             "transition": np.zeros((L.ST_TRANS, L.ST_TRANS), dtype=np.uint64),
+             "contact": np.zeros(max(P, 1), dtype=np.uint64), "radial_edges": np.zeros(L.ST_RAD_BINS + 1),
+             "transition_edges": np.zeros(L.ST_TRANS + 1), "milestone_radii": np.zeros(L.ST_MILESTONES)}
+        out = L.BdStatsOut()
+        ctypes_of = {np.float64: L.C.c_double, np.int32: L.C.c_int32, np.int8: L.C.c_int8, np.uint64: L.C.c_uint64}
+        for k, v in a.items():
+            setattr(out, k, v.ctypes.data_as(L.C.POINTER(ctypes_of[v.dtype.type])))
+        self.engine.handle.call("bd_sim_stats", L.C.byref(out))
+        a["contact"] = a["contact"][:P]
+        return a
+
+    def sim_data(self, status, steps, rets, total_steps):
+        """The reference's ``sim_data`` dict (gpu_batch_simulator.py:1511-1557) from the device statistics.
+
+        Per-step path and energy snapshots are not recorded (``path_steps`` and
+        ``energy_steps`` are empty lists).
+        """
+        a = self.read_stats()
+        outcome = status.astype(np.int32)
+        outcome[(outcome != 1) & (outcome != 2)] = 0
+        rx = np.where(outcome == 1)[0]
+        esc = np.where(outcome == 2)[0]
+        return {
+            "outcome": outcome, "n_steps": steps.astype(np.int64), "start_pos": a["start_pos"],
+            "start_q": a["start_q"], "min_dist": a["min_dist"], "step_at_min": a["step_at_min"].astype(np.int64),
+            "total_time_ps": a["total_time"], "n_returns": rets.astype(np.int64),
+            "bb_triggered": a["bridge"].astype(np.int64), "encounter_pos": a["encounter_pos"][rx],
+            "encounter_q": a["encounter_q"][rx], "encounter_traj": rx.astype(np.int64),
+            "encounter_step": a["encounter_step"][rx].astype(np.int64),
+            "encounter_n_pairs": np.full(len(rx), self._rxn_n_needed, dtype=np.int64),
+            "near_miss_pos": a["near_miss_pos"][esc], "near_miss_q": a["near_miss_q"][esc],
+            "near_miss_traj": esc.astype(np.int64), "near_miss_dist": a["min_dist"][esc],
+            "path_steps": [], "energy_steps": [],
+            "radial_bins": a["radial_edges"], "radial_counts": a["radial"].astype(np.int64),
+            "angular_theta": np.linspace(0, np.pi, _lib.ST_THETA), "angular_phi": np.linspace(0, 2 * np.pi, _lib.ST_PHI),
+            "angular_counts": a["angular"].astype(np.int64), "milestone_radii": a["milestone_radii"],
+            "milestone_flux_out": a["milestone_out"].astype(np.int64),
+            "milestone_flux_in": a["milestone_in"].astype(np.int64),
+            "contact_pair_counts": a["contact"].astype(np.int64),
+            "contact_total_steps": int(total_steps) if len(self._rxn_cutoffs) else 0,
+            "trans_bins": a["transition_edges"], "trans_matrix": a["transition"].astype(np.int64),
+        }
 
     def outcomes(self):
         N = int(self.params.n_trajectories)
@@ -318,10 +377,13 @@ class B200BatchSimulator:
         if ckpt_interval > 0 and ckpt.exists():
             ckpt.unlink()
         self.counters = c
-        outcome = status.astype(np.int32)
-        outcome[(outcome != 1) & (outcome != 2)] = 0
-        sim_data = {"outcome": outcome, "n_steps": steps.astype(np.int64), "n_returns": rets.astype(np.int64)}
         total = int(c["steps"])
+        if self.stats:
+            sim_data = self.sim_data(status, steps, rets, total)
+        else:
+            outcome = status.astype(np.int32)
+            outcome[(outcome != 1) & (outcome != 2)] = 0
+            sim_data = {"outcome": outcome, "n_steps": steps.astype(np.int64), "n_returns": rets.astype(np.int64)}
         return B200BatchResult(n_trajectories=N, n_reacted=n_reacted, n_escaped=n_escaped, n_max_steps=n_max,
                                reaction_counts={"stage_0": n_reacted}, r_start=float(self.params.r_start),
                                r_escape=float(self.params.r_escape), dt=float(getattr(self.params, "dt", 0.2)),

@@ -205,7 +205,12 @@ def gen_run(out, name, s, n_traj, seed, max_steps):
                      total_steps=int(round(res.steps_per_sec * res.elapsed_sec)), outcome=sd["outcome"],
                      n_steps=sd["n_steps"], n_returns=sd["n_returns"], return_prob=sim._return_prob, k_b=sim._k_b,
                      D_t=mob.relative_translational_diffusion(), D_r=mob.relative_rotational_diffusion(),
-                     ci=np.array(res.reaction_probability_ci(0.95)))
+                     ci=np.array(res.reaction_probability_ci(0.95)),
+                     **{f"sd_{k}": np.asarray(sd[k]) for k in (
+                         "start_pos", "start_q", "min_dist", "step_at_min", "total_time_ps", "bb_triggered",
+                         "encounter_traj", "encounter_step", "encounter_pos", "encounter_q", "near_miss_traj",
+                         "near_miss_pos", "near_miss_dist", "radial_counts", "angular_counts", "milestone_flux_out",
+                         "milestone_flux_in", "contact_pair_counts", "contact_total_steps", "trans_matrix")})
 
 
 def two_sphere_example():

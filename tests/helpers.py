@@ -60,7 +60,7 @@ def system(name):
 def oracle_engine(s, multipole=True, born_chunk_skip=True):
     if multipole and s.multipole:
         dip, quad = multipole_moments(s.rec_pos, s.rec_q)
-        ff = FarField(float(np.sum(s.rec_q)), s.debye, s.sdie, dip, quad, 4.0 * np.pi * s.sdie * 0.000142)
+        ff = FarField(float(np.sum(s.rec_q)), s.debye, s.sdie, dip, quad, 4.0 * np.pi * (s.sdie * 0.000142))
     else:
         ff = FarField(float(np.sum(s.rec_q)), s.debye, s.sdie)
     return OracleForceEngine([OracleGrid.from_dx(g) for g in s.elec_grids],
@@ -80,7 +80,9 @@ def step_system(s, engine=None):
                       rxn_cutoff=np.asarray([c for _, _, c in s.pairs], dtype=float),
                       n_needed=n_needed_of(s.n_needed, P), D_t=mob.relative_translational_diffusion(),
                       D_r=mob.relative_rotational_diffusion(), r_h_rec=s.r_hydro_rec, r_h_lig=s.r_hydro_lig,
-                      q_rec_total=float(np.sum(s.rec_q)), q_lig_total=float(np.sum(s.lig_q)), debye=s.debye)
+                      # Molecule.total_charge sums atom by atom (pystarc/structures/molecules.py:69-70)
+                      q_rec_total=sum(float(v) for v in s.rec_q), q_lig_total=sum(float(v) for v in s.lig_q),
+                      debye=s.debye)
 
 
 def step_params(s, n_traj, seed, max_steps):

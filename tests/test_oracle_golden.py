@@ -165,3 +165,31 @@ def test_stepper_reproduces_reference_run_exactly(name, sysname):
     ref_outcome = g["outcome"].copy()
     ref_outcome[ref_outcome == 0] = 3
     np.testing.assert_array_equal(res.status, ref_outcome)
+
+
+@pytest.mark.parametrize("name,sysname", [("run_two_sphere", "two_sphere"), ("run_c2", "c2"), ("run_c3", "c3")])
+def test_stepper_statistics_match_reference(name, sysname):
+    """The per-step statistics the reference collects for its output files (gpu_batch_simulator.py:1255-1317)."""
+    g = golden(name)
+    s = system(sysname)
+    res = ost.run(step_system(s), step_params(s, int(g["n_traj"]), int(g["seed"]), int(g["max_steps"])), noise="pcg64")
+    st = res.stats
+    np.testing.assert_array_equal(st.start_pos, g["sd_start_pos"])
+    np.testing.assert_array_equal(st.start_q, g["sd_start_q"])
+    np.testing.assert_array_equal(st.min_dist, g["sd_min_dist"])
+    np.testing.assert_array_equal(st.step_at_min, g["sd_step_at_min"])
+    np.testing.assert_allclose(st.total_time, g["sd_total_time_ps"], rtol=1e-12)
+    np.testing.assert_array_equal(st.bridge, g["sd_bb_triggered"])
+    for k, mine in [("radial_counts", st.rad_counts), ("angular_counts", st.ang_counts),
+                    ("milestone_flux_out", st.ms_out), ("milestone_flux_in", st.ms_in), ("trans_matrix", st.trans)]:
+        np.testing.assert_array_equal(mine, g[f"sd_{k}"], err_msg=k)
+    P = len(s.pairs)
+    np.testing.assert_array_equal(st.contact[:P], g["sd_contact_pair_counts"][:P])
+    assert st.contact_total == int(g["sd_contact_total_steps"])
+    et = g["sd_encounter_traj"]
+    np.testing.assert_array_equal(st.enc_step[et], g["sd_encounter_step"])
+    np.testing.assert_array_equal(st.enc_pos[et], g["sd_encounter_pos"])
+    np.testing.assert_array_equal(st.enc_q[et], g["sd_encounter_q"])
+    nt = g["sd_near_miss_traj"]
+    np.testing.assert_array_equal(st.nm_pos[nt], g["sd_near_miss_pos"])
+    np.testing.assert_array_equal(st.min_dist[nt], g["sd_near_miss_dist"])
