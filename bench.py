@@ -128,6 +128,9 @@ class _MP:
         self.dipole, self.quadrupole, self.four_pi_eps = s.multipole_moments()
 
 
+_OPTS = {"stage_receptor": True}
+
+
 def make_sim(s, precision, n_traj, K, id_offset=0, torque="zero"):
     from pystarc_b200.engine import B200ForceEngine
     from pystarc_b200.simulator import B200BatchSimulator
@@ -136,7 +139,8 @@ def make_sim(s, precision, n_traj, K, id_offset=0, torque="zero"):
                           device=int(os.environ.get("LOCAL_RANK", 0)))
     mol1, mol2 = s.molecules()
     sim = B200BatchSimulator(mol1, mol2, s.mobility(), s.pathway_set(), s.params(n_traj=n_traj), eng,
-                             termination="complete", steps_per_launch=K, id_offset=id_offset)
+                             termination="complete", steps_per_launch=K, id_offset=id_offset,
+                             stage_receptor=_OPTS["stage_receptor"])
     return sim
 
 
@@ -284,8 +288,10 @@ def main():
     ap.add_argument("--workload", default="protein-ligand", choices=sorted(WORKLOADS))
     ap.add_argument("--launch", default="", help="fixed launch shape GROUPxBLOCK (default: autotune)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-stage", action="store_true", help="keep the receptor table in global memory only")
     ap.add_argument("--cpu-steps", type=int, default=40)
     args = ap.parse_args()
+    _OPTS["stage_receptor"] = not args.no_stage
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -368,7 +374,7 @@ def main():
         "config": {"workload": WORKLOADS[args.workload][0], "trajectories_per_gpu": n_traj,
                    "bd_steps_per_launch": args.inner,
                    "parallelism": f"trajectory shards x{world}", "l2": "flushed (256 MiB write) between launches",
-                   "launch": launch},
+                   "launch": launch, "receptor_staged_in_smem": _OPTS["stage_receptor"]},
         "variants": {
             "mixed": {"bd_steps_per_s": d_mixed["steps"] / t_mixed, "steps": d_mixed["steps"]},
             "fp64": {"bd_steps_per_s": d_fp64["steps"] / t_fp64, "steps": d_fp64["steps"], "launch": launch64},

@@ -166,6 +166,15 @@ enum { BD_GROUP_WARP = 64, BD_GROUP_WARP_CAPPED = 65 };
 int bd_set_launch(BdHandle* h, int group, int block_threads);
 int bd_get_launch(BdHandle* h, int* group, int* block_threads, int* grid_blocks);
 
+/* Receptor staging of the stepper kernels: BD_STAGE_AUTO (default) copies an FP32 receptor
+ * table of at most BD_STAGE_MAX_BYTES (atoms + chunk spheres) into each block's shared memory
+ * for the sweeps' distance pre-tests; BD_STAGE_OFF reads the FP64 table from global memory
+ * only.  Every accept/reject decision is taken in FP64 either way, so trajectories are the
+ * same bit for bit. */
+enum { BD_STAGE_OFF = 0, BD_STAGE_AUTO = 1 };
+#define BD_STAGE_MAX_BYTES (64 * 1024)
+int bd_set_stage_receptor(BdHandle* h, int mode);
+
 /* No counterpart in the reference.  Runs p->n_traj trajectories to completion (or for
  * max_launches launches of steps_per_launch steps) on the handle's system WITHOUT
  * allocating device memory, for callers that cannot call cudaMalloc at that point: an

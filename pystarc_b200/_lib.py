@@ -89,6 +89,7 @@ SIGNATURES = {
     "bd_sim_restore": (C.c_int, [P, dp, dp, i32p, i32p, i32p, i8p, C.c_int32, u64p, i8p, i32p, i32p]),
     "bd_set_launch": (C.c_int, [P, C.c_int, C.c_int]),
     "bd_get_launch": (C.c_int, [P, i32p, i32p, i32p]),
+    "bd_set_stage_receptor": (C.c_int, [P, C.c_int]),
     "bd_sim_run_noalloc": (C.c_int, [P, C.POINTER(BdSimParams), P, P, P, P, C.c_int, C.c_int, P]),
 }
 

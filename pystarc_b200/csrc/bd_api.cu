@@ -56,6 +56,7 @@ struct BdHandle {
   std::vector<void*> sim_allocs;
   int group = 8, block = 128;
   bool launch_user = false;
+  int stage_mode = BD_STAGE_AUTO;
   // graphs: [cur][steps] cache
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   int graph_K = -1, graph_G = -1, graph_B = -1, graph_prec = -1, graph_torque = -1;
@@ -269,6 +270,19 @@ int finalize(BdHandle* h) {
     S.n_chunks = nc;
     S.n_rec_pad = nc * BD_CHUNK;
     S.rec_max_r = rmax * (1 + 1e-12) + 1e-9;
+    // FP32 copies for the stepper's shared-memory pre-tests (same order and chunking)
+    std::vector<float> rf(ra.size()), cf(cs.size());
+    for (size_t i = 0; i < ra.size(); ++i) rf[i] = (float)ra[i];
+    for (size_t i = 0; i < cs.size(); ++i) cf[i] = (float)cs[i];
+    rc = dev_alloc(h, h->sys_allocs, &p, rf.size() * sizeof(float));
+    if (rc) return rc;
+    CK(h, cudaMemcpy(p, rf.data(), rf.size() * sizeof(float), cudaMemcpyHostToDevice));
+    S.rec_f = (const float4*)p;
+    rc = dev_alloc(h, h->sys_allocs, &p, cf.size() * sizeof(float));
+    if (rc) return rc;
+    CK(h, cudaMemcpy(p, cf.data(), cf.size() * sizeof(float), cudaMemcpyHostToDevice));
+    S.chunks_f = (const float4*)p;
+    S.rec_in_smem = h->stage_mode == BD_STAGE_AUTO && (size_t)(S.n_rec_pad + nc) * sizeof(float4) <= BD_STAGE_MAX_BYTES;
   }
   // Born direction 2 needs the ligand Born grid, receptor atoms and alpha > 1e-12 (gpu_batch_engine.py:583-590)
   if (!lb.empty() && nr > 0 && fp.alpha > 1e-12) {
@@ -381,8 +395,16 @@ int persistent_blocks(BdHandle* h, void* fn, int block, size_t smem = 0) {
   return per_sm * h->n_sm;
 }
 
-// Dynamic shared memory of a stepper launch: the block's statistics histograms.
-size_t stats_smem(const BdHandle* h) { return h->P.stats ? (size_t)SH_NUM * sizeof(unsigned) : 0; }
+// Dynamic shared memory of a stepper launch (block_shared_begin's layout): the
+// staged FP32 receptor table, then the block's statistics histograms.  Raises the
+// kernel's dynamic shared-memory limit to match, so occupancy queries and launches
+// agree.
+size_t stepper_smem(const DevSystem& S, const DevSim& P, void* fn) {
+  size_t b = S.rec_in_smem ? (size_t)(S.n_rec_pad + S.n_chunks) * sizeof(float4) : 0;
+  if (P.stats) b += (size_t)SH_NUM * sizeof(unsigned);
+  if (fn) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b);
+  return b;
+}
 
 }  // namespace
 
@@ -568,6 +590,16 @@ int bd_set_launch(BdHandle* h, int group, int block) {
   return BD_OK;
 }
 
+int bd_set_stage_receptor(BdHandle* h, int mode) {
+  if (!h) return BD_ERR_ARG;
+  if (mode != BD_STAGE_OFF && mode != BD_STAGE_AUTO) return fail(h, BD_ERR_ARG, "stage mode must be 0 (off) or 1 (auto)");
+  h->stage_mode = mode;
+  const bool fits = (size_t)(h->S.n_rec_pad + h->S.n_chunks) * sizeof(float4) <= BD_STAGE_MAX_BYTES;
+  if (!h->dirty) h->S.rec_in_smem = mode == BD_STAGE_AUTO && h->S.rec_f && fits;
+  h->graph_K = -1;
+  return BD_OK;
+}
+
 int bd_get_launch(BdHandle* h, int* group, int* block, int* grid) {
   if (!h) return BD_ERR_ARG;
   const int G = launch_group(h);
@@ -575,7 +607,7 @@ int bd_get_launch(BdHandle* h, int* group, int* block, int* grid) {
   if (block) *block = h->block;
   if (grid) {
     void* fn = kernel_for(h->sp.precision, G, h->sp.torque_mode, 2);
-    *grid = fn ? persistent_blocks(h, fn, h->block) : 0;
+    *grid = fn ? persistent_blocks(h, fn, h->block, stepper_smem(h->S, h->P, fn)) : 0;
   }
   return BD_OK;
 }
@@ -600,7 +632,10 @@ int bd_sim_configure(BdHandle* h, const BdSimParams* p) {
   // live-slot capacity
   const int G = launch_group(h);
   void* fn = kernel_for(p->precision, G, p->torque_mode, 2);
-  const long long resident = (long long)persistent_blocks(h, fn, h->block) * (h->block / lanes_per_traj(G));
+  DevSim probe{};
+  probe.stats = p->stats;
+  const long long resident =
+      (long long)persistent_blocks(h, fn, h->block, stepper_smem(h->S, probe, fn)) * (h->block / lanes_per_traj(G));
   long long cap = p->slots > 0 ? p->slots : std::max<long long>(65536, 8 * resident);
   cap = std::min<long long>(cap, p->n_traj);
   const int C = (int)cap;
@@ -745,11 +780,9 @@ int bd_sim_reset(BdHandle* h, void* stream) {
 
 namespace {
 
-int enqueue_launch(BdHandle* h, int K, cudaStream_t s, int cur) {
-  const int G = launch_group(h);
-  void* fn = kernel_for(h->sp.precision, G, h->sp.torque_mode, 2);
-  const size_t smem = stats_smem(h);
-  const int blocks = persistent_blocks(h, fn, h->block, smem);
+// One stepper launch plus the compaction into the other slot buffer.  `fn`,
+// `smem` and `blocks` are fixed before stream capture starts.
+int enqueue_launch(BdHandle* h, int K, cudaStream_t s, int cur, void* fn, size_t smem, int blocks) {
   SlotBuf src = h->buf[cur], dst = h->buf[1 - cur];
   const int* live = h->d_live + cur;
   int* live_dst = h->d_live + (1 - cur);
@@ -772,10 +805,13 @@ int build_graphs(BdHandle* h, int K) {
       cudaGraphExecDestroy(g);
       g = nullptr;
     }
+  void* fn = kernel_for(h->sp.precision, G, h->sp.torque_mode, 2);
+  const size_t smem = stepper_smem(h->S, h->P, fn);
+  const int blocks = persistent_blocks(h, fn, h->block, smem);
   for (int c = 0; c < 2; ++c) {
     cudaGraph_t graph;
     CK(h, cudaStreamBeginCapture(h->own, cudaStreamCaptureModeThreadLocal));
-    int rc = enqueue_launch(h, K, h->own, c);
+    int rc = enqueue_launch(h, K, h->own, c, fn, smem, blocks);
     cudaError_t e = cudaStreamEndCapture(h->own, &graph);
     if (rc) return rc;
     CK(h, e);
@@ -1042,7 +1078,8 @@ int bd_internal_run_noalloc(BdHandle* h, const BdSimParams* p, unsigned char* sc
   CK(h, cudaStreamSynchronize(s));
   const int G = launch_group(h);
   void* fn = kernel_for(p->precision, G, p->torque_mode, 2);
-  const int blocks = persistent_blocks(h, fn, h->block);
+  const size_t smem = stepper_smem(h->S, P, fn);
+  const int blocks = persistent_blocks(h, fn, h->block, smem);
   int cur = 0;
   for (int launch = 0; launch < max_launches; ++launch) {
     SlotBuf src = B[cur], dst = B[1 - cur];
@@ -1050,7 +1087,7 @@ int bd_internal_run_noalloc(BdHandle* h, const BdSimParams* p, unsigned char* sc
     int* ldst = live + (1 - cur);
     int KK = K;
     void* args[] = {&h->S, &P, &src, &lsrc, &KK};
-    CK(h, cudaLaunchKernel(fn, dim3(blocks), dim3(h->block), args, 0, s));
+    CK(h, cudaLaunchKernel(fn, dim3(blocks), dim3(h->block), args, smem, s));
     compact_kernel<<<h->n_sm * 4, 256, 0, s>>>(src, dst, lsrc, ctr);
     CK(h, cudaGetLastError());
     finish_compact_kernel<<<1, 1, 0, s>>>(ldst, ctr);

@@ -54,6 +54,9 @@ struct DevSystem {
   int n_rec_pad, n_chunks;
   const double4* rec;     // x,y,z,q
   const double4* chunks;  // centre xyz, radius
+  const float4* rec_f;    // FP32 copies for the shared-memory pre-tests (radius not inflated)
+  const float4* chunks_f;
+  int rec_in_smem;        // stepper kernels stage rec_f / chunks_f in shared memory
   double rec_max_r;
   // grids
   int n_elec;

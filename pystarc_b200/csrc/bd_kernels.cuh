@@ -34,18 +34,36 @@ struct Counts {
   unsigned grid, rev, ff;
 };
 
+// FP32 copy of the receptor table staged in shared memory by the stepper
+// kernels (null members: read the FP64 table from global memory).  Tests on it
+// only prune: they keep every atom within the FP64 test's reach plus a margin
+// far above the FP32 rounding of coordinates of tens of Angstrom, and the FP64
+// test then decides, so results do not depend on which path ran.
+struct RecView {
+  const float4* rec;
+  const float4* chunks;
+};
+constexpr float kPruneMargin = 1e-3f;  // A
+
 // Bit j set: receptor chunk k0 + j has a bounding sphere within `reach` of c.
 // Lane j of the group tests chunk k0 + j; the mask is the same on every lane.
 template <int G>
-__device__ __forceinline__ unsigned chunk_hits(const DevSystem& S, const double c[3], double reach, int k0, int lane,
-                                               unsigned gm) {
+__device__ __forceinline__ unsigned chunk_hits(const DevSystem& S, const RecView& v, const double c[3], double reach,
+                                               int k0, int lane, unsigned gm) {
   const int k = k0 + lane;
   bool hit = false;
   if (k < S.n_chunks) {
-    const double4 sp = S.chunks[k];
-    const double dx = sp.x - c[0], dy = sp.y - c[1], dz = sp.z - c[2];
-    const double lim = reach + sp.w;
-    hit = dx * dx + dy * dy + dz * dz < lim * lim;
+    if (v.chunks) {
+      const float4 sp = v.chunks[k];
+      const float dx = sp.x - (float)c[0], dy = sp.y - (float)c[1], dz = sp.z - (float)c[2];
+      const float lim = (float)reach + sp.w + kPruneMargin;
+      hit = dx * dx + dy * dy + dz * dz < lim * lim;
+    } else {
+      const double4 sp = S.chunks[k];
+      const double dx = sp.x - c[0], dy = sp.y - c[1], dz = sp.z - c[2];
+      const double lim = reach + sp.w;
+      hit = dx * dx + dy * dy + dz * dz < lim * lim;
+    }
   }
   if constexpr (G == 1) {
     return hit ? 1u : 0u;
@@ -92,7 +110,8 @@ struct PosFromAtoms {
 // same totals.
 template <typename FT, int G, bool TORQUE, bool ENERGY, class PosFn>
 __device__ void group_forces(const DevSystem& S, const double c[3], const double R[9], int lane, unsigned gm,
-                             const PosFn& pos, double F[3], double T[3], double& E, Counts& cnt) {
+                             const PosFn& pos, double F[3], double T[3], double& E, Counts& cnt,
+                             const RecView& v = RecView{nullptr, nullptr}) {
   double f0 = 0, f1 = 0, f2 = 0, t0 = 0, t1 = 0, t2 = 0, e = 0;
   unsigned ng = 0, nf = 0, nr = 0;
   const int nl = S.n_lig;
@@ -162,12 +181,19 @@ __device__ void group_forces(const DevSystem& S, const double c[3], const double
     const double rho = S.lig_born_rho;
     if (norm3(c[0], c[1], c[2]) - S.rec_max_r < rho) {
       const double rho2 = rho * rho;
+      const float cf0 = (float)c[0], cf1 = (float)c[1], cf2 = (float)c[2];
+      const float rho_f = (float)rho + kPruneMargin, rho_f2 = rho_f * rho_f;
       for (int k0 = 0; k0 < S.n_chunks; k0 += G) {
-       unsigned hits = chunk_hits<G>(S, c, rho, k0, lane, gm);
+       unsigned hits = chunk_hits<G>(S, v, c, rho, k0, lane, gm);
        while (hits) {
         const int k = k0 + __ffs(hits) - 1;
         hits &= hits - 1;
         for (int a = lane; a < BD_CHUNK; a += G) {
+          if (v.rec) {
+            const float4 af = v.rec[k * BD_CHUNK + a];
+            const float e0 = af.x - cf0, e1 = af.y - cf1, e2 = af.z - cf2;
+            if (e0 * e0 + e1 * e1 + e2 * e2 >= rho_f2) continue;
+          }
           const double4 at = S.rec[k * BD_CHUNK + a];
           if (fabs(at.w) < 1e-9) continue;
           const double d0 = at.x - c[0], d1 = at.y - c[1], d2 = at.z - c[2];
@@ -389,16 +415,24 @@ __device__ __forceinline__ double hi_diffusion(const DevSim& P, double r) {
 // (gpu_batch_simulator.py:1106-1128)?  Chunks whose bounding sphere is farther
 // than 1.5 A are skipped; the answer is exact.
 template <int G>
-__device__ __forceinline__ bool overlap_any(const DevSystem& S, const double c[3], int lane, unsigned gm) {
+__device__ __forceinline__ bool overlap_any(const DevSystem& S, const double c[3], int lane, unsigned gm,
+                                            const RecView& v = RecView{nullptr, nullptr}) {
   bool any = false;
   if (norm3(c[0], c[1], c[2]) < S.rec_max_r + 1.5) {
+    const float cf0 = (float)c[0], cf1 = (float)c[1], cf2 = (float)c[2];
+    const float lim_f = 1.5f + kPruneMargin, lim_f2 = lim_f * lim_f;
     for (int k0 = 0; k0 < S.n_chunks && !any; k0 += G) {
-      unsigned hits = chunk_hits<G>(S, c, 1.5, k0, lane, gm);
+      unsigned hits = chunk_hits<G>(S, v, c, 1.5, k0, lane, gm);
       bool hit = false;
       while (hits) {
         const int k = k0 + __ffs(hits) - 1;
         hits &= hits - 1;
         for (int a = lane; a < BD_CHUNK; a += G) {
+          if (v.rec) {
+            const float4 af = v.rec[k * BD_CHUNK + a];
+            const float e0 = af.x - cf0, e1 = af.y - cf1, e2 = af.z - cf2;
+            if (e0 * e0 + e1 * e1 + e2 * e2 >= lim_f2) continue;
+          }
           const double4 at = S.rec[k * BD_CHUNK + a];
           if (norm3(c[0] - at.x, c[1] - at.y, c[2] - at.z) < 1.5) hit = true;
         }
@@ -590,6 +624,29 @@ __device__ __forceinline__ void stats_block_begin(const DevSim& P, unsigned* sh)
   __syncthreads();
 }
 
+// Dynamic shared memory of a stepper block, in this order: the FP32 receptor
+// atoms (n_rec_pad float4) and chunk spheres (n_chunks float4) when
+// S.rec_in_smem, then the statistics histograms (SH_NUM words) when P.stats.
+// The host sizes every stepper launch for exactly this layout.
+struct BlockShared {
+  RecView v;
+  unsigned* stats;
+};
+
+__device__ __forceinline__ BlockShared block_shared_begin(const DevSystem& S, const DevSim& P) {
+  extern __shared__ float4 sh_dyn[];
+  BlockShared b{RecView{nullptr, nullptr}, reinterpret_cast<unsigned*>(sh_dyn)};
+  if (S.rec_in_smem) {
+    const int nr = S.n_rec_pad, n = nr + S.n_chunks;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) sh_dyn[i] = i < nr ? S.rec_f[i] : S.chunks_f[i - nr];
+    b.v = RecView{sh_dyn, sh_dyn + nr};
+    b.stats = reinterpret_cast<unsigned*>(sh_dyn + n);
+    __syncthreads();
+  }
+  stats_block_begin(P, b.stats);
+  return b;
+}
+
 __device__ __forceinline__ void stats_block_end(const DevSim& P, const unsigned* sh) {
   if (!P.stats) return;
   __syncthreads();
@@ -603,7 +660,7 @@ __device__ __forceinline__ void stats_block_end(const DevSim& P, const unsigned*
 // rejection, Brownian bridge, step count.  Returns the new status.
 template <typename FT, int G, bool TORQUE>
 __device__ __forceinline__ int bd_step(const DevSystem& S, const DevSim& P, Traj& tr, int lane, unsigned gm,
-                                       Tally& tl, unsigned* sh) {
+                                       Tally& tl, unsigned* sh, const RecView& v) {
   const Keyed key = traj_key(P, tr.id);
   const uint32_t s = (uint32_t)tr.steps;
   const double r_prev = P.stats ? norm3(tr.c[0], tr.c[1], tr.c[2]) : 0.0;
@@ -614,13 +671,13 @@ __device__ __forceinline__ int bd_step(const DevSystem& S, const DevSim& P, Traj
     return st0;
   }
   double F[3], T[3], E;
-  group_forces<FT, G, TORQUE, false>(S, tr.c, R, lane, gm, PosFromPose{R, tr.c}, F, T, E, tl.cnt);
+  group_forces<FT, G, TORQUE, false>(S, tr.c, R, lane, gm, PosFromPose{R, tr.c}, F, T, E, tl.cnt, v);
   double cn[3], qn[4], dt;
   if (!step_move<FT>(P, key, s, tr, r, F, T, cn, qn, dt)) {
     tl.nonfinite += 1;
     return ST_ERROR;
   }
-  const bool moved = !(P.overlap && overlap_any<G>(S, cn, lane, gm));
+  const bool moved = !(P.overlap && overlap_any<G>(S, cn, lane, gm, v));
   const double c0[3] = {tr.c[0], tr.c[1], tr.c[2]};
   const int st = step_end(S, P, key, s, tr, R, cn, qn, moved, dt, tl);
   if (P.stats && lane == 0) {
@@ -678,8 +735,7 @@ __global__ void init_slots_kernel(DevSim P, SlotBuf B, int n_slots) {
 template <typename FT, int G, bool TORQUE>
 __global__ void __launch_bounds__(256) step_kernel(DevSystem S, DevSim P, SlotBuf B, const int* __restrict__ n_live,
                                                    int K) {
-  extern __shared__ unsigned sh_stats[];
-  stats_block_begin(P, sh_stats);
+  const BlockShared sh = block_shared_begin(S, P);
   const int lane = threadIdx.x & (G - 1);
   const unsigned gm = group_mask<G>();
   const int live = *n_live;
@@ -701,7 +757,7 @@ __global__ void __launch_bounds__(256) step_kernel(DevSystem S, DevSim P, SlotBu
         }
         start_trajectory(P, id, tr);
       }
-      const int st = bd_step<FT, G, TORQUE>(S, P, tr, lane, gm, tl, sh_stats);
+      const int st = bd_step<FT, G, TORQUE>(S, P, tr, lane, gm, tl, sh.stats, sh.v);
       if (st != ST_RUNNING) {
         tr.status = st;
         if (lane == 0) {
@@ -724,14 +780,14 @@ __global__ void __launch_bounds__(256) step_kernel(DevSystem S, DevSim P, SlotBu
   }
   // Only lane 0 of each group counts scalar events.
   flush_tally(P, tl, lane == 0);
-  stats_block_end(P, sh_stats);
+  stats_block_end(P, sh.stats);
 }
 
 // All forces of the lanes with `need`, one trajectory at a time, the whole warp
 // sweeping that trajectory's ligand atoms and receptor chunks.
 template <typename FT, bool TORQUE>
 __device__ __forceinline__ void warp_forces(const DevSystem& S, const double c[3], const double R[9], bool need,
-                                            double F[3], double T[3], int lane, Counts& cnt) {
+                                            double F[3], double T[3], int lane, Counts& cnt, const RecView& v) {
   const unsigned FULL = 0xffffffffu;
   unsigned m = __ballot_sync(FULL, need);
   while (m) {
@@ -743,7 +799,7 @@ __device__ __forceinline__ void warp_forces(const DevSystem& S, const double c[3
 #pragma unroll
     for (int k = 0; k < 9; ++k) Rj[k] = __shfl_sync(FULL, R[k], j);
     double f[3], t[3], e;
-    group_forces<FT, 32, TORQUE, false>(S, cj, Rj, lane, FULL, PosFromPose{Rj, cj}, f, t, e, cnt);
+    group_forces<FT, 32, TORQUE, false>(S, cj, Rj, lane, FULL, PosFromPose{Rj, cj}, f, t, e, cnt, v);
     if (lane == j) {
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
@@ -755,7 +811,8 @@ __device__ __forceinline__ void warp_forces(const DevSystem& S, const double c[3
 }
 
 // Overlap test of every lane with `need`, the warp sweeping the receptor chunks together.
-__device__ __forceinline__ bool warp_overlap(const DevSystem& S, const double cn[3], bool need, int lane) {
+__device__ __forceinline__ bool warp_overlap(const DevSystem& S, const double cn[3], bool need, int lane,
+                                             const RecView& v) {
   const unsigned FULL = 0xffffffffu;
   unsigned m = __ballot_sync(FULL, need);
   bool mine = false;
@@ -765,7 +822,7 @@ __device__ __forceinline__ bool warp_overlap(const DevSystem& S, const double cn
     double cj[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) cj[k] = __shfl_sync(FULL, cn[k], j);
-    const bool hit = overlap_any<32>(S, cj, lane, FULL);
+    const bool hit = overlap_any<32>(S, cj, lane, FULL, v);
     if (lane == j) mine = hit;
   }
   return mine;
@@ -803,8 +860,7 @@ __device__ __forceinline__ void warp_refill(const DevSim& P, Traj& tr, bool& dea
 template <typename FT, bool TORQUE, int MINB>
 __global__ void __launch_bounds__(256, MINB) step_kernel_warp(DevSystem S, DevSim P, SlotBuf B,
                                                               const int* __restrict__ n_live, int K) {
-  extern __shared__ unsigned sh_stats[];
-  stats_block_begin(P, sh_stats);
+  const BlockShared sh = block_shared_begin(S, P);
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int live = *n_live;
@@ -834,7 +890,7 @@ __global__ void __launch_bounds__(256, MINB) step_kernel_warp(DevSystem S, DevSi
       }
       const bool need_f = !dead && st == ST_RUNNING;
       double F[3] = {0, 0, 0}, T[3] = {0, 0, 0};
-      warp_forces<FT, TORQUE>(S, tr.c, R, need_f, F, T, lane, tl.cnt);
+      warp_forces<FT, TORQUE>(S, tr.c, R, need_f, F, T, lane, tl.cnt, sh.v);
       double cn[3] = {0, 0, 0}, qn[4] = {1, 0, 0, 0}, dt = 0;
       bool ok = true;
       if (need_f) ok = step_move<FT>(P, key, s, tr, r, F, T, cn, qn, dt);
@@ -842,12 +898,12 @@ __global__ void __launch_bounds__(256, MINB) step_kernel_warp(DevSystem S, DevSi
         tl.nonfinite += 1;
         st = ST_ERROR;
       }
-      const bool ovl = warp_overlap(S, cn, need_f && ok && P.overlap, lane);
+      const bool ovl = warp_overlap(S, cn, need_f && ok && P.overlap, lane, sh.v);
       if (need_f && ok) {
         const double c0[3] = {tr.c[0], tr.c[1], tr.c[2]};
         st = step_end(S, P, key, s, tr, R, cn, qn, !ovl, dt, tl);
         if (P.stats) {
-          stats_step(S, P, tr, s, r_prev, dt, c0, R, sh_stats);
+          stats_step(S, P, tr, s, r_prev, dt, c0, R, sh.stats);
           if (st == ST_REACTED) stats_encounter(P, tr, s, true);
         }
       }
@@ -866,7 +922,7 @@ __global__ void __launch_bounds__(256, MINB) step_kernel_warp(DevSystem S, DevSi
     if (own) store_slot(B, slot, tr);
   }
   flush_tally(P, tl, true);
-  stats_block_end(P, sh_stats);
+  stats_block_end(P, sh.stats);
 }
 
 // Sum the per-thread tallies of a warp and add them to the device counters.
