@@ -128,7 +128,7 @@ class _MP:
         self.dipole, self.quadrupole, self.four_pi_eps = s.multipole_moments()
 
 
-_OPTS = {"stage_receptor": True}
+_OPTS = {"layout": None}
 
 
 def make_sim(s, precision, n_traj, K, id_offset=0, torque="zero"):
@@ -136,11 +136,10 @@ def make_sim(s, precision, n_traj, K, id_offset=0, torque="zero"):
     from pystarc_b200.simulator import B200BatchSimulator
 
     eng = B200ForceEngine(**s.engine_kwargs(), multipole_expansion=_MP(s), precision=precision, torque_mode=torque,
-                          device=int(os.environ.get("LOCAL_RANK", 0)))
+                          device=int(os.environ.get("LOCAL_RANK", 0)), layout=_OPTS["layout"])
     mol1, mol2 = s.molecules()
     sim = B200BatchSimulator(mol1, mol2, s.mobility(), s.pathway_set(), s.params(n_traj=n_traj), eng,
-                             termination="complete", steps_per_launch=K, id_offset=id_offset,
-                             stage_receptor=_OPTS["stage_receptor"])
+                             termination="complete", steps_per_launch=K, id_offset=id_offset)
     return sim
 
 
@@ -187,8 +186,10 @@ def time_device_arm(s, precision, steps, warmup, K, n_traj, id_offset, dist, fix
     g = np.zeros(3, dtype=np.int32)
     h.call("bd_get_launch", _lib.ptr(g[0:1], _lib.C.c_int32), _lib.ptr(g[1:2], _lib.C.c_int32),
            _lib.ptr(g[2:3], _lib.C.c_int32))
+    lay = np.zeros(1, dtype=np.int32)
+    h.call("bd_get_layout", _lib.ptr(lay, _lib.C.c_int32))
     sim.engine.close()
-    launch = {"group": int(g[0]), "block": int(g[1]), "grid": int(g[2]),
+    launch = {"group": int(g[0]), "block": int(g[1]), "grid": int(g[2]), "layout_flags": int(lay[0]),
               "autotune_steps_per_s": {f"{a}x{b}": round(v) for (a, b), v in table.items()}}
     return sum(times), times, d, launch
 
@@ -288,10 +289,12 @@ def main():
     ap.add_argument("--workload", default="protein-ligand", choices=sorted(WORKLOADS))
     ap.add_argument("--launch", default="", help="fixed launch shape GROUPxBLOCK (default: autotune)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-stage", action="store_true", help="keep the receptor table in global memory only")
+    ap.add_argument("--layout", type=int, default=-1,
+                    help="device data layout flags (1 stage receptor, 2 windows for 1-channel grids, "
+                         "4 windows for the paired grid; -1: library default)")
     ap.add_argument("--cpu-steps", type=int, default=40)
     args = ap.parse_args()
-    _OPTS["stage_receptor"] = not args.no_stage
+    _OPTS["layout"] = None if args.layout < 0 else args.layout
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -374,7 +377,7 @@ def main():
         "config": {"workload": WORKLOADS[args.workload][0], "trajectories_per_gpu": n_traj,
                    "bd_steps_per_launch": args.inner,
                    "parallelism": f"trajectory shards x{world}", "l2": "flushed (256 MiB write) between launches",
-                   "launch": launch, "receptor_staged_in_smem": _OPTS["stage_receptor"]},
+                   "launch": launch},
         "variants": {
             "mixed": {"bd_steps_per_s": d_mixed["steps"] / t_mixed, "steps": d_mixed["steps"]},
             "fp64": {"bd_steps_per_s": d_fp64["steps"] / t_fp64, "steps": d_fp64["steps"], "launch": launch64},

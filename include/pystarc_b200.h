@@ -166,14 +166,22 @@ enum { BD_GROUP_WARP = 64, BD_GROUP_WARP_CAPPED = 65 };
 int bd_set_launch(BdHandle* h, int group, int block_threads);
 int bd_get_launch(BdHandle* h, int* group, int* block_threads, int* grid_blocks);
 
-/* Receptor staging of the stepper kernels: BD_STAGE_AUTO (default) copies an FP32 receptor
- * table of at most BD_STAGE_MAX_BYTES (atoms + chunk spheres) into each block's shared memory
- * for the sweeps' distance pre-tests; BD_STAGE_OFF reads the FP64 table from global memory
- * only.  Every accept/reject decision is taken in FP64 either way, so trajectories are the
- * same bit for bit. */
-enum { BD_STAGE_OFF = 0, BD_STAGE_AUTO = 1 };
+/* Device data layout (bit flags, default BD_LAYOUT_DEFAULT; applied when the device system
+ * is next built, i.e. at the next configure or force evaluation):
+ * BD_LAYOUT_STAGE_RECEPTOR: the stepper kernels copy an FP32 receptor table of at most
+ *   BD_STAGE_MAX_BYTES (atoms + chunk spheres) into each block's shared memory for the
+ *   sweeps' distance pre-tests; every accept/reject is still decided in FP64.
+ * BD_LAYOUT_WINDOWS_1: each single-channel grid (ligand Born grid, unpaired receptor grids)
+ *   gets a float4 copy whose entry n holds nodes n..n+3 of node n's z row, so one force
+ *   stencil is 8 vector loads instead of 20 scalar ones (4x the grid's memory).
+ * BD_LAYOUT_WINDOWS_2: the interleaved elec+Born grid gets a float4 copy whose entry n holds
+ *   both channels of nodes n and n+1: 12 loads per stencil instead of 20 (2x its memory).
+ * The same values enter the same arithmetic in every layout: results are identical. */
+enum { BD_LAYOUT_STAGE_RECEPTOR = 1, BD_LAYOUT_WINDOWS_1 = 2, BD_LAYOUT_WINDOWS_2 = 4 };
+#define BD_LAYOUT_DEFAULT (BD_LAYOUT_WINDOWS_1 | BD_LAYOUT_WINDOWS_2)
 #define BD_STAGE_MAX_BYTES (64 * 1024)
-int bd_set_stage_receptor(BdHandle* h, int mode);
+int bd_set_layout(BdHandle* h, int flags);
+int bd_get_layout(BdHandle* h, int* flags);
 
 /* No counterpart in the reference.  Runs p->n_traj trajectories to completion (or for
  * max_launches launches of steps_per_launch steps) on the handle's system WITHOUT

@@ -19,6 +19,8 @@ TORQUE_ZERO, TORQUE_CENTROID = 0, 1
 CTR_NAMES = ("started", "reacted", "escaped", "max_steps", "steps", "returns", "overlap", "bridge", "grid_evals",
              "rev_evals", "ff_evals", "nonfinite")
 N_CTR = len(CTR_NAMES)
+LAYOUT_STAGE_RECEPTOR, LAYOUT_WINDOWS_1, LAYOUT_WINDOWS_2 = 1, 2, 4
+LAYOUT_DEFAULT = LAYOUT_WINDOWS_1 | LAYOUT_WINDOWS_2
 
 _ERR_NAMES = {BD_ERR_ARG: "bad argument", BD_ERR_CUDA: "CUDA error", BD_ERR_OOM: "out of device memory",
               BD_ERR_NAN: "non-finite value", BD_ERR_STALL: "device watchdog", BD_ERR_STATE: "call out of order"}
@@ -89,7 +91,8 @@ SIGNATURES = {
     "bd_sim_restore": (C.c_int, [P, dp, dp, i32p, i32p, i32p, i8p, C.c_int32, u64p, i8p, i32p, i32p]),
     "bd_set_launch": (C.c_int, [P, C.c_int, C.c_int]),
     "bd_get_launch": (C.c_int, [P, i32p, i32p, i32p]),
-    "bd_set_stage_receptor": (C.c_int, [P, C.c_int]),
+    "bd_set_layout": (C.c_int, [P, C.c_int]),
+    "bd_get_layout": (C.c_int, [P, i32p]),
     "bd_sim_run_noalloc": (C.c_int, [P, C.POINTER(BdSimParams), P, P, P, P, C.c_int, C.c_int, P]),
 }
 

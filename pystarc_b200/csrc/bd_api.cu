@@ -56,7 +56,7 @@ struct BdHandle {
   std::vector<void*> sim_allocs;
   int group = 8, block = 128;
   bool launch_user = false;
-  int stage_mode = BD_STAGE_AUTO;
+  int layout = BD_LAYOUT_DEFAULT;
   // graphs: [cur][steps] cache
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   int graph_K = -1, graph_G = -1, graph_B = -1, graph_prec = -1, graph_torque = -1;
@@ -133,6 +133,18 @@ int upload_floats(BdHandle* h, const float* src, size_t n, const float** out) {
   return BD_OK;
 }
 
+// Window copy of an uploaded grid for the vector stencil loads (DevGrid::win).
+int add_window(BdHandle* h, DevGrid& g) {
+  const long n = (long)g.nx * g.ny * g.nz;
+  void* p = nullptr;
+  int rc = dev_alloc(h, h->sys_allocs, &p, (size_t)n * sizeof(float4));
+  if (rc) return rc;
+  window_kernel<<<h->n_sm * 8, 256>>>(g.data, (float4*)p, n, g.nz, g.ch);
+  CK(h, cudaGetLastError());
+  g.win = (const float4*)p;
+  return BD_OK;
+}
+
 bool same_lattice(const GridHost& a, const GridHost& b) {
   for (int i = 0; i < 3; ++i)
     if (a.n[i] != b.n[i] || a.o[i] != b.o[i] || a.sp[i] != b.sp[i]) return false;
@@ -199,6 +211,14 @@ int finalize(BdHandle* h) {
       S.paired = 1;
     }
   }
+  if (h->layout & BD_LAYOUT_WINDOWS_1) {
+    for (int k = 0; k < S.n_elec; ++k)
+      if (int rc = add_window(h, S.elec[k])) return rc;
+    if (S.has_born)
+      if (int rc = add_window(h, S.born)) return rc;
+  }
+  if (S.paired && (h->layout & BD_LAYOUT_WINDOWS_2))
+    if (int rc = add_window(h, S.pair)) return rc;
   // ligand
   const int nl = (int)(h->lig.size() / 4);
   S.n_lig = nl;
@@ -282,7 +302,8 @@ int finalize(BdHandle* h) {
     if (rc) return rc;
     CK(h, cudaMemcpy(p, cf.data(), cf.size() * sizeof(float), cudaMemcpyHostToDevice));
     S.chunks_f = (const float4*)p;
-    S.rec_in_smem = h->stage_mode == BD_STAGE_AUTO && (size_t)(S.n_rec_pad + nc) * sizeof(float4) <= BD_STAGE_MAX_BYTES;
+    S.rec_in_smem = (h->layout & BD_LAYOUT_STAGE_RECEPTOR) &&
+                    (size_t)(S.n_rec_pad + nc) * sizeof(float4) <= BD_STAGE_MAX_BYTES;
   }
   // Born direction 2 needs the ligand Born grid, receptor atoms and alpha > 1e-12 (gpu_batch_engine.py:583-590)
   if (!lb.empty() && nr > 0 && fp.alpha > 1e-12) {
@@ -290,6 +311,8 @@ int finalize(BdHandle* h) {
     int rc = upload_floats(h, lb[0].data.data(), lb[0].data.size(), &p);
     if (rc) return rc;
     grid_to_dev(lb[0], p, 1, S.lig_born);
+    if (h->layout & BD_LAYOUT_WINDOWS_1)
+      if ((rc = add_window(h, S.lig_born))) return rc;
     S.born_rev = 1;
     const DevGrid& g = S.lig_born;
     const double mx = std::max(std::fabs(g.lox), std::fabs(g.hix)), my = std::max(std::fabs(g.loy), std::fabs(g.hiy)),
@@ -307,6 +330,7 @@ int finalize(BdHandle* h) {
     S.rx_cut[p] = h->rx_cut[p];
     S.rx_deff[p] = h->rx_deff[p];
   }
+  CK(h, cudaDeviceSynchronize());  // window copies are built on the legacy stream
   h->S = S;
   h->dirty = false;
   h->graph_K = -1;  // system changed: rebuild graphs
@@ -590,13 +614,20 @@ int bd_set_launch(BdHandle* h, int group, int block) {
   return BD_OK;
 }
 
-int bd_set_stage_receptor(BdHandle* h, int mode) {
+int bd_set_layout(BdHandle* h, int flags) {
   if (!h) return BD_ERR_ARG;
-  if (mode != BD_STAGE_OFF && mode != BD_STAGE_AUTO) return fail(h, BD_ERR_ARG, "stage mode must be 0 (off) or 1 (auto)");
-  h->stage_mode = mode;
-  const bool fits = (size_t)(h->S.n_rec_pad + h->S.n_chunks) * sizeof(float4) <= BD_STAGE_MAX_BYTES;
-  if (!h->dirty) h->S.rec_in_smem = mode == BD_STAGE_AUTO && h->S.rec_f && fits;
-  h->graph_K = -1;
+  const int all = BD_LAYOUT_STAGE_RECEPTOR | BD_LAYOUT_WINDOWS_1 | BD_LAYOUT_WINDOWS_2;
+  if (flags & ~all) return fail(h, BD_ERR_ARG, "unknown layout flags 0x%x", flags & ~all);
+  if (flags != h->layout) {
+    h->layout = flags;
+    h->dirty = true;  // rebuilt by the next configure or evaluation
+  }
+  return BD_OK;
+}
+
+int bd_get_layout(BdHandle* h, int* flags) {
+  if (!h || !flags) return BD_ERR_ARG;
+  *flags = h->layout;
   return BD_OK;
 }
 

@@ -40,6 +40,7 @@ enum : int {
 
 struct DevGrid {
   const float* data;  // FP32 values; `ch` interleaved channels per node
+  const float4* win;  // optional: entry n = nodes n .. n + 4/ch - 1 of node n's z row, all channels
   int nx, ny, nz, ch;
   double ox, oy, oz;
   double isx, isy, isz;  // 1/spacing
@@ -294,27 +295,74 @@ __device__ __forceinline__ StencilOut<FT, CH> stencil(const DevGrid& g, double x
   const int zb = lz ? cz - 1 : cz;
   const int zc = lz ? 1 : 0;  // position of node cz inside the three-node run
   const int ze = lz ? 0 : 2;  // position of the extra z node
-  float r[2][2][3][CH];
+  float r[2][2][3][CH], xe[2][2][CH], ye[2][2][CH];
+  if (g.win) {
+    // window copy: one 16-byte load per z run (two for a 3-node run of two channels)
+    const float4* w = g.win;
 #pragma unroll
-  for (int i = 0; i < 2; ++i)
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const long n = (long)(cx + i) * syz + (long)(cy + j) * nz + zb;
+        const float4 t = __ldg(w + n);
+        if constexpr (CH == 1) {
+          r[i][j][0][0] = t.x;
+          r[i][j][1][0] = t.y;
+          r[i][j][2][0] = t.z;
+        } else {
+          const float4 u = __ldg(w + n + 2);
+          r[i][j][0][0] = t.x;
+          r[i][j][0][1] = t.y;
+          r[i][j][1][0] = t.z;
+          r[i][j][1][1] = t.w;
+          r[i][j][2][0] = u.x;
+          r[i][j][2][1] = u.y;
+        }
+      }
+    float4 tx[2], ty[2];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) tx[j] = __ldg(w + (long)ex * syz + (long)(cy + j) * nz + cz);
+#pragma unroll
+    for (int i = 0; i < 2; ++i) ty[i] = __ldg(w + (long)(cx + i) * syz + (long)ey * nz + cz);
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
-      const long base = ((long)(cx + i) * syz + (long)(cy + j) * nz + zb) * CH;
-#pragma unroll
-      for (int k = 0; k < 3; ++k) ld<CH>(d + base + k * CH, r[i][j][k]);
+      if constexpr (CH == 1) {
+        xe[j][0][0] = tx[j].x;
+        xe[j][1][0] = tx[j].y;
+        ye[j][0][0] = ty[j].x;
+        ye[j][1][0] = ty[j].y;
+      } else {
+        xe[j][0][0] = tx[j].x;
+        xe[j][0][1] = tx[j].y;
+        xe[j][1][0] = tx[j].z;
+        xe[j][1][1] = tx[j].w;
+        ye[j][0][0] = ty[j].x;
+        ye[j][0][1] = ty[j].y;
+        ye[j][1][0] = ty[j].z;
+        ye[j][1][1] = ty[j].w;
+      }
     }
-  float xe[2][2][CH], ye[2][2][CH];
+  } else {
 #pragma unroll
-  for (int j = 0; j < 2; ++j) {
-    const long base = ((long)ex * syz + (long)(cy + j) * nz + cz) * CH;
-    ld<CH>(d + base, xe[j][0]);
-    ld<CH>(d + base + CH, xe[j][1]);
-  }
+    for (int i = 0; i < 2; ++i)
 #pragma unroll
-  for (int i = 0; i < 2; ++i) {
-    const long base = ((long)(cx + i) * syz + (long)ey * nz + cz) * CH;
-    ld<CH>(d + base, ye[i][0]);
-    ld<CH>(d + base + CH, ye[i][1]);
+      for (int j = 0; j < 2; ++j) {
+        const long base = ((long)(cx + i) * syz + (long)(cy + j) * nz + zb) * CH;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) ld<CH>(d + base + k * CH, r[i][j][k]);
+      }
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const long base = ((long)ex * syz + (long)(cy + j) * nz + cz) * CH;
+      ld<CH>(d + base, xe[j][0]);
+      ld<CH>(d + base + CH, xe[j][1]);
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const long base = ((long)(cx + i) * syz + (long)ey * nz + cz) * CH;
+      ld<CH>(d + base, ye[i][0]);
+      ld<CH>(d + base + CH, ye[i][1]);
+    }
   }
   const FT wx[2] = {(FT)1 - sx, sx}, wy[2] = {(FT)1 - sy, sy}, wz[2] = {(FT)1 - sz, sz};
   StencilOut<FT, CH> o;

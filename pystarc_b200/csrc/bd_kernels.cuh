@@ -719,6 +719,21 @@ __device__ __forceinline__ int group_fetch(unsigned long long* p, int lane, unsi
   return v > 0x7fffffffull ? 0x7fffffff : (int)v;
 }
 
+// Window copy of a grid (DevGrid::win): entry n holds nodes n .. n + 4/ch - 1 of
+// node n's z row, all `ch` channels of each, zero past the end of the row.
+__global__ void window_kernel(const float* __restrict__ d, float4* __restrict__ w, long n_nodes, int nz, int ch) {
+  for (long n = blockIdx.x * (long)blockDim.x + threadIdx.x; n < n_nodes; n += (long)gridDim.x * blockDim.x) {
+    const int z = (int)(n % nz);
+    float v[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int node = k / ch, c = k % ch;
+      v[k] = z + node < nz ? d[(n + node) * ch + c] : 0.f;
+    }
+    w[n] = make_float4(v[0], v[1], v[2], v[3]);
+  }
+}
+
 // Fill `n_slots` slots with the first trajectories of the pending pool.
 __global__ void init_slots_kernel(DevSim P, SlotBuf B, int n_slots) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;

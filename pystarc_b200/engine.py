@@ -66,7 +66,7 @@ class B200ForceEngine:
     def __init__(self, elec_grids, born_grids, alpha: float = 0.07957747, receptor_charge: float = 0.0,
                  debye_length: float = 7.858, sdie: float = 78.0, lig_born_grids=None, rec_positions=None,
                  rec_charges=None, multipole_expansion=None, rec_radii=None, lig_radii=None, use_lj=False, *,
-                 precision: str = "fp64", torque_mode: str = "zero", device: int = 0):
+                 precision: str = "fp64", torque_mode: str = "zero", device: int = 0, layout=None):
         if use_lj:
             raise NotImplementedError("WCA contact forces (use_lj=True) are not implemented by this engine")
         if precision not in PRECISIONS or torque_mode not in TORQUES:
@@ -82,6 +82,8 @@ class B200ForceEngine:
         self.precision = precision
         self.torque_mode = torque_mode
         self.handle = EngineHandle(device)
+        if layout is not None:  # bit flags of the device data layout (identical results in every layout)
+            self.handle.call("bd_set_layout", int(layout))
         elec = sorted(list(elec_grids or []), key=_sp)
         born = sorted(list(born_grids or []), key=_sp)
         if self._has_yukawa and len(elec) > 1:

@@ -119,7 +119,7 @@ class B200BatchSimulator:
 
     def __init__(self, mol1, mol2, mob, pathway_set, params, batch_engine, *, precision=None, torque_mode=None,
                  termination="reference", steps_per_launch=64, launches_per_poll=8, slots=0, id_offset=0,
-                 stats=None, stage_receptor=True, verbose=False):
+                 stats=None, verbose=False):
         if not hasattr(batch_engine, "handle"):
             raise TypeError("batch_engine must be a B200ForceEngine")
         if any(getattr(r, "state_before", None) is not None for r in pathway_set.reactions):
@@ -137,8 +137,6 @@ class B200BatchSimulator:
         self.id_offset = int(id_offset)
         # per-step statistics for write_all: on when the pipeline attached an output config
         self.stats = bool(getattr(params, "_output_cfg", None) is not None) if stats is None else bool(stats)
-        # FP32 receptor copy in shared memory for the sweeps' pre-tests (same results either way)
-        self.stage_receptor = bool(stage_receptor)
         self.verbose = verbose
         c0 = np.asarray(mol2.centroid(), dtype=float)
         self._mol2_pos0 = np.asarray(mol2.positions_array(), dtype=float) - c0
@@ -207,7 +205,6 @@ class B200BatchSimulator:
         sp.slots = self.slots
         sp.id_offset = self.id_offset
         sp.stats = int(self.stats)
-        h.call("bd_set_stage_receptor", 1 if self.stage_receptor else 0)
         h.call("bd_sim_configure", _lib.C.byref(sp))
         return D_t
 

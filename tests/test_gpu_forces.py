@@ -18,11 +18,11 @@ class _MP:
         self.dipole, self.quadrupole, self.four_pi_eps = s.multipole_moments()
 
 
-def make_engine(s, precision="fp64", torque="zero"):
+def make_engine(s, precision="fp64", torque="zero", layout=None):
     from pystarc_b200.engine import B200ForceEngine
 
     eng = B200ForceEngine(**s.engine_kwargs(), multipole_expansion=_MP(s) if s.multipole else None,
-                          precision=precision, torque_mode=torque)
+                          precision=precision, torque_mode=torque, layout=layout)
     eng.set_ligand(s.lig_pos - s.lig_pos.mean(axis=0), s.lig_q)
     return eng
 
@@ -75,6 +75,24 @@ def test_random_poses_against_oracle(sysname, precision, tol):
     escale = np.maximum(np.abs(Eo), 1e-3 * np.abs(Eo).max() + 1e-300)
     assert np.max(np.abs(E - Eo) / escale) < max(tol, 1e-9) * 10
     eng.close()
+
+
+@pytest.mark.parametrize("sysname", ["c2", "c3"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_grid_windows_give_identical_forces(sysname, precision):
+    """Window copies (vector loads) and plain scalar loads feed the same values to the same arithmetic."""
+    from pystarc_b200 import _lib
+
+    s = system(sysname)
+    c, q = random_poses(2000, 0.5, 35.0, 5)
+    out = []
+    for layout in (0, _lib.LAYOUT_WINDOWS_1, _lib.LAYOUT_WINDOWS_2, _lib.LAYOUT_DEFAULT):
+        eng = make_engine(s, precision, "centroid", layout=layout)
+        out.append(eng.eval_poses(c, q))
+        eng.close()
+    for other in out[1:]:
+        for x, y in zip(out[0], other):
+            np.testing.assert_array_equal(x, y)
 
 
 @pytest.mark.parametrize("group", [1, 4, 8, 16, 32, 64, 65])
