@@ -107,7 +107,7 @@ class Clocks:
 
 
 WORKLOADS = {
-    "protein-ligand": ("protein+small-ligand (3200/18 atoms, 193^3+129^3 grids, 1e6 trajectories)", 1_000_000),
+    "protein-ligand": ("protein+small-ligand (3200/18 atoms, 193^3 elec+Born grids, 65^3 ligand Born grid, 1e6 trajectories)", 1_000_000),
     "two-spheres": ("two charged spheres (+5/-5 e, 129^3 grid, 1e5 trajectories, FP64 physics)", 100_000),
     "protein-protein": ("protein-protein (1700/1400 atoms, 3 x 161^3 grids, HI, 1e7 trajectories)", 10_000_000),
 }

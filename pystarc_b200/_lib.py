@@ -20,7 +20,7 @@ CTR_NAMES = ("started", "reacted", "escaped", "max_steps", "steps", "returns", "
              "rev_evals", "ff_evals", "nonfinite")
 N_CTR = len(CTR_NAMES)
 LAYOUT_STAGE_RECEPTOR, LAYOUT_WINDOWS_1, LAYOUT_WINDOWS_2 = 1, 2, 4
-LAYOUT_DEFAULT = LAYOUT_WINDOWS_1 | LAYOUT_WINDOWS_2
+LAYOUT_DEFAULT = LAYOUT_WINDOWS_1
 
 _ERR_NAMES = {BD_ERR_ARG: "bad argument", BD_ERR_CUDA: "CUDA error", BD_ERR_OOM: "out of device memory",
               BD_ERR_NAN: "non-finite value", BD_ERR_STALL: "device watchdog", BD_ERR_STATE: "call out of order"}

@@ -101,6 +101,87 @@ struct PosFromAtoms {
   }
 };
 
+// Reverse Born (direction 2) of one trajectory by a whole warp.  Receptor
+// chunks are culled against the ligand Born grid's margin box in the ligand
+// frame; the in-box atoms of the surviving chunks are queued in a per-warp ring
+// in shared memory and interpolated 32 at a time, so the stencil runs on full
+// warps however sparsely a chunk overlaps the box.  Which atoms contribute is
+// decided exactly as in the per-chunk sweep (FP64 rotation, strict margin box).
+// Blocks have at most 256 threads (every caller's launch bound): 8 rings.
+constexpr int kRevRing = 64;  // > 31 pending + 32 new candidates
+
+template <typename FT, bool TORQUE>
+__device__ __forceinline__ void warp_reverse_born(const DevSystem& S, const double c[3], const double R[9], int lane,
+                                                  double r[3], double u[3], unsigned& nr) {
+  __shared__ double4 rings[8][kRevRing];
+  double4* ring = rings[threadIdx.x >> 5];
+  const unsigned FULL = 0xffffffffu;
+  const DevGrid& g = S.lig_born;
+  const FT alpha = (FT)S.alpha;
+  unsigned head = 0, tail = 0;  // warp-uniform ring cursors
+  auto drain = [&](unsigned count) {
+    if ((unsigned)lane < count) {
+      const double4 e = ring[(tail + lane) % kRevRing];
+      const StencilOut<FT, 1> st = stencil<FT, 1>(g, e.x, e.y, e.z);
+      const FT qr = (FT)e.w;
+      const FT cf = -alpha * qr * qr;
+      const FT g0 = cf * st.gx[0], g1 = cf * st.gy[0], g2 = cf * st.gz[0];
+      r[0] += (double)g0;
+      r[1] += (double)g1;
+      r[2] += (double)g2;
+      if (TORQUE) {
+        u[0] += e.y * (double)g2 - e.z * (double)g1;
+        u[1] += e.z * (double)g0 - e.x * (double)g2;
+        u[2] += e.x * (double)g1 - e.y * (double)g0;
+      }
+      nr += 1;
+    }
+    tail += count;
+  };
+  for (int k0 = 0; k0 < S.n_chunks; k0 += 32) {
+    const int k = k0 + lane;
+    bool hit = false;
+    if (k < S.n_chunks) {
+      const double4 sp = S.chunks[k];
+      const double d0 = sp.x - c[0], d1 = sp.y - c[1], d2 = sp.z - c[2];
+      const double l0 = R[0] * d0 + R[3] * d1 + R[6] * d2;
+      const double l1 = R[1] * d0 + R[4] * d1 + R[7] * d2;
+      const double l2 = R[2] * d0 + R[5] * d1 + R[8] * d2;
+      const double ex = fmax(fmax(g.lox - l0, l0 - g.hix), 0.0);
+      const double ey = fmax(fmax(g.loy - l1, l1 - g.hiy), 0.0);
+      const double ez = fmax(fmax(g.loz - l2, l2 - g.hiz), 0.0);
+      const double lim = sp.w + 1e-9;  // the radius is already inflated against rounding
+      hit = ex * ex + ey * ey + ez * ez < lim * lim;
+    }
+    unsigned hits = __ballot_sync(FULL, hit);
+    while (hits) {
+      const int kk = k0 + __ffs(hits) - 1;
+      hits &= hits - 1;
+      const double4 at = S.rec[kk * BD_CHUNK + lane];
+      double l0 = 0, l1 = 0, l2 = 0;
+      bool cand = false;
+      if (fabs(at.w) >= 1e-9) {
+        const double d0 = at.x - c[0], d1 = at.y - c[1], d2 = at.z - c[2];
+        l0 = R[0] * d0 + R[3] * d1 + R[6] * d2;
+        l1 = R[1] * d0 + R[4] * d1 + R[7] * d2;
+        l2 = R[2] * d0 + R[5] * d1 + R[8] * d2;
+        cand = in_box(g, l0, l1, l2);
+      }
+      const unsigned m = __ballot_sync(FULL, cand);
+      if (cand) ring[(head + __popc(m & ((1u << lane) - 1u))) % kRevRing] = make_double4(l0, l1, l2, at.w);
+      head += __popc(m);
+      if (head - tail >= 32) {
+        __syncwarp();
+        drain(32);
+        __syncwarp();
+      }
+    }
+  }
+  __syncwarp();
+  drain(head - tail);
+  __syncwarp();  // the ring is reused by the next call
+}
+
 // Net force, torque (about c) and energy on the ligand of one trajectory,
 // computed cooperatively by the G lanes of a group.  Follows
 // GPUBatchForceEngine.__call__ (pystarc/forces/gpu_batch_engine.py:531-605):
@@ -177,7 +258,18 @@ __device__ void group_forces(const DevSystem& S, const double c[3], const double
   // Lanes test G receptor chunks at a time against the box's circumsphere, then
   // sweep the hit chunks' atoms together.
   double r0 = 0, r1 = 0, r2 = 0, u0 = 0, u1 = 0, u2 = 0;
-  if (S.born_rev) {
+  if constexpr (G == 32) {
+    if (S.born_rev && norm3(c[0], c[1], c[2]) - S.rec_max_r < S.lig_born_rho) {
+      double rr[3] = {0, 0, 0}, uu[3] = {0, 0, 0};
+      warp_reverse_born<FT, TORQUE>(S, c, R, lane, rr, uu, nr);
+      r0 = rr[0];
+      r1 = rr[1];
+      r2 = rr[2];
+      u0 = uu[0];
+      u1 = uu[1];
+      u2 = uu[2];
+    }
+  } else if (S.born_rev) {
     const double rho = S.lig_born_rho;
     if (norm3(c[0], c[1], c[2]) - S.rec_max_r < rho) {
       const double rho2 = rho * rho;
