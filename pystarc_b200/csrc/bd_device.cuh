@@ -277,18 +277,23 @@ __device__ __forceinline__ void ld(const float* p, float v[CH]) {
   }
 }
 
-template <typename FT, int CH>
-__device__ __forceinline__ StencilOut<FT, CH> stencil(const DevGrid& g, double x, double y, double z) {
-  const double ux = (x - g.ox) * g.isx, uy = (y - g.oy) * g.isy, uz = (z - g.oz) * g.isz;
-  const double fx = floor(ux), fy = floor(uy), fz = floor(uz);
+// PT is the type of the position and of the cell/fraction arithmetic: double
+// everywhere except the mixed-precision reverse-Born sweep, which hands in FP32
+// ligand-frame coordinates (the interpolant is continuous, so an FP32 position
+// only moves the result by its own rounding).
+template <typename FT, int CH, typename PT = double>
+__device__ __forceinline__ StencilOut<FT, CH> stencil(const DevGrid& g, PT x, PT y, PT z) {
+  const PT ux = (x - (PT)g.ox) * (PT)g.isx, uy = (y - (PT)g.oy) * (PT)g.isy, uz = (z - (PT)g.oz) * (PT)g.isz;
+  const PT fx = floor(ux), fy = floor(uy), fz = floor(uz);
   const int cx = (int)fx, cy = (int)fy, cz = (int)fz;
-  const double sxd = ux - fx, syd = uy - fy, szd = uz - fz;
-  const bool lx = sxd < 0.5, ly = syd < 0.5, lz = szd < 0.5;
+  const PT sxd = ux - fx, syd = uy - fy, szd = uz - fz;
+  const PT half = (PT)0.5;
+  const bool lx = sxd < half, ly = syd < half, lz = szd < half;
   const int ex = lx ? cx - 1 : cx + 2, ey = ly ? cy - 1 : cy + 2;
   const FT sx = (FT)sxd, sy = (FT)syd, sz = (FT)szd;
-  const FT ax = (FT)(lx ? 0.5 - sxd : sxd - 0.5);
-  const FT ay = (FT)(ly ? 0.5 - syd : syd - 0.5);
-  const FT az = (FT)(lz ? 0.5 - szd : szd - 0.5);
+  const FT ax = (FT)(lx ? half - sxd : sxd - half);
+  const FT ay = (FT)(ly ? half - syd : syd - half);
+  const FT az = (FT)(lz ? half - szd : szd - half);
   const long nz = g.nz, syz = (long)g.ny * g.nz;
   const float* d = g.data;
   // centre rows (cx+i, cy+j): three z nodes starting at zb

@@ -105,24 +105,45 @@ struct PosFromAtoms {
 // chunks are culled against the ligand Born grid's margin box in the ligand
 // frame; the in-box atoms of the surviving chunks are queued in a per-warp ring
 // in shared memory and interpolated 32 at a time, so the stencil runs on full
-// warps however sparsely a chunk overlaps the box.  Which atoms contribute is
-// decided exactly as in the per-chunk sweep (FP64 rotation, strict margin box).
+// warps however sparsely a chunk overlaps the box.
+// Geometry is in FT: FP64 in the FP64 engine; FP32 in mixed precision, where a
+// box decision within 1e-3 A of a face (far above the FP32 rotation error for
+// coordinates of hundreds of A) is taken again in FP64, so the set of
+// contributing atoms is exactly the FP64 one in both modes.
 // Blocks have at most 256 threads (every caller's launch bound): 8 rings.
 constexpr int kRevRing = 64;  // > 31 pending + 32 new candidates
+
+template <typename T>
+struct Vec4;
+template <>
+struct Vec4<float> {
+  using type = float4;
+  static __device__ __forceinline__ float4 make(float a, float b, float c, float d) { return make_float4(a, b, c, d); }
+};
+template <>
+struct Vec4<double> {
+  using type = double4;
+  static __device__ __forceinline__ double4 make(double a, double b, double c, double d) {
+    return make_double4(a, b, c, d);
+  }
+};
 
 template <typename FT, bool TORQUE>
 __device__ __forceinline__ void warp_reverse_born(const DevSystem& S, const double c[3], const double R[9], int lane,
                                                   double r[3], double u[3], unsigned& nr) {
-  __shared__ double4 rings[8][kRevRing];
-  double4* ring = rings[threadIdx.x >> 5];
+  using V4 = typename Vec4<FT>::type;
+  __shared__ V4 rings[8][kRevRing];
+  V4* ring = rings[threadIdx.x >> 5];
   const unsigned FULL = 0xffffffffu;
   const DevGrid& g = S.lig_born;
   const FT alpha = (FT)S.alpha;
+  const FT Rt[9] = {(FT)R[0], (FT)R[1], (FT)R[2], (FT)R[3], (FT)R[4], (FT)R[5], (FT)R[6], (FT)R[7], (FT)R[8]};
+  const FT lox = (FT)g.lox, loy = (FT)g.loy, loz = (FT)g.loz, hix = (FT)g.hix, hiy = (FT)g.hiy, hiz = (FT)g.hiz;
   unsigned head = 0, tail = 0;  // warp-uniform ring cursors
   auto drain = [&](unsigned count) {
     if ((unsigned)lane < count) {
-      const double4 e = ring[(tail + lane) % kRevRing];
-      const StencilOut<FT, 1> st = stencil<FT, 1>(g, e.x, e.y, e.z);
+      const V4 e = ring[(tail + lane) % kRevRing];
+      const StencilOut<FT, 1> st = stencil<FT, 1, FT>(g, e.x, e.y, e.z);
       const FT qr = (FT)e.w;
       const FT cf = -alpha * qr * qr;
       const FT g0 = cf * st.gx[0], g1 = cf * st.gy[0], g2 = cf * st.gz[0];
@@ -130,51 +151,74 @@ __device__ __forceinline__ void warp_reverse_born(const DevSystem& S, const doub
       r[1] += (double)g1;
       r[2] += (double)g2;
       if (TORQUE) {
-        u[0] += e.y * (double)g2 - e.z * (double)g1;
-        u[1] += e.z * (double)g0 - e.x * (double)g2;
-        u[2] += e.x * (double)g1 - e.y * (double)g0;
+        const double x = (double)e.x, y = (double)e.y, z = (double)e.z;
+        u[0] += y * (double)g2 - z * (double)g1;
+        u[1] += z * (double)g0 - x * (double)g2;
+        u[2] += x * (double)g1 - y * (double)g0;
       }
       nr += 1;
     }
     tail += count;
+  };
+  // one hit chunk: lane = atom; in-box atoms go to the ring in lane order
+  auto gather = [&](const double4& at) {
+    FT l0 = 0, l1 = 0, l2 = 0;
+    bool cand = false;
+    if (fabs(at.w) >= 1e-9) {
+      const FT d0 = (FT)(at.x - c[0]), d1 = (FT)(at.y - c[1]), d2 = (FT)(at.z - c[2]);
+      l0 = Rt[0] * d0 + Rt[3] * d1 + Rt[6] * d2;
+      l1 = Rt[1] * d0 + Rt[4] * d1 + Rt[7] * d2;
+      l2 = Rt[2] * d0 + Rt[5] * d1 + Rt[8] * d2;
+      cand = l0 > lox && l0 < hix && l1 > loy && l1 < hiy && l2 > loz && l2 < hiz;
+      if constexpr (sizeof(FT) == 4) {
+        const float m = fminf(fminf(fminf(l0 - lox, hix - l0), fminf(l1 - loy, hiy - l1)),
+                              fminf(l2 - loz, hiz - l2));
+        if (fabsf(m) < 1e-3f) {
+          const double e0 = at.x - c[0], e1 = at.y - c[1], e2 = at.z - c[2];
+          cand = in_box(g, R[0] * e0 + R[3] * e1 + R[6] * e2, R[1] * e0 + R[4] * e1 + R[7] * e2,
+                        R[2] * e0 + R[5] * e1 + R[8] * e2);
+        }
+      }
+    }
+    const unsigned m = __ballot_sync(FULL, cand);
+    if (cand) ring[(head + __popc(m & ((1u << lane) - 1u))) % kRevRing] = Vec4<FT>::make(l0, l1, l2, (FT)at.w);
+    head += __popc(m);
+    if (head - tail >= 32) {
+      __syncwarp();
+      drain(32);
+      __syncwarp();
+    }
   };
   for (int k0 = 0; k0 < S.n_chunks; k0 += 32) {
     const int k = k0 + lane;
     bool hit = false;
     if (k < S.n_chunks) {
       const double4 sp = S.chunks[k];
-      const double d0 = sp.x - c[0], d1 = sp.y - c[1], d2 = sp.z - c[2];
-      const double l0 = R[0] * d0 + R[3] * d1 + R[6] * d2;
-      const double l1 = R[1] * d0 + R[4] * d1 + R[7] * d2;
-      const double l2 = R[2] * d0 + R[5] * d1 + R[8] * d2;
-      const double ex = fmax(fmax(g.lox - l0, l0 - g.hix), 0.0);
-      const double ey = fmax(fmax(g.loy - l1, l1 - g.hiy), 0.0);
-      const double ez = fmax(fmax(g.loz - l2, l2 - g.hiz), 0.0);
-      const double lim = sp.w + 1e-9;  // the radius is already inflated against rounding
+      const FT d0 = (FT)(sp.x - c[0]), d1 = (FT)(sp.y - c[1]), d2 = (FT)(sp.z - c[2]);
+      const FT l0 = Rt[0] * d0 + Rt[3] * d1 + Rt[6] * d2;
+      const FT l1 = Rt[1] * d0 + Rt[4] * d1 + Rt[7] * d2;
+      const FT l2 = Rt[2] * d0 + Rt[5] * d1 + Rt[8] * d2;
+      const FT ex = fmax(fmax(lox - l0, l0 - hix), (FT)0);
+      const FT ey = fmax(fmax(loy - l1, l1 - hiy), (FT)0);
+      const FT ez = fmax(fmax(loz - l2, l2 - hiz), (FT)0);
+      // the radius is inflated against rounding; the extra margin covers FP32 geometry
+      const FT lim = (FT)sp.w + (sizeof(FT) == 4 ? (FT)1e-3 : (FT)1e-9);
       hit = ex * ex + ey * ey + ez * ez < lim * lim;
     }
     unsigned hits = __ballot_sync(FULL, hit);
-    while (hits) {
-      const int kk = k0 + __ffs(hits) - 1;
+    if (!hits) continue;
+    // software-pipelined: the next hit chunk's atoms load while this one is tested
+    int kk = k0 + __ffs(hits) - 1;
+    hits &= hits - 1;
+    double4 at = S.rec[kk * BD_CHUNK + lane];
+    for (;;) {
+      const int kn = hits ? k0 + __ffs(hits) - 1 : -1;
       hits &= hits - 1;
-      const double4 at = S.rec[kk * BD_CHUNK + lane];
-      double l0 = 0, l1 = 0, l2 = 0;
-      bool cand = false;
-      if (fabs(at.w) >= 1e-9) {
-        const double d0 = at.x - c[0], d1 = at.y - c[1], d2 = at.z - c[2];
-        l0 = R[0] * d0 + R[3] * d1 + R[6] * d2;
-        l1 = R[1] * d0 + R[4] * d1 + R[7] * d2;
-        l2 = R[2] * d0 + R[5] * d1 + R[8] * d2;
-        cand = in_box(g, l0, l1, l2);
-      }
-      const unsigned m = __ballot_sync(FULL, cand);
-      if (cand) ring[(head + __popc(m & ((1u << lane) - 1u))) % kRevRing] = make_double4(l0, l1, l2, at.w);
-      head += __popc(m);
-      if (head - tail >= 32) {
-        __syncwarp();
-        drain(32);
-        __syncwarp();
-      }
+      double4 an = at;
+      if (kn >= 0) an = S.rec[kn * BD_CHUNK + lane];
+      gather(at);
+      if (kn < 0) break;
+      at = an;
     }
   }
   __syncwarp();
