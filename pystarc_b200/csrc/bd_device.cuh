@@ -294,7 +294,8 @@ __device__ __forceinline__ StencilOut<FT, CH> stencil(const DevGrid& g, PT x, PT
   const FT ax = (FT)(lx ? half - sxd : sxd - half);
   const FT ay = (FT)(ly ? half - syd : syd - half);
   const FT az = (FT)(lz ? half - szd : szd - half);
-  const long nz = g.nz, syz = (long)g.ny * g.nz;
+  // node indices fit in int: grids are limited to 2^30 nodes of at most two channels
+  const int nz = g.nz, syz = g.ny * g.nz;
   const float* d = g.data;
   // centre rows (cx+i, cy+j): three z nodes starting at zb
   const int zb = lz ? cz - 1 : cz;
@@ -308,7 +309,7 @@ __device__ __forceinline__ StencilOut<FT, CH> stencil(const DevGrid& g, PT x, PT
     for (int i = 0; i < 2; ++i)
 #pragma unroll
       for (int j = 0; j < 2; ++j) {
-        const long n = (long)(cx + i) * syz + (long)(cy + j) * nz + zb;
+        const int n = (cx + i) * syz + (cy + j) * nz + zb;
         const float4 t = __ldg(w + n);
         if constexpr (CH == 1) {
           r[i][j][0][0] = t.x;
@@ -326,9 +327,9 @@ __device__ __forceinline__ StencilOut<FT, CH> stencil(const DevGrid& g, PT x, PT
       }
     float4 tx[2], ty[2];
 #pragma unroll
-    for (int j = 0; j < 2; ++j) tx[j] = __ldg(w + (long)ex * syz + (long)(cy + j) * nz + cz);
+    for (int j = 0; j < 2; ++j) tx[j] = __ldg(w + (ex * syz + (cy + j) * nz + cz));
 #pragma unroll
-    for (int i = 0; i < 2; ++i) ty[i] = __ldg(w + (long)(cx + i) * syz + (long)ey * nz + cz);
+    for (int i = 0; i < 2; ++i) ty[i] = __ldg(w + ((cx + i) * syz + ey * nz + cz));
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
       if constexpr (CH == 1) {
@@ -352,19 +353,19 @@ __device__ __forceinline__ StencilOut<FT, CH> stencil(const DevGrid& g, PT x, PT
     for (int i = 0; i < 2; ++i)
 #pragma unroll
       for (int j = 0; j < 2; ++j) {
-        const long base = ((long)(cx + i) * syz + (long)(cy + j) * nz + zb) * CH;
+        const int base = ((cx + i) * syz + (cy + j) * nz + zb) * CH;
 #pragma unroll
         for (int k = 0; k < 3; ++k) ld<CH>(d + base + k * CH, r[i][j][k]);
       }
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
-      const long base = ((long)ex * syz + (long)(cy + j) * nz + cz) * CH;
+      const int base = (ex * syz + (cy + j) * nz + cz) * CH;
       ld<CH>(d + base, xe[j][0]);
       ld<CH>(d + base + CH, xe[j][1]);
     }
 #pragma unroll
     for (int i = 0; i < 2; ++i) {
-      const long base = ((long)(cx + i) * syz + (long)ey * nz + cz) * CH;
+      const int base = ((cx + i) * syz + ey * nz + cz) * CH;
       ld<CH>(d + base, ye[i][0]);
       ld<CH>(d + base + CH, ye[i][1]);
     }

@@ -140,6 +140,7 @@ __device__ __forceinline__ void warp_reverse_born(const DevSystem& S, const doub
   const FT Rt[9] = {(FT)R[0], (FT)R[1], (FT)R[2], (FT)R[3], (FT)R[4], (FT)R[5], (FT)R[6], (FT)R[7], (FT)R[8]};
   const FT lox = (FT)g.lox, loy = (FT)g.loy, loz = (FT)g.loz, hix = (FT)g.hix, hiy = (FT)g.hiy, hiz = (FT)g.hiz;
   unsigned head = 0, tail = 0;  // warp-uniform ring cursors
+  FT rs0 = 0, rs1 = 0, rs2 = 0;  // per-lane sums in FT (at most a few dozen terms per lane)
   auto drain = [&](unsigned count) {
     if ((unsigned)lane < count) {
       const V4 e = ring[(tail + lane) % kRevRing];
@@ -147,9 +148,9 @@ __device__ __forceinline__ void warp_reverse_born(const DevSystem& S, const doub
       const FT qr = (FT)e.w;
       const FT cf = -alpha * qr * qr;
       const FT g0 = cf * st.gx[0], g1 = cf * st.gy[0], g2 = cf * st.gz[0];
-      r[0] += (double)g0;
-      r[1] += (double)g1;
-      r[2] += (double)g2;
+      rs0 += g0;
+      rs1 += g1;
+      rs2 += g2;
       if (TORQUE) {
         const double x = (double)e.x, y = (double)e.y, z = (double)e.z;
         u[0] += y * (double)g2 - z * (double)g1;
@@ -160,12 +161,28 @@ __device__ __forceinline__ void warp_reverse_born(const DevSystem& S, const doub
     }
     tail += count;
   };
+  // Atom rows of the sweep: the FP32 table in mixed precision (offsets from an
+  // FP32 centre are good to ~1e-5 A, far inside the 1e-3 A re-check band).
+  using AT = typename Vec4<FT>::type;
+  const AT* atoms = nullptr;
+  if constexpr (sizeof(FT) == 4) atoms = S.rec_f;
+  else atoms = S.rec;
+  const FT cx = (FT)c[0], cy = (FT)c[1], cz = (FT)c[2];
   // one hit chunk: lane = atom; in-box atoms go to the ring in lane order
-  auto gather = [&](const double4& at) {
+  auto gather = [&](const AT& at, int idx) {
     FT l0 = 0, l1 = 0, l2 = 0;
     bool cand = false;
-    if (fabs(at.w) >= 1e-9) {
-      const FT d0 = (FT)(at.x - c[0]), d1 = (FT)(at.y - c[1]), d2 = (FT)(at.z - c[2]);
+    if (fabs(at.w) >= (FT)1e-9) {
+      FT d0, d1, d2;
+      if constexpr (sizeof(FT) == 4) {
+        d0 = at.x - cx;
+        d1 = at.y - cy;
+        d2 = at.z - cz;
+      } else {
+        d0 = at.x - c[0];
+        d1 = at.y - c[1];
+        d2 = at.z - c[2];
+      }
       l0 = Rt[0] * d0 + Rt[3] * d1 + Rt[6] * d2;
       l1 = Rt[1] * d0 + Rt[4] * d1 + Rt[7] * d2;
       l2 = Rt[2] * d0 + Rt[5] * d1 + Rt[8] * d2;
@@ -174,7 +191,8 @@ __device__ __forceinline__ void warp_reverse_born(const DevSystem& S, const doub
         const float m = fminf(fminf(fminf(l0 - lox, hix - l0), fminf(l1 - loy, hiy - l1)),
                               fminf(l2 - loz, hiz - l2));
         if (fabsf(m) < 1e-3f) {
-          const double e0 = at.x - c[0], e1 = at.y - c[1], e2 = at.z - c[2];
+          const double4 a64 = S.rec[idx];
+          const double e0 = a64.x - c[0], e1 = a64.y - c[1], e2 = a64.z - c[2];
           cand = in_box(g, R[0] * e0 + R[3] * e1 + R[6] * e2, R[1] * e0 + R[4] * e1 + R[7] * e2,
                         R[2] * e0 + R[5] * e1 + R[8] * e2);
         }
@@ -210,13 +228,14 @@ __device__ __forceinline__ void warp_reverse_born(const DevSystem& S, const doub
     // software-pipelined: the next hit chunk's atoms load while this one is tested
     int kk = k0 + __ffs(hits) - 1;
     hits &= hits - 1;
-    double4 at = S.rec[kk * BD_CHUNK + lane];
+    AT at = atoms[kk * BD_CHUNK + lane];
     for (;;) {
       const int kn = hits ? k0 + __ffs(hits) - 1 : -1;
       hits &= hits - 1;
-      double4 an = at;
-      if (kn >= 0) an = S.rec[kn * BD_CHUNK + lane];
-      gather(at);
+      AT an = at;
+      if (kn >= 0) an = atoms[kn * BD_CHUNK + lane];
+      gather(at, kk * BD_CHUNK + lane);
+      kk = kn;
       if (kn < 0) break;
       at = an;
     }
@@ -224,6 +243,9 @@ __device__ __forceinline__ void warp_reverse_born(const DevSystem& S, const doub
   __syncwarp();
   drain(head - tail);
   __syncwarp();  // the ring is reused by the next call
+  r[0] += (double)rs0;
+  r[1] += (double)rs1;
+  r[2] += (double)rs2;
 }
 
 // Net force, torque (about c) and energy on the ligand of one trajectory,
