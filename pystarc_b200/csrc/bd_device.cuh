@@ -277,6 +277,21 @@ __device__ __forceinline__ void ld(const float* p, float v[CH]) {
   }
 }
 
+// floor(u) as a value and as an int, for 0 <= u < 2^23 (float) or 2^52 (double):
+// adding 2^23 (2^52) with round-down leaves exactly floor(u) in the low mantissa
+// bits, so the cell index needs no float-to-int conversion.  Every stencil
+// position is inside its grid's margin box, so u >= 3.
+__device__ __forceinline__ void floor_split(float u, float& f, int& c) {
+  const float t = __fadd_rd(u, 8388608.0f);
+  c = __float_as_int(t) - 0x4B000000;
+  f = t - 8388608.0f;
+}
+__device__ __forceinline__ void floor_split(double u, double& f, int& c) {
+  const double t = __dadd_rd(u, 4503599627370496.0);
+  c = (int)(__double_as_longlong(t) - 0x4330000000000000ll);
+  f = t - 4503599627370496.0;
+}
+
 // PT is the type of the position and of the cell/fraction arithmetic: double
 // everywhere except the mixed-precision reverse-Born sweep, which hands in FP32
 // ligand-frame coordinates (the interpolant is continuous, so an FP32 position
@@ -284,8 +299,11 @@ __device__ __forceinline__ void ld(const float* p, float v[CH]) {
 template <typename FT, int CH, typename PT = double>
 __device__ __forceinline__ StencilOut<FT, CH> stencil(const DevGrid& g, PT x, PT y, PT z) {
   const PT ux = (x - (PT)g.ox) * (PT)g.isx, uy = (y - (PT)g.oy) * (PT)g.isy, uz = (z - (PT)g.oz) * (PT)g.isz;
-  const PT fx = floor(ux), fy = floor(uy), fz = floor(uz);
-  const int cx = (int)fx, cy = (int)fy, cz = (int)fz;
+  PT fx, fy, fz;
+  int cx, cy, cz;
+  floor_split(ux, fx, cx);
+  floor_split(uy, fy, cy);
+  floor_split(uz, fz, cz);
   const PT sxd = ux - fx, syd = uy - fy, szd = uz - fz;
   const PT half = (PT)0.5;
   const bool lx = sxd < half, ly = syd < half, lz = szd < half;
