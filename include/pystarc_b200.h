@@ -201,6 +201,79 @@ int bd_sim_run_noalloc(BdHandle* h, const BdSimParams* p, int8_t* out_status, in
                        int32_t* out_returns, uint64_t* counters, int steps_per_launch, int max_launches,
                        void* stream);
 
+/* ---- Force terms of the evaluation entry points ------------------------------------------
+ * No reference counterpart: bit flags choosing which terms bd_eval_forces(_atoms) sum.
+ * BD_TERM_GRID: electrostatic and Born direction-1 grid forces on the ligand atoms;
+ * BD_TERM_FARFIELD: the Yukawa multipole far-field of atoms outside every electrostatic grid;
+ * BD_TERM_REV_BORN: Born direction 2 (ligand Born grid at the receptor atoms).  Default: all.
+ * The surrogate is trained on BD_TERM_FARFIELD | BD_TERM_REV_BORN.  The stepper always
+ * sums every term (or the surrogate's share, see bd_sim_set_surrogate). */
+enum { BD_TERM_GRID = 1, BD_TERM_FARFIELD = 2, BD_TERM_REV_BORN = 4, BD_TERM_ALL = 7 };
+int bd_set_terms(BdHandle* h, int terms);
+
+/* ---- Surrogate MLP ensemble -------------------------------------------------------------------
+ * No reference counterpart: the engine's learned part.  Every member maps in_dim inputs
+ * through n_hidden SiLU layers of width `hidden` to out_dim outputs.  BF16 weights and
+ * activations, FP32 accumulation on the tensor cores, FP32 biases, master weights and Adam
+ * moments.  A parameter vector (FP32, per member) holds, layer by layer, W (out x in,
+ * row-major) and then b (out).  Device arrays unless stated; streams follow CUDA (NULL =
+ * legacy default stream).  Errors: bd_mlp_last_error. */
+typedef struct BdMlp BdMlp;
+typedef struct {
+  int32_t n_members; /* 1..8 */
+  int32_t in_dim;    /* 1..32 */
+  int32_t hidden;    /* 128, 256, 384 or 512 */
+  int32_t n_hidden;  /* 1..8 */
+  int32_t out_dim;   /* 1..32 */
+  int32_t reserved;
+  uint64_t seed; /* weight initialisation: U(-1/sqrt(fan_in), 1/sqrt(fan_in)) */
+} BdMlpDesc;
+int bd_mlp_create(int device, const BdMlpDesc* d, BdMlp** out);
+int bd_mlp_destroy(BdMlp* m);
+int bd_mlp_last_error(const BdMlp* m, char* buf, int len);
+int bd_mlp_n_params(const BdMlp* m, int64_t* n);
+/* HOST arrays of bd_mlp_n_params floats; set also clears the member's Adam state. */
+int bd_mlp_get_params(BdMlp* m, int member, float* params);
+int bd_mlp_set_params(BdMlp* m, int member, const float* params);
+/* Y (n x out_dim) = member(X (n x in_dim)). */
+int bd_mlp_forward(BdMlp* m, int member, int64_t n, const float* X, float* Y, void* stream);
+/* Mean squared error over rows and outputs against T (n x out_dim) into *loss (device float,
+ * may be NULL) and its gradient into grad (device, parameter layout, may be NULL).
+ * n is a positive multiple of 32. */
+int bd_mlp_grad(BdMlp* m, int member, int n, const float* X, const float* T, float* grad, float* loss, void* stream);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8, bias-corrected) of one member on a batch. */
+int bd_mlp_train_step(BdMlp* m, int member, int n, const float* X, const float* T, float lr, float* loss,
+                      void* stream);
+/* All members on n rows: mean (n x out_dim) and spread (n x out_dim, RMS deviation of the
+ * members from the mean; may be NULL). */
+int bd_mlp_ensemble(BdMlp* m, int64_t n, const float* X, float* mean, float* spread, void* stream);
+
+/* Stepper with the surrogate (no reference counterpart).  While set, each BD step of
+ * bd_sim_run runs as three phases: the exact grid forces everywhere plus the exact far-field
+ * and reverse Born outside the trust region r_min <= |c| <= r_max; the ensemble on the trusted
+ * poses' features (c / r_scale, |c| / r_scale, q with w >= 0, five Gaussian radial basis values
+ * exp(-((|c| - rbf_centre[k]) / rbf_width)^2 / 2)); then the surrogate's far-field + reverse Born
+ * (mean output x out_scale x envelope) where the members agree (spread of the force <=
+ * threshold x max(|force|, force_floor x envelope)), the exact kernels elsewhere, and the rest
+ * of the step.  envelope = exp(-(|c| - env_ref) / env_length) (env_ref / |c|)^2, or 1 when
+ * env_length is 0.  The
+ * ensemble needs 13 inputs and 6 outputs (force, torque).  m = NULL returns to the fused
+ * exact stepper.  The ensemble must not be used by other calls while the stepper runs, and
+ * per-step statistics are not collected in this mode. */
+typedef struct {
+  double r_scale;
+  double rbf_centre[5];
+  double rbf_width;
+  double out_scale[6];
+  double r_min, r_max;
+  double threshold;
+  double force_floor;
+  double env_length, env_ref;
+} BdSurrogateParams;
+int bd_sim_set_surrogate(BdHandle* h, BdMlp* m, const BdSurrogateParams* p);
+/* Trusted-pose evaluations and exact fallbacks since configure: out[0], out[1]. */
+int bd_sim_surrogate_counters(BdHandle* h, uint64_t* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -21,6 +21,7 @@ CTR_NAMES = ("started", "reacted", "escaped", "max_steps", "steps", "returns", "
 N_CTR = len(CTR_NAMES)
 LAYOUT_STAGE_RECEPTOR, LAYOUT_WINDOWS_1, LAYOUT_WINDOWS_2 = 1, 2, 4
 LAYOUT_DEFAULT = LAYOUT_WINDOWS_1
+TERM_GRID, TERM_FARFIELD, TERM_REV_BORN, TERM_ALL = 1, 2, 4, 7
 
 _ERR_NAMES = {BD_ERR_ARG: "bad argument", BD_ERR_CUDA: "CUDA error", BD_ERR_OOM: "out of device memory",
               BD_ERR_NAN: "non-finite value", BD_ERR_STALL: "device watchdog", BD_ERR_STATE: "call out of order"}
@@ -56,6 +57,18 @@ class BdStatsOut(C.Structure):
 
 
 ST_RAD_BINS, ST_THETA, ST_PHI, ST_MILESTONES, ST_TRANS = 200, 36, 72, 11, 50
+
+
+class BdSurrogateParams(C.Structure):
+    _fields_ = [("r_scale", C.c_double), ("rbf_centre", C.c_double * 5), ("rbf_width", C.c_double),
+                ("out_scale", C.c_double * 6), ("r_min", C.c_double), ("r_max", C.c_double),
+                ("threshold", C.c_double), ("force_floor", C.c_double), ("env_length", C.c_double),
+                ("env_ref", C.c_double)]
+
+
+class BdMlpDesc(C.Structure):
+    _fields_ = [("n_members", C.c_int32), ("in_dim", C.c_int32), ("hidden", C.c_int32), ("n_hidden", C.c_int32),
+                ("out_dim", C.c_int32), ("reserved", C.c_int32), ("seed", C.c_uint64)]
 
 
 P = C.c_void_p
@@ -94,6 +107,19 @@ SIGNATURES = {
     "bd_set_layout": (C.c_int, [P, C.c_int]),
     "bd_get_layout": (C.c_int, [P, i32p]),
     "bd_sim_run_noalloc": (C.c_int, [P, C.POINTER(BdSimParams), P, P, P, P, C.c_int, C.c_int, P]),
+    "bd_set_terms": (C.c_int, [P, C.c_int]),
+    "bd_sim_set_surrogate": (C.c_int, [P, P, C.POINTER(BdSurrogateParams)]),
+    "bd_sim_surrogate_counters": (C.c_int, [P, u64p]),
+    "bd_mlp_create": (C.c_int, [C.c_int, C.POINTER(BdMlpDesc), C.POINTER(P)]),
+    "bd_mlp_destroy": (C.c_int, [P]),
+    "bd_mlp_last_error": (C.c_int, [P, C.c_char_p, C.c_int]),
+    "bd_mlp_n_params": (C.c_int, [P, C.POINTER(C.c_int64)]),
+    "bd_mlp_get_params": (C.c_int, [P, C.c_int, fp]),
+    "bd_mlp_set_params": (C.c_int, [P, C.c_int, fp]),
+    "bd_mlp_forward": (C.c_int, [P, C.c_int, C.c_int64, P, P, P]),
+    "bd_mlp_grad": (C.c_int, [P, C.c_int, C.c_int, P, P, P, P, P]),
+    "bd_mlp_train_step": (C.c_int, [P, C.c_int, C.c_int, P, P, C.c_float, P, P]),
+    "bd_mlp_ensemble": (C.c_int, [P, C.c_int64, P, P, P, P]),
 }
 
 _LIB = None
@@ -128,6 +154,14 @@ def check(rc, handle=None):
     if rc != BD_OK:
         buf = C.create_string_buffer(1024)
         load().bd_last_error(handle, buf, 1024)
+        raise BdError(rc, buf.value.decode(errors="replace"))
+    return rc
+
+
+def check_mlp(rc, m=None):
+    if rc != BD_OK:
+        buf = C.create_string_buffer(1024)
+        load().bd_mlp_last_error(m, buf, 1024)
         raise BdError(rc, buf.value.decode(errors="replace"))
     return rc
 

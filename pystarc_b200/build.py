@@ -11,7 +11,7 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libpystarc_b200.so"
-SOURCES = ["bd_api.cu", "bd_noalloc.cu"]
+SOURCES = ["bd_api.cu", "bd_noalloc.cu", "bd_mlp.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -9,7 +9,15 @@
 #include <vector>
 
 #include "bd_kernels.cuh"
+#include "bd_surrogate.cuh"
 #include "pystarc_b200.h"
+
+// surrogate MLP (bd_mlp.cu)
+int bd_internal_mlp_shape(const BdMlp* m, int* in_dim, int* in_pad, int* out_dim);
+int bd_internal_mlp_prepare(BdMlp* m, int rows);
+int bd_internal_mlp_ensemble_rows(BdMlp* m, int rows, const int* n_dev, const void* Xpacked, float* mean,
+                                  float* spread, cudaStream_t s);
+const char* bd_internal_mlp_error(const BdMlp* m);
 
 using namespace bd;
 
@@ -57,6 +65,13 @@ struct BdHandle {
   int group = 8, block = 128;
   bool launch_user = false;
   int layout = BD_LAYOUT_DEFAULT;
+  unsigned terms = BD_TERM_ALL;
+  // learned surrogate (bd_sim_set_surrogate): the model, its constants, per-slot scratch
+  BdMlp* sur = nullptr;
+  DevSurrogate sur_q{};
+  SurBuf sur_buf{};
+  int sur_cap = 0;
+  unsigned long long* sur_ctr_host_base = nullptr;
   // graphs: [cur][steps] cache
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   int graph_K = -1, graph_G = -1, graph_B = -1, graph_prec = -1, graph_torque = -1;
@@ -331,6 +346,7 @@ int finalize(BdHandle* h) {
     S.rx_deff[p] = h->rx_deff[p];
   }
   CK(h, cudaDeviceSynchronize());  // window copies are built on the legacy stream
+  S.terms = h->terms;
   h->S = S;
   h->dirty = false;
   h->graph_K = -1;  // system changed: rebuild graphs
@@ -625,6 +641,54 @@ int bd_set_layout(BdHandle* h, int flags) {
   return BD_OK;
 }
 
+int bd_sim_set_surrogate(BdHandle* h, BdMlp* m, const BdSurrogateParams* p) {
+  if (!h) return BD_ERR_ARG;
+  h->graph_K = -1;  // the step sequence changes
+  if (!m) {
+    h->sur = nullptr;
+    return BD_OK;
+  }
+  if (!p) return fail(h, BD_ERR_ARG, "bd_sim_set_surrogate: params are NULL");
+  int in_dim, in_pad, out_dim;
+  bd_internal_mlp_shape(m, &in_dim, &in_pad, &out_dim);
+  if (in_dim != kSurIn || in_pad != kSurInPad || out_dim != kSurOut)
+    return fail(h, BD_ERR_ARG, "the surrogate needs %d inputs and %d outputs (got %d, %d)", kSurIn, kSurOut, in_dim,
+                out_dim);
+  if (!(p->r_scale > 0) || !(p->rbf_width > 0) || !(p->threshold >= 0) || !(p->r_max >= p->r_min))
+    return fail(h, BD_ERR_ARG, "bd_sim_set_surrogate: bad feature or trust-region constants");
+  DevSurrogate& q = h->sur_q;
+  q.r_scale = p->r_scale;
+  for (int k = 0; k < 5; ++k) q.rbf_centre[k] = p->rbf_centre[k];
+  q.rbf_width = p->rbf_width;
+  for (int k = 0; k < kSurOut; ++k) q.out_scale[k] = p->out_scale[k];
+  q.r_min = p->r_min;
+  q.r_max = p->r_max;
+  q.threshold = p->threshold;
+  q.force_floor = p->force_floor;
+  q.env_length = p->env_length;
+  q.env_ref = p->env_ref;
+  if (q.env_length > 0 && !(q.env_ref > 0)) return fail(h, BD_ERR_ARG, "the envelope needs env_ref > 0");
+  h->sur = m;
+  return BD_OK;
+}
+
+int bd_sim_surrogate_counters(BdHandle* h, uint64_t* out) {
+  if (!h || !out) return BD_ERR_ARG;
+  out[0] = out[1] = 0;
+  if (!h->sur || !h->sur_buf.ctr || !h->sur_cap) return BD_OK;
+  CK(h, cudaDeviceSynchronize());
+  CK(h, cudaMemcpy(out, h->sur_buf.ctr, 2 * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+  return BD_OK;
+}
+
+int bd_set_terms(BdHandle* h, int terms) {
+  if (!h) return BD_ERR_ARG;
+  if (terms < 0 || terms > BD_TERM_ALL) return fail(h, BD_ERR_ARG, "terms must be a mask of BD_TERM_* bits");
+  h->terms = (unsigned)terms;
+  h->S.terms = (unsigned)terms;  // evaluation kernels take S by value at launch
+  return BD_OK;
+}
+
 int bd_get_layout(BdHandle* h, int* flags) {
   if (!h || !flags) return BD_ERR_ARG;
   *flags = h->layout;
@@ -659,6 +723,8 @@ int bd_sim_configure(BdHandle* h, const BdSimParams* p) {
   CK(h, cudaDeviceSynchronize());
   free_list(h->sim_allocs);
   h->sim_ready = false;
+  h->sur_cap = 0;
+  h->sur_buf = SurBuf{};
   h->sp = *p;
   // live-slot capacity
   const int G = launch_group(h);
@@ -826,6 +892,80 @@ int enqueue_launch(BdHandle* h, int K, cudaStream_t s, int cur, void* fn, size_t
   return BD_OK;
 }
 
+// Scratch of the surrogate stepper for the configured capacity (outside any capture).
+int ensure_surrogate_buffers(BdHandle* h) {
+  const int C = h->buf[0].cap;
+  if (h->sur_cap == C) return BD_OK;
+  SurBuf& U = h->sur_buf;
+  void* q;
+  int rc;
+  if ((rc = dev_alloc(h, h->sim_allocs, &q, 3 * (size_t)C * sizeof(double)))) return rc;
+  U.F = (double*)q;
+  if ((rc = dev_alloc(h, h->sim_allocs, &q, 3 * (size_t)C * sizeof(double)))) return rc;
+  U.T = (double*)q;
+  if ((rc = dev_alloc(h, h->sim_allocs, &q, (size_t)C))) return rc;
+  U.mode = (int8_t*)q;
+  if ((rc = dev_alloc(h, h->sim_allocs, &q, (size_t)C * sizeof(int)))) return rc;
+  U.row = (int*)q;
+  if ((rc = dev_alloc(h, h->sim_allocs, &q, (size_t)C * kSurInPad * 2))) return rc;
+  U.X = (__nv_bfloat16*)q;
+  if ((rc = dev_alloc(h, h->sim_allocs, &q, (size_t)C * kSurOut * sizeof(float)))) return rc;
+  U.mean = (const float*)q;
+  if ((rc = dev_alloc(h, h->sim_allocs, &q, (size_t)C * kSurOut * sizeof(float)))) return rc;
+  U.spread = (const float*)q;
+  if ((rc = dev_alloc(h, h->sim_allocs, &q, sizeof(int)))) return rc;
+  U.n_rows = (int*)q;
+  if ((rc = dev_alloc(h, h->sim_allocs, &q, 2 * sizeof(unsigned long long)))) return rc;
+  U.ctr = (unsigned long long*)q;
+  CK(h, cudaMemset(U.X, 0, (size_t)C * kSurInPad * 2));
+  CK(h, cudaMemset(U.ctr, 0, 2 * sizeof(unsigned long long)));
+  if ((rc = bd_internal_mlp_prepare(h->sur, C))) return fail(h, rc, "surrogate: %s", bd_internal_mlp_error(h->sur));
+  h->sur_cap = C;
+  return BD_OK;
+}
+
+extern "C++" {
+template <typename FT, bool TQ>
+int enqueue_surrogate_step(BdHandle* h, cudaStream_t s, int cur, int blocks) {
+  SlotBuf B = h->buf[cur];
+  const int* live = h->d_live + cur;
+  SurBuf U = h->sur_buf;
+  zero_int_kernel<<<1, 1, 0, s>>>(U.n_rows);
+  sur_begin_kernel<FT, TQ><<<blocks, 256, 0, s>>>(h->S, h->P, B, live, U, h->sur_q);
+  CK(h, cudaGetLastError());
+  int rc = bd_internal_mlp_ensemble_rows(h->sur, h->sur_cap, U.n_rows, U.X, (float*)U.mean, (float*)U.spread, s);
+  if (rc) return fail(h, rc, "surrogate: %s", bd_internal_mlp_error(h->sur));
+  sur_end_kernel<FT, TQ><<<blocks, 256, 0, s>>>(h->S, h->P, B, live, U, h->sur_q);
+  CK(h, cudaGetLastError());
+  return BD_OK;
+}
+}  // extern "C++"
+
+// K surrogate BD steps on buffer `cur`, then the compaction into the other buffer.
+int enqueue_surrogate_launch(BdHandle* h, int K, cudaStream_t s, int cur, int blocks) {
+  const bool tq = h->sp.torque_mode == BD_TORQUE_CENTROID, f64 = h->sp.precision == BD_PREC_FP64;
+  for (int k = 0; k < K; ++k) {
+    int rc = f64 ? (tq ? enqueue_surrogate_step<double, true>(h, s, cur, blocks)
+                       : enqueue_surrogate_step<double, false>(h, s, cur, blocks))
+                 : (tq ? enqueue_surrogate_step<float, true>(h, s, cur, blocks)
+                       : enqueue_surrogate_step<float, false>(h, s, cur, blocks));
+    if (rc) return rc;
+  }
+  SlotBuf src = h->buf[cur], dst = h->buf[1 - cur];
+  compact_kernel<<<h->n_sm * 4, 256, 0, s>>>(src, dst, h->d_live + cur, h->d_ctr);
+  CK(h, cudaGetLastError());
+  finish_compact_kernel<<<1, 1, 0, s>>>(h->d_live + (1 - cur), h->d_ctr);
+  CK(h, cudaGetLastError());
+  return BD_OK;
+}
+
+int surrogate_blocks(BdHandle* h) {
+  const bool tq = h->sp.torque_mode == BD_TORQUE_CENTROID, f64 = h->sp.precision == BD_PREC_FP64;
+  void* fa = f64 ? (tq ? (void*)&sur_begin_kernel<double, true> : (void*)&sur_begin_kernel<double, false>)
+                 : (tq ? (void*)&sur_begin_kernel<float, true> : (void*)&sur_begin_kernel<float, false>);
+  return persistent_blocks(h, fa, 256);
+}
+
 int build_graphs(BdHandle* h, int K) {
   const int G = launch_group(h);
   if (h->graph_K == K && h->graph_G == G && h->graph_B == h->block && h->graph_prec == h->sp.precision &&
@@ -839,10 +979,15 @@ int build_graphs(BdHandle* h, int K) {
   void* fn = kernel_for(h->sp.precision, G, h->sp.torque_mode, 2);
   const size_t smem = stepper_smem(h->S, h->P, fn);
   const int blocks = persistent_blocks(h, fn, h->block, smem);
+  const int sblocks = h->sur ? surrogate_blocks(h) : 0;
+  if (h->sur) {
+    int rc = ensure_surrogate_buffers(h);
+    if (rc) return rc;
+  }
   for (int c = 0; c < 2; ++c) {
     cudaGraph_t graph;
     CK(h, cudaStreamBeginCapture(h->own, cudaStreamCaptureModeThreadLocal));
-    int rc = enqueue_launch(h, K, h->own, c, fn, smem, blocks);
+    int rc = h->sur ? enqueue_surrogate_launch(h, K, h->own, c, sblocks) : enqueue_launch(h, K, h->own, c, fn, smem, blocks);
     cudaError_t e = cudaStreamEndCapture(h->own, &graph);
     if (rc) return rc;
     CK(h, e);
@@ -865,6 +1010,7 @@ int bd_sim_run(BdHandle* h, int n_launch, int K, void* stream) {
   if (!h->sim_ready) return fail(h, BD_ERR_STATE, "bd_sim_run before bd_sim_configure");
   if (n_launch < 0 || K <= 0) return fail(h, BD_ERR_ARG, "bd_sim_run: n_launch >= 0 and steps > 0 needed");
   if (h->dirty) return fail(h, BD_ERR_STATE, "system changed after bd_sim_reset; reset again");
+  if (h->sur && h->P.stats) return fail(h, BD_ERR_STATE, "per-step statistics are not collected by the surrogate stepper");
   int rc = build_graphs(h, K);
   if (rc) return rc;
   cudaStream_t s = pick(h, stream);

@@ -58,6 +58,7 @@ struct DevSystem {
   const float4* rec_f;    // FP32 copies for the shared-memory pre-tests (radius not inflated)
   const float4* chunks_f;
   int rec_in_smem;        // stepper kernels stage rec_f / chunks_f in shared memory
+  unsigned terms;         // BD_TERM_* summed by the evaluation kernels (the stepper sums all)
   double rec_max_r;
   // grids
   int n_elec;

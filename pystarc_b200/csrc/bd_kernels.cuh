@@ -258,8 +258,9 @@ __device__ __forceinline__ void warp_reverse_born(const DevSystem& S, const doub
 template <typename FT, int G, bool TORQUE, bool ENERGY, class PosFn>
 __device__ void group_forces(const DevSystem& S, const double c[3], const double R[9], int lane, unsigned gm,
                              const PosFn& pos, double F[3], double T[3], double& E, Counts& cnt,
-                             const RecView& v = RecView{nullptr, nullptr}) {
+                             const RecView& v = RecView{nullptr, nullptr}, unsigned terms = 7u) {
   double f0 = 0, f1 = 0, f2 = 0, t0 = 0, t1 = 0, t2 = 0, e = 0;
+  const bool t_grid = terms & 1u, t_ff = terms & 2u, t_rev = terms & 4u;
   unsigned ng = 0, nf = 0, nr = 0;
   const int nl = S.n_lig;
   for (int i = lane; i < nl; i += G) {
@@ -278,6 +279,7 @@ __device__ void group_forces(const DevSystem& S, const double c[3], const double
     const bool bin = S.has_born && in_box(S.born, x[0], x[1], x[2]);
     const FT cb = (FT)S.alpha * q * q;
     if (gi == 0 && bin && S.paired) {
+      if (!t_grid) continue;
       const StencilOut<FT, 2> s = stencil<FT, 2>(S.pair, x[0], x[1], x[2]);
       fa0 = -q * s.gx[0] - cb * s.gx[1];
       fa1 = -q * s.gy[0] - cb * s.gy[1];
@@ -286,13 +288,15 @@ __device__ void group_forces(const DevSystem& S, const double c[3], const double
       ng += 2;
     } else {
       if (gi >= 0) {
+        if (t_grid) {
         const StencilOut<FT, 1> s = stencil<FT, 1>(S.elec[gi], x[0], x[1], x[2]);
         fa0 = -q * s.gx[0];
         fa1 = -q * s.gy[0];
         fa2 = -q * s.gz[0];
         if (ENERGY) ea = q * s.phi[0];
         ng += 1;
-      } else if (S.has_yukawa) {
+        }
+      } else if (S.has_yukawa && t_ff) {
         FT ff[3], ef;
         farfield<FT>(S, x[0], x[1], x[2], q, ff, ef);
         fa0 = ff[0];
@@ -301,7 +305,7 @@ __device__ void group_forces(const DevSystem& S, const double c[3], const double
         if (ENERGY) ea = ef;
         nf += 1;
       }
-      if (bin) {
+      if (bin && t_grid) {
         const StencilOut<FT, 1> s = stencil<FT, 1>(S.born, x[0], x[1], x[2]);
         fa0 -= cb * s.gx[0];
         fa1 -= cb * s.gy[0];
@@ -325,7 +329,7 @@ __device__ void group_forces(const DevSystem& S, const double c[3], const double
   // sweep the hit chunks' atoms together.
   double r0 = 0, r1 = 0, r2 = 0, u0 = 0, u1 = 0, u2 = 0;
   if constexpr (G == 32) {
-    if (S.born_rev && norm3(c[0], c[1], c[2]) - S.rec_max_r < S.lig_born_rho) {
+    if (t_rev && S.born_rev && norm3(c[0], c[1], c[2]) - S.rec_max_r < S.lig_born_rho) {
       double rr[3] = {0, 0, 0}, uu[3] = {0, 0, 0};
       warp_reverse_born<FT, TORQUE>(S, c, R, lane, rr, uu, nr);
       r0 = rr[0];
@@ -335,7 +339,7 @@ __device__ void group_forces(const DevSystem& S, const double c[3], const double
       u1 = uu[1];
       u2 = uu[2];
     }
-  } else if (S.born_rev) {
+  } else if (t_rev && S.born_rev) {
     const double rho = S.lig_born_rho;
     if (norm3(c[0], c[1], c[2]) - S.rec_max_r < rho) {
       const double rho2 = rho * rho;
@@ -437,7 +441,8 @@ __global__ void __launch_bounds__(256) eval_pose_kernel(DevSystem S, long long n
       quat_to_rot(q, R);
     }
     double f[3], tq[3], e;
-    group_forces<FT, G, TORQUE, true>(S, c, R, lane, gm, PosFromPose{R, c}, f, tq, e, cnt);
+    group_forces<FT, G, TORQUE, true>(S, c, R, lane, gm, PosFromPose{R, c}, f, tq, e, cnt, RecView{nullptr, nullptr},
+                                      S.terms);
     if (lane == 0) {
       F[3 * t] = f[0];
       F[3 * t + 1] = f[1];
@@ -476,7 +481,7 @@ __global__ void __launch_bounds__(256) eval_atoms_kernel(DevSystem S, long long 
     for (int k = 0; k < 9; ++k) R[k] = Rm[9 * t + k];
     double f[3], tq[3], e;
     group_forces<FT, G, TORQUE, true>(S, c, R, lane, gm, PosFromAtoms{pos + (long long)t * S.n_lig * 3, c}, f,
-                                      tq, e, cnt);
+                                      tq, e, cnt, RecView{nullptr, nullptr}, S.terms);
     if (lane == 0) {
       F[3 * t] = f[0];
       F[3 * t + 1] = f[1];

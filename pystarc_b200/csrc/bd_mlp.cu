@@ -1,0 +1,861 @@
+// Surrogate MLP ensemble: training and inference on the tensor cores.
+//
+// No reference counterpart: this is the engine's learned part.  A member maps
+// in_dim inputs through n_hidden SiLU layers of width `hidden` to out_dim
+// outputs.  Weights and activations are BF16, every product accumulates in
+// FP32 (mma.sync m16n8k16), biases, pre-activations, master weights, Adam
+// moments and the loss are FP32.
+//
+// Training data flow for one member and a batch of n rows (n a multiple of 32):
+//   forward   Z_l = A_{l-1} W_l^T + b_l, A_l = SiLU(Z_l)   (Z_l FP32; A_l BF16 in both
+//             row-major [n][h] and transposed [h][n] order)
+//   loss      L = mean((Y - T)^2) over rows and real outputs; dY = 2 (Y - T) / (n out_dim)
+//   backward  dW_l = dZ_l^T A_{l-1} (split over the batch, reduced in a fixed order),
+//             db_l = column sums of dZ_l, dA_{l-1} = dZ_l W_l,
+//             dZ_{l-1} = dA_{l-1} * SiLU'(Z_{l-1})
+//   update    Adam on the FP32 masters, then fresh BF16 copies W_l and W_l^T.
+// Every GEMM has the form C = A B^T with both operands K-contiguous in memory,
+// which is why activations and gradients are also kept transposed.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "pystarc_b200.h"
+
+typedef __nv_bfloat16 bf16;
+
+namespace {
+
+constexpr int kBK = 32;        // K step of a GEMM tile
+constexpr int kMaxLayers = 9;  // n_hidden <= 8, plus the output layer
+constexpr int kChunkRows = 65536;  // inference processes this many rows at a time
+
+int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+// ---------------------------------------------------------------------------
+// GEMM C[M][N] = A[M][K] B[N][K]^T (+ epilogue), BF16 in, FP32 accumulate.
+// K and N are multiples of 32, lda/ldb multiples of 8; M is arbitrary.
+// ---------------------------------------------------------------------------
+enum { EPI_HIDDEN_FWD = 0, EPI_OUT_FWD = 1, EPI_HIDDEN_BWD = 2, EPI_PARTIAL = 3 };
+
+struct GemmArgs {
+  int M, N, K;
+  const bf16* A;
+  int lda;
+  const bf16* B;
+  int ldb;
+  int k_per_split;  // multiple of kBK; gridDim.z splits cover K
+  const float* bias;
+  int n_real;  // EPI_OUT_FWD: columns stored
+  float* C;    // Z (hidden fwd, optional), Y (out fwd) or split partials
+  int ldc;
+  long long split_stride;
+  bf16* O;  // BF16 row-major result (activation or dZ), optional
+  int ldo;
+  bf16* Ot;  // BF16 transposed result [N][ldot], optional
+  int ldot;
+  const float* Zin;  // pre-activations for the SiLU derivative
+  int ldz;
+  const int* m_dev;  // optional device row count: rows >= *m_dev are skipped
+};
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int bytes) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__device__ __forceinline__ void mma_bf16(float c[4], const unsigned a[4], const unsigned b[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+__device__ __forceinline__ float silu_grad(float z) {
+  const float s = 1.0f / (1.0f + __expf(-z));
+  return s * (1.0f + z * (1.0f - s));
+}
+
+template <int BM, int BN, int WM, int WN, int EPI>
+__global__ void __launch_bounds__(256) gemm_nt(GemmArgs g) {
+  static_assert(WM * WN == 8, "8 warps");
+  constexpr int TM = BM / WM, TN = BN / WN;  // warp tile
+  constexpr int MT = TM / 16, NT = TN / 8;
+  constexpr int LDS = kBK + 8;  // padded smem row (bank-conflict free 32-bit fragment loads)
+  __shared__ __align__(16) bf16 As[2][BM][LDS];
+  __shared__ __align__(16) bf16 Bs[2][BN][LDS];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm0 = (warp / WN) * TM, wn0 = (warp % WN) * TN;
+  const int gq = lane >> 2, tq = lane & 3;
+  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+  const int M = g.m_dev ? min(g.M, *g.m_dev) : g.M;
+  if (m0 >= M) return;  // whole block: no barrier is skipped by part of it
+  const int kb = blockIdx.z * g.k_per_split, ke = min(g.K, kb + g.k_per_split);
+  float acc[MT][NT][4];
+#pragma unroll
+  for (int i = 0; i < MT; ++i)
+#pragma unroll
+    for (int j = 0; j < NT; ++j)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.f;
+
+  auto load = [&](int st, int k) {
+    for (int c = tid; c < BM * (kBK / 8); c += 256) {
+      const int r = c / (kBK / 8), kc = (c % (kBK / 8)) * 8;
+      const int row = m0 + r;
+      const bool ok = row < M;
+      cp_async16(&As[st][r][kc], g.A + (size_t)(ok ? row : 0) * g.lda + k + kc, ok ? 16 : 0);
+    }
+    for (int c = tid; c < BN * (kBK / 8); c += 256) {
+      const int r = c / (kBK / 8), kc = (c % (kBK / 8)) * 8;
+      const int row = n0 + r;
+      const bool ok = row < g.N;
+      cp_async16(&Bs[st][r][kc], g.B + (size_t)(ok ? row : 0) * g.ldb + k + kc, ok ? 16 : 0);
+    }
+    cp_async_commit();
+  };
+
+  int st = 0;
+  if (kb < ke) load(0, kb);
+  for (int k = kb; k < ke; k += kBK) {
+    if (k + kBK < ke) {
+      load(st ^ 1, k + kBK);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kBK; kk += 16) {
+      unsigned a[MT][4], b[NT][2];
+#pragma unroll
+      for (int i = 0; i < MT; ++i) {
+        const int r = wm0 + i * 16 + gq;
+        a[i][0] = *reinterpret_cast<const unsigned*>(&As[st][r][kk + 2 * tq]);
+        a[i][1] = *reinterpret_cast<const unsigned*>(&As[st][r + 8][kk + 2 * tq]);
+        a[i][2] = *reinterpret_cast<const unsigned*>(&As[st][r][kk + 2 * tq + 8]);
+        a[i][3] = *reinterpret_cast<const unsigned*>(&As[st][r + 8][kk + 2 * tq + 8]);
+      }
+#pragma unroll
+      for (int j = 0; j < NT; ++j) {
+        const int c = wn0 + j * 8 + gq;
+        b[j][0] = *reinterpret_cast<const unsigned*>(&Bs[st][c][kk + 2 * tq]);
+        b[j][1] = *reinterpret_cast<const unsigned*>(&Bs[st][c][kk + 2 * tq + 8]);
+      }
+#pragma unroll
+      for (int i = 0; i < MT; ++i)
+#pragma unroll
+        for (int j = 0; j < NT; ++j) mma_bf16(acc[i][j], a[i], b[j]);
+    }
+    __syncthreads();
+    st ^= 1;
+  }
+
+  // epilogue: acc[i][j][h*2 + e] is row wm0 + i*16 + gq + 8h, column wn0 + j*8 + 2tq + e
+#pragma unroll
+  for (int i = 0; i < MT; ++i)
+#pragma unroll
+    for (int j = 0; j < NT; ++j)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int r = m0 + wm0 + i * 16 + gq + 8 * h;
+        const int c = n0 + wn0 + j * 8 + 2 * tq;
+        if (r >= M || c >= g.N) continue;
+        float v0 = acc[i][j][2 * h], v1 = acc[i][j][2 * h + 1];
+        if constexpr (EPI == EPI_PARTIAL) {
+          float* p = g.C + blockIdx.z * g.split_stride + (size_t)r * g.ldc + c;
+          p[0] = v0;
+          p[1] = v1;
+        } else if constexpr (EPI == EPI_OUT_FWD) {
+          if (c < g.n_real) g.C[(size_t)r * g.ldc + c] = v0 + g.bias[c];
+          if (c + 1 < g.n_real) g.C[(size_t)r * g.ldc + c + 1] = v1 + g.bias[c + 1];
+        } else {
+          float o0, o1;
+          if constexpr (EPI == EPI_HIDDEN_FWD) {
+            v0 += g.bias[c];
+            v1 += g.bias[c + 1];
+            if (g.C) {
+              g.C[(size_t)r * g.ldc + c] = v0;
+              g.C[(size_t)r * g.ldc + c + 1] = v1;
+            }
+            o0 = silu(v0);
+            o1 = silu(v1);
+          } else {  // EPI_HIDDEN_BWD: v = dA, output dZ
+            o0 = v0 * silu_grad(g.Zin[(size_t)r * g.ldz + c]);
+            o1 = v1 * silu_grad(g.Zin[(size_t)r * g.ldz + c + 1]);
+          }
+          const bf16 b0 = __float2bfloat16_rn(o0), b1 = __float2bfloat16_rn(o1);
+          if (g.O) {
+            __nv_bfloat162 pr;
+            pr.x = b0;
+            pr.y = b1;
+            *reinterpret_cast<__nv_bfloat162*>(g.O + (size_t)r * g.ldo + c) = pr;
+          }
+          if (g.Ot) {
+            g.Ot[(size_t)c * g.ldot + r] = b0;
+            g.Ot[(size_t)(c + 1) * g.ldot + r] = b1;
+          }
+        }
+      }
+}
+
+// ---------------------------------------------------------------------------
+// Small kernels
+// ---------------------------------------------------------------------------
+
+// FP32 rows (n x in_dim) -> BF16 rows padded to ld (zeros), optionally transposed [ld][ldt].
+__global__ void pack_input_kernel(const float* __restrict__ X, int n, int in_dim, bf16* __restrict__ Xb, int ld,
+                                  bf16* __restrict__ Xt, int ldt) {
+  const long long total = (long long)n * ld;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(i / ld), c = (int)(i % ld);
+    const bf16 v = __float2bfloat16_rn(c < in_dim ? X[(size_t)r * in_dim + c] : 0.f);
+    Xb[i] = v;
+    if (Xt) Xt[(size_t)c * ldt + r] = v;
+  }
+}
+
+// dY = 2 (Y - T) / (n out_dim) as BF16 rows [n][ld] and transposed [ld][ldt]; per-block loss partials.
+__global__ void loss_kernel(const float* __restrict__ Y, int ldy, const float* __restrict__ T, int n, int out_dim,
+                            bf16* __restrict__ dY, int ld, bf16* __restrict__ dYt, int ldt,
+                            float* __restrict__ partial) {
+  __shared__ float red[256];
+  const float scale = 2.0f / ((float)n * (float)out_dim);
+  float s = 0.f;
+  const long long total = (long long)n * ld;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(i / ld), c = (int)(i % ld);
+    float d = 0.f;
+    if (c < out_dim) {
+      const float e = Y[(size_t)r * ldy + c] - T[(size_t)r * out_dim + c];
+      s += e * e;
+      d = scale * e;
+    }
+    const bf16 b = __float2bfloat16_rn(d);
+    dY[i] = b;
+    dYt[(size_t)c * ldt + r] = b;
+  }
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
+}
+
+// loss = sum(partials) / (n out_dim), in a fixed order.
+__global__ void loss_finish_kernel(const float* __restrict__ partial, int nb, float denom, float* __restrict__ loss) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  float s = 0.f;
+  for (int i = 0; i < nb; ++i) s += partial[i];
+  *loss = s / denom;
+}
+
+// Weight gradient of one layer from split partials (summed in split order) and
+// bias gradient as the row sums of dZ^T [out_pad][ldt] over the first n columns.
+__global__ void grad_reduce_kernel(const float* __restrict__ part, int splits, long long split_stride, int ldp,
+                                   int out_real, int in_real, const bf16* __restrict__ dZt, int ldt, int n,
+                                   float* __restrict__ gW, float* __restrict__ gb) {
+  const int total = out_real * in_real;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total + out_real; i += gridDim.x * blockDim.x) {
+    if (i < total) {
+      const int o = i / in_real, c = i % in_real;
+      float s = 0.f;
+      for (int z = 0; z < splits; ++z) s += part[z * split_stride + (size_t)o * ldp + c];
+      gW[i] = s;
+    } else {
+      const int o = i - total;
+      float s = 0.f;
+      for (int m = 0; m < n; ++m) s += __bfloat162float(dZt[(size_t)o * ldt + m]);
+      gb[o] = s;
+    }
+  }
+}
+
+struct LayerGeom {
+  int in_real[kMaxLayers], out_real[kMaxLayers], in_pad[kMaxLayers], out_pad[kMaxLayers];
+  long long w_off[kMaxLayers], b_off[kMaxLayers];  // into the FP32 parameter vector
+  long long wb_off[kMaxLayers];                     // into the padded BF16 W / W^T buffers
+  int n_layers;
+};
+
+// Adam on the FP32 parameters, then the padded BF16 copies W [out_pad][in_pad] and W^T [in_pad][out_pad].
+__global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ grad, float* __restrict__ m1,
+                            float* __restrict__ m2, long long n_params, float lr, float b1, float b2, float eps,
+                            float c1, float c2, LayerGeom L, bf16* __restrict__ Wb, bf16* __restrict__ Wt) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n_params;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float gi = grad[i];
+    const float a = b1 * m1[i] + (1.f - b1) * gi;
+    const float b = b2 * m2[i] + (1.f - b2) * gi * gi;
+    m1[i] = a;
+    m2[i] = b;
+    const float w = p[i] - lr * (a / c1) / (sqrtf(b / c2) + eps);
+    p[i] = w;
+    for (int l = 0; l < L.n_layers; ++l) {
+      if (i >= L.w_off[l] && i < L.b_off[l]) {
+        const int k = (int)(i - L.w_off[l]);
+        const int o = k / L.in_real[l], c = k % L.in_real[l];
+        const bf16 v = __float2bfloat16_rn(w);
+        Wb[L.wb_off[l] + (size_t)o * L.in_pad[l] + c] = v;
+        Wt[L.wb_off[l] + (size_t)c * L.out_pad[l] + o] = v;
+      }
+    }
+  }
+}
+
+// BF16 copies of every weight from the FP32 parameters (after set/initialise).
+__global__ void refresh_kernel(const float* __restrict__ p, long long n_params, LayerGeom L, bf16* __restrict__ Wb,
+                               bf16* __restrict__ Wt) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n_params;
+       i += (long long)gridDim.x * blockDim.x) {
+    for (int l = 0; l < L.n_layers; ++l) {
+      if (i >= L.w_off[l] && i < L.b_off[l]) {
+        const int k = (int)(i - L.w_off[l]);
+        const int o = k / L.in_real[l], c = k % L.in_real[l];
+        const bf16 v = __float2bfloat16_rn(p[i]);
+        Wb[L.wb_off[l] + (size_t)o * L.in_pad[l] + c] = v;
+        Wt[L.wb_off[l] + (size_t)c * L.out_pad[l] + o] = v;
+      }
+    }
+  }
+}
+
+// Ensemble mean and spread (RMS deviation of the members from the mean), per output.
+__global__ void ensemble_kernel(const float* __restrict__ Ys, int members, long long stride, int n, int out_dim,
+                                float* __restrict__ mean, float* __restrict__ spread, const int* __restrict__ n_dev) {
+  if (n_dev) n = min(n, *n_dev);
+  const long long total = (long long)n * out_dim;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    float s = 0.f;
+    for (int m = 0; m < members; ++m) s += Ys[m * stride + i];
+    const float mu = s / (float)members;
+    float d = 0.f;
+    for (int m = 0; m < members; ++m) {
+      const float e = Ys[m * stride + i] - mu;
+      d += e * e;
+    }
+    mean[i] = mu;
+    if (spread) spread[i] = sqrtf(d / (float)members);
+  }
+}
+
+}  // namespace
+
+// ===========================================================================
+struct BdMlp {
+  int device = 0;
+  BdMlpDesc d{};
+  std::string err;
+  LayerGeom L{};
+  long long n_params = 0, wb_size = 0;
+  int n_sm = 148;
+  struct Member {
+    float *p = nullptr, *m1 = nullptr, *m2 = nullptr, *grad = nullptr;
+    bf16 *Wb = nullptr, *Wt = nullptr;
+    long long step = 0;
+  };
+  std::vector<Member> mem;
+  std::vector<void*> allocs;  // everything, freed at destroy
+  // training scratch (sized for `train_cap` rows)
+  int train_cap = 0;
+  std::vector<void*> train_allocs;
+  bf16 *Xb = nullptr, *Xt = nullptr, *dY = nullptr, *dYt = nullptr;
+  std::vector<float*> Z;
+  std::vector<bf16*> A, At, dZ, dZt;
+  float *Y = nullptr, *part = nullptr, *loss_part = nullptr, *loss_tmp = nullptr;
+  long long part_stride = 0;
+  // inference scratch (infer_cap rows)
+  int infer_cap = 0;
+  std::vector<void*> infer_allocs;
+  bf16 *act[2] = {nullptr, nullptr}, *Xi = nullptr;
+  float* Ys = nullptr;
+};
+
+namespace {
+
+int mfail(BdMlp* m, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (m) m->err = buf;
+  return code;
+}
+
+#define MCK(m, x)                                                                                       \
+  do {                                                                                                  \
+    cudaError_t e_ = (x);                                                                               \
+    if (e_ != cudaSuccess)                                                                              \
+      return mfail(m, e_ == cudaErrorMemoryAllocation ? BD_ERR_OOM : BD_ERR_CUDA, "%s: %s (%s:%d)", #x, \
+                   cudaGetErrorString(e_), __FILE__, __LINE__);                                         \
+  } while (0)
+
+int malloc_into(BdMlp* m, std::vector<void*>& list, void** p, size_t bytes) {
+  MCK(m, cudaMalloc(p, bytes));
+  list.push_back(*p);
+  MCK(m, cudaMemset(*p, 0, bytes));
+  return BD_OK;
+}
+
+uint64_t splitmix(uint64_t& s) {
+  uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+int grid_for(BdMlp* m, long long n) { return (int)std::min<long long>((n + 255) / 256, (long long)m->n_sm * 16); }
+
+template <int BM, int BN, int WM, int WN, int EPI>
+int launch_gemm(BdMlp* m, const GemmArgs& g, int splits, cudaStream_t s) {
+  dim3 grid((g.N + BN - 1) / BN, (g.M + BM - 1) / BM, splits);
+  gemm_nt<BM, BN, WM, WN, EPI><<<grid, 256, 0, s>>>(g);
+  MCK(m, cudaGetLastError());
+  return BD_OK;
+}
+
+// C = A B^T with the tile picked from N (hidden widths use 128-wide tiles).
+template <int EPI>
+int gemm(BdMlp* m, const GemmArgs& g, int splits, cudaStream_t s) {
+  if (g.N >= 128) return launch_gemm<128, 128, 2, 4, EPI>(m, g, splits, s);
+  return launch_gemm<128, 32, 4, 2, EPI>(m, g, splits, s);
+}
+
+int ensure_train(BdMlp* m, int n) {
+  if (n <= m->train_cap) return BD_OK;
+  for (void* p : m->train_allocs) cudaFree(p);
+  m->train_allocs.clear();
+  m->Z.assign(m->L.n_layers, nullptr);
+  m->A.assign(m->L.n_layers, nullptr);
+  m->At.assign(m->L.n_layers, nullptr);
+  m->dZ.assign(m->L.n_layers, nullptr);
+  m->dZt.assign(m->L.n_layers, nullptr);
+  const LayerGeom& L = m->L;
+  void* p;
+  int rc;
+  auto get = [&](size_t bytes) -> void* {
+    p = nullptr;
+    rc = malloc_into(m, m->train_allocs, &p, bytes);
+    return p;
+  };
+  m->Xb = (bf16*)get((size_t)n * L.in_pad[0] * 2);
+  if (rc) return rc;
+  m->Xt = (bf16*)get((size_t)n * L.in_pad[0] * 2);
+  if (rc) return rc;
+  const int nl = L.n_layers;
+  for (int l = 0; l + 1 < nl; ++l) {  // hidden layers
+    const int h = L.out_pad[l];
+    if (!(m->Z[l] = (float*)get((size_t)n * h * 4))) return rc;
+    if (!(m->A[l] = (bf16*)get((size_t)n * h * 2))) return rc;
+    if (!(m->At[l] = (bf16*)get((size_t)n * h * 2))) return rc;
+    if (!(m->dZ[l] = (bf16*)get((size_t)n * h * 2))) return rc;
+    if (!(m->dZt[l] = (bf16*)get((size_t)n * h * 2))) return rc;
+  }
+  const int op = L.out_pad[nl - 1];
+  if (!(m->Y = (float*)get((size_t)n * op * 4))) return rc;
+  if (!(m->dY = (bf16*)get((size_t)n * op * 2))) return rc;
+  if (!(m->dYt = (bf16*)get((size_t)n * op * 2))) return rc;
+  int maxw = 0;
+  for (int l = 0; l < nl; ++l) maxw = std::max(maxw, L.out_pad[l] * L.in_pad[l]);
+  m->part_stride = maxw;
+  if (!(m->part = (float*)get((size_t)64 * maxw * 4))) return rc;
+  if (!(m->loss_part = (float*)get((size_t)m->n_sm * 16 * 4))) return rc;
+  if (!(m->loss_tmp = (float*)get(4))) return rc;
+  m->train_cap = n;
+  return BD_OK;
+}
+
+// Inference buffers for `rows` rows at a time (at least kChunkRows).
+int ensure_infer(BdMlp* m, int rows = kChunkRows) {
+  rows = std::max(rows, kChunkRows);
+  if (rows <= m->infer_cap) return BD_OK;
+  MCK(m, cudaDeviceSynchronize());
+  for (void* q : m->infer_allocs) cudaFree(q);
+  m->infer_allocs.clear();
+  m->infer_cap = 0;
+  const LayerGeom& L = m->L;
+  int wmax = L.in_pad[0];
+  for (int l = 0; l < L.n_layers; ++l) wmax = std::max(wmax, L.out_pad[l]);
+  void* p;
+  int rc;
+  if ((rc = malloc_into(m, m->infer_allocs, &p, (size_t)rows * L.in_pad[0] * 2))) return rc;
+  m->Xi = (bf16*)p;
+  for (int k = 0; k < 2; ++k) {
+    if ((rc = malloc_into(m, m->infer_allocs, &p, (size_t)rows * wmax * 2))) return rc;
+    m->act[k] = (bf16*)p;
+  }
+  if ((rc = malloc_into(m, m->infer_allocs, &p, (size_t)m->d.n_members * rows * m->d.out_dim * 4))) return rc;
+  m->Ys = (float*)p;
+  m->infer_cap = rows;
+  return BD_OK;
+}
+
+// Forward of one member on packed BF16 rows Xb [n][in_pad]; writes Y [n][ldy] (FP32, real outputs).
+// Training mode keeps Z, A and A^T of every hidden layer.
+int forward(BdMlp* m, int member, int n, const bf16* Xb, float* Y, int ldy, bool train, cudaStream_t s,
+            const int* n_dev = nullptr) {
+  const LayerGeom& L = m->L;
+  const BdMlp::Member& w = m->mem[member];
+  const bf16* in = Xb;
+  int ld_in = L.in_pad[0];
+  for (int l = 0; l < L.n_layers; ++l) {
+    GemmArgs g{};
+    g.M = n;
+    g.N = L.out_pad[l];
+    g.K = L.in_pad[l];
+    g.A = in;
+    g.lda = ld_in;
+    g.B = w.Wb + L.wb_off[l];
+    g.ldb = L.in_pad[l];
+    g.k_per_split = g.K;
+    g.bias = w.p + L.b_off[l];
+    g.m_dev = n_dev;
+    int rc;
+    if (l + 1 < L.n_layers) {
+      bf16* out = train ? m->A[l] : m->act[l & 1];
+      g.C = train ? m->Z[l] : nullptr;
+      g.ldc = g.N;
+      g.O = out;
+      g.ldo = g.N;
+      g.Ot = train ? m->At[l] : nullptr;
+      g.ldot = n;
+      if ((rc = gemm<EPI_HIDDEN_FWD>(m, g, 1, s))) return rc;
+      in = out;
+      ld_in = g.N;
+    } else {
+      g.C = Y;
+      g.ldc = ldy;
+      g.n_real = L.out_real[l];
+      if ((rc = gemm<EPI_OUT_FWD>(m, g, 1, s))) return rc;
+    }
+  }
+  return BD_OK;
+}
+
+// Loss and gradient of one member on n rows (n % 32 == 0) into the member's grad buffer.
+int backward(BdMlp* m, int member, int n, const float* X, const float* T, float* loss, cudaStream_t s) {
+  const LayerGeom& L = m->L;
+  BdMlp::Member& w = m->mem[member];
+  int rc;
+  if ((rc = ensure_train(m, n))) return rc;
+  pack_input_kernel<<<grid_for(m, (long long)n * L.in_pad[0]), 256, 0, s>>>(X, n, m->d.in_dim, m->Xb, L.in_pad[0],
+                                                                             m->Xt, n);
+  MCK(m, cudaGetLastError());
+  const int nl = L.n_layers, op = L.out_pad[nl - 1];
+  if ((rc = forward(m, member, n, m->Xb, m->Y, op, true, s))) return rc;
+  const int nb = grid_for(m, (long long)n * op);
+  loss_kernel<<<nb, 256, 0, s>>>(m->Y, op, T, n, m->d.out_dim, m->dY, op, m->dYt, n, m->loss_part);
+  MCK(m, cudaGetLastError());
+  loss_finish_kernel<<<1, 32, 0, s>>>(m->loss_part, nb, (float)n * (float)m->d.out_dim, loss ? loss : m->loss_tmp);
+  MCK(m, cudaGetLastError());
+  const int splits = std::max(1, std::min(64, n / 256));
+  const int kps = round_up((n + splits - 1) / splits, kBK);
+  for (int l = nl - 1; l >= 0; --l) {
+    const bf16* dZ = l == nl - 1 ? m->dY : m->dZ[l];
+    const bf16* dZt = l == nl - 1 ? m->dYt : m->dZt[l];
+    const bf16* Ain_t = l == 0 ? m->Xt : m->At[l - 1];
+    // dW_l = dZ_l^T A_{l-1}: M = out_pad, N = in_pad, K = n
+    GemmArgs g{};
+    g.M = L.out_pad[l];
+    g.N = L.in_pad[l];
+    g.K = n;
+    g.A = dZt;
+    g.lda = n;
+    g.B = Ain_t;
+    g.ldb = n;
+    g.k_per_split = kps;
+    g.C = m->part;
+    g.ldc = L.in_pad[l];
+    g.split_stride = m->part_stride;
+    const int used = (n + kps - 1) / kps;
+    if ((rc = gemm<EPI_PARTIAL>(m, g, used, s))) return rc;
+    const int tot = L.out_real[l] * L.in_real[l] + L.out_real[l];
+    grad_reduce_kernel<<<grid_for(m, tot), 256, 0, s>>>(m->part, used, m->part_stride, L.in_pad[l], L.out_real[l],
+                                                         L.in_real[l], dZt, n, n, w.grad + L.w_off[l],
+                                                         w.grad + L.b_off[l]);
+    MCK(m, cudaGetLastError());
+    if (l == 0) break;
+    // dZ_{l-1} = (dZ_l W_l) * SiLU'(Z_{l-1}): M = n, N = in_pad (hidden), K = out_pad
+    GemmArgs b{};
+    b.M = n;
+    b.N = L.in_pad[l];
+    b.K = L.out_pad[l];
+    b.A = dZ;
+    b.lda = L.out_pad[l];
+    b.B = w.Wt + L.wb_off[l];
+    b.ldb = L.out_pad[l];
+    b.k_per_split = b.K;
+    b.Zin = m->Z[l - 1];
+    b.ldz = L.in_pad[l];
+    b.O = m->dZ[l - 1];
+    b.ldo = L.in_pad[l];
+    b.Ot = m->dZt[l - 1];
+    b.ldot = n;
+    if ((rc = gemm<EPI_HIDDEN_BWD>(m, b, 1, s))) return rc;
+  }
+  return BD_OK;
+}
+
+int check_member(BdMlp* m, int member) {
+  if (!m) return BD_ERR_ARG;
+  if (member < 0 || member >= m->d.n_members) return mfail(m, BD_ERR_ARG, "member %d out of range", member);
+  MCK(m, cudaSetDevice(m->device));
+  return BD_OK;
+}
+
+}  // namespace
+
+// Ensemble inference for the stepper (same translation unit boundary as the C ABI).
+int bd_internal_mlp_ensemble(BdMlp* m, int64_t n, const float* X, float* mean, float* spread, cudaStream_t s) {
+  int rc;
+  if ((rc = ensure_infer(m))) return rc;
+  const LayerGeom& L = m->L;
+  const int od = m->d.out_dim;
+  for (int64_t r0 = 0; r0 < n; r0 += kChunkRows) {
+    const int rows = (int)std::min<int64_t>(kChunkRows, n - r0);
+    pack_input_kernel<<<grid_for(m, (long long)rows * L.in_pad[0]), 256, 0, s>>>(
+        X + r0 * m->d.in_dim, rows, m->d.in_dim, m->Xi, L.in_pad[0], nullptr, 0);
+    MCK(m, cudaGetLastError());
+    for (int k = 0; k < m->d.n_members; ++k)
+      if ((rc = forward(m, k, rows, m->Xi, m->Ys + (size_t)k * m->infer_cap * od, od, false, s))) return rc;
+    ensemble_kernel<<<grid_for(m, (long long)rows * od), 256, 0, s>>>(
+        m->Ys, m->d.n_members, (long long)m->infer_cap * od, rows, od, mean + r0 * od,
+        spread ? spread + r0 * od : nullptr, nullptr);
+    MCK(m, cudaGetLastError());
+  }
+  return BD_OK;
+}
+
+// The stepper's view: shape checks, buffers for `rows` rows (before any graph
+// capture), and the ensemble on packed BF16 feature rows whose count is on the device.
+int bd_internal_mlp_shape(const BdMlp* m, int* in_dim, int* in_pad, int* out_dim) {
+  *in_dim = m->d.in_dim;
+  *in_pad = m->L.in_pad[0];
+  *out_dim = m->d.out_dim;
+  return BD_OK;
+}
+
+int bd_internal_mlp_prepare(BdMlp* m, int rows) {
+  MCK(m, cudaSetDevice(m->device));
+  return ensure_infer(m, rows);
+}
+
+int bd_internal_mlp_ensemble_rows(BdMlp* m, int rows, const int* n_dev, const void* Xpacked, float* mean,
+                                  float* spread, cudaStream_t s) {
+  if (rows > m->infer_cap) return mfail(m, BD_ERR_STATE, "inference buffers hold %d rows, %d asked", m->infer_cap, rows);
+  const int od = m->d.out_dim;
+  int rc;
+  for (int k = 0; k < m->d.n_members; ++k)
+    if ((rc = forward(m, k, rows, (const bf16*)Xpacked, m->Ys + (size_t)k * m->infer_cap * od, od, false, s, n_dev)))
+      return rc;
+  ensemble_kernel<<<grid_for(m, (long long)rows * od), 256, 0, s>>>(m->Ys, m->d.n_members, (long long)m->infer_cap * od,
+                                                                     rows, od, mean, spread, n_dev);
+  MCK(m, cudaGetLastError());
+  return BD_OK;
+}
+
+const char* bd_internal_mlp_error(const BdMlp* m) { return m->err.c_str(); }
+
+extern "C" {
+
+int bd_mlp_create(int device, const BdMlpDesc* d, BdMlp** out) {
+  if (!out || !d) return BD_ERR_ARG;
+  *out = nullptr;
+  if (d->n_members < 1 || d->n_members > 8 || d->in_dim < 1 || d->in_dim > 32 || d->hidden < 128 ||
+      d->hidden % 128 || d->hidden > 512 || d->n_hidden < 1 || d->n_hidden > kMaxLayers - 1 || d->out_dim < 1 ||
+      d->out_dim > 32)
+    return BD_ERR_ARG;
+  BdMlp* m = new BdMlp();
+  m->device = device;
+  m->d = *d;
+  if (cudaSetDevice(device) != cudaSuccess) {
+    delete m;
+    return BD_ERR_CUDA;
+  }
+  cudaDeviceGetAttribute(&m->n_sm, cudaDevAttrMultiProcessorCount, device);
+  LayerGeom& L = m->L;
+  L.n_layers = d->n_hidden + 1;
+  long long off = 0, woff = 0;
+  for (int l = 0; l < L.n_layers; ++l) {
+    L.in_real[l] = l == 0 ? d->in_dim : d->hidden;
+    L.out_real[l] = l + 1 == L.n_layers ? d->out_dim : d->hidden;
+    L.in_pad[l] = round_up(L.in_real[l], 32);
+    L.out_pad[l] = round_up(L.out_real[l], 32);
+    L.w_off[l] = off;
+    off += (long long)L.out_real[l] * L.in_real[l];
+    L.b_off[l] = off;
+    off += L.out_real[l];
+    L.wb_off[l] = woff;
+    woff += (long long)L.out_pad[l] * L.in_pad[l];
+  }
+  m->n_params = off;
+  m->wb_size = woff;
+  m->mem.resize(d->n_members);
+  uint64_t seed = d->seed;
+  std::vector<float> init(off);
+  for (int k = 0; k < d->n_members; ++k) {
+    BdMlp::Member& w = m->mem[k];
+    void* p;
+    int rc = 0;
+    if ((rc = malloc_into(m, m->allocs, &p, off * 4))) goto fail;
+    w.p = (float*)p;
+    if ((rc = malloc_into(m, m->allocs, &p, off * 4))) goto fail;
+    w.m1 = (float*)p;
+    if ((rc = malloc_into(m, m->allocs, &p, off * 4))) goto fail;
+    w.m2 = (float*)p;
+    if ((rc = malloc_into(m, m->allocs, &p, off * 4))) goto fail;
+    w.grad = (float*)p;
+    if ((rc = malloc_into(m, m->allocs, &p, woff * 2))) goto fail;
+    w.Wb = (bf16*)p;
+    if ((rc = malloc_into(m, m->allocs, &p, woff * 2))) goto fail;
+    w.Wt = (bf16*)p;
+    // uniform(-1/sqrt(fan_in), 1/sqrt(fan_in)) for weights and biases, member by member
+    for (int l = 0; l < L.n_layers; ++l) {
+      const float bound = 1.0f / std::sqrt((float)L.in_real[l]);
+      for (long long i = L.w_off[l]; i < L.b_off[l] + L.out_real[l]; ++i) {
+        const double u = (double)(splitmix(seed) >> 11) * (1.0 / 9007199254740992.0);
+        init[i] = (float)((2.0 * u - 1.0) * bound);
+      }
+    }
+    if (cudaMemcpy(w.p, init.data(), off * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+      rc = BD_ERR_CUDA;
+      goto fail;
+    }
+    refresh_kernel<<<grid_for(m, off), 256>>>(w.p, off, L, w.Wb, w.Wt);
+    continue;
+  fail:
+    for (void* q : m->allocs) cudaFree(q);
+    delete m;
+    return rc;
+  }
+  if (cudaDeviceSynchronize() != cudaSuccess) {
+    for (void* q : m->allocs) cudaFree(q);
+    delete m;
+    return BD_ERR_CUDA;
+  }
+  *out = m;
+  return BD_OK;
+}
+
+int bd_mlp_destroy(BdMlp* m) {
+  if (!m) return BD_OK;
+  cudaSetDevice(m->device);
+  cudaDeviceSynchronize();
+  for (void* p : m->train_allocs) cudaFree(p);
+  for (void* p : m->infer_allocs) cudaFree(p);
+  for (void* p : m->allocs) cudaFree(p);
+  delete m;
+  return BD_OK;
+}
+
+int bd_mlp_last_error(const BdMlp* m, char* buf, int len) {
+  if (!buf || len <= 0) return BD_ERR_ARG;
+  snprintf(buf, (size_t)len, "%s", m ? m->err.c_str() : "no MLP");
+  return BD_OK;
+}
+
+int bd_mlp_n_params(const BdMlp* m, int64_t* n) {
+  if (!m || !n) return BD_ERR_ARG;
+  *n = m->n_params;
+  return BD_OK;
+}
+
+int bd_mlp_get_params(BdMlp* m, int member, float* params) {
+  int rc = check_member(m, member);
+  if (rc) return rc;
+  if (!params) return mfail(m, BD_ERR_ARG, "params is NULL");
+  MCK(m, cudaDeviceSynchronize());
+  MCK(m, cudaMemcpy(params, m->mem[member].p, m->n_params * 4, cudaMemcpyDeviceToHost));
+  return BD_OK;
+}
+
+int bd_mlp_set_params(BdMlp* m, int member, const float* params) {
+  int rc = check_member(m, member);
+  if (rc) return rc;
+  if (!params) return mfail(m, BD_ERR_ARG, "params is NULL");
+  BdMlp::Member& w = m->mem[member];
+  MCK(m, cudaDeviceSynchronize());
+  MCK(m, cudaMemcpy(w.p, params, m->n_params * 4, cudaMemcpyHostToDevice));
+  MCK(m, cudaMemset(w.m1, 0, m->n_params * 4));
+  MCK(m, cudaMemset(w.m2, 0, m->n_params * 4));
+  w.step = 0;
+  refresh_kernel<<<grid_for(m, m->n_params), 256>>>(w.p, m->n_params, m->L, w.Wb, w.Wt);
+  MCK(m, cudaGetLastError());
+  MCK(m, cudaDeviceSynchronize());
+  return BD_OK;
+}
+
+int bd_mlp_forward(BdMlp* m, int member, int64_t n, const float* X, float* Y, void* stream) {
+  int rc = check_member(m, member);
+  if (rc) return rc;
+  if (n < 0 || (n > 0 && (!X || !Y))) return mfail(m, BD_ERR_ARG, "bd_mlp_forward: bad arguments");
+  if ((rc = ensure_infer(m))) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  for (int64_t r0 = 0; r0 < n; r0 += kChunkRows) {
+    const int rows = (int)std::min<int64_t>(kChunkRows, n - r0);
+    pack_input_kernel<<<grid_for(m, (long long)rows * m->L.in_pad[0]), 256, 0, s>>>(
+        X + r0 * m->d.in_dim, rows, m->d.in_dim, m->Xi, m->L.in_pad[0], nullptr, 0);
+    MCK(m, cudaGetLastError());
+    if ((rc = forward(m, member, rows, m->Xi, Y + r0 * m->d.out_dim, m->d.out_dim, false, s))) return rc;
+  }
+  return BD_OK;
+}
+
+int bd_mlp_grad(BdMlp* m, int member, int n, const float* X, const float* T, float* grad, float* loss, void* stream) {
+  int rc = check_member(m, member);
+  if (rc) return rc;
+  if (n <= 0 || n % 32 || !X || !T) return mfail(m, BD_ERR_ARG, "bd_mlp_grad: n must be a positive multiple of 32");
+  cudaStream_t s = (cudaStream_t)stream;
+  if ((rc = backward(m, member, n, X, T, loss, s))) return rc;
+  if (grad) MCK(m, cudaMemcpyAsync(grad, m->mem[member].grad, m->n_params * 4, cudaMemcpyDeviceToDevice, s));
+  return BD_OK;
+}
+
+int bd_mlp_train_step(BdMlp* m, int member, int n, const float* X, const float* T, float lr, float* loss,
+                      void* stream) {
+  int rc = check_member(m, member);
+  if (rc) return rc;
+  if (n <= 0 || n % 32 || !X || !T || !(lr > 0))
+    return mfail(m, BD_ERR_ARG, "bd_mlp_train_step: n must be a positive multiple of 32 and lr > 0");
+  cudaStream_t s = (cudaStream_t)stream;
+  if ((rc = backward(m, member, n, X, T, loss, s))) return rc;
+  BdMlp::Member& w = m->mem[member];
+  w.step += 1;
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.0f - (float)std::pow((double)b1, (double)w.step);
+  const float c2 = 1.0f - (float)std::pow((double)b2, (double)w.step);
+  adam_kernel<<<grid_for(m, m->n_params), 256, 0, s>>>(w.p, w.grad, w.m1, w.m2, m->n_params, lr, b1, b2, 1e-8f, c1,
+                                                        c2, m->L, w.Wb, w.Wt);
+  MCK(m, cudaGetLastError());
+  return BD_OK;
+}
+
+int bd_mlp_ensemble(BdMlp* m, int64_t n, const float* X, float* mean, float* spread, void* stream) {
+  if (!m) return BD_ERR_ARG;
+  MCK(m, cudaSetDevice(m->device));
+  if (n < 0 || (n > 0 && (!X || !mean))) return mfail(m, BD_ERR_ARG, "bd_mlp_ensemble: bad arguments");
+  return bd_internal_mlp_ensemble(m, n, X, mean, spread, (cudaStream_t)stream);
+}
+
+}  // extern "C"

@@ -190,9 +190,20 @@ class B200ForceEngine:
             return F, T, E
         return F.cpu().numpy(), T.cpu().numpy(), E.cpu().numpy()
 
-    def eval_poses(self, centroids, rotations, precision=None, torque_mode=None):
-        """Forces for poses (centroid + quaternion (w,x,y,z) or 3x3 matrix) with the ligand from ``set_ligand``."""
+    def eval_poses(self, centroids, rotations, precision=None, torque_mode=None, terms=None):
+        """Forces for poses (centroid + quaternion (w,x,y,z) or 3x3 matrix) with the ligand from ``set_ligand``.
+
+        ``terms`` (``_lib.TERM_*`` bits) restricts the sum to some force terms; the
+        surrogate's training targets are ``TERM_FARFIELD | TERM_REV_BORN``.
+        """
         import torch
+
+        if terms is not None:
+            self.handle.call("bd_set_terms", int(terms))
+            try:
+                return self.eval_poses(centroids, rotations, precision, torque_mode)
+            finally:
+                self.handle.call("bd_set_terms", _lib.TERM_ALL)
 
         dev = torch.device("cuda", self.handle.device)
         as_torch = isinstance(centroids, torch.Tensor)

@@ -119,7 +119,7 @@ class B200BatchSimulator:
 
     def __init__(self, mol1, mol2, mob, pathway_set, params, batch_engine, *, precision=None, torque_mode=None,
                  termination="reference", steps_per_launch=64, launches_per_poll=8, slots=0, id_offset=0,
-                 stats=None, verbose=False):
+                 stats=None, surrogate=None, verbose=False):
         if not hasattr(batch_engine, "handle"):
             raise TypeError("batch_engine must be a B200ForceEngine")
         if any(getattr(r, "state_before", None) is not None for r in pathway_set.reactions):
@@ -138,6 +138,8 @@ class B200BatchSimulator:
         # per-step statistics for write_all: on when the pipeline attached an output config
         self.stats = bool(getattr(params, "_output_cfg", None) is not None) if stats is None else bool(stats)
         self.verbose = verbose
+        # (MLPEnsemble, SurrogateSpec): far-field + reverse Born from the learned surrogate inside its trust region
+        self.surrogate = surrogate
         c0 = np.asarray(mol2.centroid(), dtype=float)
         self._mol2_pos0 = np.asarray(mol2.positions_array(), dtype=float) - c0
         self._charges = np.asarray(mol2.charges_array(), dtype=float)
@@ -206,12 +208,22 @@ class B200BatchSimulator:
         sp.id_offset = self.id_offset
         sp.stats = int(self.stats)
         h.call("bd_sim_configure", _lib.C.byref(sp))
+        if self.surrogate is not None:
+            ens, spec = self.surrogate
+            h.call("bd_sim_set_surrogate", ens.h, _lib.C.byref(spec.c_params()))
+        else:
+            h.call("bd_sim_set_surrogate", None, None)
         return D_t
 
     def read_counters(self):
         out = np.zeros(_lib.N_CTR, dtype=np.uint64)
         self.engine.handle.call("bd_sim_counters", _lib.ptr(out, _lib.C.c_uint64), _lib.N_CTR, None)
-        return dict(zip(_lib.CTR_NAMES, (int(v) for v in out)))
+        d = dict(zip(_lib.CTR_NAMES, (int(v) for v in out)))
+        if self.surrogate is not None:
+            s = np.zeros(2, dtype=np.uint64)
+            self.engine.handle.call("bd_sim_surrogate_counters", _lib.ptr(s, _lib.C.c_uint64))
+            d["surrogate_evals"], d["surrogate_fallbacks"] = int(s[0]), int(s[1])
+        return d
 
     def read_stats(self):
         """Per-step statistics as host arrays (requires ``stats=True``)."""
