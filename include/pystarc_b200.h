@@ -244,6 +244,12 @@ int bd_mlp_grad(BdMlp* m, int member, int n, const float* X, const float* T, flo
 /* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8, bias-corrected) of one member on a batch. */
 int bd_mlp_train_step(BdMlp* m, int member, int n, const float* X, const float* T, float lr, float* loss,
                       void* stream);
+/* `steps` Adam steps of one member on random batches (rows drawn with replacement by a
+ * counter-based hash of seed, member and step) of device-resident data X (n_data x in_dim),
+ * T (n_data x out_dim).  The step is captured once as a CUDA graph and replayed; loss_trace
+ * (device, `steps` floats, may be NULL) receives each step's batch loss. */
+int bd_mlp_train(BdMlp* m, int member, int64_t n_data, const float* X, const float* T, int batch, int steps,
+                 float lr, uint64_t seed, float* loss_trace, void* stream);
 /* All members on n rows: mean (n x out_dim) and spread (n x out_dim, RMS deviation of the
  * members from the mean; may be NULL). */
 int bd_mlp_ensemble(BdMlp* m, int64_t n, const float* X, float* mean, float* spread, void* stream);
@@ -255,8 +261,8 @@ int bd_mlp_ensemble(BdMlp* m, int64_t n, const float* X, float* mean, float* spr
  * exp(-((|c| - rbf_centre[k]) / rbf_width)^2 / 2)); then the surrogate's far-field + reverse Born
  * (mean output x out_scale x envelope) where the members agree (spread of the force <=
  * threshold x max(|force|, force_floor x envelope)), the exact kernels elsewhere, and the rest
- * of the step.  envelope = exp(-(|c| - env_ref) / env_length) (env_ref / |c|)^2, or 1 when
- * env_length is 0.  The
+ * of the step.  envelope(|c|) = exp of env_log interpolated linearly over 32 evenly spaced radii
+ * from env_r0 to env_r1 (clamped outside), or 1 when env_r1 <= env_r0.  The
  * ensemble needs 13 inputs and 6 outputs (force, torque).  m = NULL returns to the fused
  * exact stepper.  The ensemble must not be used by other calls while the stepper runs, and
  * per-step statistics are not collected in this mode. */
@@ -268,7 +274,8 @@ typedef struct {
   double r_min, r_max;
   double threshold;
   double force_floor;
-  double env_length, env_ref;
+  double env_r0, env_r1;
+  double env_log[32];
 } BdSurrogateParams;
 int bd_sim_set_surrogate(BdHandle* h, BdMlp* m, const BdSurrogateParams* p);
 /* Trusted-pose evaluations and exact fallbacks since configure: out[0], out[1]. */

@@ -62,8 +62,8 @@ ST_RAD_BINS, ST_THETA, ST_PHI, ST_MILESTONES, ST_TRANS = 200, 36, 72, 11, 50
 class BdSurrogateParams(C.Structure):
     _fields_ = [("r_scale", C.c_double), ("rbf_centre", C.c_double * 5), ("rbf_width", C.c_double),
                 ("out_scale", C.c_double * 6), ("r_min", C.c_double), ("r_max", C.c_double),
-                ("threshold", C.c_double), ("force_floor", C.c_double), ("env_length", C.c_double),
-                ("env_ref", C.c_double)]
+                ("threshold", C.c_double), ("force_floor", C.c_double), ("env_r0", C.c_double),
+                ("env_r1", C.c_double), ("env_log", C.c_double * 32)]
 
 
 class BdMlpDesc(C.Structure):
@@ -120,6 +120,7 @@ SIGNATURES = {
     "bd_mlp_grad": (C.c_int, [P, C.c_int, C.c_int, P, P, P, P, P]),
     "bd_mlp_train_step": (C.c_int, [P, C.c_int, C.c_int, P, P, C.c_float, P, P]),
     "bd_mlp_ensemble": (C.c_int, [P, C.c_int64, P, P, P, P]),
+    "bd_mlp_train": (C.c_int, [P, C.c_int, C.c_int64, P, P, C.c_int, C.c_int, C.c_float, C.c_uint64, P, P]),
 }
 
 _LIB = None

@@ -665,9 +665,12 @@ int bd_sim_set_surrogate(BdHandle* h, BdMlp* m, const BdSurrogateParams* p) {
   q.r_max = p->r_max;
   q.threshold = p->threshold;
   q.force_floor = p->force_floor;
-  q.env_length = p->env_length;
-  q.env_ref = p->env_ref;
-  if (q.env_length > 0 && !(q.env_ref > 0)) return fail(h, BD_ERR_ARG, "the envelope needs env_ref > 0");
+  q.env_r0 = p->env_r0;
+  q.env_r1 = p->env_r1;
+  for (int k = 0; k < kSurEnv; ++k) {
+    if (!std::isfinite(p->env_log[k])) return fail(h, BD_ERR_ARG, "envelope entry %d is not finite", k);
+    q.env_log[k] = p->env_log[k];
+  }
   h->sur = m;
   return BD_OK;
 }

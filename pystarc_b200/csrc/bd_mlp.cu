@@ -262,33 +262,60 @@ __global__ void loss_kernel(const float* __restrict__ Y, int ldy, const float* _
 }
 
 // loss = sum(partials) / (n out_dim), in a fixed order.
-__global__ void loss_finish_kernel(const float* __restrict__ partial, int nb, float denom, float* __restrict__ loss) {
+__global__ void loss_finish_kernel(const float* __restrict__ partial, int nb, float denom, float* __restrict__ loss,
+                                   float* __restrict__ trace, const long long* __restrict__ step) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   float s = 0.f;
   for (int i = 0; i < nb; ++i) s += partial[i];
-  *loss = s / denom;
+  if (loss) *loss = s / denom;
+  if (trace) trace[*step] = s / denom;
 }
 
 // Weight gradient of one layer from split partials (summed in split order) and
 // bias gradient as the row sums of dZ^T [out_pad][ldt] over the first n columns.
 __global__ void grad_reduce_kernel(const float* __restrict__ part, int splits, long long split_stride, int ldp,
-                                   int out_real, int in_real, const bf16* __restrict__ dZt, int ldt, int n,
-                                   float* __restrict__ gW, float* __restrict__ gb) {
+                                   int out_real, int in_real, float* __restrict__ gW) {
   const int total = out_real * in_real;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total + out_real; i += gridDim.x * blockDim.x) {
-    if (i < total) {
-      const int o = i / in_real, c = i % in_real;
-      float s = 0.f;
-      for (int z = 0; z < splits; ++z) s += part[z * split_stride + (size_t)o * ldp + c];
-      gW[i] = s;
-    } else {
-      const int o = i - total;
-      float s = 0.f;
-      for (int m = 0; m < n; ++m) s += __bfloat162float(dZt[(size_t)o * ldt + m]);
-      gb[o] = s;
-    }
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    const int o = i / in_real, c = i % in_real;
+    float s = 0.f;
+    for (int z = 0; z < splits; ++z) s += part[z * split_stride + (size_t)o * ldp + c];
+    gW[i] = s;
   }
 }
+
+// Bias gradient: one warp per output row o sums dZ^T[o][0..n) (lanes stride the
+// row, then a fixed-order butterfly).
+__global__ void bias_grad_kernel(const bf16* __restrict__ dZt, int ldt, int n, int out_real, float* __restrict__ gb) {
+  const int lane = threadIdx.x & 31;
+  for (int o = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; o < out_real; o += (gridDim.x * blockDim.x) >> 5) {
+    float s = 0.f;
+    for (int m = lane; m < n; m += 32) s += __bfloat162float(dZt[(size_t)o * ldt + m]);
+#pragma unroll
+    for (int w = 16; w > 0; w >>= 1) s += __shfl_xor_sync(0xffffffffu, s, w);
+    if (lane == 0) gb[o] = s;
+  }
+}
+
+// Random training batch: row i of the batch is data row hash(seed, step, i) mod n_data.
+__global__ void gather_batch_kernel(const float* __restrict__ X, const float* __restrict__ T, long long n_data,
+                                    int in_dim, int out_dim, int batch, unsigned long long seed,
+                                    const long long* __restrict__ step, float* __restrict__ Xb,
+                                    float* __restrict__ Tb) {
+  const long long st = *step;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < batch; i += gridDim.x * blockDim.x) {
+    unsigned long long z = seed ^ ((unsigned long long)st << 24) ^ (unsigned long long)i;
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    const long long r = (long long)(z % (unsigned long long)n_data);
+    for (int k = 0; k < in_dim; ++k) Xb[(size_t)i * in_dim + k] = X[r * in_dim + k];
+    for (int k = 0; k < out_dim; ++k) Tb[(size_t)i * out_dim + k] = T[r * out_dim + k];
+  }
+}
+
+__global__ void step_increment_kernel(long long* step) { *step += 1; }
 
 struct LayerGeom {
   int in_real[kMaxLayers], out_real[kMaxLayers], in_pad[kMaxLayers], out_pad[kMaxLayers];
@@ -300,7 +327,11 @@ struct LayerGeom {
 // Adam on the FP32 parameters, then the padded BF16 copies W [out_pad][in_pad] and W^T [in_pad][out_pad].
 __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ grad, float* __restrict__ m1,
                             float* __restrict__ m2, long long n_params, float lr, float b1, float b2, float eps,
-                            float c1, float c2, LayerGeom L, bf16* __restrict__ Wb, bf16* __restrict__ Wt) {
+                            const long long* __restrict__ t_prev, LayerGeom L, bf16* __restrict__ Wb,
+                            bf16* __restrict__ Wt) {
+  // bias corrections of step t = t_prev + 1
+  const double t = (double)(*t_prev + 1);
+  const float c1 = (float)(1.0 - pow((double)b1, t)), c2 = (float)(1.0 - pow((double)b2, t));
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n_params;
        i += (long long)gridDim.x * blockDim.x) {
     const float gi = grad[i];
@@ -372,8 +403,19 @@ struct BdMlp {
   struct Member {
     float *p = nullptr, *m1 = nullptr, *m2 = nullptr, *grad = nullptr;
     bf16 *Wb = nullptr, *Wt = nullptr;
-    long long step = 0;
+    long long* step = nullptr;  // device: Adam steps taken
   };
+  // graph of one training step (bd_mlp_train), rebuilt when its arguments change
+  cudaGraphExec_t train_graph = nullptr;
+  int tg_member = -1, tg_batch = 0;
+  const float *tg_X = nullptr, *tg_T = nullptr;
+  long long tg_n = 0;
+  float tg_lr = 0.f;
+  unsigned long long tg_seed = 0;
+  float* tg_trace = nullptr;
+  float *Xbatch = nullptr, *Tbatch = nullptr;
+  int batch_cap = 0;
+  long long* data_step = nullptr;  // device: batches drawn by bd_mlp_train
   std::vector<Member> mem;
   std::vector<void*> allocs;  // everything, freed at destroy
   // training scratch (sized for `train_cap` rows)
@@ -444,6 +486,10 @@ int gemm(BdMlp* m, const GemmArgs& g, int splits, cudaStream_t s) {
 
 int ensure_train(BdMlp* m, int n) {
   if (n <= m->train_cap) return BD_OK;
+  if (m->train_graph) {  // it holds the old buffers
+    cudaGraphExecDestroy(m->train_graph);
+    m->train_graph = nullptr;
+  }
   for (void* p : m->train_allocs) cudaFree(p);
   m->train_allocs.clear();
   m->Z.assign(m->L.n_layers, nullptr);
@@ -554,7 +600,8 @@ int forward(BdMlp* m, int member, int n, const bf16* Xb, float* Y, int ldy, bool
 }
 
 // Loss and gradient of one member on n rows (n % 32 == 0) into the member's grad buffer.
-int backward(BdMlp* m, int member, int n, const float* X, const float* T, float* loss, cudaStream_t s) {
+int backward(BdMlp* m, int member, int n, const float* X, const float* T, float* loss, cudaStream_t s,
+             float* trace = nullptr) {
   const LayerGeom& L = m->L;
   BdMlp::Member& w = m->mem[member];
   int rc;
@@ -567,7 +614,8 @@ int backward(BdMlp* m, int member, int n, const float* X, const float* T, float*
   const int nb = grid_for(m, (long long)n * op);
   loss_kernel<<<nb, 256, 0, s>>>(m->Y, op, T, n, m->d.out_dim, m->dY, op, m->dYt, n, m->loss_part);
   MCK(m, cudaGetLastError());
-  loss_finish_kernel<<<1, 32, 0, s>>>(m->loss_part, nb, (float)n * (float)m->d.out_dim, loss ? loss : m->loss_tmp);
+  loss_finish_kernel<<<1, 32, 0, s>>>(m->loss_part, nb, (float)n * (float)m->d.out_dim, loss ? loss : m->loss_tmp,
+                                     trace, trace ? m->data_step : nullptr);
   MCK(m, cudaGetLastError());
   const int splits = std::max(1, std::min(64, n / 256));
   const int kps = round_up((n + splits - 1) / splits, kBK);
@@ -590,10 +638,11 @@ int backward(BdMlp* m, int member, int n, const float* X, const float* T, float*
     g.split_stride = m->part_stride;
     const int used = (n + kps - 1) / kps;
     if ((rc = gemm<EPI_PARTIAL>(m, g, used, s))) return rc;
-    const int tot = L.out_real[l] * L.in_real[l] + L.out_real[l];
+    const int tot = L.out_real[l] * L.in_real[l];
     grad_reduce_kernel<<<grid_for(m, tot), 256, 0, s>>>(m->part, used, m->part_stride, L.in_pad[l], L.out_real[l],
-                                                         L.in_real[l], dZt, n, n, w.grad + L.w_off[l],
-                                                         w.grad + L.b_off[l]);
+                                                         L.in_real[l], w.grad + L.w_off[l]);
+    MCK(m, cudaGetLastError());
+    bias_grad_kernel<<<(L.out_real[l] * 32 + 255) / 256, 256, 0, s>>>(dZt, n, n, L.out_real[l], w.grad + L.b_off[l]);
     MCK(m, cudaGetLastError());
     if (l == 0) break;
     // dZ_{l-1} = (dZ_l W_l) * SiLU'(Z_{l-1}): M = n, N = in_pad (hidden), K = out_pad
@@ -644,6 +693,31 @@ int bd_internal_mlp_ensemble(BdMlp* m, int64_t n, const float* X, float* mean, f
         spread ? spread + r0 * od : nullptr, nullptr);
     MCK(m, cudaGetLastError());
   }
+  return BD_OK;
+}
+
+int adam_update(BdMlp* m, int member, float lr, cudaStream_t s) {
+  BdMlp::Member& w = m->mem[member];
+  adam_kernel<<<grid_for(m, m->n_params), 256, 0, s>>>(w.p, w.grad, w.m1, w.m2, m->n_params, lr, 0.9f, 0.999f, 1e-8f,
+                                                        w.step, m->L, w.Wb, w.Wt);
+  MCK(m, cudaGetLastError());
+  step_increment_kernel<<<1, 1, 0, s>>>(w.step);
+  MCK(m, cudaGetLastError());
+  return BD_OK;
+}
+
+// One training step on a random batch of device-resident data: gather, forward,
+// loss, backward, Adam.  Enqueued once under stream capture and replayed.
+int enqueue_train_step(BdMlp* m, int member, long long n_data, const float* X, const float* T, int batch, float lr,
+                       unsigned long long seed, float* trace, cudaStream_t s) {
+  gather_batch_kernel<<<grid_for(m, batch), 256, 0, s>>>(X, T, n_data, m->d.in_dim, m->d.out_dim, batch, seed,
+                                                         m->data_step, m->Xbatch, m->Tbatch);
+  MCK(m, cudaGetLastError());
+  int rc = backward(m, member, batch, m->Xbatch, m->Tbatch, nullptr, s, trace);
+  if (rc) return rc;
+  if ((rc = adam_update(m, member, lr, s))) return rc;
+  step_increment_kernel<<<1, 1, 0, s>>>(m->data_step);
+  MCK(m, cudaGetLastError());
   return BD_OK;
 }
 
@@ -730,6 +804,8 @@ int bd_mlp_create(int device, const BdMlpDesc* d, BdMlp** out) {
     w.Wb = (bf16*)p;
     if ((rc = malloc_into(m, m->allocs, &p, woff * 2))) goto fail;
     w.Wt = (bf16*)p;
+    if ((rc = malloc_into(m, m->allocs, &p, sizeof(long long)))) goto fail;
+    w.step = (long long*)p;
     // uniform(-1/sqrt(fan_in), 1/sqrt(fan_in)) for weights and biases, member by member
     for (int l = 0; l < L.n_layers; ++l) {
       const float bound = 1.0f / std::sqrt((float)L.in_real[l]);
@@ -762,6 +838,7 @@ int bd_mlp_destroy(BdMlp* m) {
   if (!m) return BD_OK;
   cudaSetDevice(m->device);
   cudaDeviceSynchronize();
+  if (m->train_graph) cudaGraphExecDestroy(m->train_graph);
   for (void* p : m->train_allocs) cudaFree(p);
   for (void* p : m->infer_allocs) cudaFree(p);
   for (void* p : m->allocs) cudaFree(p);
@@ -799,7 +876,7 @@ int bd_mlp_set_params(BdMlp* m, int member, const float* params) {
   MCK(m, cudaMemcpy(w.p, params, m->n_params * 4, cudaMemcpyHostToDevice));
   MCK(m, cudaMemset(w.m1, 0, m->n_params * 4));
   MCK(m, cudaMemset(w.m2, 0, m->n_params * 4));
-  w.step = 0;
+  MCK(m, cudaMemset(w.step, 0, sizeof(long long)));
   refresh_kernel<<<grid_for(m, m->n_params), 256>>>(w.p, m->n_params, m->L, w.Wb, w.Wt);
   MCK(m, cudaGetLastError());
   MCK(m, cudaDeviceSynchronize());
@@ -840,14 +917,70 @@ int bd_mlp_train_step(BdMlp* m, int member, int n, const float* X, const float* 
     return mfail(m, BD_ERR_ARG, "bd_mlp_train_step: n must be a positive multiple of 32 and lr > 0");
   cudaStream_t s = (cudaStream_t)stream;
   if ((rc = backward(m, member, n, X, T, loss, s))) return rc;
-  BdMlp::Member& w = m->mem[member];
-  w.step += 1;
-  const float b1 = 0.9f, b2 = 0.999f;
-  const float c1 = 1.0f - (float)std::pow((double)b1, (double)w.step);
-  const float c2 = 1.0f - (float)std::pow((double)b2, (double)w.step);
-  adam_kernel<<<grid_for(m, m->n_params), 256, 0, s>>>(w.p, w.grad, w.m1, w.m2, m->n_params, lr, b1, b2, 1e-8f, c1,
-                                                        c2, m->L, w.Wb, w.Wt);
-  MCK(m, cudaGetLastError());
+  return adam_update(m, member, lr, s);
+}
+
+int bd_mlp_train(BdMlp* m, int member, int64_t n_data, const float* X, const float* T, int batch, int steps,
+                 float lr, uint64_t seed, float* loss_trace, void* stream) {
+  int rc = check_member(m, member);
+  if (rc) return rc;
+  if (n_data <= 0 || !X || !T || batch <= 0 || batch % 32 || steps < 0 || !(lr > 0))
+    return mfail(m, BD_ERR_ARG, "bd_mlp_train: need data, a batch that is a positive multiple of 32, lr > 0");
+  cudaStream_t s = (cudaStream_t)stream;
+  if ((rc = ensure_train(m, batch))) return rc;
+  if (batch > m->batch_cap) {
+    void* p;
+    MCK(m, cudaDeviceSynchronize());
+    if ((rc = malloc_into(m, m->allocs, &p, (size_t)batch * m->d.in_dim * 4))) return rc;
+    m->Xbatch = (float*)p;
+    if ((rc = malloc_into(m, m->allocs, &p, (size_t)batch * m->d.out_dim * 4))) return rc;
+    m->Tbatch = (float*)p;
+    m->batch_cap = batch;
+    if (m->train_graph) {
+      cudaGraphExecDestroy(m->train_graph);
+      m->train_graph = nullptr;
+    }
+  }
+  if (!m->data_step) {
+    void* p;
+    if ((rc = malloc_into(m, m->allocs, &p, sizeof(long long)))) return rc;
+    m->data_step = (long long*)p;
+  }
+  // the loss trace is indexed by batches drawn since this call began
+  MCK(m, cudaMemsetAsync(m->data_step, 0, sizeof(long long), s));
+  if (!m->train_graph || m->tg_member != member || m->tg_batch != batch || m->tg_X != X || m->tg_T != T ||
+      m->tg_n != n_data || m->tg_lr != lr || m->tg_seed != seed || m->tg_trace != loss_trace) {
+    if (m->train_graph) {
+      cudaGraphExecDestroy(m->train_graph);
+      m->train_graph = nullptr;
+    }
+    cudaStream_t cs;
+    MCK(m, cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaGraph_t g;
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+      cudaStreamDestroy(cs);
+      MCK(m, e);
+    }
+    rc = enqueue_train_step(m, member, n_data, X, T, batch, lr, seed ^ ((unsigned long long)member << 56), loss_trace,
+                            cs);
+    e = cudaStreamEndCapture(cs, &g);
+    cudaStreamDestroy(cs);
+    if (rc) return rc;
+    MCK(m, e);
+    e = cudaGraphInstantiate(&m->train_graph, g, 0);
+    cudaGraphDestroy(g);
+    MCK(m, e);
+    m->tg_member = member;
+    m->tg_batch = batch;
+    m->tg_X = X;
+    m->tg_T = T;
+    m->tg_n = n_data;
+    m->tg_lr = lr;
+    m->tg_seed = seed;
+    m->tg_trace = loss_trace;
+  }
+  for (int i = 0; i < steps; ++i) MCK(m, cudaGraphLaunch(m->train_graph, s));
   return BD_OK;
 }
 

@@ -26,20 +26,27 @@ namespace bd {
 
 constexpr int kSurIn = 13, kSurInPad = 32, kSurOut = 6;
 
+constexpr int kSurEnv = 32;  // radial envelope table entries
+
 struct DevSurrogate {
   double r_scale, rbf_centre[5], rbf_width;
   double out_scale[kSurOut];
   double r_min, r_max, threshold, force_floor;
-  double env_length, env_ref;  // radial envelope of the outputs (env_length 0: none)
+  double env_r0, env_r1;       // envelope table range (env_r1 <= env_r0: no envelope)
+  double env_log[kSurEnv];     // log of the force size at kSurEnv evenly spaced radii
 };
 
-// Outputs are normalised by out_scale and by exp(-(r - env_ref) / env_length) (env_ref / r)^2,
-// the radial fall-off of a screened monopole, so that the network sees targets of similar
-// size at every distance.
+// Outputs are normalised by out_scale and by a radial envelope: the RMS force
+// size of the training targets as a function of |c|, interpolated linearly in
+// its log between table entries (clamped at the ends), so that the network sees
+// targets of similar size at every distance.
 __device__ __forceinline__ double sur_envelope(const DevSurrogate& Q, double r) {
-  if (!(Q.env_length > 0)) return 1.0;
-  const double x = Q.env_ref / r;
-  return exp(-(r - Q.env_ref) / Q.env_length) * x * x;
+  if (!(Q.env_r1 > Q.env_r0)) return 1.0;
+  double u = (r - Q.env_r0) / (Q.env_r1 - Q.env_r0) * (kSurEnv - 1);
+  u = fmin(fmax(u, 0.0), (double)(kSurEnv - 1));
+  const int i = min((int)u, kSurEnv - 2);
+  const double t = u - i;
+  return exp((1.0 - t) * Q.env_log[i] + t * Q.env_log[i + 1]);
 }
 
 // Per-slot scratch of one BD step.

@@ -43,8 +43,9 @@ class SurrogateSpec:
     r_max: float = 80.0  # upper end of the training poses
     threshold: float = 0.02  # ensemble force spread / force size above which the exact path runs
     force_floor: float = 0.0  # in envelope units: force sizes below force_floor * envelope count as that
-    env_length: float = 0.0  # radial envelope exp(-(r - env_ref) / env_length) (env_ref / r)^2; 0: none
-    env_ref: float = 25.0
+    env_r0: float = 0.0  # radial envelope: log force size at N_ENV radii from env_r0 to env_r1
+    env_r1: float = 0.0
+    env_log: tuple = (0.0,) * 32
 
     def features(self, c, q):
         """(n, 13) float32 features of centroids c (n, 3) and quaternions q (n, 4, w first)."""
@@ -58,10 +59,34 @@ class SurrogateSpec:
         return f.astype(np.float32)
 
     def envelope(self, r):
+        """Radial envelope of the outputs (the device's sur_envelope)."""
         r = np.asarray(r, dtype=np.float64)
-        if not self.env_length > 0:
+        if not self.env_r1 > self.env_r0:
             return np.ones_like(r)
-        return np.exp(-(r - self.env_ref) / self.env_length) * (self.env_ref / r) ** 2
+        k = len(self.env_log)
+        u = np.clip((r - self.env_r0) / (self.env_r1 - self.env_r0) * (k - 1), 0.0, k - 1.0)
+        i = np.minimum(u.astype(np.int64), k - 2)
+        t = u - i
+        lg = np.asarray(self.env_log)
+        return np.exp((1.0 - t) * lg[i] + t * lg[i + 1])
+
+    def fit_envelope(self, r, force, bins=32):
+        """Envelope from training targets: log RMS force size in evenly spaced radial bins."""
+        r = np.asarray(r, dtype=np.float64)
+        f2 = np.sum(np.asarray(force, dtype=np.float64) ** 2, axis=1)
+        lo, hi = float(r.min()), float(r.max())
+        edges = np.linspace(lo, hi, bins + 1)
+        idx = np.clip(np.searchsorted(edges, r, side="right") - 1, 0, bins - 1)
+        cnt = np.bincount(idx, minlength=bins)
+        rms = np.sqrt(np.bincount(idx, weights=f2, minlength=bins) / np.maximum(cnt, 1))
+        ok = (cnt > 0) & (rms > 0)
+        centres = 0.5 * (edges[:-1] + edges[1:])
+        grid = np.linspace(lo, hi, bins)
+        if ok.sum() == 0:
+            self.env_r0 = self.env_r1 = 0.0
+            return
+        self.env_log = tuple(float(v) for v in np.interp(grid, centres[ok], np.log(rms[ok])))
+        self.env_r0, self.env_r1 = lo, hi
 
     def c_params(self):
         """The ``BdSurrogateParams`` of this spec."""
@@ -73,7 +98,9 @@ class SurrogateSpec:
         for k in range(N_OUT):
             p.out_scale[k] = self.out_scale[k]
         p.r_min, p.r_max, p.threshold, p.force_floor = self.r_min, self.r_max, self.threshold, self.force_floor
-        p.env_length, p.env_ref = self.env_length, self.env_ref
+        p.env_r0, p.env_r1 = self.env_r0, self.env_r1
+        for k in range(32):
+            p.env_log[k] = self.env_log[k]
         return p
 
     def trusted(self, c):
@@ -152,6 +179,17 @@ class MLPEnsemble:
         """One Adam step; ``loss`` (a 1-element CUDA tensor) receives the batch loss if given."""
         self._call("bd_mlp_train_step", int(member), X.shape[0], _lib.P(X.data_ptr()), _lib.P(T.data_ptr()),
                    C.c_float(lr), _lib.P(loss.data_ptr() if loss is not None else 0), self._stream())
+
+    def train(self, member, X, T, batch, steps, lr, seed=0, trace=True):
+        """``steps`` Adam steps on random batches of device-resident (X, T); returns the loss trace."""
+        import torch
+
+        X, T = self._dev(X), self._dev(T)
+        tr = torch.zeros(max(steps, 1), dtype=torch.float32, device=X.device) if trace else None
+        self._call("bd_mlp_train", int(member), X.shape[0], _lib.P(X.data_ptr()), _lib.P(T.data_ptr()), int(batch),
+                   int(steps), C.c_float(lr), int(seed) & 0xFFFFFFFFFFFFFFFF,
+                   _lib.P(tr.data_ptr() if tr is not None else 0), self._stream())
+        return tr
 
     def ensemble(self, X):
         import torch
@@ -246,7 +284,9 @@ def fit(ens, spec, c, q, targets, steps=20000, batch=8192, lr=1e-3, seed=0, log=
     """
     import torch
 
-    env = spec.envelope(np.linalg.norm(np.asarray(c, dtype=np.float64), axis=1))[:, None]
+    rr = np.linalg.norm(np.asarray(c, dtype=np.float64), axis=1)
+    spec.fit_envelope(rr, np.asarray(targets)[:, :3])
+    env = spec.envelope(rr)[:, None]
     t = np.asarray(targets, dtype=np.float64) / env
     rms = np.sqrt(np.mean(t ** 2, axis=0))
     spec.out_scale = tuple(float(max(v, 1e-12)) for v in rms)
@@ -256,20 +296,18 @@ def fit(ens, spec, c, q, targets, steps=20000, batch=8192, lr=1e-3, seed=0, log=
     Y = torch.as_tensor((t / np.asarray(spec.out_scale)).astype(np.float32), device=dev)
     n = X.shape[0]
     batch = min(batch, n - n % 32)
-    loss = torch.zeros(1, dtype=torch.float32, device=dev)
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
     finals = []
     for m in range(ens.n_members):
-        g = torch.Generator(device=dev)
-        g.manual_seed(int(seed) * 1000 + m)
-        for s in range(steps):
-            idx = torch.randint(0, n, (batch,), device=dev, generator=g)
-            xb, yb = X[idx].contiguous(), Y[idx].contiguous()
-            ens.train_step(m, xb, yb, lr, loss)
-            if log and (s % max(1, steps // 10) == 0 or s == steps - 1):
-                log(f"member {m} step {s} loss {float(loss.item()):.4e}")
-        finals.append(float(loss.item()))
+        tr = ens.train(m, X, Y, batch, steps, lr, seed=int(seed) * 1000 + m)
+        t = tr.cpu().numpy()
+        tail = t[-max(1, steps // 20):]
+        finals.append(float(tail.mean()))
+        if log:
+            for s in range(0, steps, max(1, steps // 10)):
+                log(f"member {m} step {s} loss {t[s]:.4e}")
+            log(f"member {m} final loss {finals[-1]:.4e}")
     torch.cuda.synchronize(dev)
     return TrainReport(steps=steps, batch=batch, seconds=time.perf_counter() - t0, final_loss=finals)
 

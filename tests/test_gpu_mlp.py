@@ -96,3 +96,20 @@ def test_bad_batch_is_rejected():
     with pytest.raises(BdError, match="multiple of 32"):
         e.grad(0, X, T)
     e.close()
+
+
+def test_device_training_loop_matches_eager_steps_in_effect():
+    """bd_mlp_train (graph-replayed) lowers the loss like the eager steps do."""
+    e = _ens(1)
+    rng = np.random.default_rng(3)
+    X = rng.uniform(-1, 1, (20000, 13)).astype(np.float32)
+    T = np.stack([np.sin(2 * X[:, 0]) + X[:, 1] * X[:, 2], np.cos(X[:, 3])] + [X[:, 5]] * 4, axis=1).astype(np.float32)
+    l0, _ = e.grad(0, X[:4096], T[:4096])
+    tr = e.train(0, X, T, 1024, 600, 1e-3, seed=5).cpu().numpy()
+    l1, _ = e.grad(0, X[:4096], T[:4096])
+    assert np.all(np.isfinite(tr)) and tr[-50:].mean() < 0.1 * tr[:5].mean()
+    assert l1 < 0.05 * l0, (l0, l1)
+    # a second call continues from the trained weights (Adam state kept)
+    tr2 = e.train(0, X, T, 1024, 50, 1e-3, seed=6).cpu().numpy()
+    assert tr2.mean() < 2 * tr[-50:].mean()
+    e.close()

@@ -74,8 +74,8 @@ def test_trained_surrogate_gains_over_omitting_it_and_keeps_k_on():
     from pystarc_b200 import surrogate as sg
 
     s = system("c2")
-    ens = sg.MLPEnsemble(n_members=5, seed=11)
-    spec = sg.SurrogateSpec(env_length=s.debye, env_ref=25.0)
+    ens = sg.MLPEnsemble(n_members=3, seed=11)
+    spec = sg.SurrogateSpec()
     spec.r_min = sg.contact_distance(s.rec_pos, s.lig_pos) + 8.0
     spec.r_max = 80.0
     sampler = make_sim(s, 20000, 100000, "mixed", steps_per_launch=16)
@@ -85,7 +85,7 @@ def test_trained_surrogate_gains_over_omitting_it_and_keeps_k_on():
     eng.set_ligand(lig, s.lig_q)
     T = sg.exact_targets(eng, c, q)
     n_tr = 50000
-    rep = sg.fit(ens, spec, c[:n_tr], q[:n_tr], T[:n_tr], steps=3000, batch=4096, lr=1e-3)
+    rep = sg.fit(ens, spec, c[:n_tr], q[:n_tr], T[:n_tr], steps=4000, batch=4096, lr=1e-3)
     err = sg.heldout_error(ens, spec, c[n_tr:], q[n_tr:], T[n_tr:])
     # what the trained network gains: its error against leaving the two terms out
     assert err["median"] < 0.2 * err["without_surrogate_median"], err

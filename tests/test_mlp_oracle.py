@@ -64,3 +64,17 @@ def test_features_identify_q_and_minus_q():
     np.testing.assert_array_equal(f1, f2)
     assert f1.shape == (1, 13) and f1.dtype == np.float32
     assert abs(f1[0, 3] - np.linalg.norm(c) / spec.r_scale) < 1e-7
+
+
+def test_envelope_follows_a_radial_profile():
+    rng = np.random.default_rng(4)
+    r = rng.uniform(20, 60, 200000)
+    size = np.exp(-r / 8.0) / r
+    d = rng.normal(size=(r.size, 3))
+    f = d / np.linalg.norm(d, axis=1, keepdims=True) * size[:, None]
+    spec = SurrogateSpec()
+    spec.fit_envelope(r, f)
+    probe = np.linspace(22, 58, 50)
+    ratio = spec.envelope(probe) / (np.exp(-probe / 8.0) / probe)
+    assert np.all(np.abs(np.log(ratio)) < 0.05), ratio
+    assert spec.envelope(np.array([5.0]))[0] == spec.envelope(np.array([spec.env_r0]))[0]  # clamped
