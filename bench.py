@@ -131,15 +131,15 @@ class _MP:
 _OPTS = {"layout": None}
 
 
-def make_sim(s, precision, n_traj, K, id_offset=0, torque="zero"):
+def make_sim(s, precision, n_traj, K, id_offset=0, torque="zero", surrogate=None, termination="complete", seed=None):
     from pystarc_b200.engine import B200ForceEngine
     from pystarc_b200.simulator import B200BatchSimulator
 
     eng = B200ForceEngine(**s.engine_kwargs(), multipole_expansion=_MP(s), precision=precision, torque_mode=torque,
                           device=int(os.environ.get("LOCAL_RANK", 0)), layout=_OPTS["layout"])
     mol1, mol2 = s.molecules()
-    sim = B200BatchSimulator(mol1, mol2, s.mobility(), s.pathway_set(), s.params(n_traj=n_traj), eng,
-                             termination="complete", steps_per_launch=K, id_offset=id_offset)
+    sim = B200BatchSimulator(mol1, mol2, s.mobility(), s.pathway_set(), s.params(n_traj=n_traj, seed=seed), eng,
+                             termination=termination, steps_per_launch=K, id_offset=id_offset, surrogate=surrogate)
     return sim
 
 
@@ -213,6 +213,99 @@ def e2e_arm(s, precision, steps, K, n_traj, id_offset, launch):
     launches = max(1, steps)
     sim.engine.close()
     return res.total_steps / el, h2d / launches, d2h / launches, res
+
+
+def surrogate_arm(s, steps, warmup, K, n_traj, n_poses, train_steps, members, kon_traj, kon_launches=300, log=None):
+    """Config 4: train the surrogate on exact-kernel BD poses, judge it on held-out poses, time the
+    surrogate stepper like the exact one, and compare k_on of exact and surrogate runs."""
+    import torch
+
+    from pystarc_b200 import surrogate as sg
+
+    out = {}
+    t0 = time.perf_counter()
+    say = log or (lambda m: None)
+    r_lo, r_hi = 25.0, min(80.0, float(s.r_escape))
+    sampler = make_sim(s, "mixed", n_traj, 16)
+    n_held = max(n_poses // 10, 1024)
+    c, q = sg.sample_poses(sampler, n_poses + n_held, r_lo=r_lo, r_hi=r_hi)
+    eng = sampler.engine
+    eng.set_ligand(s.lig_pos - s.lig_pos.mean(axis=0), s.lig_q)
+    T = sg.exact_targets(eng, c, q)
+    eng.close()
+    out["data_s"] = round(time.perf_counter() - t0, 1)
+    say(f"surrogate: {len(c)} poses and exact targets in {out['data_s']} s")
+    spec = sg.SurrogateSpec(r_scale=80.0)
+    spec.r_min = sg.contact_distance(s.rec_pos, s.lig_pos) + 8.0
+    spec.r_max = r_hi
+    ens = sg.MLPEnsemble(n_members=members, seed=20261203)
+    rep = sg.fit(ens, spec, c[:n_poses], q[:n_poses], T[:n_poses], steps=train_steps, batch=8192, lr=1e-3, log=log)
+    out["training"] = {"poses": int(n_poses), "steps": rep.steps, "batch": rep.batch, "members": members,
+                       "seconds": round(rep.seconds, 2), "final_loss": [round(v, 6) for v in rep.final_loss],
+                       "tflops": round(members * train_steps * rep.batch * 3 * 2 *
+                                       sum(i * o for i, o in ens.dims) / rep.seconds / 1e12, 1)}
+    out["heldout"] = sg.heldout_error(ens, spec, c[n_poses:], q[n_poses:], T[n_poses:])
+    say(f"surrogate: trained in {rep.seconds:.1f} s, held-out {out['heldout']}")
+    out["trust_region_A"] = [round(spec.r_min, 2), round(spec.r_max, 2)]
+    # timed like the exact arm: graph launches of K steps, L2 flushed in between
+    sim = make_sim(s, "mixed", n_traj, K, surrogate=(ens, spec))
+    sim._setup()
+    h = sim.engine.handle
+    h.call("bd_sim_reset", None)
+    stream = torch.cuda.current_stream()
+    sptr = _lib_P(stream.cuda_stream)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    for _ in range(warmup):
+        h.call("bd_sim_run", 1, K, sptr)
+    c0 = sim.read_counters()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    torch.cuda.synchronize()
+    for i in range(steps):
+        flush.zero_()
+        ev[i][0].record(stream)
+        h.call("bd_sim_run", 1, K, sptr)
+        ev[i][1].record(stream)
+    torch.cuda.synchronize()
+    t = sum(a.elapsed_time(b) for a, b in ev) / 1e3
+    c1 = sim.read_counters()
+    d = {k: c1[k] - c0[k] for k in c1}
+    sim.engine.close()
+    out["bd_steps_per_s"] = d["steps"] / t
+    out["surrogate_share"] = d["surrogate_evals"] / max(d["steps"], 1)
+    out["fallback_fraction"] = d["surrogate_fallbacks"] / max(d["surrogate_evals"], 1)
+    out["counters"] = {k: int(v) for k, v in d.items()}
+    say(f"surrogate: stepper {out['bd_steps_per_s']:.3e} steps/s, fallback {out['fallback_fraction']:.3f}")
+    # k_on: the same trajectories (seed, keyed noise) with and without the surrogate, each given the same
+    # budget of kon_launches x K steps per slot; trajectories unfinished by then are left out of both
+    kon = {}
+    D_rel = s.mobility().relative_translational_diffusion()
+    for name, sur in (("plain", None), ("surrogate", (ens, spec))):
+        sm = make_sim(s, "mixed", kon_traj, K, surrogate=sur, termination="reference", seed=4242)
+        t1 = time.perf_counter()
+        res = sm.run(max_launches=kon_launches)
+        lo, hi = res.reaction_probability_ci()
+        kon[name] = {"n": int(kon_traj), "reacted": int(res.n_reacted), "escaped": int(res.n_escaped),
+                     "p_rxn": res.n_reacted / max(res.n_reacted + res.n_escaped, 1), "wilson95": [lo, hi],
+                     "k_on": res.rate_constant(D_rel, sm._k_b), "k_on_wilson95": list(res.rate_constant_ci(D_rel, sm._k_b)),
+                     "max_steps_or_unfinished": int(kon_traj - res.n_reacted - res.n_escaped),
+                     "wall_s": round(time.perf_counter() - t1, 1)}
+        say(f"surrogate: k_on run {name}: {kon[name]}")
+        sm.engine.close()
+    a, b = kon["plain"]["wilson95"], kon["surrogate"]["wilson95"]
+    kon["cis_overlap"] = bool(a[0] <= b[1] and b[0] <= a[1])
+    out["k_on"] = kon
+    ens.close()
+    return out
+
+
+def _progress(msg):
+    print(f"[bench {time.strftime('%H:%M:%S')}] {msg}", file=sys.stderr, flush=True)
+
+
+def _lib_P(v):
+    from pystarc_b200 import _lib
+
+    return _lib.P(v)
 
 
 # --------------------------------------------------------------------------- CPU baseline
@@ -293,6 +386,11 @@ def main():
                     help="device data layout flags (1 stage receptor, 2 windows for 1-channel grids, "
                          "4 windows for the paired grid; -1: library default)")
     ap.add_argument("--cpu-steps", type=int, default=40)
+    ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate arm (config 4)")
+    ap.add_argument("--sur-poses", type=int, default=200_000)
+    ap.add_argument("--sur-train-steps", type=int, default=8000)
+    ap.add_argument("--sur-members", type=int, default=5)
+    ap.add_argument("--sur-kon-traj", type=int, default=20_000)
     args = ap.parse_args()
     _OPTS["layout"] = None if args.layout < 0 else args.layout
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -343,8 +441,10 @@ def main():
     ck = clocks.stop()
     t_fp64, tl_fp64, d_fp64, launch64 = time_device_arm(s, "fp64", args.steps, args.warmup, args.inner, n_traj,
                                                         id_offset, dist, fixed)
+    _progress(f"exact arms: mixed {d_mixed['steps'] / t_mixed:.3e}, fp64 {d_fp64['steps'] / t_fp64:.3e} steps/s")
     e2e_val, h2d, d2h, e2e_res = e2e_arm(s, "mixed", max(args.steps, 20), args.inner, n_traj, id_offset,
                                          (launch["group"], launch["block"]))
+    _progress(f"e2e arm: {e2e_val:.3e} steps/s")
     t_max = t_mixed
     steps_all = d_mixed["steps"]
     if dist is not None:
@@ -392,6 +492,10 @@ def main():
         "gpu_launches": 3 * args.steps,
         "clocks": ck,
     }
+    if world == 1 and not args.no_surrogate and args.workload != "two-spheres":
+        line["variants"]["surrogate"] = surrogate_arm(s, args.steps, args.warmup, args.inner, n_traj, args.sur_poses,
+                                                      args.sur_train_steps, args.sur_members, args.sur_kon_traj,
+                                                      log=_progress)
     if world == 1 and not args.no_cpu_baseline:
         _, info = cpu_baseline(s, os.cpu_count() or 1, n_steps=args.cpu_steps)
         line["cpu_baseline"] = info

@@ -102,10 +102,11 @@ __global__ void __launch_bounds__(256) gemm_nt(GemmArgs g) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm0 = (warp / WN) * TM, wn0 = (warp % WN) * TN;
   const int gq = lane >> 2, tq = lane & 3;
-  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+  const int n0 = blockIdx.x * BN;
   const int M = g.m_dev ? min(g.M, *g.m_dev) : g.M;
-  if (m0 >= M) return;  // whole block: no barrier is skipped by part of it
   const int kb = blockIdx.z * g.k_per_split, ke = min(g.K, kb + g.k_per_split);
+  // row tiles are shared out over gridDim.y blocks (block-uniform loop: barriers stay whole)
+  for (int m0 = blockIdx.y * BM; m0 < M; m0 += gridDim.y * BM) {
   float acc[MT][NT][4];
 #pragma unroll
   for (int i = 0; i < MT; ++i)
@@ -212,6 +213,7 @@ __global__ void __launch_bounds__(256) gemm_nt(GemmArgs g) {
           }
         }
       }
+  }  // row tiles
 }
 
 // ---------------------------------------------------------------------------
@@ -471,7 +473,10 @@ int grid_for(BdMlp* m, long long n) { return (int)std::min<long long>((n + 255) 
 
 template <int BM, int BN, int WM, int WN, int EPI>
 int launch_gemm(BdMlp* m, const GemmArgs& g, int splits, cudaStream_t s) {
-  dim3 grid((g.N + BN - 1) / BN, (g.M + BM - 1) / BM, splits);
+  const int nx = (g.N + BN - 1) / BN, tiles = (g.M + BM - 1) / BM;
+  // enough blocks for two per SM; each loops over its share of the row tiles
+  const int ny = std::max(1, std::min(tiles, (2 * m->n_sm + nx * splits - 1) / (nx * splits)));
+  dim3 grid(nx, ny, splits);
   gemm_nt<BM, BN, WM, WN, EPI><<<grid, 256, 0, s>>>(g);
   MCK(m, cudaGetLastError());
   return BD_OK;
