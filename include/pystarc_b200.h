@@ -281,6 +281,24 @@ int bd_sim_set_surrogate(BdHandle* h, BdMlp* m, const BdSurrogateParams* p);
 /* Trusted-pose evaluations and exact fallbacks since configure: out[0], out[1]. */
 int bd_sim_surrogate_counters(BdHandle* h, uint64_t* out);
 
+/* ---- Heterogeneous batch -----------------------------------------------------------------
+ * No reference counterpart (the reference runs one system per process).  Trajectories of n
+ * configured handles (each with its own grids, atoms, reactions and BdSimParams; the same
+ * precision and torque mode) share one slot pool and one persistent launch; a slot holds the
+ * trajectory's index in the concatenation of the systems' ranges.  Outcomes land in each
+ * handle's own arrays (read them with bd_sim_outcomes); the counters are summed over the
+ * systems.  The handles must stay configured and unchanged while the batch exists.  Noise keys
+ * are each handle's (seed, id_offset + local id, step), so a trajectory runs exactly as it
+ * would in its handle's own stepper. */
+typedef struct BdMulti BdMulti;
+int bd_multi_create(BdHandle* const* handles, int n, BdMulti** out);
+int bd_multi_destroy(BdMulti* m);
+int bd_multi_last_error(const BdMulti* m, char* buf, int len);
+int bd_multi_reset(BdMulti* m, void* stream);
+int bd_multi_run(BdMulti* m, int n_launch, int steps_per_launch, void* stream);
+int bd_multi_counters(BdMulti* m, uint64_t* out, int n, void* stream);
+int bd_multi_live(BdMulti* m, int32_t* n_live);
+
 #ifdef __cplusplus
 }
 #endif

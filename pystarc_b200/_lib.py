@@ -109,6 +109,13 @@ SIGNATURES = {
     "bd_sim_run_noalloc": (C.c_int, [P, C.POINTER(BdSimParams), P, P, P, P, C.c_int, C.c_int, P]),
     "bd_set_terms": (C.c_int, [P, C.c_int]),
     "bd_sim_set_surrogate": (C.c_int, [P, P, C.POINTER(BdSurrogateParams)]),
+    "bd_multi_create": (C.c_int, [C.POINTER(P), C.c_int, C.POINTER(P)]),
+    "bd_multi_destroy": (C.c_int, [P]),
+    "bd_multi_last_error": (C.c_int, [P, C.c_char_p, C.c_int]),
+    "bd_multi_reset": (C.c_int, [P, P]),
+    "bd_multi_run": (C.c_int, [P, C.c_int, C.c_int, P]),
+    "bd_multi_counters": (C.c_int, [P, u64p, C.c_int, P]),
+    "bd_multi_live": (C.c_int, [P, i32p]),
     "bd_sim_surrogate_counters": (C.c_int, [P, u64p]),
     "bd_mlp_create": (C.c_int, [C.c_int, C.POINTER(BdMlpDesc), C.POINTER(P)]),
     "bd_mlp_destroy": (C.c_int, [P]),
@@ -155,6 +162,14 @@ def check(rc, handle=None):
     if rc != BD_OK:
         buf = C.create_string_buffer(1024)
         load().bd_last_error(handle, buf, 1024)
+        raise BdError(rc, buf.value.decode(errors="replace"))
+    return rc
+
+
+def check_multi(rc, m=None):
+    if rc != BD_OK:
+        buf = C.create_string_buffer(1024)
+        load().bd_multi_last_error(m, buf, 1024)
         raise BdError(rc, buf.value.decode(errors="replace"))
     return rc
 

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "bd_kernels.cuh"
+#include "bd_multi.cuh"
 #include "bd_surrogate.cuh"
 #include "pystarc_b200.h"
 
@@ -1290,3 +1291,253 @@ int bd_internal_run_noalloc(BdHandle* h, const BdSimParams* p, unsigned char* sc
   CK(h, cudaStreamSynchronize(s));
   return BD_OK;
 }
+
+// ===========================================================================
+// Heterogeneous batch (bd_multi_*): several configured handles in one pool.
+// ===========================================================================
+struct BdMulti {
+  int device = 0, n_sm = 148;
+  std::vector<BdHandle*> hs;
+  int precision = BD_PREC_MIXED, torque = BD_TORQUE_ZERO;
+  MultiTab T{};
+  SlotBuf buf[2]{};
+  int* d_live = nullptr;
+  int cap = 0, cur = 0, blocks = 0;
+  std::vector<void*> allocs;
+  cudaStream_t own = nullptr;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  int graph_K = -1;
+  std::string err;
+};
+
+namespace {
+
+int mfail(BdMulti* m, int code, const char* fmt, ...) {
+  char b[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(b, sizeof b, fmt, ap);
+  va_end(ap);
+  if (m) m->err = b;
+  return code;
+}
+
+#define MCK(m, x)                                                                                      \
+  do {                                                                                                 \
+    cudaError_t e_ = (x);                                                                              \
+    if (e_ != cudaSuccess)                                                                             \
+      return mfail(m, e_ == cudaErrorMemoryAllocation ? BD_ERR_OOM : BD_ERR_CUDA, "%s: %s (%s:%d)", #x, \
+                   cudaGetErrorString(e_), __FILE__, __LINE__);                                        \
+  } while (0)
+
+int malloc_multi(BdMulti* m, void** p, size_t bytes) {
+  MCK(m, cudaMalloc(p, bytes ? bytes : 16));
+  m->allocs.push_back(*p);
+  return BD_OK;
+}
+
+void* multi_kernel(int prec, int torque) {
+  const bool tq = torque == BD_TORQUE_CENTROID;
+  if (prec == BD_PREC_FP64) return tq ? (void*)&step_kernel_multi<double, true> : (void*)&step_kernel_multi<double, false>;
+  return tq ? (void*)&step_kernel_multi<float, true> : (void*)&step_kernel_multi<float, false>;
+}
+
+int multi_graphs(BdMulti* m, int K) {
+  if (m->graph_K == K) return BD_OK;
+  for (auto& g : m->graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+  void* fn = multi_kernel(m->precision, m->torque);
+  for (int c = 0; c < 2; ++c) {
+    cudaGraph_t graph;
+    MCK(m, cudaStreamBeginCapture(m->own, cudaStreamCaptureModeThreadLocal));
+    SlotBuf src = m->buf[c], dst = m->buf[1 - c];
+    const int* live = m->d_live + c;
+    int KK = K;
+    MultiTab T = m->T;
+    void* args[] = {&T, &src, &live, &KK};
+    cudaError_t e = cudaLaunchKernel(fn, dim3(m->blocks), dim3(256), args, 0, m->own);
+    if (e == cudaSuccess) {
+      compact_kernel<<<m->n_sm * 4, 256, 0, m->own>>>(src, dst, live, m->T.ctr);
+      finish_compact_kernel<<<1, 1, 0, m->own>>>(m->d_live + (1 - c), m->T.ctr);
+      e = cudaGetLastError();
+    }
+    cudaError_t e2 = cudaStreamEndCapture(m->own, &graph);
+    MCK(m, e);
+    MCK(m, e2);
+    e = cudaGraphInstantiate(&m->graph[c], graph, 0);
+    cudaGraphDestroy(graph);
+    MCK(m, e);
+  }
+  m->graph_K = K;
+  return BD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bd_multi_create(BdHandle* const* handles, int n, BdMulti** out) {
+  if (!out) return BD_ERR_ARG;
+  *out = nullptr;
+  if (!handles || n < 1 || n > 1024) return BD_ERR_ARG;
+  BdMulti* m = new BdMulti();
+  auto bail = [&](int rc) {
+    for (void* p : m->allocs) cudaFree(p);
+    if (m->own) cudaStreamDestroy(m->own);
+    g_create_error = m->err;
+    delete m;
+    return rc;
+  };
+  m->device = handles[0] ? handles[0]->device : 0;
+  std::vector<DevSystem> sys(n);
+  std::vector<DevSim> sim(n);
+  std::vector<long long> base(n + 1, 0);
+  for (int i = 0; i < n; ++i) {
+    BdHandle* h = handles[i];
+    if (!h || !h->sim_ready || h->dirty)
+      return bail(mfail(m, BD_ERR_STATE, "handle %d is not configured (bd_sim_configure after its last change)", i));
+    if (h->device != m->device) return bail(mfail(m, BD_ERR_ARG, "handle %d is on another device", i));
+    if (i == 0) {
+      m->precision = h->sp.precision;
+      m->torque = h->sp.torque_mode;
+    } else if (h->sp.precision != m->precision || h->sp.torque_mode != m->torque) {
+      return bail(mfail(m, BD_ERR_ARG, "handle %d: every system needs the same precision and torque mode", i));
+    }
+    if (h->sur) return bail(mfail(m, BD_ERR_ARG, "handle %d has a surrogate; the batch runs the exact kernels", i));
+    sys[i] = h->S;
+    sys[i].rec_in_smem = 0;
+    sim[i] = h->P;
+    sim[i].stats = 0;
+    base[i + 1] = base[i] + h->P.n_traj;
+  }
+  if (base[n] > 0x7fffffffll) return bail(mfail(m, BD_ERR_ARG, "more than 2^31 - 1 trajectories in the batch"));
+  if (cudaSetDevice(m->device) != cudaSuccess) return bail(mfail(m, BD_ERR_CUDA, "cudaSetDevice failed"));
+  cudaDeviceGetAttribute(&m->n_sm, cudaDevAttrMultiProcessorCount, m->device);
+  void* p;
+  int rc;
+  if ((rc = malloc_multi(m, &p, C_NUM * sizeof(unsigned long long)))) return bail(rc);
+  unsigned long long* ctr = (unsigned long long*)p;
+  for (auto& q : sim) q.ctr = ctr;
+  if ((rc = malloc_multi(m, &p, n * sizeof(DevSystem)))) return bail(rc);
+  if (cudaMemcpy(p, sys.data(), n * sizeof(DevSystem), cudaMemcpyHostToDevice) != cudaSuccess)
+    return bail(mfail(m, BD_ERR_CUDA, "upload of the system table failed"));
+  m->T.sys = (const DevSystem*)p;
+  if ((rc = malloc_multi(m, &p, n * sizeof(DevSim)))) return bail(rc);
+  if (cudaMemcpy(p, sim.data(), n * sizeof(DevSim), cudaMemcpyHostToDevice) != cudaSuccess)
+    return bail(mfail(m, BD_ERR_CUDA, "upload of the run-parameter table failed"));
+  m->T.sim = (const DevSim*)p;
+  if ((rc = malloc_multi(m, &p, (n + 1) * sizeof(long long)))) return bail(rc);
+  if (cudaMemcpy(p, base.data(), (n + 1) * sizeof(long long), cudaMemcpyHostToDevice) != cudaSuccess)
+    return bail(mfail(m, BD_ERR_CUDA, "upload of the index table failed"));
+  m->T.base = (const long long*)p;
+  m->T.n_sys = n;
+  m->T.total = base[n];
+  m->T.ctr = ctr;
+  m->hs.assign(handles, handles + n);
+  // slot pool: eight resident waves, at least 65536, at most every trajectory
+  void* fn = multi_kernel(m->precision, m->torque);
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, 0) != cudaSuccess || per_sm < 1) per_sm = 1;
+  m->blocks = per_sm * m->n_sm;
+  const long long cap = std::min<long long>(base[n], std::max<long long>(65536, 8ll * m->blocks * 256));
+  m->cap = (int)cap;
+  for (int b = 0; b < 2; ++b) {
+    SlotBuf& B = m->buf[b];
+    if ((rc = malloc_multi(m, &p, 3 * (size_t)cap * sizeof(double)))) return bail(rc);
+    B.c = (double*)p;
+    if ((rc = malloc_multi(m, &p, 4 * (size_t)cap * sizeof(double)))) return bail(rc);
+    B.q = (double*)p;
+    if ((rc = malloc_multi(m, &p, (size_t)cap * sizeof(int)))) return bail(rc);
+    B.traj = (int*)p;
+    if ((rc = malloc_multi(m, &p, (size_t)cap * sizeof(int)))) return bail(rc);
+    B.steps = (int*)p;
+    if ((rc = malloc_multi(m, &p, (size_t)cap * sizeof(int)))) return bail(rc);
+    B.rets = (int*)p;
+    if ((rc = malloc_multi(m, &p, (size_t)cap))) return bail(rc);
+    B.status = (int8_t*)p;
+    B.cap = (int)cap;
+  }
+  if ((rc = malloc_multi(m, &p, 2 * sizeof(int)))) return bail(rc);
+  m->d_live = (int*)p;
+  if (cudaStreamCreateWithFlags(&m->own, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(mfail(m, BD_ERR_CUDA, "stream creation failed"));
+  *out = m;
+  return BD_OK;
+}
+
+int bd_multi_destroy(BdMulti* m) {
+  if (!m) return BD_OK;
+  cudaSetDevice(m->device);
+  cudaDeviceSynchronize();
+  for (auto& g : m->graph)
+    if (g) cudaGraphExecDestroy(g);
+  for (void* p : m->allocs) cudaFree(p);
+  if (m->own) cudaStreamDestroy(m->own);
+  delete m;
+  return BD_OK;
+}
+
+int bd_multi_last_error(const BdMulti* m, char* buf, int len) {
+  if (!buf || len <= 0) return BD_ERR_ARG;
+  snprintf(buf, (size_t)len, "%s", m ? m->err.c_str() : g_create_error.c_str());
+  return BD_OK;
+}
+
+int bd_multi_reset(BdMulti* m, void* stream) {
+  if (!m) return BD_ERR_ARG;
+  MCK(m, cudaSetDevice(m->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  MCK(m, cudaMemsetAsync(m->T.ctr, 0, C_NUM * sizeof(unsigned long long), s));
+  for (BdHandle* h : m->hs) {
+    const size_t n = (size_t)h->P.n_traj;
+    MCK(m, cudaMemsetAsync(h->P.out_status, 0, n, s));
+    MCK(m, cudaMemsetAsync(h->P.out_steps, 0, n * sizeof(int), s));
+    MCK(m, cudaMemsetAsync(h->P.out_returns, 0, n * sizeof(int), s));
+  }
+  init_slots_multi_kernel<<<(m->cap + 255) / 256, 256, 0, s>>>(m->T, m->buf[0], m->cap);
+  MCK(m, cudaGetLastError());
+  const unsigned long long started = (unsigned long long)m->cap;
+  const int live[2] = {m->cap, 0};
+  MCK(m, cudaMemcpyAsync(m->T.ctr + C_PENDING, &started, sizeof started, cudaMemcpyHostToDevice, s));
+  MCK(m, cudaMemcpyAsync(m->d_live, live, sizeof live, cudaMemcpyHostToDevice, s));
+  MCK(m, cudaStreamSynchronize(s));
+  m->cur = 0;
+  return BD_OK;
+}
+
+int bd_multi_run(BdMulti* m, int n_launch, int K, void* stream) {
+  if (!m) return BD_ERR_ARG;
+  if (n_launch < 0 || K <= 0) return mfail(m, BD_ERR_ARG, "bd_multi_run: n_launch >= 0 and steps > 0 needed");
+  MCK(m, cudaSetDevice(m->device));
+  int rc = multi_graphs(m, K);
+  if (rc) return rc;
+  for (int i = 0; i < n_launch; ++i) {
+    MCK(m, cudaGraphLaunch(m->graph[m->cur], (cudaStream_t)stream));
+    m->cur = 1 - m->cur;
+  }
+  return BD_OK;
+}
+
+int bd_multi_counters(BdMulti* m, uint64_t* out, int n, void* stream) {
+  if (!m || !out) return BD_ERR_ARG;
+  unsigned long long c[C_NUM];
+  cudaStream_t s = (cudaStream_t)stream;
+  MCK(m, cudaMemcpyAsync(c, m->T.ctr, sizeof c, cudaMemcpyDeviceToHost, s));
+  MCK(m, cudaStreamSynchronize(s));
+  const int k = std::min(n, (int)BD_CTR_NUM);
+  for (int i = 0; i < k; ++i) out[i] = c[i];
+  if (k > 0) out[0] = std::min<unsigned long long>(c[C_PENDING], (unsigned long long)m->T.total);
+  return BD_OK;
+}
+
+int bd_multi_live(BdMulti* m, int32_t* n_live) {
+  if (!m || !n_live) return BD_ERR_ARG;
+  MCK(m, cudaDeviceSynchronize());
+  MCK(m, cudaMemcpy(n_live, m->d_live + m->cur, sizeof(int), cudaMemcpyDeviceToHost));
+  return BD_OK;
+}
+
+}  // extern "C"
