@@ -110,12 +110,16 @@ WORKLOADS = {
     "protein-ligand": ("protein+small-ligand (3200/18 atoms, 193^3 elec+Born grids, 65^3 ligand Born grid, 1e6 trajectories)", 1_000_000),
     "two-spheres": ("two charged spheres (+5/-5 e, 129^3 grid, 1e5 trajectories, FP64 physics)", 100_000),
     "protein-protein": ("protein-protein (1700/1400 atoms, 3 x 161^3 grids, HI, 1e7 trajectories)", 10_000_000),
+    "heterogeneous": ("16 synthetic receptor-ligand systems in one persistent launch (500-8000 / 10-2000 atoms, "
+                      "97^3-225^3 grids at 0.5-1.0 A, 1e4-1e6 trajectories each, b 50-90 A)", 0),
 }
 
 
 def build_system(device, workload="protein-ligand"):
     from pystarc_b200 import synth
 
+    if workload == "heterogeneous":
+        return synth.config5(0, device=device)
     if workload == "two-spheres":
         return synth.config1()
     if workload == "protein-protein":
@@ -298,6 +302,93 @@ def surrogate_arm(s, steps, warmup, K, n_traj, n_poses, train_steps, members, ko
     return out
 
 
+def hetero_arm(systems, precision, steps, warmup, K):
+    """BD steps/s of the 16-system batch: graph launches of K steps, L2 flushed in between."""
+    import torch
+
+    from pystarc_b200.multi import B200MultiBatch
+
+    sims = [make_sim(s, precision, s.n_traj, K) for s in systems]
+    batch = B200MultiBatch(sims, steps_per_launch=K)
+    batch.setup()
+    batch._call("bd_multi_reset", None)
+    stream = torch.cuda.current_stream()
+    sptr = _lib_P(stream.cuda_stream)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    for _ in range(warmup):
+        batch._call("bd_multi_run", 1, K, sptr)
+    c0 = batch.counters()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    torch.cuda.synchronize()
+    for i in range(steps):
+        flush.zero_()
+        ev[i][0].record(stream)
+        batch._call("bd_multi_run", 1, K, sptr)
+        ev[i][1].record(stream)
+    torch.cuda.synchronize()
+    t = sum(a.elapsed_time(b) for a, b in ev) / 1e3
+    c1 = batch.counters()
+    batch.close()
+    for sm in sims:
+        sm.engine.close()
+    return t, {k: c1[k] - c0[k] for k in c1}
+
+
+def hetero_main(args):
+    import torch
+
+    from pystarc_b200 import synth
+
+    t0 = time.perf_counter()
+    systems = [synth.config5(i, device="cuda") for i in range(16)]
+    _progress(f"16 systems built in {time.perf_counter() - t0:.1f} s")
+    clocks = Clocks(0)
+    clocks.start()
+    t_mixed, d_mixed = hetero_arm(systems, "mixed", args.steps, args.warmup, args.inner)
+    ck = clocks.stop()
+    t_fp64, d_fp64 = hetero_arm(systems, "fp64", args.steps, args.warmup, args.inner)
+    _progress(f"mixed {d_mixed['steps'] / t_mixed:.3e}, fp64 {d_fp64['steps'] / t_fp64:.3e} steps/s")
+    # end to end through the public API (engines built from host arrays inside the timed region)
+    from pystarc_b200.multi import B200MultiBatch
+
+    torch.cuda.synchronize()
+    te = time.perf_counter()
+    sims = [make_sim(s, "mixed", s.n_traj, args.inner) for s in systems]
+    batch = B200MultiBatch(sims, steps_per_launch=args.inner, launches_per_poll=1)
+    res = batch.run(max_launches=max(args.steps, 20))
+    torch.cuda.synchronize()
+    e2e = sum(r.total_steps for r in res) / (time.perf_counter() - te)
+    batch.close()
+    h2d = sum(np.asarray(g.data).nbytes for s in systems for g in s.elec_grids + s.born_grids + s.lig_born_grids)
+    d2h = sum(s.n_traj * 9 for s in systems)
+    peak, peak_kind = peaks()
+    gathers = d_mixed["grid_evals"] + d_mixed["rev_evals"]
+    achieved = (gathers * ALGO_BYTES_PER_GATHER + d_mixed["steps"] * STATE_BYTES_PER_STEP) / t_mixed / 1e9
+    line = {
+        "metric": METRIC, "value": d_mixed["steps"] / t_mixed, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t_mixed / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 forces / f64 poses", "data": "synthetic",
+        "config": {"workload": WORKLOADS["heterogeneous"][0], "bd_steps_per_launch": args.inner,
+                   "systems": [s.meta | {"n_traj": s.n_traj} for s in systems],
+                   "l2": "flushed (256 MiB write) between launches", "parallelism": "one persistent launch"},
+        "variants": {"fp64": {"bd_steps_per_s": d_fp64["steps"] / t_fp64, "steps": d_fp64["steps"]}},
+        "counters": {k: int(v) for k, v in d_mixed.items()},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_kind": peak_kind,
+                     "algorithmic_bytes": "224 B per (atom, grid) stencil + 128 B per trajectory-step"},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d / max(args.steps, 20)),
+                "d2h_bytes_per_step": int(d2h / max(args.steps, 20)),
+                "note": "B200ForceEngine x16 + B200MultiBatch.run() from host arrays, incl. grid upload"},
+        "gpu_launches": 3 * args.steps,
+        "clocks": ck,
+    }
+    if not args.no_cpu_baseline:
+        _, info = cpu_baseline(systems[0], os.cpu_count() or 1, n_steps=args.cpu_steps)
+        info["sample"] = "system 0 of the batch only: " + info["sample"]
+        line["cpu_baseline"] = info
+    print(json.dumps(line))
+
+
 def _progress(msg):
     print(f"[bench {time.strftime('%H:%M:%S')}] {msg}", file=sys.stderr, flush=True)
 
@@ -417,6 +508,13 @@ def main():
                                      "(PCG64 order), CPU"},
                           "cpu_baseline": info, "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0,
                                                         "d2h_bytes_per_step": 0}}))
+        return
+
+    if args.workload == "heterogeneous":
+        if world > 1:
+            print(json.dumps({"error": "the heterogeneous batch is a single-GPU workload"}))
+            return
+        hetero_main(args)
         return
 
     import torch

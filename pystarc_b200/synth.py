@@ -296,3 +296,50 @@ def config3(n_traj=10_000_000, scale=1.0, device=None, seed=20261203):
                     elec, born, lig_born, pairs, 3, r_start=b, r_escape=2 * b, r_hydro_rec=17.5 * scale,
                     r_hydro_lig=16.5 * scale, debye=lam, sdie=sdie, max_dt=100.0, hi=True, overlap=True,
                     n_traj=n_traj, seed=seed)
+
+
+C5_DIMS = (97, 129, 161, 193, 225)
+
+
+def config5(index, device=None, seed_base=5000, traj_scale=1.0):
+    """System ``index`` of the heterogeneous batch (16 systems, seed 5000 + index).
+
+    Receptor atoms log-uniform 500-8000, ligand atoms log-uniform 10-2000, at
+    the atom density of config 2 (3200 atoms in a 22 A ball); charges N(0, 0.35)
+    shifted to a net receptor charge of +2..+8 e and a ligand charge of -1..-4 e;
+    radii U(1.2, 2.0).  Receptor elec and Born grids share one lattice with dims
+    drawn from {97, 129, 161, 193, 225} at 0.5-1.0 A; the ligand Born grid spans
+    the ligand plus 10 A at 0.5 A (at most 129^3).  Trajectories log-uniform
+    1e4-1e6 (times ``traj_scale``), b-surface U(50, 90) A (at least contact +
+    10 A), r_escape = 2b, max_dt 20 ps, no HI, overlap on.  Reaction: 3 pairs at
+    the poles, cutoff 4.5 A, 2 needed.
+    """
+    rng = np.random.default_rng(seed_base + index)
+    lam = debye_length(0.15)
+    sdie = 78.5
+    rho = 3200 / (4.0 / 3.0 * math.pi * 22.0 ** 3)
+    n_rec = int(round(math.exp(rng.uniform(math.log(500), math.log(8000)))))
+    n_lig = int(round(math.exp(rng.uniform(math.log(10), math.log(2000)))))
+    R_rec = (3 * n_rec / (4 * math.pi * rho)) ** (1 / 3)
+    R_lig = max(2.0, (3 * n_lig / (4 * math.pi * rho)) ** (1 / 3))
+    q_rec = float(rng.integers(2, 9))
+    q_lig = -float(rng.integers(1, 5))
+    rec_pos, rec_q, rec_r = _protein(n_rec, R_rec, q_rec, 0.35, seed_base * 10 + 2 * index)
+    lig_pos, lig_q, lig_r = _protein(n_lig, R_lig, q_lig, 0.35, seed_base * 10 + 2 * index + 1)
+    dims = int(rng.choice(C5_DIMS))
+    sp = float(rng.uniform(0.5, 1.0))
+    eps_e, eps_b = sdie * EPS0, 4.0 * EPS0
+    elec = [fill_sum_grid(rec_pos, rec_q, rec_r, (dims,) * 3, sp, lam, eps_e, device=device)]
+    born = [fill_sum_grid(rec_pos, rec_q, rec_r, (dims,) * 3, sp, 0, eps_b, device=device)]
+    ld = min(129, int(2 * (R_lig + 10.0) / 0.5) | 1)
+    lig_born = [fill_sum_grid(lig_pos, lig_q, lig_r, (ld,) * 3, 0.5, 0, eps_b, device=device)]
+    rec_idx = _pole_atoms(rec_pos, 3, (1, 0, 0))
+    lig_idx = _pole_atoms(lig_pos, 3, (-1, 0, 0))
+    pairs = [(int(a), int(b), 4.5) for a, b in zip(rec_idx, lig_idx)]
+    b = max(float(rng.uniform(50.0, 90.0)), R_rec + R_lig + 10.0)
+    n_traj = max(1, int(round(math.exp(rng.uniform(math.log(1e4), math.log(1e6))) * traj_scale)))
+    return BDSystem(f"config5_{index:02d}", rec_pos, rec_q, rec_r, lig_pos, lig_q, lig_r, elec, born, lig_born,
+                    pairs, 2, r_start=b, r_escape=2 * b, r_hydro_rec=R_rec + 1.4, r_hydro_lig=R_lig + 1.4,
+                    debye=lam, sdie=sdie, max_dt=20.0, hi=False, overlap=True, n_traj=n_traj,
+                    seed=20261203 + index,
+                    meta={"n_rec": n_rec, "n_lig": n_lig, "grid": dims, "spacing": round(sp, 3), "b": round(b, 1)})
