@@ -244,6 +244,11 @@ int bd_mlp_grad(BdMlp* m, int member, int n, const float* X, const float* T, flo
 /* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8, bias-corrected) of one member on a batch. */
 int bd_mlp_train_step(BdMlp* m, int member, int n, const float* X, const float* T, float lr, float* loss,
                       void* stream);
+/* Inference kernels of bd_mlp_forward / bd_mlp_ensemble and of the surrogate stepper:
+ * 1 (default) = tcgen05 MMAs with TMEM accumulators, one CTA per 128 rows running every layer
+ * (hidden <= 256, in_dim <= 32, out_dim <= 32; other shapes use 0); 0 = the mma.sync GEMM chain
+ * the training kernels use.  Both give the same values up to FP32 summation order. */
+int bd_mlp_set_inference(BdMlp* m, int mode);
 /* `steps` Adam steps of one member on random batches (rows drawn with replacement by a
  * counter-based hash of seed, member and step) of device-resident data X (n_data x in_dim),
  * T (n_data x out_dim).  The step is captured once as a CUDA graph and replayed; loss_trace

@@ -128,6 +128,7 @@ SIGNATURES = {
     "bd_mlp_train_step": (C.c_int, [P, C.c_int, C.c_int, P, P, C.c_float, P, P]),
     "bd_mlp_ensemble": (C.c_int, [P, C.c_int64, P, P, P, P]),
     "bd_mlp_train": (C.c_int, [P, C.c_int, C.c_int64, P, P, C.c_int, C.c_int, C.c_float, C.c_uint64, P, P]),
+    "bd_mlp_set_inference": (C.c_int, [P, C.c_int]),
 }
 
 _LIB = None

@@ -326,6 +326,184 @@ struct LayerGeom {
   int n_layers;
 };
 
+// ---------------------------------------------------------------------------
+// Inference on the 5th-generation tensor cores (tcgen05).  One CTA of 128
+// threads runs every layer of one member on 128 rows: the activation tile
+// (128 x K, BF16) and the layer's weights (N x K, BF16) sit in shared memory in
+// the canonical K-major no-swizzle layout (8-row x 16-byte core matrices; K
+// chunks 128 B apart, 8-row groups SBO apart), one elected thread issues the
+// 128 x N x 16 MMAs into a TMEM accumulator of N FP32 columns, and the four
+// warps read their 32 TMEM lanes back (tcgen05.ld 32x32b) for the epilogue:
+// bias + SiLU into the next activation tile, or bias into the FP32 outputs.
+// Hidden widths up to 256; the input and output are padded to 32.
+// ---------------------------------------------------------------------------
+constexpr int kTcRows = 128;
+constexpr int kTcK = 256;                        // widest K held in the activation tile
+constexpr int kTcSboA = kTcK / 8 * 128;          // bytes between 8-row groups of the activation tile
+constexpr int kTcBytesA = kTcRows * kTcK * 2;    // 64 KB
+constexpr int kTcBytesB = 256 * kTcK * 2;        // 128 KB
+constexpr int kTcSmem = kTcBytesA + kTcBytesB + 64;  // + mbarrier and TMEM address
+constexpr int kTcMaxMembers = 8;
+
+struct TcArgs {
+  const bf16* X;  // n x 32 packed BF16 input rows
+  int n;
+  const int* n_dev;  // optional device row count
+  const bf16* Wb[kTcMaxMembers];
+  const float* P[kTcMaxMembers];  // FP32 parameter vectors (biases)
+  LayerGeom L;
+  float* Y;  // per member: rows x ldy, members y_stride apart (member0's block first)
+  int ldy;
+  long long y_stride;
+  int member0;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Byte offset of element (row, k) in a canonical K-major no-swizzle tile.
+__device__ __forceinline__ uint32_t kmajor_off(int row, int k, int sbo) {
+  return (uint32_t)((row >> 3) * sbo + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
+}
+
+// Shared-memory matrix descriptor (sm100): start, leading and stride byte offsets
+// (>> 4), version 1, no swizzle.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both K-major, M x N.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  // bounded: a wait that never completes returns false instead of hanging the GPU
+  for (int it = 0; it < (1 << 22); ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__global__ void __launch_bounds__(128, 1) mlp_forward_tc_kernel(TcArgs a) {
+  extern __shared__ __align__(1024) unsigned char tc_smem[];
+  unsigned char* As = tc_smem;
+  unsigned char* Bs = tc_smem + kTcBytesA;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tc_smem + kTcBytesA + kTcBytesB);
+  uint32_t* taddr_slot = reinterpret_cast<uint32_t*>(tc_smem + kTcBytesA + kTcBytesB + 8);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int member = a.member0 + blockIdx.y;
+  const int n = a.n_dev ? min(a.n, *a.n_dev) : a.n;
+  const int r0 = blockIdx.x * kTcRows;
+  if (r0 >= n) return;  // whole block, before any allocation
+  const LayerGeom& L = a.L;
+  int width = 32;  // columns of TMEM used
+  for (int l = 0; l < L.n_layers; ++l) width = max(width, L.out_pad[l]);
+  const uint32_t ncols = width <= 32 ? 32 : width <= 64 ? 64 : width <= 128 ? 128 : 256;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(taddr_slot)),
+                 "r"(ncols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // input rows: 32 BF16 (four 16-byte chunks) per row; rows past n are zero
+  for (int c = tid; c < kTcRows * 4; c += blockDim.x) {
+    const int r = c >> 2, kc = c & 3;
+    uint4 v = make_uint4(0, 0, 0, 0);
+    if (r0 + r < n) v = *reinterpret_cast<const uint4*>(a.X + (size_t)(r0 + r) * 32 + kc * 8);
+    *reinterpret_cast<uint4*>(As + kmajor_off(r, kc * 8, kTcSboA)) = v;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *taddr_slot;
+  bool ok = true;
+  for (int l = 0; l < L.n_layers; ++l) {
+    const int N = L.out_pad[l], K = L.in_pad[l], sbo_b = K / 8 * 128;
+    const bf16* W = a.Wb[member] + L.wb_off[l];
+    for (int c = tid; c < N * (K / 8); c += blockDim.x) {
+      const int row = c / (K / 8), kc = c % (K / 8);
+      *reinterpret_cast<uint4*>(Bs + kmajor_off(row, kc * 8, sbo_b)) =
+          *reinterpret_cast<const uint4*>(W + (size_t)row * K + kc * 8);
+    }
+    // generic-proxy shared-memory writes become visible to the tensor core
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t idesc = umma_idesc_bf16(kTcRows, N);
+      for (int j = 0; j < K / 16; ++j) {
+        const uint64_t ad = umma_desc(smem_u32(As) + j * 256, 128, kTcSboA);
+        const uint64_t bd = umma_desc(smem_u32(Bs) + j * 256, 128, sbo_b);
+        const uint32_t acc = j > 0;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+            "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                   : "memory");
+    }
+    ok = mbar_wait(smem_u32(bar), (uint32_t)(l & 1)) && ok;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // epilogue: this thread's row is TMEM lane 32 * warp + lane
+    const int row = warp * 32 + lane;
+    const float* bias = a.P[member] + L.b_off[l];
+    const bool last = l + 1 == L.n_layers;
+    for (int c0 = 0; c0 < N; c0 += 32) {
+      uint32_t v[32];
+      const uint32_t addr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+          "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+            "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+            "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+          : "r"(addr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (last) {
+        if (r0 + row < n) {
+          float* y = a.Y + blockIdx.y * a.y_stride + (size_t)(r0 + row) * a.ldy;
+#pragma unroll
+          for (int k = 0; k < 32; ++k) {
+            const int c = c0 + k;
+            if (c < L.out_real[l]) y[c] = ok ? __uint_as_float(v[k]) + bias[c] : __int_as_float(0x7fc00000);
+          }
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          uint32_t pk[4];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const int c = c0 + q * 8 + 2 * e;
+            const float z0 = __uint_as_float(v[q * 8 + 2 * e]) + bias[c];
+            const float z1 = __uint_as_float(v[q * 8 + 2 * e + 1]) + bias[c + 1];
+            __nv_bfloat162 h2 = __floats2bfloat162_rn(silu(z0), silu(z1));
+            pk[e] = *reinterpret_cast<uint32_t*>(&h2);
+          }
+          *reinterpret_cast<uint4*>(As + kmajor_off(row, c0 + q * 8, kTcSboA)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+        }
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+  }
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
+}
+
+
 // Adam on the FP32 parameters, then the padded BF16 copies W [out_pad][in_pad] and W^T [in_pad][out_pad].
 __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ grad, float* __restrict__ m1,
                             float* __restrict__ m2, long long n_params, float lr, float b1, float b2, float eps,
@@ -428,6 +606,8 @@ struct BdMlp {
   std::vector<bf16*> A, At, dZ, dZt;
   float *Y = nullptr, *part = nullptr, *loss_part = nullptr, *loss_tmp = nullptr;
   long long part_stride = 0;
+  int inference = 1;  // 1: tcgen05 kernel when the shape allows, 0: mma.sync GEMM chain
+  bool tc_attr = false;
   // inference scratch (infer_cap rows)
   int infer_cap = 0;
   std::vector<void*> infer_allocs;
@@ -604,6 +784,51 @@ int forward(BdMlp* m, int member, int n, const bf16* Xb, float* Y, int ldy, bool
   return BD_OK;
 }
 
+bool tc_eligible(const BdMlp* m) {
+  if (m->inference != 1 || m->L.in_pad[0] != 32 || m->d.hidden > kTcK) return false;
+  for (int l = 0; l < m->L.n_layers; ++l)
+    if (m->L.out_pad[l] > 256 || m->L.in_pad[l] > kTcK) return false;
+  return true;
+}
+
+// Members [member0, member0 + count) on packed rows Xp (n x 32 BF16): Y block of member k at
+// Y + k * y_stride, rows ldy apart.  tcgen05 kernel, one CTA per (128-row tile, member).
+int forward_tc(BdMlp* m, int member0, int count, int n, const bf16* Xp, float* Y, int ldy, long long y_stride,
+               cudaStream_t s, const int* n_dev = nullptr) {
+  if (!m->tc_attr) {
+    MCK(m, cudaFuncSetAttribute(mlp_forward_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
+    m->tc_attr = true;
+  }
+  TcArgs a{};
+  a.X = Xp;
+  a.n = n;
+  a.n_dev = n_dev;
+  for (int k = 0; k < count; ++k) {
+    a.Wb[k] = m->mem[member0 + k].Wb;
+    a.P[k] = m->mem[member0 + k].p;
+  }
+  // the kernel indexes Wb / P by member0 + blockIdx.y: shift the tables so that works
+  TcArgs b = a;
+  for (int k = 0; k < kTcMaxMembers; ++k) {
+    b.Wb[k] = nullptr;
+    b.P[k] = nullptr;
+  }
+  for (int k = 0; k < count; ++k) {
+    b.Wb[member0 + k] = a.Wb[k];
+    b.P[member0 + k] = a.P[k];
+  }
+  b.L = m->L;
+  b.Y = Y;
+  b.ldy = ldy;
+  b.y_stride = y_stride;
+  b.member0 = member0;
+  dim3 grid((n + kTcRows - 1) / kTcRows, count);
+  if (grid.x == 0) return BD_OK;
+  mlp_forward_tc_kernel<<<grid, kTcRows, kTcSmem, s>>>(b);
+  MCK(m, cudaGetLastError());
+  return BD_OK;
+}
+
 // Loss and gradient of one member on n rows (n % 32 == 0) into the member's grad buffer.
 int backward(BdMlp* m, int member, int n, const float* X, const float* T, float* loss, cudaStream_t s,
              float* trace = nullptr) {
@@ -691,8 +916,12 @@ int bd_internal_mlp_ensemble(BdMlp* m, int64_t n, const float* X, float* mean, f
     pack_input_kernel<<<grid_for(m, (long long)rows * L.in_pad[0]), 256, 0, s>>>(
         X + r0 * m->d.in_dim, rows, m->d.in_dim, m->Xi, L.in_pad[0], nullptr, 0);
     MCK(m, cudaGetLastError());
-    for (int k = 0; k < m->d.n_members; ++k)
-      if ((rc = forward(m, k, rows, m->Xi, m->Ys + (size_t)k * m->infer_cap * od, od, false, s))) return rc;
+    if (tc_eligible(m)) {
+      if ((rc = forward_tc(m, 0, m->d.n_members, rows, m->Xi, m->Ys, od, (long long)m->infer_cap * od, s))) return rc;
+    } else {
+      for (int k = 0; k < m->d.n_members; ++k)
+        if ((rc = forward(m, k, rows, m->Xi, m->Ys + (size_t)k * m->infer_cap * od, od, false, s))) return rc;
+    }
     ensemble_kernel<<<grid_for(m, (long long)rows * od), 256, 0, s>>>(
         m->Ys, m->d.n_members, (long long)m->infer_cap * od, rows, od, mean + r0 * od,
         spread ? spread + r0 * od : nullptr, nullptr);
@@ -745,9 +974,16 @@ int bd_internal_mlp_ensemble_rows(BdMlp* m, int rows, const int* n_dev, const vo
   if (rows > m->infer_cap) return mfail(m, BD_ERR_STATE, "inference buffers hold %d rows, %d asked", m->infer_cap, rows);
   const int od = m->d.out_dim;
   int rc;
-  for (int k = 0; k < m->d.n_members; ++k)
-    if ((rc = forward(m, k, rows, (const bf16*)Xpacked, m->Ys + (size_t)k * m->infer_cap * od, od, false, s, n_dev)))
+  if (tc_eligible(m)) {
+    if ((rc = forward_tc(m, 0, m->d.n_members, rows, (const bf16*)Xpacked, m->Ys, od, (long long)m->infer_cap * od,
+                         s, n_dev)))
       return rc;
+  } else {
+    for (int k = 0; k < m->d.n_members; ++k)
+      if ((rc = forward(m, k, rows, (const bf16*)Xpacked, m->Ys + (size_t)k * m->infer_cap * od, od, false, s,
+                        n_dev)))
+        return rc;
+  }
   ensemble_kernel<<<grid_for(m, (long long)rows * od), 256, 0, s>>>(m->Ys, m->d.n_members, (long long)m->infer_cap * od,
                                                                      rows, od, mean, spread, n_dev);
   MCK(m, cudaGetLastError());
@@ -899,7 +1135,11 @@ int bd_mlp_forward(BdMlp* m, int member, int64_t n, const float* X, float* Y, vo
     pack_input_kernel<<<grid_for(m, (long long)rows * m->L.in_pad[0]), 256, 0, s>>>(
         X + r0 * m->d.in_dim, rows, m->d.in_dim, m->Xi, m->L.in_pad[0], nullptr, 0);
     MCK(m, cudaGetLastError());
-    if ((rc = forward(m, member, rows, m->Xi, Y + r0 * m->d.out_dim, m->d.out_dim, false, s))) return rc;
+    if (tc_eligible(m)) {
+      if ((rc = forward_tc(m, member, 1, rows, m->Xi, Y + r0 * m->d.out_dim, m->d.out_dim, 0, s))) return rc;
+    } else if ((rc = forward(m, member, rows, m->Xi, Y + r0 * m->d.out_dim, m->d.out_dim, false, s))) {
+      return rc;
+    }
   }
   return BD_OK;
 }
@@ -986,6 +1226,13 @@ int bd_mlp_train(BdMlp* m, int member, int64_t n_data, const float* X, const flo
     m->tg_trace = loss_trace;
   }
   for (int i = 0; i < steps; ++i) MCK(m, cudaGraphLaunch(m->train_graph, s));
+  return BD_OK;
+}
+
+int bd_mlp_set_inference(BdMlp* m, int mode) {
+  if (!m) return BD_ERR_ARG;
+  if (mode != 0 && mode != 1) return mfail(m, BD_ERR_ARG, "inference mode must be 0 (mma.sync) or 1 (tcgen05)");
+  m->inference = mode;
   return BD_OK;
 }
 

@@ -180,6 +180,10 @@ class MLPEnsemble:
         self._call("bd_mlp_train_step", int(member), X.shape[0], _lib.P(X.data_ptr()), _lib.P(T.data_ptr()),
                    C.c_float(lr), _lib.P(loss.data_ptr() if loss is not None else 0), self._stream())
 
+    def set_inference(self, mode):
+        """1: tcgen05 inference kernel (default), 0: the mma.sync GEMM chain."""
+        self._call("bd_mlp_set_inference", int(mode))
+
     def train(self, member, X, T, batch, steps, lr, seed=0, trace=True):
         """``steps`` Adam steps on random batches of device-resident (X, T); returns the loss trace."""
         import torch

@@ -113,3 +113,25 @@ def test_device_training_loop_matches_eager_steps_in_effect():
     tr2 = e.train(0, X, T, 1024, 50, 1e-3, seed=6).cpu().numpy()
     assert tr2.mean() < 2 * tr[-50:].mean()
     e.close()
+
+
+@pytest.mark.parametrize("shape,n", [((13, 256, 4, 6), 1000), ((13, 256, 4, 6), 300_000), ((7, 128, 2, 3), 333)])
+def test_tcgen05_inference_matches_mma_sync_and_oracle(shape, n):
+    in_dim, hidden, n_hidden, out_dim = shape
+    e = _ens(3, in_dim, hidden, n_hidden, out_dim, seed=21)
+    X, _ = _data(n, in_dim, out_dim, seed=4)
+    e.set_inference(1)
+    Y_tc = e.forward(1, X).cpu().numpy()
+    mean_tc, spread_tc = (t.cpu().numpy() for t in e.ensemble(X))
+    e.set_inference(0)
+    Y_mma = e.forward(1, X).cpu().numpy()
+    mean_mma, spread_mma = (t.cpu().numpy() for t in e.ensemble(X))
+    scale = np.max(np.abs(Y_mma))
+    assert np.all(np.isfinite(Y_tc))
+    assert np.max(np.abs(Y_tc - Y_mma)) <= 2e-2 * scale, np.max(np.abs(Y_tc - Y_mma))
+    assert np.median(np.abs(Y_tc - Y_mma)) <= 1e-3 * scale
+    np.testing.assert_allclose(mean_tc, mean_mma, atol=2e-2 * np.max(np.abs(mean_mma)))
+    k = min(n, 2000)
+    Yo, _ = om.forward(e.get_params(1).astype(np.float64), e.dims, X[:k], rounding=True)
+    assert np.max(np.abs(Y_tc[:k] - Yo)) <= 2e-2 * np.max(np.abs(Yo)) + 1e-4
+    e.close()
