@@ -86,6 +86,13 @@ __device__ __forceinline__ void mma_bf16(float c[4], const unsigned a[4], const 
 }
 
 __device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+// z * sigmoid(z) with sigmoid(z) = (1 + tanh(z / 2)) / 2 on the hardware tanh (relative error
+// ~2^-11, below the BF16 rounding the result goes through next)
+__device__ __forceinline__ float silu_fast(float z) {
+  float t;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(0.5f * z));
+  return 0.5f * z * (1.0f + t);
+}
 __device__ __forceinline__ float silu_grad(float z) {
   const float s = 1.0f / (1.0f + __expf(-z));
   return s * (1.0f + z * (1.0f - s));
@@ -342,14 +349,14 @@ constexpr int kTcK = 256;                        // widest K held in the activat
 constexpr int kTcSboA = kTcK / 8 * 128;          // bytes between 8-row groups of the activation tile
 constexpr int kTcBytesA = kTcRows * kTcK * 2;    // 64 KB
 constexpr int kTcBytesB = 256 * kTcK * 2;        // 128 KB
-constexpr int kTcSmem = kTcBytesA + kTcBytesB + 64;  // + mbarrier and TMEM address
+constexpr int kTcSmem = kTcBytesA + kTcBytesB + 64;  // + two mbarriers and the TMEM address
 constexpr int kTcMaxMembers = 8;
 
 struct TcArgs {
   const bf16* X;  // n x 32 packed BF16 input rows
   int n;
   const int* n_dev;  // optional device row count
-  const bf16* Wb[kTcMaxMembers];
+  const bf16* Wc[kTcMaxMembers];  // per member: each layer's weights as the canonical shared-memory image
   const float* P[kTcMaxMembers];  // FP32 parameter vectors (biases)
   LayerGeom L;
   float* Y;  // per member: rows x ldy, members y_stride apart (member0's block first)
@@ -392,12 +399,29 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
   return false;
 }
 
-__global__ void __launch_bounds__(128, 1) mlp_forward_tc_kernel(TcArgs a) {
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
+// Thread 0: stream layer l's weight image (already in the canonical layout) into the B tile.
+__device__ __forceinline__ void load_weights_async(const TcArgs& a, int member, int l, unsigned char* Bs,
+                                                   uint32_t bar) {
+  const LayerGeom& L = a.L;
+  const uint32_t bytes = (uint32_t)(L.out_pad[l] * L.in_pad[l] * 2);
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+  const unsigned char* src = reinterpret_cast<const unsigned char*>(a.Wc[member] + L.wb_off[l]);
+  for (uint32_t off = 0; off < bytes; off += 32768u)
+    bulk_g2s(smem_u32(Bs) + off, src + off, min(32768u, bytes - off), bar);
+}
+
+__global__ void __launch_bounds__(512, 1) mlp_forward_tc_kernel(TcArgs a) {
   extern __shared__ __align__(1024) unsigned char tc_smem[];
   unsigned char* As = tc_smem;
   unsigned char* Bs = tc_smem + kTcBytesA;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(tc_smem + kTcBytesA + kTcBytesB);
-  uint32_t* taddr_slot = reinterpret_cast<uint32_t*>(tc_smem + kTcBytesA + kTcBytesB + 8);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tc_smem + kTcBytesA + kTcBytesB);  // [0] MMA done, [1] weights in
+  uint32_t* taddr_slot = reinterpret_cast<uint32_t*>(tc_smem + kTcBytesA + kTcBytesB + 16);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int member = a.member0 + blockIdx.y;
   const int n = a.n_dev ? min(a.n, *a.n_dev) : a.n;
@@ -407,14 +431,18 @@ __global__ void __launch_bounds__(128, 1) mlp_forward_tc_kernel(TcArgs a) {
   int width = 32;  // columns of TMEM used
   for (int l = 0; l < L.n_layers; ++l) width = max(width, L.out_pad[l]);
   const uint32_t ncols = width <= 32 ? 32 : width <= 64 ? 64 : width <= 128 ? 128 : 256;
+  const uint32_t bar_mma = smem_u32(bar), bar_w = smem_u32(bar + 1);
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(taddr_slot)),
                  "r"(ncols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
   }
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(1));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_mma), "r"(1));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_w), "r"(1));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    load_weights_async(a, member, 0, Bs, bar_w);
   }
   // input rows: 32 BF16 (four 16-byte chunks) per row; rows past n are zero
   for (int c = tid; c < kTcRows * 4; c += blockDim.x) {
@@ -423,23 +451,19 @@ __global__ void __launch_bounds__(128, 1) mlp_forward_tc_kernel(TcArgs a) {
     if (r0 + r < n) v = *reinterpret_cast<const uint4*>(a.X + (size_t)(r0 + r) * 32 + kc * 8);
     *reinterpret_cast<uint4*>(As + kmajor_off(r, kc * 8, kTcSboA)) = v;
   }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *taddr_slot;
   bool ok = true;
+  // epilogue split: warp w reads TMEM lanes 32 (w % 4) .. + 31 and every fourth 32-column chunk
+  const int quarter = warp & 3, colgroup = warp >> 2;
+  const int row = quarter * 32 + lane;
   for (int l = 0; l < L.n_layers; ++l) {
     const int N = L.out_pad[l], K = L.in_pad[l], sbo_b = K / 8 * 128;
-    const bf16* W = a.Wb[member] + L.wb_off[l];
-    for (int c = tid; c < N * (K / 8); c += blockDim.x) {
-      const int row = c / (K / 8), kc = c % (K / 8);
-      *reinterpret_cast<uint4*>(Bs + kmajor_off(row, kc * 8, sbo_b)) =
-          *reinterpret_cast<const uint4*>(W + (size_t)row * K + kc * 8);
-    }
-    // generic-proxy shared-memory writes become visible to the tensor core
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
     if (tid == 0) {
+      ok = mbar_wait(bar_w, (uint32_t)(l & 1)) && ok;  // this layer's weights are in
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t idesc = umma_idesc_bf16(kTcRows, N);
       for (int j = 0; j < K / 16; ++j) {
@@ -451,18 +475,18 @@ __global__ void __launch_bounds__(128, 1) mlp_forward_tc_kernel(TcArgs a) {
             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
             "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
       }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_mma)
                    : "memory");
     }
-    ok = mbar_wait(smem_u32(bar), (uint32_t)(l & 1)) && ok;
+    ok = mbar_wait(bar_mma, (uint32_t)(l & 1)) && ok;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    // epilogue: this thread's row is TMEM lane 32 * warp + lane
-    const int row = warp * 32 + lane;
+    // the B tile is free again: the next layer's weights stream in during this epilogue
+    if (tid == 0 && l + 1 < L.n_layers) load_weights_async(a, member, l + 1, Bs, bar_w);
     const float* bias = a.P[member] + L.b_off[l];
     const bool last = l + 1 == L.n_layers;
-    for (int c0 = 0; c0 < N; c0 += 32) {
+    for (int c0 = 32 * colgroup; c0 < N; c0 += 128) {
       uint32_t v[32];
-      const uint32_t addr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+      const uint32_t addr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c0;
       asm volatile(
           "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
           "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
@@ -490,13 +514,14 @@ __global__ void __launch_bounds__(128, 1) mlp_forward_tc_kernel(TcArgs a) {
             const int c = c0 + q * 8 + 2 * e;
             const float z0 = __uint_as_float(v[q * 8 + 2 * e]) + bias[c];
             const float z1 = __uint_as_float(v[q * 8 + 2 * e + 1]) + bias[c + 1];
-            __nv_bfloat162 h2 = __floats2bfloat162_rn(silu(z0), silu(z1));
+            __nv_bfloat162 h2 = __floats2bfloat162_rn(silu_fast(z0), silu_fast(z1));
             pk[e] = *reinterpret_cast<uint32_t*>(&h2);
           }
           *reinterpret_cast<uint4*>(As + kmajor_off(row, c0 + q * 8, kTcSboA)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
         }
       }
     }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
   }
@@ -508,7 +533,7 @@ __global__ void __launch_bounds__(128, 1) mlp_forward_tc_kernel(TcArgs a) {
 __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ grad, float* __restrict__ m1,
                             float* __restrict__ m2, long long n_params, float lr, float b1, float b2, float eps,
                             const long long* __restrict__ t_prev, LayerGeom L, bf16* __restrict__ Wb,
-                            bf16* __restrict__ Wt) {
+                            bf16* __restrict__ Wt, bf16* __restrict__ Wc) {
   // bias corrections of step t = t_prev + 1
   const double t = (double)(*t_prev + 1);
   const float c1 = (float)(1.0 - pow((double)b1, t)), c2 = (float)(1.0 - pow((double)b2, t));
@@ -528,6 +553,7 @@ __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ gra
         const bf16 v = __float2bfloat16_rn(w);
         Wb[L.wb_off[l] + (size_t)o * L.in_pad[l] + c] = v;
         Wt[L.wb_off[l] + (size_t)c * L.out_pad[l] + o] = v;
+        Wc[L.wb_off[l] + kmajor_off(o, c, L.in_pad[l] / 8 * 128) / 2] = v;
       }
     }
   }
@@ -535,7 +561,7 @@ __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ gra
 
 // BF16 copies of every weight from the FP32 parameters (after set/initialise).
 __global__ void refresh_kernel(const float* __restrict__ p, long long n_params, LayerGeom L, bf16* __restrict__ Wb,
-                               bf16* __restrict__ Wt) {
+                               bf16* __restrict__ Wt, bf16* __restrict__ Wc) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n_params;
        i += (long long)gridDim.x * blockDim.x) {
     for (int l = 0; l < L.n_layers; ++l) {
@@ -545,6 +571,7 @@ __global__ void refresh_kernel(const float* __restrict__ p, long long n_params, 
         const bf16 v = __float2bfloat16_rn(p[i]);
         Wb[L.wb_off[l] + (size_t)o * L.in_pad[l] + c] = v;
         Wt[L.wb_off[l] + (size_t)c * L.out_pad[l] + o] = v;
+        Wc[L.wb_off[l] + kmajor_off(o, c, L.in_pad[l] / 8 * 128) / 2] = v;
       }
     }
   }
@@ -582,7 +609,7 @@ struct BdMlp {
   int n_sm = 148;
   struct Member {
     float *p = nullptr, *m1 = nullptr, *m2 = nullptr, *grad = nullptr;
-    bf16 *Wb = nullptr, *Wt = nullptr;
+    bf16 *Wb = nullptr, *Wt = nullptr, *Wc = nullptr;  // W, W^T, and W as canonical tcgen05 tiles
     long long* step = nullptr;  // device: Adam steps taken
   };
   // graph of one training step (bd_mlp_train), rebuilt when its arguments change
@@ -803,19 +830,11 @@ int forward_tc(BdMlp* m, int member0, int count, int n, const bf16* Xp, float* Y
   a.X = Xp;
   a.n = n;
   a.n_dev = n_dev;
-  for (int k = 0; k < count; ++k) {
-    a.Wb[k] = m->mem[member0 + k].Wb;
-    a.P[k] = m->mem[member0 + k].p;
-  }
-  // the kernel indexes Wb / P by member0 + blockIdx.y: shift the tables so that works
+  // the kernel indexes the tables by member0 + blockIdx.y
   TcArgs b = a;
-  for (int k = 0; k < kTcMaxMembers; ++k) {
-    b.Wb[k] = nullptr;
-    b.P[k] = nullptr;
-  }
   for (int k = 0; k < count; ++k) {
-    b.Wb[member0 + k] = a.Wb[k];
-    b.P[member0 + k] = a.P[k];
+    b.Wc[member0 + k] = m->mem[member0 + k].Wc;
+    b.P[member0 + k] = m->mem[member0 + k].p;
   }
   b.L = m->L;
   b.Y = Y;
@@ -824,7 +843,7 @@ int forward_tc(BdMlp* m, int member0, int count, int n, const bf16* Xp, float* Y
   b.member0 = member0;
   dim3 grid((n + kTcRows - 1) / kTcRows, count);
   if (grid.x == 0) return BD_OK;
-  mlp_forward_tc_kernel<<<grid, kTcRows, kTcSmem, s>>>(b);
+  mlp_forward_tc_kernel<<<grid, 512, kTcSmem, s>>>(b);
   MCK(m, cudaGetLastError());
   return BD_OK;
 }
@@ -933,7 +952,7 @@ int bd_internal_mlp_ensemble(BdMlp* m, int64_t n, const float* X, float* mean, f
 int adam_update(BdMlp* m, int member, float lr, cudaStream_t s) {
   BdMlp::Member& w = m->mem[member];
   adam_kernel<<<grid_for(m, m->n_params), 256, 0, s>>>(w.p, w.grad, w.m1, w.m2, m->n_params, lr, 0.9f, 0.999f, 1e-8f,
-                                                        w.step, m->L, w.Wb, w.Wt);
+                                                        w.step, m->L, w.Wb, w.Wt, w.Wc);
   MCK(m, cudaGetLastError());
   step_increment_kernel<<<1, 1, 0, s>>>(w.step);
   MCK(m, cudaGetLastError());
@@ -1045,6 +1064,8 @@ int bd_mlp_create(int device, const BdMlpDesc* d, BdMlp** out) {
     w.Wb = (bf16*)p;
     if ((rc = malloc_into(m, m->allocs, &p, woff * 2))) goto fail;
     w.Wt = (bf16*)p;
+    if ((rc = malloc_into(m, m->allocs, &p, woff * 2))) goto fail;
+    w.Wc = (bf16*)p;
     if ((rc = malloc_into(m, m->allocs, &p, sizeof(long long)))) goto fail;
     w.step = (long long*)p;
     // uniform(-1/sqrt(fan_in), 1/sqrt(fan_in)) for weights and biases, member by member
@@ -1059,7 +1080,7 @@ int bd_mlp_create(int device, const BdMlpDesc* d, BdMlp** out) {
       rc = BD_ERR_CUDA;
       goto fail;
     }
-    refresh_kernel<<<grid_for(m, off), 256>>>(w.p, off, L, w.Wb, w.Wt);
+    refresh_kernel<<<grid_for(m, off), 256>>>(w.p, off, L, w.Wb, w.Wt, w.Wc);
     continue;
   fail:
     for (void* q : m->allocs) cudaFree(q);
@@ -1118,7 +1139,7 @@ int bd_mlp_set_params(BdMlp* m, int member, const float* params) {
   MCK(m, cudaMemset(w.m1, 0, m->n_params * 4));
   MCK(m, cudaMemset(w.m2, 0, m->n_params * 4));
   MCK(m, cudaMemset(w.step, 0, sizeof(long long)));
-  refresh_kernel<<<grid_for(m, m->n_params), 256>>>(w.p, m->n_params, m->L, w.Wb, w.Wt);
+  refresh_kernel<<<grid_for(m, m->n_params), 256>>>(w.p, m->n_params, m->L, w.Wb, w.Wt, w.Wc);
   MCK(m, cudaGetLastError());
   MCK(m, cudaDeviceSynchronize());
   return BD_OK;
