@@ -114,112 +114,112 @@ __global__ void __launch_bounds__(256) gemm_nt(GemmArgs g) {
   const int kb = blockIdx.z * g.k_per_split, ke = min(g.K, kb + g.k_per_split);
   // row tiles are shared out over gridDim.y blocks (block-uniform loop: barriers stay whole)
   for (int m0 = blockIdx.y * BM; m0 < M; m0 += gridDim.y * BM) {
-  float acc[MT][NT][4];
+    float acc[MT][NT][4];
 #pragma unroll
-  for (int i = 0; i < MT; ++i)
+    for (int i = 0; i < MT; ++i)
 #pragma unroll
-    for (int j = 0; j < NT; ++j)
+      for (int j = 0; j < NT; ++j)
 #pragma unroll
-      for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.f;
+        for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.f;
 
-  auto load = [&](int st, int k) {
-    for (int c = tid; c < BM * (kBK / 8); c += 256) {
-      const int r = c / (kBK / 8), kc = (c % (kBK / 8)) * 8;
-      const int row = m0 + r;
-      const bool ok = row < M;
-      cp_async16(&As[st][r][kc], g.A + (size_t)(ok ? row : 0) * g.lda + k + kc, ok ? 16 : 0);
-    }
-    for (int c = tid; c < BN * (kBK / 8); c += 256) {
-      const int r = c / (kBK / 8), kc = (c % (kBK / 8)) * 8;
-      const int row = n0 + r;
-      const bool ok = row < g.N;
-      cp_async16(&Bs[st][r][kc], g.B + (size_t)(ok ? row : 0) * g.ldb + k + kc, ok ? 16 : 0);
-    }
-    cp_async_commit();
-  };
-
-  int st = 0;
-  if (kb < ke) load(0, kb);
-  for (int k = kb; k < ke; k += kBK) {
-    if (k + kBK < ke) {
-      load(st ^ 1, k + kBK);
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
-    }
-    __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < kBK; kk += 16) {
-      unsigned a[MT][4], b[NT][2];
-#pragma unroll
-      for (int i = 0; i < MT; ++i) {
-        const int r = wm0 + i * 16 + gq;
-        a[i][0] = *reinterpret_cast<const unsigned*>(&As[st][r][kk + 2 * tq]);
-        a[i][1] = *reinterpret_cast<const unsigned*>(&As[st][r + 8][kk + 2 * tq]);
-        a[i][2] = *reinterpret_cast<const unsigned*>(&As[st][r][kk + 2 * tq + 8]);
-        a[i][3] = *reinterpret_cast<const unsigned*>(&As[st][r + 8][kk + 2 * tq + 8]);
+    auto load = [&](int st, int k) {
+      for (int c = tid; c < BM * (kBK / 8); c += 256) {
+        const int r = c / (kBK / 8), kc = (c % (kBK / 8)) * 8;
+        const int row = m0 + r;
+        const bool ok = row < M;
+        cp_async16(&As[st][r][kc], g.A + (size_t)(ok ? row : 0) * g.lda + k + kc, ok ? 16 : 0);
       }
-#pragma unroll
-      for (int j = 0; j < NT; ++j) {
-        const int c = wn0 + j * 8 + gq;
-        b[j][0] = *reinterpret_cast<const unsigned*>(&Bs[st][c][kk + 2 * tq]);
-        b[j][1] = *reinterpret_cast<const unsigned*>(&Bs[st][c][kk + 2 * tq + 8]);
+      for (int c = tid; c < BN * (kBK / 8); c += 256) {
+        const int r = c / (kBK / 8), kc = (c % (kBK / 8)) * 8;
+        const int row = n0 + r;
+        const bool ok = row < g.N;
+        cp_async16(&Bs[st][r][kc], g.B + (size_t)(ok ? row : 0) * g.ldb + k + kc, ok ? 16 : 0);
       }
-#pragma unroll
-      for (int i = 0; i < MT; ++i)
-#pragma unroll
-        for (int j = 0; j < NT; ++j) mma_bf16(acc[i][j], a[i], b[j]);
-    }
-    __syncthreads();
-    st ^= 1;
-  }
+      cp_async_commit();
+    };
 
-  // epilogue: acc[i][j][h*2 + e] is row wm0 + i*16 + gq + 8h, column wn0 + j*8 + 2tq + e
+    int st = 0;
+    if (kb < ke) load(0, kb);
+    for (int k = kb; k < ke; k += kBK) {
+      if (k + kBK < ke) {
+        load(st ^ 1, k + kBK);
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
+      __syncthreads();
 #pragma unroll
-  for (int i = 0; i < MT; ++i)
+      for (int kk = 0; kk < kBK; kk += 16) {
+        unsigned a[MT][4], b[NT][2];
 #pragma unroll
-    for (int j = 0; j < NT; ++j)
+        for (int i = 0; i < MT; ++i) {
+          const int r = wm0 + i * 16 + gq;
+          a[i][0] = *reinterpret_cast<const unsigned*>(&As[st][r][kk + 2 * tq]);
+          a[i][1] = *reinterpret_cast<const unsigned*>(&As[st][r + 8][kk + 2 * tq]);
+          a[i][2] = *reinterpret_cast<const unsigned*>(&As[st][r][kk + 2 * tq + 8]);
+          a[i][3] = *reinterpret_cast<const unsigned*>(&As[st][r + 8][kk + 2 * tq + 8]);
+        }
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int r = m0 + wm0 + i * 16 + gq + 8 * h;
-        const int c = n0 + wn0 + j * 8 + 2 * tq;
-        if (r >= M || c >= g.N) continue;
-        float v0 = acc[i][j][2 * h], v1 = acc[i][j][2 * h + 1];
-        if constexpr (EPI == EPI_PARTIAL) {
-          float* p = g.C + blockIdx.z * g.split_stride + (size_t)r * g.ldc + c;
-          p[0] = v0;
-          p[1] = v1;
-        } else if constexpr (EPI == EPI_OUT_FWD) {
-          if (c < g.n_real) g.C[(size_t)r * g.ldc + c] = v0 + g.bias[c];
-          if (c + 1 < g.n_real) g.C[(size_t)r * g.ldc + c + 1] = v1 + g.bias[c + 1];
-        } else {
-          float o0, o1;
-          if constexpr (EPI == EPI_HIDDEN_FWD) {
-            v0 += g.bias[c];
-            v1 += g.bias[c + 1];
-            if (g.C) {
-              g.C[(size_t)r * g.ldc + c] = v0;
-              g.C[(size_t)r * g.ldc + c + 1] = v1;
+        for (int j = 0; j < NT; ++j) {
+          const int c = wn0 + j * 8 + gq;
+          b[j][0] = *reinterpret_cast<const unsigned*>(&Bs[st][c][kk + 2 * tq]);
+          b[j][1] = *reinterpret_cast<const unsigned*>(&Bs[st][c][kk + 2 * tq + 8]);
+        }
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+          for (int j = 0; j < NT; ++j) mma_bf16(acc[i][j], a[i], b[j]);
+      }
+      __syncthreads();
+      st ^= 1;
+    }
+
+    // epilogue: acc[i][j][h*2 + e] is row wm0 + i*16 + gq + 8h, column wn0 + j*8 + 2tq + e
+#pragma unroll
+    for (int i = 0; i < MT; ++i)
+#pragma unroll
+      for (int j = 0; j < NT; ++j)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int r = m0 + wm0 + i * 16 + gq + 8 * h;
+          const int c = n0 + wn0 + j * 8 + 2 * tq;
+          if (r >= M || c >= g.N) continue;
+          float v0 = acc[i][j][2 * h], v1 = acc[i][j][2 * h + 1];
+          if constexpr (EPI == EPI_PARTIAL) {
+            float* p = g.C + blockIdx.z * g.split_stride + (size_t)r * g.ldc + c;
+            p[0] = v0;
+            p[1] = v1;
+          } else if constexpr (EPI == EPI_OUT_FWD) {
+            if (c < g.n_real) g.C[(size_t)r * g.ldc + c] = v0 + g.bias[c];
+            if (c + 1 < g.n_real) g.C[(size_t)r * g.ldc + c + 1] = v1 + g.bias[c + 1];
+          } else {
+            float o0, o1;
+            if constexpr (EPI == EPI_HIDDEN_FWD) {
+              v0 += g.bias[c];
+              v1 += g.bias[c + 1];
+              if (g.C) {
+                g.C[(size_t)r * g.ldc + c] = v0;
+                g.C[(size_t)r * g.ldc + c + 1] = v1;
+              }
+              o0 = silu(v0);
+              o1 = silu(v1);
+            } else {  // EPI_HIDDEN_BWD: v = dA, output dZ
+              o0 = v0 * silu_grad(g.Zin[(size_t)r * g.ldz + c]);
+              o1 = v1 * silu_grad(g.Zin[(size_t)r * g.ldz + c + 1]);
             }
-            o0 = silu(v0);
-            o1 = silu(v1);
-          } else {  // EPI_HIDDEN_BWD: v = dA, output dZ
-            o0 = v0 * silu_grad(g.Zin[(size_t)r * g.ldz + c]);
-            o1 = v1 * silu_grad(g.Zin[(size_t)r * g.ldz + c + 1]);
-          }
-          const bf16 b0 = __float2bfloat16_rn(o0), b1 = __float2bfloat16_rn(o1);
-          if (g.O) {
-            __nv_bfloat162 pr;
-            pr.x = b0;
-            pr.y = b1;
-            *reinterpret_cast<__nv_bfloat162*>(g.O + (size_t)r * g.ldo + c) = pr;
-          }
-          if (g.Ot) {
-            g.Ot[(size_t)c * g.ldot + r] = b0;
-            g.Ot[(size_t)(c + 1) * g.ldot + r] = b1;
+            const bf16 b0 = __float2bfloat16_rn(o0), b1 = __float2bfloat16_rn(o1);
+            if (g.O) {
+              __nv_bfloat162 pr;
+              pr.x = b0;
+              pr.y = b1;
+              *reinterpret_cast<__nv_bfloat162*>(g.O + (size_t)r * g.ldo + c) = pr;
+            }
+            if (g.Ot) {
+              g.Ot[(size_t)c * g.ldot + r] = b0;
+              g.Ot[(size_t)(c + 1) * g.ldot + r] = b1;
+            }
           }
         }
-      }
   }  // row tiles
 }
 
