@@ -228,9 +228,10 @@ int finalize(BdHandle* h) {
     }
   }
   if (h->layout & BD_LAYOUT_WINDOWS_1) {
-    for (int k = 0; k < S.n_elec; ++k)
+    // a paired lattice is read through the pair copy only: its single-channel grids need no window
+    for (int k = S.paired ? 1 : 0; k < S.n_elec; ++k)
       if (int rc = add_window(h, S.elec[k])) return rc;
-    if (S.has_born)
+    if (S.has_born && !S.paired)
       if (int rc = add_window(h, S.born)) return rc;
   }
   if (S.paired && (h->layout & BD_LAYOUT_WINDOWS_2))
