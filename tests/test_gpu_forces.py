@@ -158,3 +158,23 @@ def test_reference_chunk_skip_quirk_only_when_batch_is_far():
     a = o_skip(g["positions"], s.lig_q, g["R"], g["centroids"])[0]
     b = o_exact(g["positions"], s.lig_q, g["R"], g["centroids"])[0]
     np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("sysname", ["c2", "c3"])
+def test_force_terms_add_up(sysname):
+    """bd_set_terms: grid + far-field + reverse Born evaluated apart sum to the full force."""
+    from pystarc_b200 import _lib
+
+    s = system(sysname)
+    eng = make_engine(s, "fp64", "centroid")
+    c, q = random_poses(1500, 0.5, 60.0, 23)
+    F, T, E = eng.eval_poses(c, q)
+    parts = [eng.eval_poses(c, q, terms=t) for t in (_lib.TERM_GRID, _lib.TERM_FARFIELD, _lib.TERM_REV_BORN)]
+    Fs = sum(p[0] for p in parts)
+    Ts = sum(p[1] for p in parts)
+    np.testing.assert_allclose(Fs, F, rtol=1e-9, atol=1e-12 * np.abs(F).max())
+    np.testing.assert_allclose(Ts, T, rtol=1e-9, atol=1e-12 * np.abs(T).max())
+    # the mask is restored after each call
+    F2, _, _ = eng.eval_poses(c, q)
+    np.testing.assert_array_equal(F2, F)
+    eng.close()
