@@ -135,7 +135,8 @@ class _MP:
 _OPTS = {"layout": None}
 
 
-def make_sim(s, precision, n_traj, K, id_offset=0, torque="zero", surrogate=None, termination="complete", seed=None):
+def make_sim(s, precision, n_traj, K, id_offset=0, torque="zero", surrogate=None, termination="complete", seed=None,
+             slots=0):
     from pystarc_b200.engine import B200ForceEngine
     from pystarc_b200.simulator import B200BatchSimulator
 
@@ -143,26 +144,50 @@ def make_sim(s, precision, n_traj, K, id_offset=0, torque="zero", surrogate=None
                           device=int(os.environ.get("LOCAL_RANK", 0)), layout=_OPTS["layout"])
     mol1, mol2 = s.molecules()
     sim = B200BatchSimulator(mol1, mol2, s.mobility(), s.pathway_set(), s.params(n_traj=n_traj, seed=seed), eng,
-                             termination=termination, steps_per_launch=K, id_offset=id_offset, surrogate=surrogate)
+                             termination=termination, steps_per_launch=K, id_offset=id_offset, surrogate=surrogate,
+                             slots=slots)
     return sim
 
 
-def time_device_arm(s, precision, steps, warmup, K, n_traj, id_offset, dist, fixed_launch=None):
-    """Per-launch CUDA-event times (graph launches) with L2 flushes in between."""
+def pool_slots(n_traj):
+    """One slot-pool size for every arm (8 waves of 512 threads per SM), so aged pools can be restored."""
+    import torch
+
+    n_sm = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    return int(min(n_traj, 8 * n_sm * 512))
+
+
+def age_pool(sim, K, age, path):
+    """Advance a fresh pool by ``age`` launches (untimed) and save it, so that every arm times the
+    same state past the start-up transient (trajectories start on the b-sphere, where steps are
+    cheap; the per-step cost rises several-fold as they reach the receptor)."""
+    sim._setup()
+    h = sim.engine.handle
+    h.call("bd_sim_reset", None)
+    for _ in range(age):
+        h.call("bd_sim_run", 1, K, None)
+    return sim.save_checkpoint(path)
+
+
+def time_device_arm(s, precision, steps, warmup, K, n_traj, id_offset, dist, fixed_launch=None, aged=None,
+                    surrogate=None):
+    """Per-launch CUDA-event times (graph launches) with L2 flushes in between, from the aged pool."""
     import torch
 
     from pystarc_b200 import _lib
     from pystarc_b200.autotune import autotune
 
-    sim = make_sim(s, precision, n_traj, K, id_offset)
+    sim = make_sim(s, precision, n_traj, K, id_offset, surrogate=surrogate, slots=pool_slots(n_traj))
+    table = {}
     if fixed_launch:
-        table = {}
         sim.engine.handle.call("bd_set_launch", fixed_launch[0], fixed_launch[1])
-    else:
-        best, table = autotune(sim)  # untimed; the run below starts from a fresh reset
+    elif surrogate is None:
+        best, table = autotune(sim)  # untimed; the run below starts from the restored pool
     sim._setup()
     h = sim.engine.handle
     h.call("bd_sim_reset", None)
+    if aged is not None:
+        sim.load_checkpoint(aged)
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
@@ -198,13 +223,27 @@ def time_device_arm(s, precision, steps, warmup, K, n_traj, id_offset, dist, fix
     return sum(times), times, d, launch
 
 
+def aged_poses(path, n, seed=7):
+    """A sample of running poses (centroids, quaternions) from a saved pool."""
+    d = np.load(path)
+    C = int(d["cap"])
+    live = int(d["n_live"])
+    run = np.nonzero(d["status"][:live] == 0)[0]
+    rng = np.random.default_rng(seed)
+    pick = rng.choice(run, size=min(n, run.size), replace=False)
+    c = d["c"].reshape(3, C)[:, pick].T.copy()
+    q = d["q"].reshape(4, C)[:, pick].T.copy()
+    return c, q
+
+
 def e2e_arm(s, precision, steps, K, n_traj, id_offset, launch):
-    """Through the public API from host arrays: engine construction (grid uploads), run(), outcomes."""
+    """Through the public API from host arrays: engine construction (grid uploads), run() of the
+    first ``steps`` launches from the b-sphere (the aging and the timed window together), outcomes."""
     import torch
 
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    sim = make_sim(s, precision, n_traj, K, id_offset)
+    sim = make_sim(s, precision, n_traj, K, id_offset, slots=pool_slots(n_traj))
     sim.engine.handle.call("bd_set_launch", launch[0], launch[1])
     sim.M = 1
     res = sim.run(max_launches=steps)
@@ -219,7 +258,8 @@ def e2e_arm(s, precision, steps, K, n_traj, id_offset, launch):
     return res.total_steps / el, h2d / launches, d2h / launches, res
 
 
-def surrogate_arm(s, steps, warmup, K, n_traj, n_poses, train_steps, members, kon_traj, kon_launches=300, log=None):
+def surrogate_arm(s, steps, warmup, K, n_traj, n_poses, train_steps, members, kon_traj, kon_launches=300, log=None,
+                  aged=None):
     """Config 4: train the surrogate on exact-kernel BD poses, judge it on held-out poses, time the
     surrogate stepper like the exact one, and compare k_on of exact and surrogate runs."""
     import torch
@@ -252,10 +292,12 @@ def surrogate_arm(s, steps, warmup, K, n_traj, n_poses, train_steps, members, ko
     say(f"surrogate: trained in {rep.seconds:.1f} s, held-out {out['heldout']}")
     out["trust_region_A"] = [round(spec.r_min, 2), round(spec.r_max, 2)]
     # timed like the exact arm: graph launches of K steps, L2 flushed in between
-    sim = make_sim(s, "mixed", n_traj, K, surrogate=(ens, spec))
+    sim = make_sim(s, "mixed", n_traj, K, surrogate=(ens, spec), slots=pool_slots(n_traj))
     sim._setup()
     h = sim.engine.handle
     h.call("bd_sim_reset", None)
+    if aged is not None:
+        sim.load_checkpoint(aged)
     stream = torch.cuda.current_stream()
     sptr = _lib_P(stream.cuda_stream)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -401,7 +443,7 @@ def _lib_P(v):
 
 # --------------------------------------------------------------------------- CPU baseline
 def _cpu_worker(args):
-    grid_file, n_traj, seed, n_steps = args
+    grid_file, n_traj, seed, n_steps, init = args
     from oracle import stepper as ost
     from oracle.forces import FarField, OracleForceEngine, OracleGrid
 
@@ -420,7 +462,7 @@ def _cpu_worker(args):
     prm = ost.StepParams(n_traj=n_traj, seed=seed, r_b=float(d["r_b"]), r_esc=float(d["r_esc"]), max_steps=n_steps,
                          max_dt=float(d["max_dt"]), use_hi=bool(d["hi"]), overlap=bool(d["overlap"]))
     t0 = time.perf_counter()
-    res = ost.run(ss, prm, noise="pcg64", termination="reference")
+    res = ost.run(ss, prm, noise="pcg64", termination="reference", init=init)
     return res.total_steps, time.perf_counter() - t0
 
 
@@ -443,21 +485,34 @@ def save_cpu_inputs(s, path):
     np.savez(path, **arr)
 
 
-def cpu_baseline(s, cores, traj_per_proc=256, n_steps=40):
-    """The reference's step loop restated in NumPy on `cores` processes, each a bounded sample."""
+def cpu_baseline(s, cores, traj_per_proc=256, n_steps=40, init=None):
+    """The reference's step loop restated in NumPy on `cores` processes, each a bounded sample.
+
+    ``init`` = (centroids, quaternions): start the processes' trajectories from these poses (a
+    sample of the GPU arm's aged pool) instead of the b-sphere, so both arms time the same regime.
+    """
+    if init is not None:
+        traj_per_proc = max(1, min(traj_per_proc, len(init[0]) // cores))
+    jobs = []
+    for i in range(cores):
+        sl = None
+        if init is not None:
+            sl = (init[0][i * traj_per_proc:(i + 1) * traj_per_proc], init[1][i * traj_per_proc:(i + 1) * traj_per_proc])
+        jobs.append((traj_per_proc, 1000 + i, n_steps, sl))
     with tempfile.TemporaryDirectory() as td:
         f = os.path.join(td, "inputs.npz")
         save_cpu_inputs(s, f)
         ctx = mp.get_context("spawn")
         t0 = time.perf_counter()
         with ctx.Pool(cores) as pool:
-            out = pool.map(_cpu_worker, [(f, traj_per_proc, 1000 + i, n_steps) for i in range(cores)])
+            out = pool.map(_cpu_worker, [(f, n, sd, ns, sl) for n, sd, ns, sl in jobs])
         wall = time.perf_counter() - t0
     steps = sum(o[0] for o in out)
     busy = max(o[1] for o in out)
+    where = "poses sampled from the GPU arm's aged pool" if init is not None else "the b-sphere"
     return steps / busy, {"value": steps / busy, "unit": UNIT, "cores": cores, "kind": "port",
                           "sample": f"{cores} processes x {traj_per_proc} trajectories x <= {n_steps} steps of the "
-                                    f"same system from the b-sphere ({steps} trajectory-steps, {busy:.1f} s)",
+                                    f"same system from {where} ({steps} trajectory-steps, {busy:.1f} s)",
                           "wall_s": round(wall, 1)}
 
 
@@ -478,6 +533,8 @@ def main():
                          "4 windows for the paired grid; -1: library default)")
     ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate arm (config 4)")
+    ap.add_argument("--age", type=int, default=64,
+                    help="untimed launches that age the pool before every timed arm (0: time from the b-sphere)")
     ap.add_argument("--sur-poses", type=int, default=200_000)
     ap.add_argument("--sur-train-steps", type=int, default=8000)
     ap.add_argument("--sur-members", type=int, default=5)
@@ -532,15 +589,24 @@ def main():
     n_traj = args.n_traj or WORKLOADS[args.workload][1]
     id_offset = rank * n_traj
     clocks = Clocks(local)
-    clocks.start()
     fixed = tuple(int(v) for v in args.launch.split("x")) if args.launch else None
+    work = tempfile.mkdtemp(prefix="bench_pool_")
+    aged = None
+    if args.age > 0:
+        t_age = time.perf_counter()
+        ager = make_sim(s, "mixed", n_traj, args.inner, id_offset, slots=pool_slots(n_traj))
+        aged = age_pool(ager, args.inner, args.age, os.path.join(work, "aged.npz"))
+        ager.engine.close()
+        _progress(f"pool aged {args.age} launches ({args.age * args.inner} BD steps) in "
+                  f"{time.perf_counter() - t_age:.1f} s")
+    clocks.start()
     t_mixed, tl_mixed, d_mixed, launch = time_device_arm(s, "mixed", args.steps, args.warmup, args.inner, n_traj,
-                                                         id_offset, dist, fixed)
+                                                         id_offset, dist, fixed, aged=aged)
     ck = clocks.stop()
     t_fp64, tl_fp64, d_fp64, launch64 = time_device_arm(s, "fp64", args.steps, args.warmup, args.inner, n_traj,
-                                                        id_offset, dist, fixed)
+                                                        id_offset, dist, fixed, aged=aged)
     _progress(f"exact arms: mixed {d_mixed['steps'] / t_mixed:.3e}, fp64 {d_fp64['steps'] / t_fp64:.3e} steps/s")
-    e2e_val, h2d, d2h, e2e_res = e2e_arm(s, "mixed", max(args.steps, 20), args.inner, n_traj, id_offset,
+    e2e_val, h2d, d2h, e2e_res = e2e_arm(s, "mixed", args.age + max(args.steps, 20), args.inner, n_traj, id_offset,
                                          (launch["group"], launch["block"]))
     _progress(f"e2e arm: {e2e_val:.3e} steps/s")
     t_max = t_mixed
@@ -574,6 +640,10 @@ def main():
         "dtype": "f32 forces / f64 poses", "data": "synthetic",
         "config": {"workload": WORKLOADS[args.workload][0], "trajectories_per_gpu": n_traj,
                    "bd_steps_per_launch": args.inner,
+                   "timed_window": (f"BD steps {(args.age + args.warmup) * args.inner}-"
+                                    f"{(args.age + args.warmup + args.steps) * args.inner} of the run: the pool is "
+                                    f"aged {args.age} launches (restored for each arm), then {args.warmup} warm-up "
+                                    f"launches"),
                    "parallelism": f"trajectory shards x{world}", "l2": "flushed (256 MiB write) between launches",
                    "launch": launch},
         "variants": {
@@ -593,11 +663,16 @@ def main():
     if world == 1 and not args.no_surrogate and args.workload != "two-spheres":
         line["variants"]["surrogate"] = surrogate_arm(s, args.steps, args.warmup, args.inner, n_traj, args.sur_poses,
                                                       args.sur_train_steps, args.sur_members, args.sur_kon_traj,
-                                                      log=_progress)
+                                                      log=_progress, aged=aged)
     if world == 1 and not args.no_cpu_baseline:
-        _, info = cpu_baseline(s, os.cpu_count() or 1, n_steps=args.cpu_steps)
+        cores = os.cpu_count() or 1
+        init = aged_poses(aged, cores * 64) if aged is not None else None
+        _, info = cpu_baseline(s, cores, n_steps=args.cpu_steps, init=init)
         line["cpu_baseline"] = info
     print(json.dumps(line))
+    import shutil
+
+    shutil.rmtree(work, ignore_errors=True)
     if dist is not None:
         dist.destroy_process_group()
 

@@ -303,13 +303,16 @@ def _forces(sys, R_sr, cen_sr, force_batch=None):
 
 
 def run(sys: StepSystem, prm: StepParams, noise: str = "pcg64", termination: str = "reference",
-        force_batch=None, id_offset: int = 0) -> StepResult:
+        force_batch=None, id_offset: int = 0, init=None) -> StepResult:
     """Run ``prm.n_traj`` trajectories; see the module docstring for the two noise modes.
 
     ``termination="reference"`` stops the loop when 99.5 % are done or on a stall
     (gpu_batch_simulator.py:1347-1356); ``"complete"`` runs until every
     trajectory has reacted, escaped or used ``max_steps`` steps.  With keyed
     noise, local trajectory i draws as global trajectory ``id_offset + i``.
+    ``init`` = (centroids (N, 3), quaternions (N, 4)) starts the trajectories
+    from given poses instead of the b-sphere (used to time the loop on an aged
+    pool; not part of the reference).
     """
     N = prm.n_traj
     keyed = noise == "philox"
@@ -331,6 +334,9 @@ def run(sys: StepSystem, prm: StepParams, noise: str = "pcg64", termination: str
     v /= np.linalg.norm(v, axis=1, keepdims=True)
     pos = v * r_b
     q = shoemake(draws.start_uniforms(all_ids) if keyed else rng.random((N, 3)).astype(np.float64))
+    if init is not None:
+        pos = np.array(init[0], dtype=np.float64).reshape(N, 3)
+        q = np.array(init[1], dtype=np.float64).reshape(N, 4)
     status = np.zeros(N, dtype=np.int32)
     n_steps = np.zeros(N, dtype=np.int64)
     n_returns = np.zeros(N, dtype=np.int64)
