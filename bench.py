@@ -631,6 +631,9 @@ def main():
         m = re.search(r"dram_bytes_per_launch \| (\d+)", tf.read_text())
         traffic = int(m.group(1)) if m else None
     if rank != 0:
+        import shutil
+
+        shutil.rmtree(work, ignore_errors=True)
         if dist is not None:
             dist.destroy_process_group()
         return
