@@ -107,6 +107,15 @@ int bd_set_ligand(BdHandle* h, int n, const double* body_xyz, const double* char
  * rec_positions / rec_charges and the stepper's overlap table (gpu_batch_engine.py:207-217,
  * gpu_batch_simulator.py:771-781). */
 int bd_set_receptor(BdHandle* h, int n, const double* xyz, const double* charges);
+/* WCA contact forces (the repulsive part of Lennard-Jones) between every ligand and receptor
+ * atom, from their radii: sigma = r_lig + r_rec, force eps (12 (sigma/r)^12 - 6 (sigma/r)^6) / r^2
+ * along the pair for r < 1.122462 sigma, only for poses whose centroid is within `activation`
+ * of the origin.  Radii follow the order of bd_set_ligand / bd_set_receptor (all atoms, charged
+ * or not); activation < 0 selects 2.5 (max r_rec + max r_lig).  n_rec = 0 turns the term off.
+ * Replaces GPUBatchForceEngine's rec_radii / lig_radii / use_lj and _wca_forces_gpu
+ * (gpu_batch_engine.py:233-246, :474-529, :600-602); eps is the reference's 0.17 kBT. */
+int bd_set_contact(BdHandle* h, int n_rec, const double* rec_radii, int n_lig, const double* lig_radii, double eps,
+                   double activation);
 /* Add a FP32 grid (host array, C order, z fastest).  kind = BD_GRID_*.  Grids are sorted
  * finest-first and dropped as the reference does (gpu_batch_engine.py:179-211, :248-287). */
 int bd_add_grid(BdHandle* h, int kind, const float* data, int nx, int ny, int nz, const double* origin,
@@ -205,10 +214,11 @@ int bd_sim_run_noalloc(BdHandle* h, const BdSimParams* p, int8_t* out_status, in
  * No reference counterpart: bit flags choosing which terms bd_eval_forces(_atoms) sum.
  * BD_TERM_GRID: electrostatic and Born direction-1 grid forces on the ligand atoms;
  * BD_TERM_FARFIELD: the Yukawa multipole far-field of atoms outside every electrostatic grid;
- * BD_TERM_REV_BORN: Born direction 2 (ligand Born grid at the receptor atoms).  Default: all.
+ * BD_TERM_REV_BORN: Born direction 2 (ligand Born grid at the receptor atoms);
+ * BD_TERM_CONTACT: WCA contact forces (bd_set_contact).  Default: all.
  * The surrogate is trained on BD_TERM_FARFIELD | BD_TERM_REV_BORN.  The stepper always
  * sums every term (or the surrogate's share, see bd_sim_set_surrogate). */
-enum { BD_TERM_GRID = 1, BD_TERM_FARFIELD = 2, BD_TERM_REV_BORN = 4, BD_TERM_ALL = 7 };
+enum { BD_TERM_GRID = 1, BD_TERM_FARFIELD = 2, BD_TERM_REV_BORN = 4, BD_TERM_CONTACT = 8, BD_TERM_ALL = 15 };
 int bd_set_terms(BdHandle* h, int terms);
 
 /* ---- Surrogate MLP ensemble -------------------------------------------------------------------

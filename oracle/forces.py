@@ -10,6 +10,7 @@ function follows one piece of pystarc/forces/gpu_batch_engine.py:
 * ``eval_batch``       -- ``_eval_batch`` (:289-391)
 * ``yukawa_forces``    -- ``_yukawa_forces_gpu`` (:393-472)
 * ``born_reverse``     -- ``_eval_born_reverse`` (:607-657)
+* ``wca_forces``       -- ``_wca_forces_gpu`` and its activation radius (:233-246, :474-529)
 * ``OracleForceEngine.__call__`` -- ``GPUBatchForceEngine.__call__`` (:531-605)
 
 Beyond the reference, ``OracleForceEngine`` can also return the torque about the
@@ -314,6 +315,49 @@ def born_reverse(R, centroids, rec_pos, rec_q, lig_born_grid, alpha, chunk_skip=
     return out, -np.einsum("nij,nj->ni", R, f_lig_tot)
 
 
+WCA_EPSILON = 0.17  # kBT, gpu_batch_engine.py:239
+WCA_CUTOFF = 1.122462  # in units of sigma, gpu_batch_engine.py:512
+
+
+def wca_activation(rec_radii, lig_radii):
+    """Centroid distance below which the contact term is evaluated (gpu_batch_engine.py:241-242)."""
+    return (float(np.max(rec_radii)) + float(np.max(lig_radii))) * 2.5
+
+
+def wca_forces(lig_positions, centroids, rec_pos, rec_radii, lig_radii, eps=WCA_EPSILON, activation=None):
+    """WCA contact forces on the ligand atoms (gpu_batch_engine.py:474-529).
+
+    Every (ligand, receptor) atom pair with sigma = r_lig + r_rec and
+    r = sqrt(max(r^2, 1e-6)) < 1.122462 sigma contributes
+    eps (12 (sigma/r)^12 - 6 (sigma/r)^6) / r^2 * (x_lig - x_rec) / r, with the
+    unclamped r^2 as divisor.  Trajectories whose centroid is at or beyond the
+    activation radius get zero.  Returns per-ligand-atom forces (N, A, 3) and
+    their totals (N, 3).
+    """
+    lig_positions = np.asarray(lig_positions, dtype=np.float64)
+    N, A, _ = lig_positions.shape
+    rec_pos = np.asarray(rec_pos, dtype=np.float64)
+    rr = np.asarray(rec_radii, dtype=np.float64)
+    rl = np.asarray(lig_radii, dtype=np.float64)
+    act = wca_activation(rr, rl) if activation is None else float(activation)
+    f_atoms = np.zeros((N, A, 3))
+    active = np.linalg.norm(np.asarray(centroids, dtype=np.float64), axis=1) < act
+    sig = rl[:, None] + rr[None, :]
+    for n in np.flatnonzero(active):
+        diff = lig_positions[n][:, None, :] - rec_pos[None, :, :]
+        r2 = (diff * diff).sum(axis=2)
+        r = np.sqrt(np.maximum(r2, 1e-6))
+        in_range = r < WCA_CUTOFF * sig
+        sr = sig / r
+        sr2 = sr * sr
+        sr6 = sr2 * sr2 * sr2
+        sr12 = sr6 * sr6
+        with np.errstate(divide="ignore", invalid="ignore"):
+            f_mag = np.where(in_range, eps * (12.0 * sr12 - 6.0 * sr6) / r2, 0.0)
+        f_atoms[n] = (f_mag[:, :, None] * diff / r[:, :, None]).sum(axis=1)
+    return f_atoms, f_atoms.sum(axis=1)
+
+
 # --------------------------------------------------------------------------
 # Engine
 # --------------------------------------------------------------------------
@@ -329,7 +373,8 @@ class OracleForceEngine:
     """
 
     def __init__(self, elec_grids, born_grids, alpha=0.07957747, farfield: FarField | None = None,
-                 lig_born_grids=None, rec_positions=None, rec_charges=None, born_chunk_skip=True):
+                 lig_born_grids=None, rec_positions=None, rec_charges=None, born_chunk_skip=True,
+                 rec_radii=None, lig_radii=None, use_lj=False):
         self.alpha = float(alpha)
         self.ff = farfield
         self.elec = sort_finest_first(list(elec_grids or []))
@@ -346,11 +391,15 @@ class OracleForceEngine:
             self.rec_pos = np.asarray(rec_positions, dtype=np.float64)
             self.rec_q = np.asarray(rec_charges, dtype=np.float64)
         self.born_chunk_skip = born_chunk_skip
+        self.wca = None  # (receptor positions, receptor radii, ligand radii): gpu_batch_engine.py:233-246
+        if use_lj and rec_radii is not None and lig_radii is not None:
+            self.wca = (np.asarray(rec_positions, dtype=np.float64), np.asarray(rec_radii, dtype=np.float64),
+                        np.asarray(lig_radii, dtype=np.float64))
 
     def atoms(self, lig_positions, lig_charges, R_matrices=None, centroids=None):
         """Per-atom terms and totals: (direct ligand forces (N,A,3), energies (N,A), receptor
         reverse-Born forces (N,Nr,3) or None, net force (N,3), energy (N,)).  The totals are
-        summed in the reference's order: elec, Born direction 1, Born direction 2 (:556-596)."""
+        summed in the reference's order: elec, Born direction 1, Born direction 2, WCA contact (:556-602)."""
         N, A, _ = lig_positions.shape
         f = np.zeros((N, A, 3))
         e = np.zeros((N, A))
@@ -381,6 +430,10 @@ class OracleForceEngine:
             f_rec, f2_tot = born_reverse(np.asarray(R_matrices), np.asarray(centroids), self.rec_pos, self.rec_q,
                                          self.lig_born[0], self.alpha, self.born_chunk_skip)
             forces += f2_tot
+        if self.wca is not None:
+            fw, tw = wca_forces(lig_positions, centroids, *self.wca)
+            f += fw
+            forces += tw
         return f, e, f_rec, forces, energies
 
     def __call__(self, lig_positions, lig_charges, R_matrices=None, centroids=None, torque_mode="zero",

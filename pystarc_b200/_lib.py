@@ -21,7 +21,7 @@ CTR_NAMES = ("started", "reacted", "escaped", "max_steps", "steps", "returns", "
 N_CTR = len(CTR_NAMES)
 LAYOUT_STAGE_RECEPTOR, LAYOUT_WINDOWS_1, LAYOUT_WINDOWS_2 = 1, 2, 4
 LAYOUT_DEFAULT = LAYOUT_WINDOWS_1
-TERM_GRID, TERM_FARFIELD, TERM_REV_BORN, TERM_ALL = 1, 2, 4, 7
+TERM_GRID, TERM_FARFIELD, TERM_REV_BORN, TERM_CONTACT, TERM_ALL = 1, 2, 4, 8, 15
 
 _ERR_NAMES = {BD_ERR_ARG: "bad argument", BD_ERR_CUDA: "CUDA error", BD_ERR_OOM: "out of device memory",
               BD_ERR_NAN: "non-finite value", BD_ERR_STALL: "device watchdog", BD_ERR_STATE: "call out of order"}
@@ -86,6 +86,7 @@ SIGNATURES = {
     "bd_last_error": (C.c_int, [P, C.c_char_p, C.c_int]),
     "bd_set_ligand": (C.c_int, [P, C.c_int, dp, dp]),
     "bd_set_receptor": (C.c_int, [P, C.c_int, dp, dp]),
+    "bd_set_contact": (C.c_int, [P, C.c_int, dp, C.c_int, dp, C.c_double, C.c_double]),
     "bd_add_grid": (C.c_int, [P, C.c_int, fp, C.c_int, C.c_int, C.c_int, dp, dp]),
     "bd_clear_grids": (C.c_int, [P]),
     "bd_set_force_params": (C.c_int, [P, C.POINTER(BdForceParams)]),

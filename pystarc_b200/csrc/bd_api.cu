@@ -45,6 +45,8 @@ struct BdHandle {
   // host-side inputs
   std::vector<double> lig;  // x,y,z,q
   std::vector<double> rec;  // x,y,z,q
+  std::vector<double> rec_rad, lig_rad;  // WCA contact radii (empty: term off)
+  double wca_eps = 0.0, wca_act = -1.0;
   std::vector<GridHost> grids[3];
   BdForceParams fp{};
   bool fp_set = false;
@@ -321,7 +323,31 @@ int finalize(BdHandle* h) {
     S.chunks_f = (const float4*)p;
     S.rec_in_smem = (h->layout & BD_LAYOUT_STAGE_RECEPTOR) &&
                     (size_t)(S.n_rec_pad + nc) * sizeof(float4) <= BD_STAGE_MAX_BYTES;
+    // WCA radii in the same order; padding entries never come within a cutoff
+    if (!h->rec_rad.empty()) {
+      if (h->rec_rad.size() != (size_t)nr || h->lig_rad.size() != (size_t)nl)
+        return fail(h, BD_ERR_ARG, "contact radii (%zu receptor, %zu ligand) do not match the atoms (%d, %d)",
+                    h->rec_rad.size(), h->lig_rad.size(), nr, nl);
+      std::vector<double> rd((size_t)nc * BD_CHUNK, -1e300);
+      for (int j = 0; j < nr; ++j) rd[j] = h->rec_rad[order[j]];
+      rc = dev_alloc(h, h->sys_allocs, &p, rd.size() * sizeof(double));
+      if (rc) return rc;
+      CK(h, cudaMemcpy(p, rd.data(), rd.size() * sizeof(double), cudaMemcpyHostToDevice));
+      S.rec_rad = (const double*)p;
+      rc = dev_alloc(h, h->sys_allocs, &p, h->lig_rad.size() * sizeof(double));
+      if (rc) return rc;
+      CK(h, cudaMemcpy(p, h->lig_rad.data(), h->lig_rad.size() * sizeof(double), cudaMemcpyHostToDevice));
+      S.lig_rad = (const double*)p;
+      const double mr = *std::max_element(h->rec_rad.begin(), h->rec_rad.end()),
+                   ml = *std::max_element(h->lig_rad.begin(), h->lig_rad.end());
+      S.wca = 1;
+      S.wca_eps = h->wca_eps;
+      // activation radius 2.5 x the largest sigma (gpu_batch_engine.py:241-242)
+      S.wca_act = h->wca_act >= 0 ? h->wca_act : (mr + ml) * 2.5;
+      S.wca_cut = std::max(0.0, kWcaCut * (mr + ml)) * (1 + 1e-12);
+    }
   }
+  if (!h->rec_rad.empty() && nr == 0) return fail(h, BD_ERR_ARG, "contact forces need the receptor atoms");
   // Born direction 2 needs the ligand Born grid, receptor atoms and alpha > 1e-12 (gpu_batch_engine.py:583-590)
   if (!lb.empty() && nr > 0 && fp.alpha > 1e-12) {
     const float* p;
@@ -683,6 +709,28 @@ int bd_sim_surrogate_counters(BdHandle* h, uint64_t* out) {
   if (!h->sur || !h->sur_buf.ctr || !h->sur_cap) return BD_OK;
   CK(h, cudaDeviceSynchronize());
   CK(h, cudaMemcpy(out, h->sur_buf.ctr, 2 * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+  return BD_OK;
+}
+
+int bd_set_contact(BdHandle* h, int n_rec, const double* rec_radii, int n_lig, const double* lig_radii, double eps,
+                   double activation) {
+  if (!h) return BD_ERR_ARG;
+  if (n_rec < 0 || n_lig < 0 || (n_rec > 0 && (!rec_radii || !lig_radii || n_lig == 0)))
+    return fail(h, BD_ERR_ARG, "bd_set_contact: bad arguments");
+  if (!std::isfinite(eps) || !std::isfinite(activation)) return fail(h, BD_ERR_NAN, "contact eps/activation not finite");
+  h->rec_rad.clear();
+  h->lig_rad.clear();
+  if (n_rec > 0) {
+    h->rec_rad.assign(rec_radii, rec_radii + n_rec);
+    h->lig_rad.assign(lig_radii, lig_radii + n_lig);
+    for (double r : h->rec_rad)
+      if (!std::isfinite(r)) return fail(h, BD_ERR_NAN, "receptor radius is not finite");
+    for (double r : h->lig_rad)
+      if (!std::isfinite(r)) return fail(h, BD_ERR_NAN, "ligand radius is not finite");
+  }
+  h->wca_eps = eps;
+  h->wca_act = activation;
+  h->dirty = true;
   return BD_OK;
 }
 

@@ -75,6 +75,11 @@ struct DevSystem {
   double V_factor, inv_debye, inv_fpe;
   double dip[3], quad[9];
   double alpha;
+  // WCA contact term (wca = 0: off): epsilon, centroid activation radius, largest pair cutoff
+  int wca;
+  double wca_eps, wca_act, wca_cut;
+  const double* rec_rad;  // n_rec_pad, receptor table order (padding -1e300: never within a cutoff)
+  const double* lig_rad;  // n_lig
   // reaction pairs (flattened)
   int n_pairs, n_needed;
   double rx_rec[BD_MAX_PAIRS][3];

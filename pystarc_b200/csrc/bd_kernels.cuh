@@ -248,17 +248,85 @@ __device__ __forceinline__ void warp_reverse_born(const DevSystem& S, const doub
   r[2] += (double)rs2;
 }
 
+template <int G>
+__device__ __forceinline__ double gmax(double v, unsigned m) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(m, v, o, G));
+  return v;
+}
+
+constexpr double kWcaCut = 1.122462;  // the WCA cutoff in units of sigma (2^(1/6) to 7 digits)
+
+// WCA contact forces of one pose (gpu_batch_engine.py:474-529): every ligand atom
+// against every receptor atom, charged or not, with sigma = r_lig + r_rec and
+// force eps (12 (sigma/r)^12 - 6 (sigma/r)^6) / r^2 along (x_lig - x_rec) / r for
+// r < 1.122462 sigma, where r = sqrt(max(r^2, 1e-6)) and the r^2 divisor is the
+// unclamped one, as the reference computes them.  Only receptor chunks whose
+// bounding spheres come within the largest pair cutoff of the ligand's bounding
+// sphere about c are read.  Lanes own ligand atoms and read each hit chunk's
+// receptor atoms together (same address on every lane).  Adds this lane's share
+// of the force, and of the torque about c, to f / t.
+template <int G, bool TORQUE, class PosFn>
+__device__ void group_contact(const DevSystem& S, const double c[3], int lane, unsigned gm, const PosFn& pos,
+                              double f[3], double t[3]) {
+  const int nl = S.n_lig;
+  double ext2 = 0;
+  for (int i = lane; i < nl; i += G) {
+    double ro[3], x[3];
+    pos(i, S.lig[i], ro, x);
+    ext2 = fmax(ext2, ro[0] * ro[0] + ro[1] * ro[1] + ro[2] * ro[2]);
+  }
+  if constexpr (G > 1) ext2 = gmax<G>(ext2, gm);
+  const double reach = sqrt(ext2) * (1 + 1e-12) + S.wca_cut + 1e-6;
+  for (int k0 = 0; k0 < S.n_chunks; k0 += G) {
+    unsigned hits = chunk_hits<G>(S, RecView{nullptr, nullptr}, c, reach, k0, lane, gm);
+    while (hits) {
+      const int k = k0 + __ffs(hits) - 1;
+      hits &= hits - 1;
+      const double4* ra = S.rec + (size_t)k * BD_CHUNK;
+      const double* rr = S.rec_rad + (size_t)k * BD_CHUNK;
+      for (int i = lane; i < nl; i += G) {
+        double ro[3], x[3];
+        pos(i, S.lig[i], ro, x);
+        const double rl = S.lig_rad[i];
+        double g0 = 0, g1 = 0, g2 = 0;
+        for (int a = 0; a < BD_CHUNK; ++a) {
+          const double4 at = ra[a];
+          const double d0 = x[0] - at.x, d1 = x[1] - at.y, d2 = x[2] - at.z;
+          const double r2 = d0 * d0 + d1 * d1 + d2 * d2;
+          const double r = sqrt(fmax(r2, 1e-6));
+          const double sig = rl + rr[a];
+          if (!(r < kWcaCut * sig)) continue;
+          const double sr = sig / r, sr2 = sr * sr, sr6 = sr2 * sr2 * sr2, sr12 = sr6 * sr6;
+          const double fm = S.wca_eps * (12.0 * sr12 - 6.0 * sr6) / r2;
+          g0 += fm * d0 / r;
+          g1 += fm * d1 / r;
+          g2 += fm * d2 / r;
+        }
+        f[0] += g0;
+        f[1] += g1;
+        f[2] += g2;
+        if (TORQUE) {
+          t[0] += ro[1] * g2 - ro[2] * g1;
+          t[1] += ro[2] * g0 - ro[0] * g2;
+          t[2] += ro[0] * g1 - ro[1] * g0;
+        }
+      }
+    }
+  }
+}
+
 // Net force, torque (about c) and energy on the ligand of one trajectory,
 // computed cooperatively by the G lanes of a group.  Follows
 // GPUBatchForceEngine.__call__ (pystarc/forces/gpu_batch_engine.py:531-605):
 // elec grid (finest containing grid) or Yukawa multipole far-field, Born
 // direction 1 on the receptor Born grid, Born direction 2 on the ligand Born
-// grid at the receptor atoms with the force negated.  Every lane returns the
-// same totals.
+// grid at the receptor atoms with the force negated, and the WCA contact forces
+// when they are on.  Every lane returns the same totals.
 template <typename FT, int G, bool TORQUE, bool ENERGY, class PosFn>
 __device__ void group_forces(const DevSystem& S, const double c[3], const double R[9], int lane, unsigned gm,
                              const PosFn& pos, double F[3], double T[3], double& E, Counts& cnt,
-                             const RecView& v = RecView{nullptr, nullptr}, unsigned terms = 7u) {
+                             const RecView& v = RecView{nullptr, nullptr}, unsigned terms = 15u) {
   double f0 = 0, f1 = 0, f2 = 0, t0 = 0, t1 = 0, t2 = 0, e = 0;
   const bool t_grid = terms & 1u, t_ff = terms & 2u, t_rev = terms & 4u;
   unsigned ng = 0, nf = 0, nr = 0;
@@ -323,6 +391,17 @@ __device__ void group_forces(const DevSystem& S, const double c[3], const double
       t1 += ro[2] * (double)fa0 - ro[0] * (double)fa2;
       t2 += ro[0] * (double)fa1 - ro[1] * (double)fa0;
     }
+  }
+  // WCA contact forces, for centroids within the activation radius (gpu_batch_engine.py:488-490)
+  if ((terms & 8u) && S.wca && norm3(c[0], c[1], c[2]) < S.wca_act) {
+    double wf[3] = {f0, f1, f2}, wt[3] = {t0, t1, t2};
+    group_contact<G, TORQUE>(S, c, lane, gm, pos, wf, wt);
+    f0 = wf[0];
+    f1 = wf[1];
+    f2 = wf[2];
+    t0 = wt[0];
+    t1 = wt[1];
+    t2 = wt[2];
   }
   // Born direction 2: ligand Born grid at the receptor atoms, in the ligand frame.
   // Lanes test G receptor chunks at a time against the box's circumsphere, then

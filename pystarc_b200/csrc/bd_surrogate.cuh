@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(256, 2) sur_begin_kernel(DevSystem S, DevSim P
     const bool need = run && st == ST_RUNNING;
     const bool trusted = need && r >= Q.r_min && r <= Q.r_max;
     double F[3] = {0, 0, 0}, T[3] = {0, 0, 0};
-    warp_forces_terms<FT, TORQUE>(S, tr.c, R, need, trusted ? (unsigned)1 : 7u, F, T, lane, tl.cnt);
+    warp_forces_terms<FT, TORQUE>(S, tr.c, R, need, trusted ? 9u : 15u, F, T, lane, tl.cnt);
     if (run && st != ST_RUNNING) {
       tr.status = st;
       record_end(P, tr, st, tl);

@@ -6,6 +6,9 @@ and :531-605; the attributes the reference stepper reads (``_debye``,
 ``_born_grids_gpu``, ``alpha``) exist with the same meaning.  The arithmetic
 runs in ``libpystarc_b200.so`` on the GPU; there is no CPU path.
 
+``use_lj`` with ``rec_radii`` / ``lig_radii`` adds the WCA contact forces
+(gpu_batch_engine.py:474-529) to every force evaluation, the stepper's included.
+
 Beyond the reference: ``precision`` ("fp64" or "mixed": FP32 force arithmetic
 with FP64 geometry and sums) and ``torque_mode`` ("zero", the reference GPU
 path's placeholder, or "centroid": torque about the ligand centroid argument).
@@ -67,8 +70,6 @@ class B200ForceEngine:
                  debye_length: float = 7.858, sdie: float = 78.0, lig_born_grids=None, rec_positions=None,
                  rec_charges=None, multipole_expansion=None, rec_radii=None, lig_radii=None, use_lj=False, *,
                  precision: str = "fp64", torque_mode: str = "zero", device: int = 0, layout=None):
-        if use_lj:
-            raise NotImplementedError("WCA contact forces (use_lj=True) are not implemented by this engine")
         if precision not in PRECISIONS or torque_mode not in TORQUES:
             raise ValueError(f"precision in {list(PRECISIONS)}, torque_mode in {list(TORQUES)}")
         self.alpha = float(alpha)
@@ -108,6 +109,23 @@ class B200ForceEngine:
                 self._lig_born_grids_gpu = [self._grid_info(g) for g in lb]
                 for g in lb:
                     self._add(_lib.GRID_LIG_BORN, g)
+        # WCA contact forces from the atom radii (gpu_batch_engine.py:233-246): on when use_lj and both
+        # radii are given; every receptor atom, charged or not, takes part
+        self._use_lj = bool(use_lj)
+        self._rec_radii_gpu = None
+        self._lig_radii_gpu = None
+        if use_lj and rec_radii is not None and lig_radii is not None:
+            if self.rec_positions is None:
+                raise ValueError("use_lj needs rec_positions and rec_charges")
+            self._rec_radii_gpu = np.ascontiguousarray(rec_radii, dtype=np.float64).reshape(-1)
+            self._lig_radii_gpu = np.ascontiguousarray(lig_radii, dtype=np.float64).reshape(-1)
+            if self._rec_radii_gpu.shape[0] != self.rec_positions.shape[0]:
+                raise ValueError("rec_radii does not match rec_positions")
+            self._lj_epsilon = 0.17
+            self._lj_activation = float(self._rec_radii_gpu.max() + self._lig_radii_gpu.max()) * 2.5
+            self.handle.call("bd_set_contact", len(self._rec_radii_gpu), _lib.ptr(self._rec_radii_gpu),
+                             len(self._lig_radii_gpu), _lib.ptr(self._lig_radii_gpu), self._lj_epsilon,
+                             self._lj_activation)
         fp = _lib.BdForceParams()
         fp.receptor_charge = self._rec_charge
         fp.debye_length = self._debye

@@ -65,7 +65,7 @@ def ref_molecules(mod, s):
     return mk("receptor", s.rec_pos, s.rec_q, s.rec_r), mk("ligand", s.lig_pos, s.lig_q, s.lig_r)
 
 
-def make_engine(ref, s, multipole=True):
+def make_engine(ref, s, multipole=True, use_lj=False):
     from pystarc.forces.gpu_batch_engine import GPUBatchForceEngine
     from pystarc.forces.multipole_farfield import MultipoleExpansion
     from pystarc.forces.electrostatic.grid_force import DXGrid
@@ -77,7 +77,8 @@ def make_engine(ref, s, multipole=True):
             born_grids=[ref_grid(DXGrid, g) for g in s.born_grids], alpha=s.alpha,
             receptor_charge=float(np.sum(s.rec_q)), debye_length=s.debye, sdie=s.sdie,
             lig_born_grids=[ref_grid(DXGrid, g) for g in s.lig_born_grids] or None,
-            rec_positions=s.rec_pos, rec_charges=s.rec_q, multipole_expansion=mp)
+            rec_positions=s.rec_pos, rec_charges=s.rec_q, multipole_expansion=mp,
+            rec_radii=s.rec_r if use_lj else None, lig_radii=s.lig_r if use_lj else None, use_lj=use_lj)
     return eng
 
 
@@ -127,6 +128,25 @@ def gen_engine(out, name, s, n_poses, rmin, rmax, seed):
     out[name] = dict(digest=system_digest(s), centroids=c, quats=q, R=R, positions=pos, F=F, T=T, E=E,
                      V_factor=eng._V_factor, has_yukawa=eng._has_yukawa, n_elec=len(eng._elec_grids_gpu),
                      n_born=len(eng._born_grids_gpu), n_lig_born=len(eng._lig_born_grids_gpu))
+
+
+def gen_engine_wca(out, name, s, n_poses, rmin, rmax, seed):
+    """The engine with WCA contact forces on (use_lj=True), at centroids around the activation
+    radius: the totals and the contact term alone (``_wca_forces_gpu``)."""
+    from pystarc.simulation.gpu_batch_simulator import GPUBatchSimulator
+
+    eng = make_engine(None, s, use_lj=True)
+    rng = np.random.default_rng(seed)
+    c, q = random_poses(n_poses, rmin, rmax, rng)
+    sim = GPUBatchSimulator.__new__(GPUBatchSimulator)
+    R = sim._quats_to_rotmats(q)
+    body = s.lig_pos - s.lig_pos.mean(axis=0)
+    pos = np.einsum("nij,kj->nki", R, body) + c[:, None, :]
+    with quiet():
+        F, T, E = eng(pos, s.lig_q.astype(np.float64), R_matrices=R, centroids=c)
+        F_wca = eng._wca_forces_gpu(pos, c)
+    out[name] = dict(digest=system_digest(s), centroids=c, quats=q, R=R, positions=pos, F=F, T=T, E=E, F_wca=F_wca,
+                     activation=eng._lj_activation, epsilon=eng._lj_epsilon)
 
 
 def gen_physics(out):
@@ -229,6 +249,7 @@ def two_sphere_example():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--only", nargs="*", help="regenerate only these fixtures (the manifest keeps the others)")
     args = ap.parse_args()
     sys.path.insert(0, str(REPO / "oracle" / "cupy_standin"))
     sys.path.insert(0, str(REPO))
@@ -236,20 +257,28 @@ def main():
     from pystarc_b200 import synth
 
     out = {}
-    gen_k1(out)
-    gen_physics(out)
     c2 = synth.config2(scale=0.3)
     c3 = synth.config3(scale=0.25)
-    gen_engine(out, "engine_c2", c2, 96, 3.0, 40.0, 21)
-    gen_engine(out, "engine_c3", c3, 64, 4.0, 40.0, 22)
-    gen_run(out, "run_two_sphere", two_sphere_example(), 2000, 11111113, 1_000_000)
-    gen_run(out, "run_c2", c2, 160, 424242, 400)
-    gen_run(out, "run_c3", c3, 64, 515151, 150)
-    meta = {}
+    jobs = {
+        "k1": lambda: gen_k1(out),
+        "physics": lambda: gen_physics(out),
+        "engine_c2": lambda: gen_engine(out, "engine_c2", c2, 96, 3.0, 40.0, 21),
+        "engine_c3": lambda: gen_engine(out, "engine_c3", c3, 64, 4.0, 40.0, 22),
+        "engine_wca_c2": lambda: gen_engine_wca(out, "engine_wca_c2", c2, 64, 5.0, 11.0, 23),
+        "engine_wca_c3": lambda: gen_engine_wca(out, "engine_wca_c3", c3, 48, 5.0, 11.0, 24),
+        "run_two_sphere": lambda: gen_run(out, "run_two_sphere", two_sphere_example(), 2000, 11111113, 1_000_000),
+        "run_c2": lambda: gen_run(out, "run_c2", c2, 160, 424242, 400),
+        "run_c3": lambda: gen_run(out, "run_c3", c3, 64, 515151, 150),
+    }
+    for k, job in jobs.items():
+        if not args.only or k in args.only:
+            job()
+    manifest = HERE / "MANIFEST.json"
+    meta = json.loads(manifest.read_text()) if args.only and manifest.exists() else {}
     for k, v in out.items():
         np.savez_compressed(HERE / f"{k}.npz", **{kk: np.asarray(vv) for kk, vv in v.items()})
         meta[k] = sorted(v.keys())
-    (HERE / "MANIFEST.json").write_text(json.dumps(meta, indent=1, sort_keys=True) + "\n")
+    manifest.write_text(json.dumps(meta, indent=1, sort_keys=True) + "\n")
     print("wrote", ", ".join(sorted(out)))
 
 

@@ -57,7 +57,7 @@ def system(name):
     return _CACHE[name]
 
 
-def oracle_engine(s, multipole=True, born_chunk_skip=True):
+def oracle_engine(s, multipole=True, born_chunk_skip=True, use_lj=False):
     if multipole and s.multipole:
         dip, quad = multipole_moments(s.rec_pos, s.rec_q)
         ff = FarField(float(np.sum(s.rec_q)), s.debye, s.sdie, dip, quad, 4.0 * np.pi * (s.sdie * 0.000142))
@@ -66,7 +66,7 @@ def oracle_engine(s, multipole=True, born_chunk_skip=True):
     return OracleForceEngine([OracleGrid.from_dx(g) for g in s.elec_grids],
                              [OracleGrid.from_dx(g) for g in s.born_grids], s.alpha, ff,
                              [OracleGrid.from_dx(g) for g in s.lig_born_grids] or None, s.rec_pos, s.rec_q,
-                             born_chunk_skip=born_chunk_skip)
+                             born_chunk_skip=born_chunk_skip, rec_radii=s.rec_r, lig_radii=s.lig_r, use_lj=use_lj)
 
 
 def step_system(s, engine=None):

@@ -18,11 +18,12 @@ class _MP:
         self.dipole, self.quadrupole, self.four_pi_eps = s.multipole_moments()
 
 
-def make_engine(s, precision="fp64", torque="zero", layout=None):
+def make_engine(s, precision="fp64", torque="zero", layout=None, use_lj=False):
     from pystarc_b200.engine import B200ForceEngine
 
+    lj = dict(rec_radii=s.rec_r, lig_radii=s.lig_r, use_lj=True) if use_lj else {}
     eng = B200ForceEngine(**s.engine_kwargs(), multipole_expansion=_MP(s) if s.multipole else None,
-                          precision=precision, torque_mode=torque, layout=layout)
+                          precision=precision, torque_mode=torque, layout=layout, **lj)
     eng.set_ligand(s.lig_pos - s.lig_pos.mean(axis=0), s.lig_q)
     return eng
 
@@ -178,3 +179,86 @@ def test_force_terms_add_up(sysname):
     F2, _, _ = eng.eval_poses(c, q)
     np.testing.assert_array_equal(F2, F)
     eng.close()
+
+
+# ---- WCA contact forces (use_lj=True) ---------------------------------------------------------
+
+@pytest.mark.parametrize("name,sysname", [("engine_wca_c2", "c2"), ("engine_wca_c3", "c3")])
+@pytest.mark.parametrize("path", ["atoms", "poses"])
+@pytest.mark.parametrize("precision,tol", [("fp64", FP64_TOL), ("mixed", MIXED_TOL)])
+def test_contact_forces_match_reference_outputs(name, sysname, path, precision, tol):
+    from oracle.forces import wca_forces
+    from pystarc_b200 import _lib
+
+    g = golden(name)
+    s = system(sysname)
+    assert system_digest(s) == str(g["digest"])
+    eng = make_engine(s, precision, use_lj=True)
+    assert eng._lj_activation == float(g["activation"]) and eng._lj_epsilon == float(g["epsilon"])
+    if path == "atoms":
+        F, T, E = eng(g["positions"], s.lig_q, g["R"], g["centroids"])
+    else:
+        F, T, E = eng.eval_poses(g["centroids"], g["quats"])
+    _, _, _, scale = oracle_engine(s, use_lj=True)(g["positions"], s.lig_q, g["R"], g["centroids"],
+                                                    return_scale=True)
+    err = force_error(F, g["F"], scale)
+    assert err.max() < tol, err.max()
+    assert np.all(T == 0)
+    # the contact term alone, against the reference's _wca_forces_gpu
+    Fw, _, Ew = eng.eval_poses(g["centroids"], g["quats"], terms=_lib.TERM_CONTACT)
+    fa, _ = wca_forces(g["positions"], g["centroids"], s.rec_pos, s.rec_r, s.lig_r)
+    werr = force_error(Fw, g["F_wca"], np.linalg.norm(fa, axis=2).sum(axis=1))
+    assert werr.max() < FP64_TOL, werr.max()
+    inactive = np.linalg.norm(g["centroids"], axis=1) >= eng._lj_activation
+    assert np.all(Fw[inactive] == 0) and np.all(Ew == 0)
+    eng.close()
+
+
+@pytest.mark.parametrize("sysname", ["c2", "c3"])
+@pytest.mark.parametrize("precision,tol", [("fp64", FP64_TOL), ("mixed", MIXED_TOL)])
+@pytest.mark.parametrize("group", [None, 1, 8])
+def test_contact_random_poses_against_oracle(sysname, precision, tol, group):
+    """Poses from deep overlap to beyond the activation radius, with the torque about the centroid."""
+    s = system(sysname)
+    eng = make_engine(s, precision, "centroid", use_lj=True)
+    if group is not None:
+        eng.handle.call("bd_set_launch", group, 64)
+    c, q = random_poses(600, 0.5, 1.3 * eng._lj_activation, 29)
+    F, T, E = eng.eval_poses(c, q)
+    R = rotmats(q)
+    body = s.lig_pos - s.lig_pos.mean(axis=0)
+    pos = np.einsum("nij,kj->nki", R, body) + c[:, None, :]
+    o = oracle_engine(s, born_chunk_skip=False, use_lj=True)
+    Fo, To, Eo, scale = o(pos, s.lig_q, R, c, torque_mode="centroid", return_scale=True)
+    err = force_error(F, Fo, scale)
+    assert err.max() < tol, (err.max(), np.percentile(err, 99))
+    lever = np.max(np.linalg.norm(body, axis=1)) + 1e-12
+    terr = force_error(T, To, scale * lever)
+    assert terr.max() < tol, terr.max()
+    eng.close()
+
+
+def test_contact_term_adds_up_and_is_off_without_radii():
+    from pystarc_b200 import _lib
+
+    s = system("c2")
+    eng = make_engine(s, "fp64", "centroid", use_lj=True)
+    c, q = random_poses(800, 0.5, 14.0, 31)
+    F, T, E = eng.eval_poses(c, q)
+    parts = [eng.eval_poses(c, q, terms=t)
+             for t in (_lib.TERM_GRID, _lib.TERM_FARFIELD, _lib.TERM_REV_BORN, _lib.TERM_CONTACT)]
+    np.testing.assert_allclose(sum(p[0] for p in parts), F, rtol=1e-9, atol=1e-12 * np.abs(F).max())
+    np.testing.assert_allclose(sum(p[1] for p in parts), T, rtol=1e-9, atol=1e-12 * np.abs(T).max())
+    assert np.any(parts[3][0] != 0)
+    plain = make_engine(s, "fp64", "centroid")
+    F0, T0, E0 = plain.eval_poses(c, q)
+    np.testing.assert_allclose(F0, F - parts[3][0], rtol=1e-9, atol=1e-12 * np.abs(F).max())
+    np.testing.assert_array_equal(E0, E)
+    # use_lj without radii evaluates no contact term (gpu_batch_engine.py:233-236)
+    from pystarc_b200.engine import B200ForceEngine
+
+    e2 = B200ForceEngine(**s.engine_kwargs(), multipole_expansion=_MP(s), torque_mode="centroid", use_lj=True)
+    e2.set_ligand(s.lig_pos - s.lig_pos.mean(axis=0), s.lig_q)
+    np.testing.assert_array_equal(e2.eval_poses(c, q)[0], F0)
+    for e in (eng, plain, e2):
+        e.close()

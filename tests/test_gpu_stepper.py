@@ -14,20 +14,21 @@ class _MP:
         self.dipole, self.quadrupole, self.four_pi_eps = s.multipole_moments()
 
 
-def make_sim(s, n_traj, max_steps, precision="fp64", torque="zero", seed=None, layout=None, **kw):
+def make_sim(s, n_traj, max_steps, precision="fp64", torque="zero", seed=None, layout=None, use_lj=False, **kw):
     from pystarc_b200.engine import B200ForceEngine
     from pystarc_b200.simulator import B200BatchSimulator
 
+    lj = dict(rec_radii=s.rec_r, lig_radii=s.lig_r, use_lj=True) if use_lj else {}
     eng = B200ForceEngine(**s.engine_kwargs(), multipole_expansion=_MP(s) if s.multipole else None,
-                          precision=precision, torque_mode=torque, layout=layout)
+                          precision=precision, torque_mode=torque, layout=layout, **lj)
     mol1, mol2 = s.molecules()
     kw.setdefault("termination", "complete")
     return B200BatchSimulator(mol1, mol2, s.mobility(), s.pathway_set(),
                               s.params(n_traj=n_traj, max_steps=max_steps, seed=seed), eng, **kw)
 
 
-def oracle_keyed(s, n_traj, max_steps, torque="zero", seed=None):
-    eng = oracle_engine(s, born_chunk_skip=False)
+def oracle_keyed(s, n_traj, max_steps, torque="zero", seed=None, use_lj=False):
+    eng = oracle_engine(s, born_chunk_skip=False, use_lj=use_lj)
     fn = (lambda *a, **k: eng(*a, torque_mode="centroid", **k)) if torque == "centroid" else eng
     return ost.run(step_system(s, fn), step_params(s, n_traj, seed or s.seed, max_steps), noise="philox",
                    termination="complete")
@@ -49,6 +50,26 @@ def test_fp64_trajectories_match_oracle_exactly(sysname, n, max_steps, torque):
     assert res.total_steps == o.total_steps
     assert sim._return_prob == o.return_prob and sim._k_b == o.k_b
     assert res.n_reacted == o.n_reacted and res.n_escaped == o.n_escaped
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_contact_forces_in_the_stepper(precision):
+    """use_lj=True: the stepper's forces include the WCA term, trajectory for trajectory as the oracle's."""
+    s = system("c2")
+    n, max_steps = 96, 300
+    sim = make_sim(s, n, max_steps, precision, use_lj=True, steps_per_launch=16, launches_per_poll=4)
+    sim.run()
+    st, steps, rets = sim.outcomes()
+    o = oracle_keyed(s, n, max_steps, use_lj=True)
+    plain = oracle_keyed(s, n, max_steps)
+    moved = (o.status != plain.status) | (o.n_steps != plain.n_steps)
+    assert moved.any()  # the contact term changes some fates at these sizes
+    same = (st == o.status) & (steps == o.n_steps)
+    if precision == "fp64":
+        assert same.all(), np.flatnonzero(~same)
+        np.testing.assert_array_equal(rets, o.n_returns)
+    else:
+        assert same.mean() >= 0.9, same.mean()
 
 
 @pytest.mark.parametrize("sysname,n,max_steps,torque", CASES[1:])

@@ -53,6 +53,44 @@ def test_engine_matches_reference(name, sysname):
     assert np.isclose(eng.ff.V_factor, float(g["V_factor"]), rtol=1e-15)
 
 
+@pytest.mark.parametrize("name,sysname", [("engine_wca_c2", "c2"), ("engine_wca_c3", "c3")])
+def test_contact_forces_match_reference(name, sysname):
+    """WCA contact forces (use_lj=True): the totals and the contact term alone, at centroids on both
+    sides of the activation radius."""
+    from oracle.forces import WCA_EPSILON, wca_activation, wca_forces
+
+    g = golden(name)
+    s = system(sysname)
+    assert system_digest(s) == str(g["digest"])
+    assert wca_activation(s.rec_r, s.lig_r) == float(g["activation"]) and WCA_EPSILON == float(g["epsilon"])
+    fa, fw = wca_forces(g["positions"], g["centroids"], s.rec_pos, s.rec_r, s.lig_r)
+    scale = np.linalg.norm(fa, axis=2).sum(axis=1)
+    np.testing.assert_allclose(fw, g["F_wca"], rtol=1e-12, atol=1e-14 * scale.max())
+    inactive = np.linalg.norm(g["centroids"], axis=1) >= float(g["activation"])
+    assert inactive.any() and (~inactive).any()
+    assert np.all(g["F_wca"][inactive] == 0) and np.all(fw[inactive] == 0)
+    eng = oracle_engine(s, use_lj=True)
+    F, T, E = eng(g["positions"], s.lig_q, R_matrices=g["R"], centroids=g["centroids"])
+    np.testing.assert_allclose(F, g["F"], rtol=1e-11, atol=1e-13 * np.abs(g["F"]).max())
+    np.testing.assert_allclose(E, g["E"], rtol=1e-11, atol=1e-12 * np.abs(g["E"]).max())
+    assert np.all(T == 0) and np.all(g["T"] == 0)
+
+
+def test_contact_force_cutoff_and_sign():
+    """One receptor and one ligand atom on the x axis: repulsive below 1.122462 sigma, zero from it on."""
+    from oracle.forces import wca_forces
+
+    sig = 3.0
+    for x, nonzero in ((2.5, True), (3.0, True), (3.3673, True), (3.3674, False), (4.0, False)):
+        pos = np.array([[[x, 0.0, 0.0]]])
+        fa, fw = wca_forces(pos, np.zeros((1, 3)), np.zeros((1, 3)), [1.0], [2.0], activation=10.0)
+        assert (fw[0, 0] > 0) == nonzero and fw[0, 1] == 0 and fw[0, 2] == 0, (x, fw)
+    # beyond the activation radius nothing is evaluated
+    fa, fw = wca_forces(np.array([[[2.5, 0, 0]]]), np.array([[10.0, 0, 0]]), np.zeros((1, 3)), [1.0], [2.0],
+                        activation=10.0)
+    assert np.all(fw == 0)
+
+
 def test_torque_centroid_is_consistent():
     s = system("c2")
     g = golden("engine_c2")
