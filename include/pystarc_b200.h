@@ -67,6 +67,8 @@ typedef struct {
   int32_t slots;             /* live-slot capacity; 0 = automatic */
   int64_t id_offset;         /* global id of local trajectory 0 (keys the noise; shards across GPUs) */
   int32_t stats;             /* 1: collect the per-step statistics read by bd_sim_stats */
+  double min_core_rxn_dt;    /* state-machine mode: floor of the reaction-surface dt refinement
+                              * (params.minimum_core_reaction_dt, gpu_batch_simulator.py:636) */
 } BdSimParams;
 
 /* Host arrays filled by bd_sim_stats (NULL members are skipped).  Per trajectory
@@ -107,6 +109,16 @@ int bd_set_ligand(BdHandle* h, int n, const double* body_xyz, const double* char
  * rec_positions / rec_charges and the stepper's overlap table (gpu_batch_engine.py:207-217,
  * gpu_batch_simulator.py:771-781). */
 int bd_set_receptor(BdHandle* h, int n, const double* xyz, const double* charges);
+/* State-machine reactions (gpu_batch_simulator.py:216-319): reaction p is reaction pair p of
+ * bd_set_reactions (one pair per reaction) and fires only while the trajectory is in state
+ * state_before[p]; it then moves to state_after[p], and the trajectory has reacted when that
+ * state is terminal (terminal[k] != 0: no reaction leaves state k).  States are 0..n_states-1,
+ * 0 the first state; -1 stands for an unlabelled state and is looked up in `terminal` from the
+ * end, as the reference's arrays index.  The lowest-numbered reaction that can fire wins, in the
+ * discrete test (:818-854) and in the Brownian bridge (:1185-1234); near a reachable reaction
+ * surface dt is refined (:1005-1060).  n_pairs = 0 returns to the flattened-pairs mode. */
+int bd_set_reaction_states(BdHandle* h, int n_pairs, const int32_t* state_before, const int32_t* state_after,
+                           int n_states, const uint8_t* terminal);
 /* WCA contact forces (the repulsive part of Lennard-Jones) between every ligand and receptor
  * atom, from their radii: sigma = r_lig + r_rec, force eps (12 (sigma/r)^12 - 6 (sigma/r)^6) / r^2
  * along the pair for r < 1.122462 sigma, only for poses whose centroid is within `activation`
@@ -160,6 +172,14 @@ int bd_sim_live(BdHandle* h, int32_t* n_live);
 /* Checkpoint: host copies of the live slots (cap entries each; c: 3*cap, q: 4*cap, SoA)
  * plus counters and outcomes are enough to resume exactly (bd_sim_restore). */
 int bd_sim_capacity(BdHandle* h, int32_t* cap);
+/* State-machine mode: the per-reaction fire counts since bd_sim_reset, by the discrete test
+ * (discrete[n]) and by the Brownian bridge (bridge[n]); replaces the reference's
+ * _sm_rxn_fire_counts_discrete / _bridge (gpu_batch_simulator.py:531-541). */
+int bd_sim_reaction_fires(BdHandle* h, uint64_t* discrete, uint64_t* bridge, int n);
+/* State-machine state of each live slot (cap entries, slot order of bd_sim_snapshot), read
+ * after bd_sim_snapshot and written after bd_sim_restore. */
+int bd_sim_get_states(BdHandle* h, int8_t* state);
+int bd_sim_set_states(BdHandle* h, const int8_t* state);
 int bd_sim_snapshot(BdHandle* h, double* c, double* q, int32_t* traj, int32_t* steps, int32_t* rets,
                     int8_t* status, int32_t* n_live, uint64_t* counters);
 int bd_sim_restore(BdHandle* h, const double* c, const double* q, const int32_t* traj, const int32_t* steps,
@@ -197,7 +217,7 @@ int bd_get_layout(BdHandle* h, int* flags);
  * allocating device memory, for callers that cannot call cudaMalloc at that point: an
  * application whose allocator already holds the GPU's memory, a process under a memory
  * quota, or code running while another library captures a CUDA graph.  The live-slot
- * pool, live counts and counters use a fixed file-scope device array of 9.1 MB, enough for
+ * pool, live counts and counters use a fixed file-scope device array of 9.2 MB, enough for
  * BD_NOALLOC_MAX_SLOTS live slots; p->slots above that is rejected with BD_ERR_ARG
  * (0 = use the maximum).  Outputs are DEVICE arrays the caller owns: out_status,
  * out_steps, out_returns (p->n_traj each, as bd_sim_outcomes) and counters (BD_CTR_NUM).

@@ -1,20 +1,21 @@
 """FP64 NumPy restatement of the reference's batched BD step loop (test infrastructure).
 
 Follows ``GPUBatchSimulator.run`` (pystarc/simulation/gpu_batch_simulator.py:462-1594)
-in its flattened-pairs mode, one vectorised operation per reference operation and
+in its flattened-pairs and state-machine modes, one vectorised operation per reference operation and
 in the same order, so that with ``noise="pcg64"`` it consumes NumPy's PCG64
 stream exactly as the reference does and reproduces its tallies bit for bit:
 
   start poses                       :509-513, :1597-1609
-  discrete reaction test            :856-878, :1737-1751
+  discrete reaction test            :818-878, :1690-1751
   escape / return at r_esc          :879-911
   forces                            :929-943  (the force engine is a callable)
   old pair distances                :950-960
-  adaptive dt                       :961-1067 (without the state-machine term)
+  adaptive dt                       :961-1067 (state-machine refinement :1005-1060)
   HI D(r)                           :741-751, :1074-1084
   translation, rotation             :1085-1101, :1631-1660
   overlap rejection                 :1102-1128
-  Brownian bridge                   :637-671, :1142-1252
+  Brownian bridge                   :637-671, :1142-1252 (state machine :1170-1234)
+  state-machine tables              :216-319, :523-545
   counters, termination             :1253-1254, :1341-1356, :1485-1489
 
 With ``noise="philox"`` every draw is keyed by (trajectory, its own step index)
@@ -54,6 +55,11 @@ class StepSystem:
     q_rec_total: float
     q_lig_total: float
     debye: float  # engine._debye
+    # state-machine reactions (None: flattened pairs): per reaction pair its source and
+    # destination state index, and per state whether no reaction leaves it (sm_tables)
+    sm_before: np.ndarray | None = None
+    sm_after: np.ndarray | None = None
+    sm_terminal: np.ndarray | None = None
 
 
 @dataclass
@@ -70,6 +76,7 @@ class StepParams:
     kT_scale: float = 1.0
     return_prob: float | None = None
     k_b: float | None = None
+    min_core_rxn_dt: float = 0.0  # params.minimum_core_reaction_dt (:636)
 
 
 @dataclass
@@ -86,6 +93,38 @@ class StepResult:
     n_returns: np.ndarray = field(default=None)
     n_overlap_rejected: int = 0
     stats: "StepStats" = None
+    state: np.ndarray = field(default=None)  # state-machine state of every trajectory at the end
+    sm_fires_discrete: np.ndarray = field(default=None)  # per reaction
+    sm_fires_bridge: np.ndarray = field(default=None)
+
+
+def sm_tables(state_before, state_after, first_state=None):
+    """State indices of the state-machine reactions (gpu_batch_simulator.py:262-299).
+
+    The first state (``first_state``, else the first reaction's source) gets index
+    0; every other label gets the next index the first time it is met, in the order
+    source, destination of each reaction; an unlabelled state is -1.  A state is
+    terminal when no reaction has it as its source.  Returns (before, after, terminal).
+    """
+    index = {}
+
+    def idx(label):
+        if label is None:
+            return -1
+        if label not in index:
+            index[label] = len(index)
+        return index[label]
+
+    fs = first_state if first_state is not None else (state_before[0] if state_before else None)
+    if fs is not None:
+        idx(fs)
+    before, after = [], []
+    for b, a in zip(state_before, state_after):
+        before.append(idx(b))
+        after.append(idx(a))
+    sources = set(before)
+    terminal = np.array([k not in sources for k in range(len(index))], dtype=bool)
+    return np.array(before, dtype=np.int64), np.array(after, dtype=np.int64), terminal
 
 
 def n_needed_of(n_needed_raw, n_pairs):
@@ -160,8 +199,9 @@ def hi_constants(r_h_rec, r_h_lig):
     return Df, pi8, a2, ainv
 
 
-def adaptive_dt(r_sr, sys: StepSystem, prm: StepParams):
-    """Per-trajectory dt (gpu_batch_simulator.py:961-1067, no state-machine term)."""
+def adaptive_dt(r_sr, sys: StepSystem, prm: StepParams, rxn_coord=None):
+    """Per-trajectory dt (gpu_batch_simulator.py:961-1067).  ``rxn_coord`` (state-machine mode):
+    per trajectory, the distance above the nearest reaction surface reachable from its state."""
     D_t = sys.D_t
     r_b, r_esc = prm.r_b, prm.r_esc
     adt_debye = float(sys.debye)
@@ -185,6 +225,13 @@ def adaptive_dt(r_sr, sys: StepSystem, prm: StepParams):
     dt_outer = np.minimum(np.minimum(dt_force, dt_edge), dt_pair)
     dt_inner = np.minimum(dt_force, dt_pair)
     dt_arr = np.where(in_outer, dt_outer, dt_inner)
+    if rxn_coord is not None:
+        # reaction-surface refinement: 12 sigma must stay below the reaction coordinate (:1034-1060)
+        sigma_now = np.sqrt(2.0 * D_t * dt_arr)
+        needs = 12.0 * sigma_now > rxn_coord
+        crit = rxn_coord * rxn_coord / (288.0 * D_t)
+        floored = np.maximum(crit, prm.min_core_rxn_dt) if prm.min_core_rxn_dt > 0 else crit
+        dt_arr = np.where(needs, np.minimum(dt_arr, floored), dt_arr)
     if prm.max_dt > 0:
         dt_arr = np.minimum(dt_arr, np.full_like(dt_arr, prm.max_dt))
     if prm.min_core_dt > 0:
@@ -350,6 +397,16 @@ def run(sys: StepSystem, prm: StepParams, noise: str = "pcg64", termination: str
     cutoffs = np.asarray(sys.rxn_cutoff, dtype=np.float64)
     n_needed = sys.n_needed
     D_eff = bridge_D_eff(sys)
+    sm = sys.sm_before is not None and have_pairs
+    state = np.zeros(N, dtype=np.int64)
+    fires_d = np.zeros(P, dtype=np.int64)
+    fires_b = np.zeros(P, dtype=np.int64)
+    if sm:
+        before = np.asarray(sys.sm_before, dtype=np.int64)
+        after = np.asarray(sys.sm_after, dtype=np.int64)
+        terminal = np.asarray(sys.sm_terminal, dtype=bool)
+        # bridge draws of state-machine mode come from their own stream (:473-479)
+        rng_bb = None if keyed else np.random.default_rng(int(prm.seed) + 1)
     loop_steps = 0
     max_loop = prm.max_steps if termination == "reference" else 1 << 62
     stats = StepStats(pos, q, N, r_b, r_esc, P)
@@ -366,14 +423,31 @@ def run(sys: StepSystem, prm: StepParams, noise: str = "pcg64", termination: str
         pos_run = pos[run_idx]
         q_run = q[run_idx]
         R = rotmats(q_run)
-        if have_pairs:
+        still_running_mask = status[run_idx] == 0
+        if sm:
+            # lowest-numbered reaction from the current state within its cutoff (:818-852, :1690-1735)
             gho_pos = np.einsum("nij,kj->nki", R, gho_body) + pos_run[:, None, :]
             d = np.linalg.norm(gho_pos - rec_gho[None, :, :], axis=2)
-            reacted = (d < cutoffs[None, :]).sum(axis=1) >= n_needed
+            fire = (d < cutoffs[None, :]) & (state[run_idx][:, None] == before[None, :])
+            reacted = fire.any(axis=1)
+            fidx = np.argmax(fire, axis=1)
+            fm = reacted & still_running_mask
+            newly = run_idx[:0]
+            if np.any(fm):
+                fg = run_idx[fm]
+                fr = fidx[fm]
+                ns = after[fr]
+                state[fg] = ns
+                np.add.at(fires_d, fr, 1)
+                newly = fg[terminal[ns]]
         else:
-            reacted = np.zeros(len(run_idx), dtype=bool)
-        still_running_mask = status[run_idx] == 0
-        newly = run_idx[reacted & still_running_mask]
+            if have_pairs:
+                gho_pos = np.einsum("nij,kj->nki", R, gho_body) + pos_run[:, None, :]
+                d = np.linalg.norm(gho_pos - rec_gho[None, :, :], axis=2)
+                reacted = (d < cutoffs[None, :]).sum(axis=1) >= n_needed
+            else:
+                reacted = np.zeros(len(run_idx), dtype=bool)
+            newly = run_idx[reacted & still_running_mask]
         status[newly] = 1
         stats.encounter(newly, pos, q, n_steps, bridge=False)
         r_mag = np.linalg.norm(pos_run, axis=1)
@@ -420,7 +494,12 @@ def run(sys: StepSystem, prm: StepParams, noise: str = "pcg64", termination: str
             lig_old = np.einsum("nij,kj->nki", R_sr, gho_body) + cen_sr[:, None, :]
             old_d = np.linalg.norm(lig_old - rec_gho[None, :, :], axis=2)
         r_sr = r_mag[sr_mask]
-        dt_arr = adaptive_dt(r_sr, sys, prm)
+        rxn_coord = None
+        if sm:
+            reach = state[sr_idx][:, None] == before[None, :]
+            coord = np.maximum(old_d - cutoffs[None, :], np.zeros_like(old_d))
+            rxn_coord = np.min(np.where(reach, coord, 1.0e30), axis=1)
+        dt_arr = adaptive_dt(r_sr, sys, prm, rxn_coord)
         D_arr = hi_diffusion(r_sr, sys, prm)
         if keyed:
             xi_t, xi_r = draws.step_normals(n_steps[sr_idx], sr_idx)
@@ -464,15 +543,33 @@ def run(sys: StepSystem, prm: StepParams, noise: str = "pcg64", termination: str
                 p_cross = np.where(both, p_cross, np.zeros_like(p_cross))
                 if keyed:
                     u_bb = draws.bridge_uniforms(n_steps[sr_idx], sr_idx, P)
+                elif sm:
+                    u_bb = rng_bb.random(p_cross.shape)
                 else:
                     u_bb = rng.random(p_cross.shape)
                 fired = (u_bb < p_cross) | (new_d < cutoffs[None, :])
-                bb = fired.sum(axis=1) >= n_needed
-                if np.any(bb):
-                    g = sr_idx[bb]
-                    g = g[status[g] == 0]
-                    status[g] = 1
-                    stats.encounter(g, pos, q, n_steps, bridge=True)
+                if sm:
+                    fm = fired & (state[sr_idx][:, None] == before[None, :])
+                    anyf = fm.any(axis=1)
+                    if np.any(anyf):
+                        fidx = np.argmax(fm, axis=1)
+                        proceed = anyf & (status[sr_idx] == 0)
+                        if np.any(proceed):
+                            g = sr_idx[proceed]
+                            fr = fidx[proceed]
+                            ns = after[fr]
+                            state[g] = ns
+                            np.add.at(fires_b, fr, 1)
+                            gt = g[terminal[ns]]
+                            status[gt] = 1
+                            stats.encounter(gt, pos, q, n_steps, bridge=True)
+                else:
+                    bb = fired.sum(axis=1) >= n_needed
+                    if np.any(bb):
+                        g = sr_idx[bb]
+                        g = g[status[g] == 0]
+                        status[g] = 1
+                        stats.encounter(g, pos, q, n_steps, bridge=True)
         stats.step(sr_idx, pos, q, n_steps, dt_arr, old_d, cutoffs)
         n_steps[sr_idx] += 1
         total_steps += int(sr_mask.sum())
@@ -492,4 +589,5 @@ def run(sys: StepSystem, prm: StepParams, noise: str = "pcg64", termination: str
     return StepResult(status=status, n_steps=n_steps, n_reacted=int((status == 1).sum()),
                       n_escaped=int((status == 2).sum()), n_max_steps=n_max, total_steps=total_steps,
                       loop_steps=loop_steps, return_prob=rp, k_b=kb, n_returns=n_returns,
-                      n_overlap_rejected=n_overlap, stats=stats)
+                      n_overlap_rejected=n_overlap, stats=stats, state=state, sm_fires_discrete=fires_d,
+                      sm_fires_bridge=fires_b)

@@ -46,6 +46,9 @@ struct BdHandle {
   std::vector<double> lig;  // x,y,z,q
   std::vector<double> rec;  // x,y,z,q
   std::vector<double> rec_rad, lig_rad;  // WCA contact radii (empty: term off)
+  int sm_n = 0, sm_states = 0;  // state-machine reactions (bd_set_reaction_states; 0: off)
+  int sm_before[BD_MAX_PAIRS] = {}, sm_after[BD_MAX_PAIRS] = {};
+  unsigned long long sm_terminal = 0;
   double wca_eps = 0.0, wca_act = -1.0;
   std::vector<GridHost> grids[3];
   BdForceParams fp{};
@@ -372,6 +375,18 @@ int finalize(BdHandle* h) {
     }
     S.rx_cut[p] = h->rx_cut[p];
     S.rx_deff[p] = h->rx_deff[p];
+  }
+  if (h->sm_n > 0) {
+    if (h->sm_n != h->n_pairs)
+      return fail(h, BD_ERR_ARG, "state-machine reactions: %d reactions but %d reaction pairs (one pair each)",
+                  h->sm_n, h->n_pairs);
+    S.sm = 1;
+    S.n_states = h->sm_states;
+    S.terminal = h->sm_terminal;
+    for (int p = 0; p < h->sm_n; ++p) {
+      S.rx_before[p] = h->sm_before[p];
+      S.rx_after[p] = h->sm_after[p];
+    }
   }
   CK(h, cudaDeviceSynchronize());  // window copies are built on the legacy stream
   S.terms = h->terms;
@@ -712,6 +727,28 @@ int bd_sim_surrogate_counters(BdHandle* h, uint64_t* out) {
   return BD_OK;
 }
 
+int bd_set_reaction_states(BdHandle* h, int n_pairs, const int32_t* state_before, const int32_t* state_after,
+                           int n_states, const uint8_t* terminal) {
+  if (!h) return BD_ERR_ARG;
+  if (n_pairs < 0 || n_pairs > BD_MAX_PAIRS) return fail(h, BD_ERR_ARG, "n_pairs must be in [0, %d]", BD_MAX_PAIRS);
+  if (n_pairs > 0 && (!state_before || !state_after || !terminal || n_states < 1 || n_states > 64))
+    return fail(h, BD_ERR_ARG, "bd_set_reaction_states: bad arguments (1 <= n_states <= 64)");
+  unsigned long long term = 0;
+  for (int p = 0; p < n_pairs; ++p) {
+    if (state_before[p] < -1 || state_before[p] >= n_states || state_after[p] < -1 || state_after[p] >= n_states)
+      return fail(h, BD_ERR_ARG, "reaction %d: state index out of [-1, %d)", p, n_states);
+    h->sm_before[p] = state_before[p];
+    h->sm_after[p] = state_after[p];
+  }
+  for (int k = 0; k < n_states && n_pairs > 0; ++k)
+    if (terminal[k]) term |= 1ull << k;
+  h->sm_n = n_pairs;
+  h->sm_states = n_pairs > 0 ? n_states : 0;
+  h->sm_terminal = term;
+  h->dirty = true;
+  return BD_OK;
+}
+
 int bd_set_contact(BdHandle* h, int n_rec, const double* rec_radii, int n_lig, const double* lig_radii, double eps,
                    double activation) {
   if (!h) return BD_ERR_ARG;
@@ -804,6 +841,8 @@ int bd_sim_configure(BdHandle* h, const BdSimParams* p) {
     B.rets = (int*)q;
     if ((rc = dev_alloc(h, h->sim_allocs, &q, (size_t)C))) return rc;
     B.status = (int8_t*)q;
+    if ((rc = dev_alloc(h, h->sim_allocs, &q, (size_t)C))) return rc;
+    B.state = (int8_t*)q;
     B.cap = C;
   }
   void* q;
@@ -823,6 +862,7 @@ int bd_sim_configure(BdHandle* h, const BdSimParams* p) {
   P.max_steps = p->max_steps;
   P.max_dt = p->max_dt;
   P.min_core_dt = p->min_core_dt;
+  P.min_core_rxn_dt = p->min_core_rxn_dt;
   P.use_hi = p->use_hi;
   P.overlap = p->overlap && h->S.n_chunks > 0;
   P.D_t = p->D_t;
@@ -1151,6 +1191,38 @@ int bd_sim_capacity(BdHandle* h, int32_t* cap) {
   return BD_OK;
 }
 
+int bd_sim_reaction_fires(BdHandle* h, uint64_t* discrete, uint64_t* bridge, int n) {
+  if (!h || n < 0 || n > BD_MAX_PAIRS || (n > 0 && (!discrete || !bridge)))
+    return fail(h, BD_ERR_ARG, "bd_sim_reaction_fires: bad arguments");
+  if (!h->sim_ready) return fail(h, BD_ERR_STATE, "no simulation configured");
+  CK(h, cudaDeviceSynchronize());
+  unsigned long long ctr[C_NUM];
+  CK(h, cudaMemcpy(ctr, h->d_ctr, sizeof ctr, cudaMemcpyDeviceToHost));
+  for (int p = 0; p < n; ++p) {
+    discrete[p] = ctr[C_SM_DISCRETE + p];
+    bridge[p] = ctr[C_SM_BRIDGE + p];
+  }
+  return BD_OK;
+}
+
+int bd_sim_get_states(BdHandle* h, int8_t* state) {
+  if (!h || !state) return fail(h, BD_ERR_ARG, "bd_sim_get_states: NULL");
+  if (!h->sim_ready) return fail(h, BD_ERR_STATE, "no simulation configured");
+  CK(h, cudaDeviceSynchronize());
+  const SlotBuf& B = h->buf[h->cur];
+  CK(h, cudaMemcpy(state, B.state, (size_t)B.cap, cudaMemcpyDeviceToHost));
+  return BD_OK;
+}
+
+int bd_sim_set_states(BdHandle* h, const int8_t* state) {
+  if (!h || !state) return fail(h, BD_ERR_ARG, "bd_sim_set_states: NULL");
+  if (!h->sim_ready) return fail(h, BD_ERR_STATE, "no simulation configured");
+  CK(h, cudaDeviceSynchronize());
+  const SlotBuf& B = h->buf[h->cur];
+  CK(h, cudaMemcpy(B.state, state, (size_t)B.cap, cudaMemcpyHostToDevice));
+  return BD_OK;
+}
+
 int bd_sim_snapshot(BdHandle* h, double* c, double* q, int32_t* traj, int32_t* steps, int32_t* rets, int8_t* status,
                     int32_t* n_live, uint64_t* counters) {
   if (!h || !c || !q || !traj || !steps || !rets || !status || !n_live || !counters)
@@ -1260,6 +1332,7 @@ int bd_internal_run_noalloc(BdHandle* h, const BdSimParams* p, unsigned char* sc
     B[b].steps = (int*)carve(cur_p, (size_t)C * sizeof(int));
     B[b].rets = (int*)carve(cur_p, (size_t)C * sizeof(int));
     B[b].status = (int8_t*)carve(cur_p, (size_t)C);
+    B[b].state = (int8_t*)carve(cur_p, (size_t)C);
     B[b].cap = C;
   }
   int* live = (int*)carve(cur_p, 2 * sizeof(int));
@@ -1276,6 +1349,7 @@ int bd_internal_run_noalloc(BdHandle* h, const BdSimParams* p, unsigned char* sc
   P.max_steps = p->max_steps;
   P.max_dt = p->max_dt;
   P.min_core_dt = p->min_core_dt;
+  P.min_core_rxn_dt = p->min_core_rxn_dt;
   P.use_hi = p->use_hi;
   P.overlap = p->overlap && h->S.n_chunks > 0;
   P.D_t = p->D_t;
@@ -1507,6 +1581,8 @@ int bd_multi_create(BdHandle* const* handles, int n, BdMulti** out) {
     B.rets = (int*)p;
     if ((rc = malloc_multi(m, &p, (size_t)cap))) return bail(rc);
     B.status = (int8_t*)p;
+    if ((rc = malloc_multi(m, &p, (size_t)cap))) return bail(rc);
+    B.state = (int8_t*)p;
     B.cap = (int)cap;
   }
   if ((rc = malloc_multi(m, &p, 2 * sizeof(int)))) return bail(rc);

@@ -35,7 +35,9 @@ enum : int {
   C_NONFINITE,      // steps that produced a non-finite pose (trajectory stopped)
   C_SLOT_CURSOR,    // dynamic slot cursor of the current launch
   C_LIVE_NEXT,      // live-slot count being built by the compaction
-  C_NUM
+  C_SM_DISCRETE,    // BD_MAX_PAIRS counters: state-machine reactions fired by the discrete test
+  C_SM_BRIDGE = C_SM_DISCRETE + BD_MAX_PAIRS,  // BD_MAX_PAIRS counters: fired by the Brownian bridge
+  C_NUM = C_SM_BRIDGE + BD_MAX_PAIRS
 };
 
 struct DevGrid {
@@ -86,6 +88,10 @@ struct DevSystem {
   double rx_body[BD_MAX_PAIRS][3];
   double rx_cut[BD_MAX_PAIRS];
   double rx_deff[BD_MAX_PAIRS];
+  // state-machine reactions (sm = 1): reaction p is pair p and fires only from state rx_before[p]
+  int sm, n_states;
+  int rx_before[BD_MAX_PAIRS], rx_after[BD_MAX_PAIRS];
+  unsigned long long terminal;  // bit k: state k has no reaction leaving it
 };
 
 // Per-step statistics of the reference's stepper (gpu_batch_simulator.py:577-620,
@@ -127,7 +133,7 @@ struct DevSim {
   uint32_t k0, k1;  // seed words
   double r_b, r_esc, return_prob;
   int max_steps;
-  double max_dt, min_core_dt;
+  double max_dt, min_core_dt, min_core_rxn_dt;
   int use_hi, overlap;
   double D_t, D_r;
   double adt_V0, adt_inv_debye, adt_debye;
@@ -148,6 +154,7 @@ struct SlotBuf {
   int* steps;
   int* rets;
   int8_t* status;
+  int8_t* state;  // state-machine reaction state (0 = the first state)
   int cap;
 };
 

@@ -579,6 +579,7 @@ __global__ void __launch_bounds__(256) eval_atoms_kernel(DevSystem S, long long 
 struct Traj {
   double c[3], q[4];
   int id, steps, rets, status;
+  int state;  // state-machine reaction state
 };
 
 struct Tally {
@@ -610,6 +611,7 @@ __device__ __forceinline__ void start_trajectory(const DevSim& P, int id, Traj& 
   tr.steps = 0;
   tr.rets = 0;
   tr.status = ST_RUNNING;
+  tr.state = 0;
   if (P.stats) {
 #pragma unroll
     for (int k = 0; k < 3; ++k) P.st.start_c[3 * id + k] = tr.c[k];
@@ -618,8 +620,11 @@ __device__ __forceinline__ void start_trajectory(const DevSim& P, int id, Traj& 
   }
 }
 
-// Adaptive dt (pystarc/simulation/gpu_batch_simulator.py:961-1067, flattened-pairs mode).
-__device__ __forceinline__ double adaptive_dt(const DevSim& P, double r) {
+// Adaptive dt (pystarc/simulation/gpu_batch_simulator.py:961-1067).
+// rc >= 0: state-machine mode, rc the distance to the nearest reaction surface reachable
+// from the current state (1e30 if none): where 12 sqrt(2 D_t dt) exceeds it, dt drops to
+// rc^2 / (288 D_t), floored at min_core_rxn_dt (gpu_batch_simulator.py:1005-1060).
+__device__ __forceinline__ double adaptive_dt(const DevSim& P, double r, double rc = -1.0) {
   const double D_t = P.D_t;
   const double dt_pair = (0.1 * 0.1 / 2.0) * r * r / D_t;
   double dt_force = dt_pair;
@@ -635,6 +640,10 @@ __device__ __forceinline__ double adaptive_dt(const DevSim& P, double r) {
   const double de = fmin(dist_b, dist_esc);
   const double dt_edge = de * de / (18.0 * D_t);
   double dt = (r > 1.1 * P.r_b) ? fmin(fmin(dt_force, dt_edge), dt_pair) : fmin(dt_force, dt_pair);
+  if (rc >= 0.0 && 12.0 * sqrt(2.0 * D_t * dt) > rc) {
+    const double crit = rc * rc / (288.0 * D_t);
+    dt = fmin(dt, P.min_core_rxn_dt > 0 ? fmax(crit, P.min_core_rxn_dt) : crit);
+  }
   if (P.max_dt > 0) dt = fmin(dt, P.max_dt);
   if (P.min_core_dt > 0) dt = fmax(dt, P.min_core_dt);
   return dt;
@@ -693,19 +702,49 @@ __device__ __forceinline__ double pair_distance(const DevSystem& S, const double
   return norm3(lx, ly, lz);
 }
 
+// Terminal flag of state k; k = -1 (an unlabelled state) reads the last entry, as the
+// reference's state arrays index.
+__device__ __forceinline__ bool sm_terminal(const DevSystem& S, int k) {
+  const int i = k < 0 ? k + S.n_states : k;
+  return i >= 0 && i < 64 && ((S.terminal >> i) & 1ull);
+}
+
+// Distance above the nearest reaction surface reachable from the current state
+// (pose c, R), 1e30 if no reaction leaves it (gpu_batch_simulator.py:1018-1033).
+__device__ __forceinline__ double sm_rxn_coord(const DevSystem& S, const Traj& tr, const double R[9]) {
+  double rc = 1.0e30;
+  for (int p = 0; p < S.n_pairs; ++p)
+    if (S.rx_before[p] == tr.state) rc = fmin(rc, fmax(pair_distance(S, tr.c, R, p) - S.rx_cut[p], 0.0));
+  return rc;
+}
+
 // Discrete reaction test and escape/return at the start of a step
-// (gpu_batch_simulator.py:856-911).  Returns ST_RUNNING if the trajectory
+// (gpu_batch_simulator.py:818-911).  Returns ST_RUNNING if the trajectory
 // goes on to the force evaluation; sets R = R(q) and r = |c| of that pose.
+// State-machine mode: the lowest-numbered reaction whose source state is the
+// trajectory's and whose pair is within its cutoff fires; the trajectory moves
+// to the reaction's destination state and has reacted if that state is terminal.
+// A trajectory that fired skips the escape test of this step (:880).
 __device__ __forceinline__ int step_begin(const DevSystem& S, const DevSim& P, const Keyed& key, uint32_t s, Traj& tr,
                                           double R[9], double& r, Tally& tl) {
   quat_to_rot(tr.q, R);
-  if (S.n_pairs > 0) {
+  bool fired = false;
+  if (S.sm) {
+    for (int p = 0; p < S.n_pairs; ++p)
+      if (S.rx_before[p] == tr.state && pair_distance(S, tr.c, R, p) < S.rx_cut[p]) {
+        tr.state = S.rx_after[p];
+        atomicAdd(P.ctr + C_SM_DISCRETE + p, 1ull);
+        if (sm_terminal(S, tr.state)) return ST_REACTED;
+        fired = true;
+        break;
+      }
+  } else if (S.n_pairs > 0) {
     int nsat = 0;
     for (int p = 0; p < S.n_pairs; ++p) nsat += pair_distance(S, tr.c, R, p) < S.rx_cut[p];
     if (nsat >= S.n_needed) return ST_REACTED;
   }
   r = norm3(tr.c[0], tr.c[1], tr.c[2]);
-  if (r >= P.r_esc) {
+  if (r >= P.r_esc && !fired) {
     const W4 w = key.w(s, SUB_ESCAPE);
     if (u53(w.a, w.b) < P.return_prob) {
       tr.c[0] = tr.c[0] / r * P.r_b;
@@ -727,10 +766,10 @@ __device__ __forceinline__ int step_begin(const DevSystem& S, const DevSim& P, c
 // Adaptive dt, D(r), Ermak-McCammon translation and the body-frame rotation
 // (gpu_batch_simulator.py:961-1101).  Writes the proposed pose; false if it is not finite.
 template <typename FT>
-__device__ __forceinline__ bool step_move(const DevSim& P, const Keyed& key, uint32_t s, const Traj& tr, double r,
-                                          const double F[3], const double T[3], double cn[3], double qn[4],
-                                          double& dt) {
-  dt = adaptive_dt(P, r);
+__device__ __forceinline__ bool step_move(const DevSystem& S, const DevSim& P, const Keyed& key, uint32_t s,
+                                          const Traj& tr, const double R[9], double r, const double F[3],
+                                          const double T[3], double cn[3], double qn[4], double& dt) {
+  dt = adaptive_dt(P, r, S.sm ? sm_rxn_coord(S, tr, R) : -1.0);
   const double D = hi_diffusion<FT>(P, r);
   double xt[3], xr[3];
   {
@@ -775,7 +814,7 @@ __device__ __forceinline__ int step_end(const DevSystem& S, const DevSim& P, con
 #pragma unroll
       for (int k = 0; k < 9; ++k) Rn[k] = R[k];
     }
-    int fired = 0;
+    int fired = 0, first = -1;
     for (int p = 0; p < S.n_pairs; ++p) {
       const double d0 = pair_distance(S, c0, R, p), d1 = pair_distance(S, tr.c, Rn, p);
       const double x0 = d0 - S.rx_cut[p], x1 = d1 - S.rx_cut[p];
@@ -783,9 +822,21 @@ __device__ __forceinline__ int step_end(const DevSystem& S, const DevSim& P, con
       if (x0 > 0 && x1 > 0) pc = exp(-x0 * x1 / fmax(S.rx_deff[p] * dt, 1e-30));
       const W4 w = key.w(s, SUB_BRIDGE + (uint32_t)(p >> 1));
       const double u = (p & 1) ? u53(w.c, w.d) : u53(w.a, w.b);
-      fired += (u < pc) || (d1 < S.rx_cut[p]);
+      const bool f = (u < pc) || (d1 < S.rx_cut[p]);
+      fired += f;
+      if (f && first < 0 && S.rx_before[p] == tr.state) first = p;
     }
-    if (fired >= S.n_needed) {
+    if (S.sm) {
+      // the lowest-numbered reaction from the current state whose pair fired (:1185-1234)
+      if (first >= 0) {
+        tr.state = S.rx_after[first];
+        atomicAdd(P.ctr + C_SM_BRIDGE + first, 1ull);
+        if (sm_terminal(S, tr.state)) {
+          st = ST_REACTED;
+          tl.bridge += 1;
+        }
+      }
+    } else if (fired >= S.n_needed) {
       st = ST_REACTED;
       tl.bridge += 1;
     }
@@ -915,7 +966,7 @@ __device__ __forceinline__ int bd_step(const DevSystem& S, const DevSim& P, Traj
   double F[3], T[3], E;
   group_forces<FT, G, TORQUE, false>(S, tr.c, R, lane, gm, PosFromPose{R, tr.c}, F, T, E, tl.cnt, v);
   double cn[3], qn[4], dt;
-  if (!step_move<FT>(P, key, s, tr, r, F, T, cn, qn, dt)) {
+  if (!step_move<FT>(S, P, key, s, tr, R, r, F, T, cn, qn, dt)) {
     tl.nonfinite += 1;
     return ST_ERROR;
   }
@@ -939,6 +990,7 @@ __device__ __forceinline__ void load_slot(const SlotBuf& B, int s, Traj& tr) {
   tr.steps = B.steps[s];
   tr.rets = B.rets[s];
   tr.status = B.status[s];
+  tr.state = B.state[s];
 }
 
 __device__ __forceinline__ void store_slot(const SlotBuf& B, int s, const Traj& tr) {
@@ -951,6 +1003,7 @@ __device__ __forceinline__ void store_slot(const SlotBuf& B, int s, const Traj& 
   B.steps[s] = tr.steps;
   B.rets[s] = tr.rets;
   B.status[s] = (int8_t)tr.status;
+  B.state[s] = (int8_t)tr.state;
 }
 
 template <int G>
@@ -1150,7 +1203,7 @@ __global__ void __launch_bounds__(256, MINB) step_kernel_warp(DevSystem S, DevSi
       warp_forces<FT, TORQUE>(S, tr.c, R, need_f, F, T, lane, tl.cnt, sh.v);
       double cn[3] = {0, 0, 0}, qn[4] = {1, 0, 0, 0}, dt = 0;
       bool ok = true;
-      if (need_f) ok = step_move<FT>(P, key, s, tr, r, F, T, cn, qn, dt);
+      if (need_f) ok = step_move<FT>(S, P, key, s, tr, R, r, F, T, cn, qn, dt);
       if (need_f && !ok) {
         tl.nonfinite += 1;
         st = ST_ERROR;

@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(256, 2) step_kernel_multi(MultiTab T, SlotBuf 
       warp_forces_multi<FT, TORQUE>(T, sys, tr.c, R, need_f, F, Tq, lane, tl.cnt);
       double cn[3] = {0, 0, 0}, qn[4] = {1, 0, 0, 0}, dt = 0;
       bool ok = true;
-      if (need_f) ok = step_move<FT>(P, key, s, tr, r, F, Tq, cn, qn, dt);
+      if (need_f) ok = step_move<FT>(S, P, key, s, tr, R, r, F, Tq, cn, qn, dt);
       if (need_f && !ok) {
         tl.nonfinite += 1;
         st = ST_ERROR;

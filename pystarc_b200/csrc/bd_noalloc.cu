@@ -9,7 +9,7 @@
 // counts and the counters live in the file-scope device array below, and the
 // per-trajectory outputs and final counters go to arrays the caller owns.
 //
-// The array is a fixed 9.1 MB (room for BD_NOALLOC_MAX_SLOTS = 65536 live slots);
+// The array is a fixed 9.2 MB (room for BD_NOALLOC_MAX_SLOTS = 65536 live slots);
 // every GPU that loads the library keeps it until the process exits.  All calls
 // share it and it keeps the last call's contents, so each call clears the counters
 // it uses; two calls whose work overlaps on the GPU race on it.
@@ -25,9 +25,9 @@
 namespace {
 
 constexpr int kMaxSlots = BD_NOALLOC_MAX_SLOTS;
-// two slot buffers of 69 B per slot (each array rounded up to 256 B), two live
+// two slot buffers of 70 B per slot (each array rounded up to 256 B), two live
 // counts and the counters, with slack for the per-array alignment
-constexpr size_t kScratchBytes = 2 * (size_t)kMaxSlots * 69 + 64 * 1024;
+constexpr size_t kScratchBytes = 2 * (size_t)kMaxSlots * 70 + 64 * 1024;
 
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 

@@ -236,7 +236,7 @@ __global__ void __launch_bounds__(256, 2) sur_end_kernel(DevSystem S, DevSim P, 
     const uint32_t s = (uint32_t)tr.steps;
     double cn[3] = {0, 0, 0}, qn[4] = {1, 0, 0, 0}, dt = 0;
     bool ok = true;
-    if (need) ok = step_move<FT>(P, key, s, tr, r, F, T, cn, qn, dt);
+    if (need) ok = step_move<FT>(S, P, key, s, tr, R, r, F, T, cn, qn, dt);
     int st = tr.status;
     if (need && !ok) {
       tl.nonfinite += 1;

@@ -107,6 +107,55 @@ def flatten_pairs(pathway_set):
     return rec_idx, lig_idx, np.asarray(cut, dtype=float), n_needed
 
 
+def state_machine(pathway_set):
+    """State-machine reaction tables of ``pathway_set`` (gpu_batch_simulator.py:216-319), or None.
+
+    Active when some reaction carries a ``state_before`` label.  Each reaction with
+    pairs contributes its first pair; states are numbered in the reference's order
+    (the first state, then each reaction's source and destination as met), an
+    unlabelled state is -1, and a state is terminal when no reaction leaves it.
+    Returns a dict with the reaction names, labels, state indices and terminal flags.
+    """
+    reactions = list(pathway_set.reactions)
+    if not any(getattr(r, "state_before", None) is not None for r in reactions):
+        return None
+    names, sb, sa = [], [], []
+    for rxn in reactions:
+        if not rxn.criteria.pairs:
+            continue
+        if len(rxn.criteria.pairs) != 1:
+            raise ValueError(f"state-machine reaction {rxn.name!r} has {len(rxn.criteria.pairs)} pairs; "
+                             "each reaction needs exactly one")
+        names.append(rxn.name)
+        sb.append(getattr(rxn, "state_before", None))
+        sa.append(getattr(rxn, "state_after", None))
+    if not names:
+        return None
+    first = getattr(pathway_set, "first_state", None)
+    if first is None:
+        first = sb[0]
+    index, labels = {}, []
+
+    def idx(label):
+        if label is None:
+            return -1
+        if label not in index:
+            index[label] = len(labels)
+            labels.append(label)
+        return index[label]
+
+    if first is not None:
+        idx(first)
+    before, after = [], []
+    for b, a in zip(sb, sa):
+        before.append(idx(b))
+        after.append(idx(a))
+    sources = set(before)
+    terminal = [k not in sources for k in range(len(labels))]
+    return {"names": names, "state_before": sb, "state_after": sa, "before": before, "after": after,
+            "states": list(labels), "terminal": terminal, "first_state": first}
+
+
 class B200BatchSimulator:
     """Batched BD of all trajectories on one GPU.
 
@@ -122,8 +171,6 @@ class B200BatchSimulator:
                  stats=None, surrogate=None, verbose=False):
         if not hasattr(batch_engine, "handle"):
             raise TypeError("batch_engine must be a B200ForceEngine")
-        if any(getattr(r, "state_before", None) is not None for r in pathway_set.reactions):
-            raise NotImplementedError("state-machine reactions are not implemented by this engine")
         self.mol1, self.mol2, self.mob = mol1, mol2, mob
         self.pathway_set = pathway_set
         self.params = params
@@ -151,6 +198,9 @@ class B200BatchSimulator:
         self._rxn_lig_body = self._mol2_pos0[lig_idx].reshape(-1, 3) if lig_idx else np.zeros((0, 3))
         self._rxn_cutoffs = cut
         self._rxn_n_needed = n_needed
+        # state-machine reactions: reaction p is reaction pair p (one pair each)
+        self._sm = state_machine(pathway_set)
+        self._sm_active = self._sm is not None
         self._return_prob = 0.0
         self._k_b = 0.0
         self._qb_factor = 1.1
@@ -184,6 +234,17 @@ class B200BatchSimulator:
                    int(self._rxn_n_needed))
         else:
             h.call("bd_set_reactions", 0, None, None, None, None, 1)
+        if self._sm_active:
+            sm = self._sm
+            before = np.ascontiguousarray(sm["before"], dtype=np.int32)
+            after = np.ascontiguousarray(sm["after"], dtype=np.int32)
+            n_states = max(1, len(sm["states"]))
+            term = np.zeros(n_states, dtype=np.uint8)
+            term[:len(sm["terminal"])] = sm["terminal"]
+            h.call("bd_set_reaction_states", len(before), _lib.ptr(before, _lib.C.c_int32),
+                   _lib.ptr(after, _lib.C.c_int32), n_states, _lib.ptr(term, _lib.C.c_uint8))
+        else:
+            h.call("bd_set_reaction_states", 0, None, None, 0, None)
         sp = _lib.BdSimParams()
         sp.n_traj = int(p.n_trajectories)
         sp.seed = int(p.seed if p.seed is not None else 0) & 0xFFFFFFFFFFFFFFFF
@@ -193,6 +254,7 @@ class B200BatchSimulator:
         sp.max_steps = int(min(p.max_steps, 2 ** 31 - 1))
         sp.max_dt = float(getattr(p, "max_dt", 0.0) or 0.0)
         sp.min_core_dt = float(getattr(p, "minimum_core_dt", 0.0) or 0.0)
+        sp.min_core_rxn_dt = float(getattr(p, "minimum_core_reaction_dt", 0.0) or 0.0)
         sp.use_hi = int(self._use_hi)
         sp.overlap = int(bool(getattr(p, "_overlap_check", True)))
         sp.D_t = D_t
@@ -293,6 +355,14 @@ class B200BatchSimulator:
     def _checkpoint_path(self):
         return Path(getattr(self.params, "_work_dir", "bd_sims")) / "checkpoint_b200.npz"
 
+    def reaction_fires(self):
+        """State-machine mode: per-reaction fire counts (discrete test, Brownian bridge) since the reset."""
+        n = len(self._sm["names"]) if self._sm_active else 0
+        d = np.zeros(max(n, 1), dtype=np.uint64)
+        b = np.zeros(max(n, 1), dtype=np.uint64)
+        self.engine.handle.call("bd_sim_reaction_fires", _lib.ptr(d, _lib.C.c_uint64), _lib.ptr(b, _lib.C.c_uint64), n)
+        return d[:n].astype(np.int64), b[:n].astype(np.int64)
+
     def save_checkpoint(self, path=None):
         """Slots, counters and outcomes: enough to resume the same trajectories exactly."""
         h = self.engine.handle
@@ -308,10 +378,13 @@ class B200BatchSimulator:
         h.call("bd_sim_snapshot", _lib.ptr(c), _lib.ptr(q), _lib.ptr(traj, _lib.C.c_int32),
                _lib.ptr(steps, _lib.C.c_int32), _lib.ptr(rets, _lib.C.c_int32), _lib.ptr(status, _lib.C.c_int8),
                _lib.C.byref(live), _lib.ptr(ctr, _lib.C.c_uint64))
+        state = np.zeros(C, dtype=np.int8)
+        h.call("bd_sim_get_states", _lib.ptr(state, _lib.C.c_int8))
         o_st, o_steps, o_rets = self.outcomes()
         path = Path(path or self._checkpoint_path())
         path.parent.mkdir(parents=True, exist_ok=True)
-        np.savez_compressed(path, c=c, q=q, traj=traj, steps=steps, rets=rets, status=status, n_live=live.value,
+        np.savez_compressed(path, c=c, q=q, traj=traj, steps=steps, rets=rets, status=status, state=state,
+                            n_live=live.value,
                             counters=ctr, out_status=o_st, out_steps=o_steps, out_returns=o_rets,
                             n_traj=int(self.params.n_trajectories), seed=int(self.params.seed or 0), cap=C)
         return path
@@ -332,6 +405,8 @@ class B200BatchSimulator:
                _lib.ptr(arr["status"], _lib.C.c_int8), int(arr["n_live"]), _lib.ptr(arr["counters"], _lib.C.c_uint64),
                _lib.ptr(arr["out_status"], _lib.C.c_int8), _lib.ptr(arr["out_steps"], _lib.C.c_int32),
                _lib.ptr(arr["out_returns"], _lib.C.c_int32))
+        state = np.ascontiguousarray(arr["state"], dtype=np.int8) if "state" in arr else np.zeros(cap.value, np.int8)
+        h.call("bd_sim_set_states", _lib.ptr(state, _lib.C.c_int8))
 
     # ------------------------------------------------------------------
     def run(self, max_launches=None) -> B200BatchResult:
@@ -396,6 +471,13 @@ class B200BatchSimulator:
             outcome = status.astype(np.int32)
             outcome[(outcome != 1) & (outcome != 2)] = 0
             sim_data = {"outcome": outcome, "n_steps": steps.astype(np.int64), "n_returns": rets.astype(np.int64)}
+        if self._sm_active:
+            # per-reaction fire counts (gpu_batch_simulator.py:1571-1581)
+            d, b = self.reaction_fires()
+            sim_data["completed_reactions"] = [
+                {"name": self._sm["names"][i], "n_fired": int(d[i] + b[i]),
+                 "state_before": self._sm["state_before"][i], "state_after": self._sm["state_after"][i]}
+                for i in range(len(self._sm["names"]))]
         return B200BatchResult(n_trajectories=N, n_reacted=n_reacted, n_escaped=n_escaped, n_max_steps=n_max,
                                reaction_counts={"stage_0": n_reacted}, r_start=float(self.params.r_start),
                                r_escape=float(self.params.r_escape), dt=float(getattr(self.params, "dt", 0.2)),

@@ -188,7 +188,7 @@ def gen_physics(out):
                             pts=pts, V=np.array([mp.potential(p) for p in pts]))
 
 
-def build_sim(s, n_traj, seed, max_steps, work):
+def build_sim(s, n_traj, seed, max_steps, work, sm=None):
     from pystarc.simulation.gpu_batch_simulator import GPUBatchSimulator
     from pystarc.simulation.nam_simulator import NAMParameters
     from pystarc.hydrodynamics.rotne_prager import MobilityTensor
@@ -200,6 +200,13 @@ def build_sim(s, n_traj, seed, max_steps, work):
     mob = MobilityTensor.from_radii(s.r_hydro_rec, s.r_hydro_lig, eta=s.eta, T=s.temperature)
     pairs = [ContactPair(int(a), int(b), float(c)) for a, b, c in s.pairs]
     ps = PathwaySet([ReactionInterface("stage_0", ReactionCriteria("stage_0", pairs, n_needed=s.n_needed))])
+    if sm is not None:
+        rx = []
+        for name, before, after, (a, b, c) in sm["reactions"]:
+            crit = ReactionCriteria(name, [ContactPair(int(a), int(b), float(c))], n_needed=1, state_before=before,
+                                    state_after=after)
+            rx.append(ReactionInterface(name, crit, state_before=before, state_after=after))
+        ps = PathwaySet(rx, first_state=sm["first_state"])
     params = NAMParameters(n_trajectories=n_traj, max_steps=max_steps, r_start=s.r_start, r_escape=s.r_escape,
                            seed=seed, hydrodynamic_interactions=s.hi)
     params.max_dt = s.max_dt
@@ -208,6 +215,8 @@ def build_sim(s, n_traj, seed, max_steps, work):
     params._work_dir = str(work)
     params._kT_scale = s.temperature / 298.15
     params._overlap_check = s.overlap
+    if sm is not None:
+        params.minimum_core_reaction_dt = sm["min_core_rxn_dt"]
     eng = make_engine(None, s, multipole=s.multipole)
     with quiet():
         sim = GPUBatchSimulator(mol1, mol2, mob, ps, params, eng)
@@ -231,6 +240,37 @@ def gen_run(out, name, s, n_traj, seed, max_steps):
                          "encounter_traj", "encounter_step", "encounter_pos", "encounter_q", "near_miss_traj",
                          "near_miss_pos", "near_miss_dist", "radial_counts", "angular_counts", "milestone_flux_out",
                          "milestone_flux_in", "contact_pair_counts", "contact_total_steps", "trans_matrix")})
+
+
+# State-machine reaction sets: (name, state_before, state_after, (receptor atom, ligand atom, cutoff)).
+SM_TWO_SPHERE = {"first_state": "b_surface", "min_core_rxn_dt": 0.0,
+                 "reactions": [("b_6", "b_surface", "6", (1, 1, 6.0)), ("6_3", "6", "3", (1, 1, 3.0))]}
+SM_C2 = {"first_state": "A", "min_core_rxn_dt": 0.05,
+         "reactions": [("A_B", "A", "B", (29, 0, 15.0)), ("B_C", "B", "C", (1, 1, 14.0)), ("B_A", "B", "A", (3, 2, 12.0))]}
+
+
+def gen_run_sm(out, name, s, sm, n_traj, seed, max_steps):
+    """A reference run with state-machine reactions: outcomes, step and return counts, per-reaction
+    fire counts (discrete test and Brownian bridge) and the completed_reactions record."""
+    with tempfile.TemporaryDirectory() as work:
+        sim, mob = build_sim(s, n_traj, seed, max_steps, work, sm=sm)
+        with quiet():
+            res = sim.run()
+    sd = res.sim_data
+    rx = sm["reactions"]
+    out[name] = dict(digest=system_digest(s), n_traj=n_traj, seed=seed, max_steps=max_steps,
+                     n_reacted=res.n_reacted, n_escaped=res.n_escaped, n_max_steps=res.n_max_steps,
+                     outcome=sd["outcome"], n_steps=sd["n_steps"], n_returns=sd["n_returns"],
+                     return_prob=sim._return_prob, k_b=sim._k_b,
+                     fires_discrete=np.asarray(sim._sm_rxn_fire_counts_discrete),
+                     fires_bridge=np.asarray(sim._sm_rxn_fire_counts_bridge),
+                     n_fired=np.array([r["n_fired"] for r in sd["completed_reactions"]]),
+                     state_index_before=np.asarray(sim._sm_rxn_state_before_idx),
+                     state_index_after=np.asarray(sim._sm_rxn_state_after_idx),
+                     state_terminal=np.asarray(sim._sm_state_is_terminal),
+                     rx_names=np.array([r[0] for r in rx]), rx_before=np.array([r[1] for r in rx]),
+                     rx_after=np.array([r[2] for r in rx]), rx_pairs=np.array([r[3] for r in rx], dtype=float),
+                     first_state=sm["first_state"], min_core_rxn_dt=sm["min_core_rxn_dt"])
 
 
 def two_sphere_example():
@@ -269,6 +309,9 @@ def main():
         "run_two_sphere": lambda: gen_run(out, "run_two_sphere", two_sphere_example(), 2000, 11111113, 1_000_000),
         "run_c2": lambda: gen_run(out, "run_c2", c2, 160, 424242, 400),
         "run_c3": lambda: gen_run(out, "run_c3", c3, 64, 515151, 150),
+        "run_sm_two_sphere": lambda: gen_run_sm(out, "run_sm_two_sphere", two_sphere_example(), SM_TWO_SPHERE, 1000,
+                                                31337, 1_000_000),
+        "run_sm_c2": lambda: gen_run_sm(out, "run_sm_c2", c2, SM_C2, 160, 434343, 600),
     }
     for k, job in jobs.items():
         if not args.only or k in args.only:

@@ -85,6 +85,40 @@ def step_system(s, engine=None):
                       debye=s.debye)
 
 
+def sm_spec(g):
+    """State-machine reaction set of a golden run: names, source and destination labels, pairs, first state."""
+    pairs = [(int(a), int(b), float(c)) for a, b, c in np.asarray(g["rx_pairs"])]
+    return ([str(x) for x in g["rx_names"]], [str(x) for x in g["rx_before"]], [str(x) for x in g["rx_after"]],
+            pairs, str(g["first_state"]))
+
+
+def sm_step_system(s, g, engine=None):
+    """Oracle stepper system with the state-machine reactions of golden run ``g``."""
+    from oracle.stepper import sm_tables
+
+    names, sb, sa, pairs, first = sm_spec(g)
+    ss = step_system(s, engine)
+    P = len(pairs)
+    ss.rxn_rec_pos = np.asarray([s.rec_pos[a] for a, _, _ in pairs], dtype=float).reshape(P, 3)
+    ss.rxn_lig_idx = np.asarray([b for _, b, _ in pairs], dtype=np.int64)
+    ss.rxn_cutoff = np.asarray([c for _, _, c in pairs], dtype=float)
+    ss.n_needed = n_needed_of(1, P)
+    ss.sm_before, ss.sm_after, ss.sm_terminal = sm_tables(sb, sa, first)
+    return ss
+
+
+def sm_pathway(g):
+    """The same reaction set as a PathwaySet of labelled reactions (the drop-in's input)."""
+    from pystarc_b200 import structures as st
+
+    names, sb, sa, pairs, first = sm_spec(g)
+    rx = []
+    for name, b, a, (i, j, c) in zip(names, sb, sa, pairs):
+        crit = st.ReactionCriteria(name, [st.ContactPair(i, j, c)], n_needed=1, state_before=b, state_after=a)
+        rx.append(st.ReactionInterface(name, crit, state_before=b, state_after=a))
+    return st.PathwaySet(rx, first_state=first)
+
+
 def step_params(s, n_traj, seed, max_steps):
     return StepParams(n_traj=n_traj, seed=seed, r_b=s.r_start, r_esc=s.r_escape, max_steps=max_steps,
                       max_dt=s.max_dt, use_hi=s.hi, overlap=s.overlap, kT_scale=s.temperature / 298.15)

@@ -14,7 +14,8 @@ class _MP:
         self.dipole, self.quadrupole, self.four_pi_eps = s.multipole_moments()
 
 
-def make_sim(s, n_traj, max_steps, precision="fp64", torque="zero", seed=None, layout=None, use_lj=False, **kw):
+def make_sim(s, n_traj, max_steps, precision="fp64", torque="zero", seed=None, layout=None, use_lj=False,
+             pathway=None, min_core_rxn_dt=0.0, **kw):
     from pystarc_b200.engine import B200ForceEngine
     from pystarc_b200.simulator import B200BatchSimulator
 
@@ -23,8 +24,9 @@ def make_sim(s, n_traj, max_steps, precision="fp64", torque="zero", seed=None, l
                           precision=precision, torque_mode=torque, layout=layout, **lj)
     mol1, mol2 = s.molecules()
     kw.setdefault("termination", "complete")
-    return B200BatchSimulator(mol1, mol2, s.mobility(), s.pathway_set(),
-                              s.params(n_traj=n_traj, max_steps=max_steps, seed=seed), eng, **kw)
+    params = s.params(n_traj=n_traj, max_steps=max_steps, seed=seed)
+    params.minimum_core_reaction_dt = min_core_rxn_dt
+    return B200BatchSimulator(mol1, mol2, s.mobility(), pathway or s.pathway_set(), params, eng, **kw)
 
 
 def oracle_keyed(s, n_traj, max_steps, torque="zero", seed=None, use_lj=False):
@@ -50,6 +52,97 @@ def test_fp64_trajectories_match_oracle_exactly(sysname, n, max_steps, torque):
     assert res.total_steps == o.total_steps
     assert sim._return_prob == o.return_prob and sim._k_b == o.k_b
     assert res.n_reacted == o.n_reacted and res.n_escaped == o.n_escaped
+
+
+# The reaction-surface dt refinement shrinks dt with the squared height above the surface; with
+# no floor (minimum_core_reaction_dt = 0) that height is a difference of nearly equal distances,
+# and a 1-ulp change of any input moves about a tenth of the fates (the oracle alone shows it).
+# Exact trajectory parity is therefore tested with the floor the reference pipeline sets (0.05 ps);
+# without it the test is statistical.
+SM_CASES = [("run_sm_two_sphere", "two_sphere", 200, 100000, "zero", 0.05),
+            ("run_sm_c2", "c2", 96, 600, "centroid", 0.05)]
+
+
+def _sm_oracle(s, g, n, max_steps, torque, floor):
+    from dataclasses import replace
+
+    from tests.helpers import sm_step_system
+
+    eng = oracle_engine(s, born_chunk_skip=False)
+    fn = (lambda *a, **k: eng(*a, torque_mode="centroid", **k)) if torque == "centroid" else eng
+    prm = replace(step_params(s, n, s.seed, max_steps), min_core_rxn_dt=floor)
+    return ost.run(sm_step_system(s, g, fn), prm, noise="philox", termination="complete")
+
+
+@pytest.mark.parametrize("name,sysname,n,max_steps,torque,floor", SM_CASES)
+def test_state_machine_trajectories_match_oracle_exactly(name, sysname, n, max_steps, torque, floor):
+    """State-machine reactions (reference rxns.xml state labels): per trajectory the same fate, step and
+    return count as the oracle with the same keyed draws, and the same per-reaction fire counts."""
+    from tests.helpers import sm_pathway
+
+    g = golden(name)
+    s = system(sysname)
+    sim = make_sim(s, n, max_steps, "fp64", torque, pathway=sm_pathway(g), min_core_rxn_dt=floor,
+                   steps_per_launch=16, launches_per_poll=4)
+    res = sim.run()
+    st, steps, rets = sim.outcomes()
+    o = _sm_oracle(s, g, n, max_steps, torque, floor)
+    np.testing.assert_array_equal(st, o.status)
+    np.testing.assert_array_equal(steps, o.n_steps)
+    np.testing.assert_array_equal(rets, o.n_returns)
+    d, b = sim.reaction_fires()
+    np.testing.assert_array_equal(d, o.sm_fires_discrete)
+    np.testing.assert_array_equal(b, o.sm_fires_bridge)
+    assert ((o.sm_fires_discrete + o.sm_fires_bridge) > 0).sum() >= 2  # the test sees transitions
+    rec = res.sim_data["completed_reactions"]
+    assert [r["name"] for r in rec] == [str(x) for x in g["rx_names"]]
+    assert [r["n_fired"] for r in rec] == list(d + b)
+    assert res.n_reacted == o.n_reacted
+
+
+def test_state_machine_without_dt_floor_is_statistically_the_oracle():
+    """No reaction-surface dt floor (ill-conditioned near the surface): most fates agree and the
+    reaction probabilities' Wilson intervals overlap."""
+    from pystarc_b200.hostphys import wilson_ci
+    from tests.helpers import sm_pathway
+
+    g = golden("run_sm_two_sphere")
+    s = system("two_sphere")
+    n = 200
+    sim = make_sim(s, n, 100000, "fp64", pathway=sm_pathway(g), min_core_rxn_dt=0.0, steps_per_launch=16,
+                   launches_per_poll=4)
+    res = sim.run()
+    st, _, _ = sim.outcomes()
+    o = _sm_oracle(s, g, n, 100000, "zero", 0.0)
+    assert (st == o.status).mean() >= 0.75
+    lo_a, hi_a = wilson_ci(res.n_reacted, res.n_escaped)
+    lo_b, hi_b = wilson_ci(o.n_reacted, o.n_escaped)
+    assert lo_a <= hi_b and lo_b <= hi_a
+
+
+def test_state_machine_checkpoint_keeps_states(tmp_path):
+    """A resumed state-machine run continues every trajectory from its saved state."""
+    from tests.helpers import sm_pathway
+
+    g = golden("run_sm_c2")
+    s = system("c2")
+    kw = dict(pathway=sm_pathway(g), min_core_rxn_dt=float(g["min_core_rxn_dt"]), slots=256, steps_per_launch=8,
+              launches_per_poll=1)
+    sim = make_sim(s, 200, 600, "fp64", **kw)
+    sim._setup()
+    sim.engine.handle.call("bd_sim_reset", None)
+    sim.engine.handle.call("bd_sim_run", 40, 8, None)  # 320 steps: a few trajectories have left the first state
+    path = sim.save_checkpoint(tmp_path / "ck.npz")
+    assert np.any(np.load(path)["state"] != 0)
+    _run_to_completion(sim, 8)
+    a = sim.outcomes()
+    sim2 = make_sim(s, 200, 600, "fp64", **kw)
+    sim2._setup()
+    sim2.engine.handle.call("bd_sim_reset", None)
+    sim2.load_checkpoint(path)
+    _run_to_completion(sim2, 8)
+    for x, y in zip(a, sim2.outcomes()):
+        np.testing.assert_array_equal(x, y)
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])

@@ -205,6 +205,58 @@ def test_stepper_reproduces_reference_run_exactly(name, sysname):
     np.testing.assert_array_equal(res.status, ref_outcome)
 
 
+@pytest.mark.parametrize("name,sysname", [("run_sm_two_sphere", "two_sphere"), ("run_sm_c2", "c2")])
+def test_state_machine_run_reproduces_reference_exactly(name, sysname):
+    """State-machine reactions: state numbering, every trajectory's fate and step count, and the
+    per-reaction fire counts of the discrete test and the Brownian bridge."""
+    from dataclasses import replace
+
+    from oracle.stepper import sm_tables
+    from tests.helpers import sm_spec, sm_step_system
+
+    g = golden(name)
+    s = system(sysname)
+    assert system_digest(s) == str(g["digest"])
+    _, sb, sa, _, first = sm_spec(g)
+    before, after, terminal = sm_tables(sb, sa, first)
+    np.testing.assert_array_equal(before, g["state_index_before"])
+    np.testing.assert_array_equal(after, g["state_index_after"])
+    np.testing.assert_array_equal(terminal, g["state_terminal"])
+    ss = sm_step_system(s, g)
+    prm = replace(step_params(s, int(g["n_traj"]), int(g["seed"]), int(g["max_steps"])),
+                  min_core_rxn_dt=float(g["min_core_rxn_dt"]))
+    res = ost.run(ss, prm, noise="pcg64")
+    assert res.return_prob == float(g["return_prob"]) and res.k_b == float(g["k_b"])
+    assert (res.n_reacted, res.n_escaped, res.n_max_steps) == (int(g["n_reacted"]), int(g["n_escaped"]),
+                                                              int(g["n_max_steps"]))
+    np.testing.assert_array_equal(res.n_steps, g["n_steps"])
+    np.testing.assert_array_equal(res.n_returns, g["n_returns"])
+    ref_outcome = g["outcome"].copy()
+    ref_outcome[ref_outcome == 0] = 3
+    np.testing.assert_array_equal(res.status, ref_outcome)
+    np.testing.assert_array_equal(res.sm_fires_discrete, g["fires_discrete"])
+    np.testing.assert_array_equal(res.sm_fires_bridge, g["fires_bridge"])
+    np.testing.assert_array_equal(res.sm_fires_discrete + res.sm_fires_bridge, g["n_fired"])
+
+
+def test_state_machine_tables_of_the_drop_in():
+    """pystarc_b200.simulator.state_machine numbers states as the reference does, labels unset included."""
+    from oracle.stepper import sm_tables
+    from pystarc_b200.simulator import state_machine
+    from tests.helpers import sm_pathway, sm_spec
+
+    for name in ("run_sm_two_sphere", "run_sm_c2"):
+        g = golden(name)
+        sm = state_machine(sm_pathway(g))
+        np.testing.assert_array_equal(sm["before"], g["state_index_before"])
+        np.testing.assert_array_equal(sm["after"], g["state_index_after"])
+        np.testing.assert_array_equal(sm["terminal"], g["state_terminal"])
+        assert sm["names"] == sm_spec(g)[0]
+    # a destination without a label is -1; the first state defaults to the first reaction's source
+    b, a, t = sm_tables(["x", "y"], ["y", None])
+    assert list(b) == [0, 1] and list(a) == [1, -1] and list(t) == [False, False]
+
+
 @pytest.mark.parametrize("name,sysname", [("run_two_sphere", "two_sphere"), ("run_c2", "c2"), ("run_c3", "c3")])
 def test_stepper_statistics_match_reference(name, sysname):
     """The per-step statistics the reference collects for its output files (gpu_batch_simulator.py:1255-1317)."""
