@@ -273,6 +273,159 @@ def gen_run_sm(out, name, s, sm, n_traj, seed, max_steps):
                      first_state=sm["first_state"], min_core_rxn_dt=sm["min_core_rxn_dt"])
 
 
+PIPE_DIR = HERE / "pipeline"
+
+PIPE_INPUT = """<?xml version="1.0" encoding="UTF-8"?>
+<pystarc>
+  <receptor_pqr>rec.pqr</receptor_pqr>
+  <ligand_pqr>lig.pqr</ligand_pqr>
+  <rxns_xml>rxns_sm.xml</rxns_xml>
+  <work_dir>work</work_dir>
+  <bd_milestone_radius>12.5</bd_milestone_radius>
+  <bd_milestone_radius_inner> 4.0 </bd_milestone_radius_inner>
+  <debye_length> 9.5 </debye_length>
+  <sdie>80</sdie>
+  <desolvation_alpha></desolvation_alpha>
+  <hydrodynamic_interactions>yes</hydrodynamic_interactions>
+  <overlap_check>0</overlap_check>
+  <lj_forces>1</lj_forces>
+  <multipole_fallback>False</multipole_fallback>
+  <n_trajectories>321</n_trajectories>
+  <max_steps>4321</max_steps>
+  <seed>99</seed>
+  <r_hydro_rec>2.25</r_hydro_rec>
+  <minimum_core_reaction_dt>0.05</minimum_core_reaction_dt>
+  <state_machine_reactions>TRUE</state_machine_reactions>
+  <ghost_atoms>auto</ghost_atoms>
+  <temperature>310.0</temperature>
+  <outputs>
+    <save_interval>5</save_interval>
+    <p_commit>false</p_commit>
+    <energetics>no</energetics>
+  </outputs>
+</pystarc>
+"""
+
+PIPE_REC = """REMARK synthetic receptor: chain column, element column, a 4-letter residue
+ATOM      1  N   ALA A   1      11.104   6.134  -6.504 -0.3000 1.8240
+ATOM      2  CA  ALA A   1      11.639   6.071  -5.147  0.0337 1.9080 C
+ATOM      3  CB  NTHR    2       9.000   1.000   2.000  0.1000 1.5000
+HETATM    4  O1  LIG     3      -2.345  -7.890  10.000 -0.5000 1.6612
+ATOM      5  C   ALA A   4       1.250  -3.500   0.750  0.6500 1.7000
+END
+"""
+
+PIPE_LIG = """ATOM      1  C1  BEN     1       0.500   0.250  -0.125  0.2500 1.7000
+ATOM      2  C2  BEN     1      -0.500   1.250   0.875 -0.1250 1.7000
+ATOM      3  N1  BEN     1       1.500  -1.000   0.000  0.8750 1.5500
+"""
+
+PIPE_RXNS_FLAT = """<?xml version="1.0"?>
+<roottag>
+  <reactions>
+    <reaction>
+      <n>first</n>
+      <criterion>
+        <n_needed>2</n_needed>
+        <pair><atoms>1 2</atoms><distance>5.5</distance></pair>
+        <pair><atom1>3 -0.5 6.25</atom1><atom2>1 0.2</atom2></pair>
+      </criterion>
+    </reaction>
+    <reaction>
+      <n>second</n>
+      <criterion>
+        <pair><atom1>5</atom1><atom2>3</atom2></pair>
+        <pair><atoms>4 4</atoms><distance>3.0</distance></pair>
+      </criterion>
+    </reaction>
+  </reactions>
+</roottag>
+"""
+
+PIPE_RXNS_SM = """<?xml version="1.0"?>
+<roottag>
+  <first_state> outer </first_state>
+  <reactions>
+    <reaction>
+      <n> outer_mid </n>
+      <state_before> outer </state_before>
+      <state_after> mid </state_after>
+      <criterion><n_needed>1</n_needed><pair><atoms>6 4</atoms><distance>9.0</distance></pair></criterion>
+    </reaction>
+    <reaction>
+      <n> empty </n>
+      <state_before> mid </state_before>
+      <state_after> nowhere </state_after>
+      <criterion><n_needed>1</n_needed></criterion>
+    </reaction>
+    <reaction>
+      <n> mid_in </n>
+      <state_before> mid </state_before>
+      <state_after> inner </state_after>
+      <criterion><pair><atoms>6 4</atoms><distance>4.0</distance></pair></criterion>
+    </reaction>
+    <reaction>
+      <n> mid_back </n>
+      <state_before> mid </state_before>
+      <state_after></state_after>
+      <criterion><pair><atoms>1 1</atoms><distance>7.5</distance></pair></criterion>
+    </reaction>
+  </reactions>
+</roottag>
+"""
+
+
+def gen_pipeline(out):
+    """Input files of the pipeline tests (synthetic, written here) and what the reference's
+    input parser, PQR reader/writer, GHO injection, rxns parsers and hydrodynamic-radius cache make
+    of them."""
+    import os
+    import dataclasses
+    from pystarc.pipeline import input_parser, geometry
+    from pystarc.pipeline import prepare_bd_surface as pbs
+    from pystarc.structures.pqr_io import parse_pqr_records
+
+    PIPE_DIR.mkdir(exist_ok=True)
+    files = {"input.xml": PIPE_INPUT, "rec.pqr": PIPE_REC, "lig.pqr": PIPE_LIG, "rxns_flat.xml": PIPE_RXNS_FLAT,
+             "rxns_sm.xml": PIPE_RXNS_SM}
+    for k, v in files.items():
+        (PIPE_DIR / k).write_text(v)
+    ref = {}
+    cwd = os.getcwd()
+    with tempfile.TemporaryDirectory() as tmp:
+        os.chdir(tmp)  # the reference parser creates its work_dir relative to the working directory
+        try:
+            with quiet():
+                cfg = input_parser.parse(PIPE_DIR / "input.xml")
+        finally:
+            os.chdir(cwd)
+        ref["config"] = {f.name: (str(getattr(cfg, f.name)) if isinstance(getattr(cfg, f.name), Path)
+                                  else getattr(cfg, f.name))
+                         for f in dataclasses.fields(cfg) if f.name != "outputs"}
+        ref["outputs"] = dataclasses.asdict(cfg.outputs)
+        for name in ("rec.pqr", "lig.pqr"):
+            recs = parse_pqr_records(PIPE_DIR / name)
+            ref[name] = [[r.serial, r.name, r.resname, r.resid, r.x, r.y, r.z, r.charge, r.radius] for r in recs]
+            atoms = pbs.centre_at_origin(pbs.read_pqr(PIPE_DIR / name))
+            atoms = pbs.inject_gho(atoms)
+            w = Path(tmp) / name
+            pbs.write_pqr(atoms, w)
+            ref[name + ".written"] = w.read_text()
+            with quiet():
+                g = geometry.analyse_molecule(w, srad=1.5)
+            cache = sorted(Path(tmp).glob(name + ".r_hydro_*.cache"))
+            ref[name + ".cache"] = [cache[0].name, cache[0].read_text()] if cache else None
+            ref[name + ".r_hydro"] = g.hydrodynamic_r
+        for name in ("rxns_flat.xml", "rxns_sm.xml"):
+            pairs, nn = geometry._parse_rxns_xml_criteria(PIPE_DIR / name)
+            ref[name + ".flat"] = [[[p.rec_index, p.lig_index, p.cutoff] for p in pairs], nn]
+            groups, first = geometry._parse_rxns_xml_reaction_groups(PIPE_DIR / name)
+            ref[name + ".groups"] = [[[g.name, g.state_before, g.state_after,
+                                       [[p.rec_index, p.lig_index, p.cutoff] for p in g.pairs], g.n_needed]
+                                      for g in groups], first]
+    (HERE / "pipeline_ref.json").write_text(json.dumps(ref, indent=1, sort_keys=True) + "\n")
+
+
 def two_sphere_example():
     """The reference's two-charged-spheres example (examples/two_charged_spheres) on a synthetic grid."""
     from pystarc_b200.synth import BDSystem, sphere_dh_grid
@@ -313,6 +466,7 @@ def main():
                                                 31337, 1_000_000),
         "run_sm_c2": lambda: gen_run_sm(out, "run_sm_c2", c2, SM_C2, 160, 434343, 600),
     }
+    jobs["pipeline"] = lambda: gen_pipeline(out)
     for k, job in jobs.items():
         if not args.only or k in args.only:
             job()
