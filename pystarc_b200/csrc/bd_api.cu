@@ -143,6 +143,12 @@ void grid_to_dev(const GridHost& g, const float* dptr, int ch, DevGrid& d) {
   d.hix = g.o[0] + ((double)g.n[0] - 1 - m) * g.sp[0];
   d.hiy = g.o[1] + ((double)g.n[1] - 1 - m) * g.sp[1];
   d.hiz = g.o[2] + ((double)g.n[2] - 1 - m) * g.sp[2];
+  d.oxf = (float)d.ox;
+  d.oyf = (float)d.oy;
+  d.ozf = (float)d.oz;
+  d.isxf = (float)d.isx;
+  d.isyf = (float)d.isy;
+  d.iszf = (float)d.isz;
 }
 
 int upload_floats(BdHandle* h, const float* src, size_t n, const float** out) {

@@ -47,6 +47,7 @@ struct DevGrid {
   double ox, oy, oz;
   double isx, isy, isz;  // 1/spacing
   double lox, loy, loz, hix, hiy, hiz;  // strict margin box
+  float oxf, oyf, ozf, isxf, isyf, iszf;  // FP32 origin and 1/spacing (the FP32-position stencil)
 };
 
 struct DevSystem {
@@ -311,7 +312,23 @@ __device__ __forceinline__ void floor_split(double u, double& f, int& c) {
 // only moves the result by its own rounding).
 template <typename FT, int CH, typename PT = double>
 __device__ __forceinline__ StencilOut<FT, CH> stencil(const DevGrid& g, PT x, PT y, PT z) {
-  const PT ux = (x - (PT)g.ox) * (PT)g.isx, uy = (y - (PT)g.oy) * (PT)g.isy, uz = (z - (PT)g.oz) * (PT)g.isz;
+  PT ox, oy, oz, isx, isy, isz;
+  if constexpr (sizeof(PT) == 4) {  // the host-rounded FP32 copies: no conversion per evaluation
+    ox = g.oxf;
+    oy = g.oyf;
+    oz = g.ozf;
+    isx = g.isxf;
+    isy = g.isyf;
+    isz = g.iszf;
+  } else {
+    ox = g.ox;
+    oy = g.oy;
+    oz = g.oz;
+    isx = g.isx;
+    isy = g.isy;
+    isz = g.isz;
+  }
+  const PT ux = (x - ox) * isx, uy = (y - oy) * isy, uz = (z - oz) * isz;
   PT fx, fy, fz;
   int cx, cy, cz;
   floor_split(ux, fx, cx);

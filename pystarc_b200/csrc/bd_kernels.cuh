@@ -211,8 +211,20 @@ __device__ __forceinline__ void warp_reverse_born(const DevSystem& S, const doub
     const int k = k0 + lane;
     bool hit = false;
     if (k < S.n_chunks) {
-      const double4 sp = S.chunks[k];
-      const FT d0 = (FT)(sp.x - c[0]), d1 = (FT)(sp.y - c[1]), d2 = (FT)(sp.z - c[2]);
+      FT d0, d1, d2, rad;
+      if constexpr (sizeof(FT) == 4) {  // FP32 centres: ~1e-5 A off, inside the 1e-3 A margin below
+        const float4 sp = S.chunks_f[k];
+        d0 = sp.x - cx;
+        d1 = sp.y - cy;
+        d2 = sp.z - cz;
+        rad = sp.w;
+      } else {
+        const double4 sp = S.chunks[k];
+        d0 = sp.x - c[0];
+        d1 = sp.y - c[1];
+        d2 = sp.z - c[2];
+        rad = sp.w;
+      }
       const FT l0 = Rt[0] * d0 + Rt[3] * d1 + Rt[6] * d2;
       const FT l1 = Rt[1] * d0 + Rt[4] * d1 + Rt[7] * d2;
       const FT l2 = Rt[2] * d0 + Rt[5] * d1 + Rt[8] * d2;
@@ -220,7 +232,7 @@ __device__ __forceinline__ void warp_reverse_born(const DevSystem& S, const doub
       const FT ey = fmax(fmax(loy - l1, l1 - hiy), (FT)0);
       const FT ez = fmax(fmax(loz - l2, l2 - hiz), (FT)0);
       // the radius is inflated against rounding; the extra margin covers FP32 geometry
-      const FT lim = (FT)sp.w + (sizeof(FT) == 4 ? (FT)1e-3 : (FT)1e-9);
+      const FT lim = rad + (sizeof(FT) == 4 ? (FT)1e-3 : (FT)1e-9);
       hit = ex * ex + ey * ey + ez * ez < lim * lim;
     }
     unsigned hits = __ballot_sync(FULL, hit);
