@@ -1198,6 +1198,11 @@ __global__ void __launch_bounds__(256, MINB) step_kernel_warp(DevSystem S, DevSi
     tr.status = ST_EMPTY;
     if (own) load_slot(B, slot, tr);
     bool dead = !own;
+    // F, T hold the forces at the lane's current pose while `fresh`: a step that the
+    // overlap test rejected leaves the pose, and so the forces, unchanged, and the next
+    // step reuses them instead of evaluating the same pose again
+    double F[3] = {0, 0, 0}, T[3] = {0, 0, 0};
+    bool fresh = false;
     for (int k = 0; k < K; ++k) {
       warp_refill(P, tr, dead, lane);
       if (__all_sync(FULL, dead)) break;
@@ -1207,12 +1212,13 @@ __global__ void __launch_bounds__(256, MINB) step_kernel_warp(DevSystem S, DevSi
       const double r_prev = P.stats ? norm3(tr.c[0], tr.c[1], tr.c[2]) : 0.0;
       int st = ST_EMPTY;
       if (!dead) {
+        const int rets0 = tr.rets;
         st = step_begin(S, P, key, s, tr, R, r, tl);
+        if (tr.rets != rets0) fresh = false;  // returned to the b-sphere: a new pose
         if (P.stats && st == ST_REACTED) stats_encounter(P, tr, s, false);
       }
       const bool need_f = !dead && st == ST_RUNNING;
-      double F[3] = {0, 0, 0}, T[3] = {0, 0, 0};
-      warp_forces<FT, TORQUE>(S, tr.c, R, need_f, F, T, lane, tl.cnt, sh.v);
+      warp_forces<FT, TORQUE>(S, tr.c, R, need_f && !fresh, F, T, lane, tl.cnt, sh.v);
       double cn[3] = {0, 0, 0}, qn[4] = {1, 0, 0, 0}, dt = 0;
       bool ok = true;
       if (need_f) ok = step_move<FT>(S, P, key, s, tr, R, r, F, T, cn, qn, dt);
@@ -1221,6 +1227,7 @@ __global__ void __launch_bounds__(256, MINB) step_kernel_warp(DevSystem S, DevSi
         st = ST_ERROR;
       }
       const bool ovl = warp_overlap(S, cn, need_f && ok && P.overlap, lane, sh.v);
+      fresh = need_f && ok && ovl;
       if (need_f && ok) {
         const double c0[3] = {tr.c[0], tr.c[1], tr.c[2]};
         st = step_end(S, P, key, s, tr, R, cn, qn, !ovl, dt, tl);
@@ -1229,6 +1236,7 @@ __global__ void __launch_bounds__(256, MINB) step_kernel_warp(DevSystem S, DevSi
           if (st == ST_REACTED) stats_encounter(P, tr, s, true);
         }
       }
+      if (st != ST_RUNNING) fresh = false;
       if (!dead && st != ST_RUNNING) {
         tr.status = st;
         P.out_status[tr.id] = (int8_t)st;

@@ -134,6 +134,8 @@ __global__ void __launch_bounds__(256, 2) step_kernel_multi(MultiTab T, SlotBuf 
       tr.id = (int)(tr.id - T.base[sys]);
     }
     bool dead = !own;
+    double F[3] = {0, 0, 0}, Tq[3] = {0, 0, 0};
+    bool fresh = false;  // F, Tq are the forces at the current pose (kept over rejected steps)
     for (int k = 0; k < K; ++k) {
       multi_refill(T, tr, sys, dead, lane);
       if (__all_sync(FULL, dead)) break;
@@ -143,10 +145,13 @@ __global__ void __launch_bounds__(256, 2) step_kernel_multi(MultiTab T, SlotBuf 
       const uint32_t s = (uint32_t)tr.steps;
       double R[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, r = 0;
       int st = ST_EMPTY;
-      if (!dead) st = step_begin(S, P, key, s, tr, R, r, tl);
+      if (!dead) {
+        const int rets0 = tr.rets;
+        st = step_begin(S, P, key, s, tr, R, r, tl);
+        if (tr.rets != rets0) fresh = false;
+      }
       const bool need_f = !dead && st == ST_RUNNING;
-      double F[3] = {0, 0, 0}, Tq[3] = {0, 0, 0};
-      warp_forces_multi<FT, TORQUE>(T, sys, tr.c, R, need_f, F, Tq, lane, tl.cnt);
+      warp_forces_multi<FT, TORQUE>(T, sys, tr.c, R, need_f && !fresh, F, Tq, lane, tl.cnt);
       double cn[3] = {0, 0, 0}, qn[4] = {1, 0, 0, 0}, dt = 0;
       bool ok = true;
       if (need_f) ok = step_move<FT>(S, P, key, s, tr, R, r, F, Tq, cn, qn, dt);
@@ -155,7 +160,9 @@ __global__ void __launch_bounds__(256, 2) step_kernel_multi(MultiTab T, SlotBuf 
         st = ST_ERROR;
       }
       const bool ovl = warp_overlap_multi(T, sys, cn, need_f && ok && P.overlap, lane);
+      fresh = need_f && ok && ovl;
       if (need_f && ok) st = step_end(S, P, key, s, tr, R, cn, qn, !ovl, dt, tl);
+      if (st != ST_RUNNING) fresh = false;
       if (!dead && st != ST_RUNNING) {
         tr.status = st;
         P.out_status[tr.id] = (int8_t)st;
