@@ -115,13 +115,29 @@ void free_list(std::vector<void*>& list) {
   list.clear();
 }
 
-uint32_t spread3(uint32_t v) {
-  v &= 0x3ff;
-  v = (v | (v << 16)) & 0x030000FF;
-  v = (v | (v << 8)) & 0x0300F00F;
-  v = (v | (v << 4)) & 0x030C30C3;
-  v = (v | (v << 2)) & 0x09249249;
-  return v;
+// Receptor atoms order[b, e) split at the median of their widest axis until every
+// group holds at most BD_CHUNK atoms; the left part of each split is a whole number
+// of chunks, so only the last chunk can be partial.  The chunks are compact
+// (median-split boxes), which keeps their bounding spheres small for the culls.
+void kd_chunks(const std::vector<double>& rec, std::vector<int>& order, int b, int e) {
+  const int n = e - b;
+  if (n <= BD_CHUNK) return;
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (int i = b; i < e; ++i)
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = std::min(lo[k], rec[4 * order[i] + k]);
+      hi[k] = std::max(hi[k], rec[4 * order[i] + k]);
+    }
+  int ax = 0;
+  for (int k = 1; k < 3; ++k)
+    if (hi[k] - lo[k] > hi[ax] - lo[ax]) ax = k;
+  const int left = ((n + BD_CHUNK - 1) / BD_CHUNK / 2) * BD_CHUNK;
+  std::nth_element(order.begin() + b, order.begin() + b + left, order.begin() + e, [&](int x, int y) {
+    const double u = rec[4 * x + ax], v = rec[4 * y + ax];
+    return u < v || (u == v && x < y);
+  });
+  kd_chunks(rec, order, b, b + left);
+  kd_chunks(rec, order, b + left, e);
 }
 
 void grid_to_dev(const GridHost& g, const float* dptr, int ch, DevGrid& d) {
@@ -257,32 +273,16 @@ int finalize(BdHandle* h) {
     CK(h, cudaMemcpy(p, h->lig.data(), h->lig.size() * sizeof(double), cudaMemcpyHostToDevice));
     S.lig = (const double4*)p;
   }
-  // receptor: spatial (Morton) order, chunks of BD_CHUNK with bounding spheres
+  // receptor: spatial (k-d median split) order, chunks of BD_CHUNK with bounding spheres
   const int nr = (int)(h->rec.size() / 4);
   if (nr > 0) {
-    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
     double rmax = 0;
-    for (int i = 0; i < nr; ++i) {
-      for (int k = 0; k < 3; ++k) {
-        lo[k] = std::min(lo[k], h->rec[4 * i + k]);
-        hi[k] = std::max(hi[k], h->rec[4 * i + k]);
-      }
+    for (int i = 0; i < nr; ++i)
       rmax = std::max(rmax, std::sqrt(h->rec[4 * i] * h->rec[4 * i] + h->rec[4 * i + 1] * h->rec[4 * i + 1] +
                                       h->rec[4 * i + 2] * h->rec[4 * i + 2]));
-    }
-    std::vector<uint32_t> code(nr);
-    for (int i = 0; i < nr; ++i) {
-      uint32_t c = 0;
-      for (int k = 0; k < 3; ++k) {
-        const double w = hi[k] - lo[k];
-        const uint32_t v = w > 0 ? (uint32_t)std::min(1023.0, (h->rec[4 * i + k] - lo[k]) / w * 1023.0) : 0u;
-        c |= spread3(v) << k;
-      }
-      code[i] = c;
-    }
     std::vector<int> order(nr);
     std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return code[a] < code[b]; });
+    kd_chunks(h->rec, order, 0, nr);
     const int nc = (nr + BD_CHUNK - 1) / BD_CHUNK;
     std::vector<double> ra(4 * (size_t)nc * BD_CHUNK), cs(4 * (size_t)nc);
     for (int j = 0; j < nc * BD_CHUNK; ++j) {
