@@ -650,7 +650,9 @@ def main():
                    "parallelism": f"trajectory shards x{world}", "l2": "flushed (256 MiB write) between launches",
                    "launch": launch},
         "variants": {
-            "mixed": {"bd_steps_per_s": d_mixed["steps"] / t_mixed, "steps": d_mixed["steps"]},
+            "mixed": {"bd_steps_per_s": d_mixed["steps"] / t_mixed, "steps": d_mixed["steps"],
+                      # trajectories this rank finished in the timed window (reacted, escaped or max steps)
+                      "trajectories_per_s": (d_mixed["reacted"] + d_mixed["escaped"] + d_mixed["max_steps"]) / t_mixed},
             "fp64": {"bd_steps_per_s": d_fp64["steps"] / t_fp64, "steps": d_fp64["steps"], "launch": launch64},
             "mixed_over_fp64": (d_mixed["steps"] / t_mixed) / (d_fp64["steps"] / t_fp64),
         },
