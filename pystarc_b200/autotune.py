@@ -14,8 +14,6 @@ simulator is reset afterwards, so results do not depend on it.
 
 from __future__ import annotations
 
-import numpy as np
-
 from . import _lib
 
 DEFAULT_CANDIDATES = ((1, 128), (8, 128), (16, 128), (32, 128), (64, 128), (64, 256), (65, 128), (65, 256))

@@ -34,7 +34,7 @@ import re
 import shutil
 import sys
 import xml.etree.ElementTree as ET
-from dataclasses import dataclass, field, fields
+from dataclasses import dataclass, field
 from pathlib import Path
 from typing import List, Optional
 

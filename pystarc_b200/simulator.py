@@ -28,7 +28,7 @@ from typing import Dict
 import numpy as np
 
 from . import _lib
-from .hostphys import CONV, bridge_d_eff, rate_constant, return_prob_and_kb, wilson_ci
+from .hostphys import bridge_d_eff, rate_constant, return_prob_and_kb, wilson_ci
 
 
 @dataclass

@@ -5,7 +5,6 @@ import math
 import numpy as np
 import pytest
 
-from oracle import physics as oph
 from pystarc_b200 import hostphys, structures as st, synth
 from pystarc_b200.dx import DXGrid
 from pystarc_b200.simulator import B200BatchResult, flatten_pairs

@@ -7,7 +7,7 @@ import pytest
 
 from oracle import physics as oph
 from oracle import stepper as ost
-from oracle.forces import OracleGrid, k1_batch_force, _interp, multipole_moments, yukawa_forces, FarField
+from oracle.forces import k1_batch_force, _interp, multipole_moments, yukawa_forces, FarField
 from oracle.philox import philox4x32_10, KeyedDraws
 from tests.helpers import golden, system, system_digest, oracle_engine, step_system, step_params
 
