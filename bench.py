@@ -45,11 +45,27 @@ ALGO_BYTES_PER_GATHER = 224  # 7 trilinear interpolations x 8 corners x 4 B per 
 STATE_BYTES_PER_STEP = 128  # FP64 pose read + write and status/counters per trajectory-step
 
 
+def _find_key(d, key):
+    if isinstance(d, dict):
+        if key in d and isinstance(d[key], (int, float)):
+            return float(d[key])
+        for v in d.values():
+            r = _find_key(v, key)
+            if r is not None:
+                return r
+    return None
+
+
 def peaks():
+    """The measured HBM copy bandwidth (GB/s) of MEASURED_PEAKS.json, else the pool's earlier figure."""
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
-        d = json.loads(p.read_text())
-        return float(d["hbm_gbs"]), "measured"
+        try:
+            v = _find_key(json.loads(p.read_text()), "hbm_gbs")
+            if v and v > 0:
+                return v, "measured"
+        except (OSError, ValueError):
+            pass
     return 6650.0, "fallback"
 
 
