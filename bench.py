@@ -275,7 +275,7 @@ def e2e_arm(s, precision, steps, K, n_traj, id_offset, launch):
 
 def surrogate_arm(s, steps, warmup, K, n_traj, n_poses, train_steps, members, kon_traj, kon_launches=300, log=None,
                   aged=None):
-    """Config 4: train the surrogate on exact-kernel BD poses, judge it on held-out poses, time the
+    """Config 4: train the surrogate on exact-kernel BD poses, evaluate it on held-out poses, time the
     surrogate stepper like the exact one, and compare k_on of exact and surrogate runs."""
     import torch
 

@@ -10,7 +10,7 @@ from tests.helpers import golden, oracle_engine, system, system_digest
 pytestmark = pytest.mark.gpu
 
 FP64_TOL = 1e-9   # error metric of oracle.forces.force_error, FP64 engine
-MIXED_TOL = 1e-4  # FP32 force arithmetic, FP64 geometry and sums (north-star bound for mixed precision)
+MIXED_TOL = 1e-4  # FP32 force arithmetic, FP64 geometry and sums (the bound required of mixed precision)
 
 
 class _MP:
