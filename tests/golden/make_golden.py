@@ -188,7 +188,7 @@ def gen_physics(out):
                             pts=pts, V=np.array([mp.potential(p) for p in pts]))
 
 
-def build_sim(s, n_traj, seed, max_steps, work, sm=None):
+def build_sim(s, n_traj, seed, max_steps, work, sm=None, use_lj=False):
     from pystarc.simulation.gpu_batch_simulator import GPUBatchSimulator
     from pystarc.simulation.nam_simulator import NAMParameters
     from pystarc.hydrodynamics.rotne_prager import MobilityTensor
@@ -217,15 +217,15 @@ def build_sim(s, n_traj, seed, max_steps, work, sm=None):
     params._overlap_check = s.overlap
     if sm is not None:
         params.minimum_core_reaction_dt = sm["min_core_rxn_dt"]
-    eng = make_engine(None, s, multipole=s.multipole)
+    eng = make_engine(None, s, multipole=s.multipole, use_lj=use_lj)
     with quiet():
         sim = GPUBatchSimulator(mol1, mol2, mob, ps, params, eng)
     return sim, mob
 
 
-def gen_run(out, name, s, n_traj, seed, max_steps):
+def gen_run(out, name, s, n_traj, seed, max_steps, use_lj=False):
     with tempfile.TemporaryDirectory() as work:
-        sim, mob = build_sim(s, n_traj, seed, max_steps, work)
+        sim, mob = build_sim(s, n_traj, seed, max_steps, work, use_lj=use_lj)
         with quiet():
             res = sim.run()
     sd = res.sim_data
@@ -462,6 +462,7 @@ def main():
         "run_two_sphere": lambda: gen_run(out, "run_two_sphere", two_sphere_example(), 2000, 11111113, 1_000_000),
         "run_c2": lambda: gen_run(out, "run_c2", c2, 160, 424242, 400),
         "run_c3": lambda: gen_run(out, "run_c3", c3, 64, 515151, 150),
+        "run_lj_c2": lambda: gen_run(out, "run_lj_c2", c2, 160, 424242, 400, use_lj=True),
         "run_sm_two_sphere": lambda: gen_run_sm(out, "run_sm_two_sphere", two_sphere_example(), SM_TWO_SPHERE, 1000,
                                                 31337, 1_000_000),
         "run_sm_c2": lambda: gen_run_sm(out, "run_sm_c2", c2, SM_C2, 160, 434343, 600),

@@ -205,6 +205,25 @@ def test_stepper_reproduces_reference_run_exactly(name, sysname):
     np.testing.assert_array_equal(res.status, ref_outcome)
 
 
+def test_stepper_with_contact_forces_reproduces_reference_run_exactly():
+    """use_lj=True in the stepper: the reference run with WCA contact forces, trajectory for trajectory."""
+    g = golden("run_lj_c2")
+    s = system("c2")
+    assert system_digest(s) == str(g["digest"])
+    res = ost.run(step_system(s, oracle_engine(s, use_lj=True)),
+                  step_params(s, int(g["n_traj"]), int(g["seed"]), int(g["max_steps"])), noise="pcg64")
+    assert (res.n_reacted, res.n_escaped, res.n_max_steps) == (int(g["n_reacted"]), int(g["n_escaped"]),
+                                                              int(g["n_max_steps"]))
+    np.testing.assert_array_equal(res.n_steps, g["n_steps"])
+    np.testing.assert_array_equal(res.n_returns, g["n_returns"])
+    ref_outcome = g["outcome"].copy()
+    ref_outcome[ref_outcome == 0] = 3
+    np.testing.assert_array_equal(res.status, ref_outcome)
+    # the same seed without the contact term takes other paths
+    plain = golden("run_c2")
+    assert np.any(plain["n_steps"] != g["n_steps"])
+
+
 @pytest.mark.parametrize("name,sysname", [("run_sm_two_sphere", "two_sphere"), ("run_sm_c2", "c2")])
 def test_state_machine_run_reproduces_reference_exactly(name, sysname):
     """State-machine reactions: state numbering, every trajectory's fate and step count, and the
