@@ -31,3 +31,16 @@ def allreduce_tallies(tallies: dict, group=None, device=None) -> dict:
     t = torch.tensor([int(tallies.get(k, 0)) for k in TALLY_KEYS], dtype=torch.int64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
     return dict(zip(TALLY_KEYS, (int(v) for v in t.cpu())))
+
+
+def allreduce_reaction_fires(discrete, bridge, group=None, device=None):
+    """Sum the per-reaction fire counts of state-machine runs over all ranks
+    (``B200BatchSimulator.reaction_fires``); returns (discrete, bridge) as lists."""
+    import torch
+    import torch.distributed as dist
+
+    n = len(discrete)
+    t = torch.tensor([int(v) for v in discrete] + [int(v) for v in bridge], dtype=torch.int64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    v = [int(x) for x in t.cpu()]
+    return v[:n], v[n:]

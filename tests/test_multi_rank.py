@@ -82,3 +82,46 @@ def test_two_rank_pooling_equals_single_process():
     np.testing.assert_array_equal(status, single.status)
     np.testing.assert_array_equal(steps, single.n_steps)
     assert set(TALLY_KEYS) >= set(pooled)
+
+
+def _run_sm_shard(n_total, rank, world):
+    from dataclasses import replace
+
+    from oracle import stepper as ost
+    from tests.helpers import golden, sm_step_system, step_params, system
+
+    s = system("two_sphere")
+    off, n = shard_range(n_total, rank, world)
+    prm = replace(step_params(s, n, s.seed, 20000), min_core_rxn_dt=0.05)
+    return ost.run(sm_step_system(s, golden("run_sm_two_sphere")), prm, noise="philox", termination="complete",
+                   id_offset=off)
+
+
+def _sm_worker(rank, world, port, n_total, out):
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from pystarc_b200.shard import allreduce_reaction_fires
+
+        res = _run_sm_shard(n_total, rank, world)
+        out[rank] = allreduce_reaction_fires(res.sm_fires_discrete, res.sm_fires_bridge)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_state_machine_fire_counts_pool():
+    """Per-reaction fire counts of sharded state-machine runs add up to the single-process counts."""
+    n_total = 40
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as mgr:
+        out = mgr.dict()
+        port = _free_port()
+        mp.start_processes(_sm_worker, args=(2, port, n_total, out), nprocs=2, join=True, start_method="spawn")
+        results = dict(out)
+    single = _run_sm_shard(n_total, 0, 1)
+    assert results[0] == results[1]
+    assert results[0] == (single.sm_fires_discrete.tolist(), single.sm_fires_bridge.tolist())
+    assert sum(results[0][0]) + sum(results[0][1]) > 0
