@@ -38,6 +38,11 @@ def test_errors_are_codes_not_crashes():
     assert lib.bd_last_error(None, buf, 256) == 0 and b"NULL" in buf.value
     assert lib.bd_destroy(None) == 0
     assert lib.bd_set_ligand(None, 1, None, None) == _lib.BD_ERR_ARG
+    assert lib.bd_set_contact(None, 0, None, 0, None, 0.17, -1.0) == _lib.BD_ERR_ARG
+    assert lib.bd_set_reaction_states(None, 0, None, None, 0, None) == _lib.BD_ERR_ARG
+    assert lib.bd_sim_reaction_fires(None, None, None, 0) == _lib.BD_ERR_ARG
+    assert lib.bd_sim_get_states(None, None) == _lib.BD_ERR_ARG
+    assert lib.bd_sim_set_states(None, None) == _lib.BD_ERR_ARG
 
 
 def test_create_without_gpu_reports_cuda_error():
