@@ -663,7 +663,10 @@ def main():
                                     f"aged {args.age} launches (restored for each arm), then {args.warmup} warm-up "
                                     f"launches"),
                    "parallelism": f"trajectory shards x{world}", "l2": "flushed (256 MiB write) between launches",
-                   "launch": launch},
+                   "launch": launch,
+                   "force_reuse": ("a step rejected by the overlap test leaves the pose unchanged; the next step "
+                                   "reuses its forces instead of evaluating the same pose again (trajectories are "
+                                   "bit-identical to evaluating every step)")},
         "variants": {
             "mixed": {"bd_steps_per_s": d_mixed["steps"] / t_mixed, "steps": d_mixed["steps"],
                       # trajectories this rank finished in the timed window (reacted, escaped or max steps)
