@@ -7,7 +7,8 @@ batch shares one slot pool across the systems (``bd_multi_*``): trajectories
 of every system are refilled into free slots as others finish, so small and
 large systems keep the GPU full together.  Each trajectory runs exactly as in
 its own simulator (same keyed noise), and outcomes land in each simulator's
-arrays.
+arrays.  The counters are the batch's: state-machine fire counts are summed over
+the systems, so the per-system results carry no ``completed_reactions`` record.
 """
 
 from __future__ import annotations
