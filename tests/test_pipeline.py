@@ -129,3 +129,22 @@ def test_prepare_molecules_copies_centres_and_reads_back(ref, tmp_path):
     assert (tmp_path / "work" / "ligand.pqr").read_text() == ref["lig.pqr.written"]
     assert mol_rec.atoms[-1].name == "GHO" and len(mol_lig) == 4
     np.testing.assert_allclose(mol_rec.positions_array()[0], [4.974, 5.771, -6.724])
+
+
+def test_missing_grids_or_radii_name_the_missing_step(tmp_path):
+    """Without APBS's DX files, or without a hydrodynamic radius, the run stops before any GPU work."""
+    for f in ("rec.pqr", "lig.pqr", "rxns_sm.xml"):
+        shutil.copy(PIPE / f, tmp_path / f)
+    xml = (PIPE / "input.xml").read_text()
+    (tmp_path / "input.xml").write_text(xml.replace("<r_hydro_rec>2.25</r_hydro_rec>",
+                                                    "<r_hydro_rec>2.25</r_hydro_rec><r_hydro_lig>1.5</r_hydro_lig>"))
+    with pytest.raises(FileNotFoundError, match="APBS"):
+        pl.build(tmp_path / "input.xml")
+    (tmp_path / "input.xml").write_text(xml)  # no ligand radius and no cached Monte-Carlo value
+    with pytest.raises(FileNotFoundError, match="r_hydro"):
+        pl.build(tmp_path / "input.xml")
+
+
+def test_main_prints_usage(capsys):
+    assert pl.main(["--help"]) == 0
+    assert "input.xml" in capsys.readouterr().out
