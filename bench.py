@@ -500,7 +500,44 @@ def save_cpu_inputs(s, path):
     np.savez(path, **arr)
 
 
-def cpu_baseline(s, cores, traj_per_proc=256, n_steps=40, init=None):
+def force_error_check(s, c, q):
+    """Force and torque error of the engine against the FP64 oracle on the poses (c, q), both
+    precisions: plain relative error ||F - F_ref|| / ||F_ref|| (max, p99) and the tested metric
+    of ``oracle.forces.force_error``.  The oracle is the checker here, never the thing timed."""
+    from oracle.forces import FarField, OracleForceEngine, OracleGrid, force_error
+    from oracle.stepper import rotmats
+    from pystarc_b200.engine import B200ForceEngine
+
+    dip, quad, fpe = s.multipole_moments()
+    ff = FarField(float(np.sum(s.rec_q)), s.debye, s.sdie, dip, quad, fpe)
+    oe = OracleForceEngine([OracleGrid.from_dx(g) for g in s.elec_grids], [OracleGrid.from_dx(g) for g in s.born_grids],
+                           s.alpha, ff, [OracleGrid.from_dx(g) for g in s.lig_born_grids] or None, s.rec_pos, s.rec_q,
+                           born_chunk_skip=False)
+    body = s.lig_pos - s.lig_pos.mean(axis=0)
+    R = rotmats(q)
+    pos = np.einsum("nij,kj->nki", R, body) + c[:, None, :]
+    Fo, To, _, scale = oe(pos, s.lig_q, R, c, torque_mode="centroid", return_scale=True)
+    out = {"poses": int(len(c)), "poses_from": "the GPU arm's aged pool", "reference": "FP64 oracle of "
+           "GPUBatchForceEngine.__call__ on identical poses (torque about the centroid)"}
+    nf, nt = np.linalg.norm(Fo, axis=1), np.linalg.norm(To, axis=1)
+    okf, okt = nf > 1e-6 * np.median(nf), nt > 1e-6 * np.median(nt)
+    lever = float(np.max(np.linalg.norm(body, axis=1)))
+    for prec in ("fp64", "mixed"):
+        eng = B200ForceEngine(**s.engine_kwargs(), multipole_expansion=_MP(s), precision=prec, torque_mode="centroid",
+                              device=int(os.environ.get("LOCAL_RANK", 0)))
+        eng.set_ligand(body, s.lig_q)
+        F, T, _ = eng.eval_poses(c, q)
+        eng.close()
+        pf = np.linalg.norm(F - Fo, axis=1)[okf] / nf[okf]
+        pt = np.linalg.norm(T - To, axis=1)[okt] / nt[okt]
+        out[prec] = {"force_rel_max": float(pf.max()), "force_rel_p99": float(np.percentile(pf, 99)),
+                     "torque_rel_max": float(pt.max()), "torque_rel_p99": float(np.percentile(pt, 99)),
+                     "force_metric_max": float(force_error(F, Fo, scale).max()),
+                     "torque_metric_max": float(force_error(T, To, scale * lever).max())}
+    return out
+
+
+def cpu_baseline(s, cores, traj_per_proc=256, n_steps=40, init=None, where=None):
     """The reference's step loop restated in NumPy on `cores` processes, each a bounded sample.
 
     ``init`` = (centroids, quaternions): start the processes' trajectories from these poses (a
@@ -524,7 +561,8 @@ def cpu_baseline(s, cores, traj_per_proc=256, n_steps=40, init=None):
         wall = time.perf_counter() - t0
     steps = sum(o[0] for o in out)
     busy = max(o[1] for o in out)
-    where = "poses sampled from the GPU arm's aged pool" if init is not None else "the b-sphere"
+    if where is None:
+        where = "poses sampled from the GPU arm's aged pool" if init is not None else "the b-sphere"
     return steps / busy, {"value": steps / busy, "unit": UNIT, "cores": cores, "kind": "port",
                           "sample": f"{cores} processes x {traj_per_proc} trajectories x <= {n_steps} steps of the "
                                     f"same system from {where} ({steps} trajectory-steps, {busy:.1f} s)",
@@ -565,9 +603,17 @@ def main():
             return
         s = build_system(None if not _has_cuda() else "cuda", args.workload)
         cores = os.cpu_count() or 1
+        init, where = None, "the b-sphere"
+        sample = ROOT / "oracle" / "samples" / "aged_protein_ligand.npz"
+        if args.workload == "protein-ligand" and args.age > 0 and sample.exists():
+            d = np.load(sample)
+            init = (d["c"], d["q"])
+            where = (f"a committed sample of {len(d['c'])} poses aged {int(d['aged_steps'])} BD steps from the "
+                     f"b-sphere by the oracle alone ({sample.name})")
         vals = []
         for i in range(args.warmup + args.steps):
-            v, info = cpu_baseline(s, cores, n_steps=max(4, args.cpu_steps // 4))
+            v, info = cpu_baseline(s, cores, traj_per_proc=64, n_steps=max(4, args.cpu_steps // 4), init=init,
+                                   where=where)
             if i >= args.warmup:
                 vals.append(v)
         val = float(np.mean(vals))
@@ -638,13 +684,14 @@ def main():
     gathers = d_mixed["grid_evals"] + d_mixed["rev_evals"]
     algo_bytes = gathers * ALGO_BYTES_PER_GATHER + d_mixed["steps"] * STATE_BYTES_PER_STEP
     achieved = algo_bytes / t_mixed / 1e9
-    traffic = None  # DRAM bytes per launch of the stepper, from the committed ncu capture summary
-    tf = ROOT / "profiles" / "step_kernel_warp_protein_ligand.md"
+    traffic, traffic_note = None, None
+    tf = ROOT / "profiles" / "step_kernel_warp_traffic.json"
     if args.workload == "protein-ligand" and tf.exists():
-        import re
-
-        m = re.search(r"dram_bytes_per_launch \| (\d+)", tf.read_text())
-        traffic = int(m.group(1)) if m else None
+        # DRAM bytes (read + write) of one stepper launch, from the ncu capture of a small case scaled by the
+        # trajectory-steps of this launch (the figure and its scaling are stated in the file)
+        t = json.loads(tf.read_text())
+        traffic = int(t["dram_bytes_per_trajectory_step"] * d_mixed["steps"] / args.steps)
+        traffic_note = t["note"]
     if rank != 0:
         import shutil
 
@@ -676,8 +723,9 @@ def main():
         },
         "counters": {k: int(v) for k, v in d_mixed.items()},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "peak_kind": peak_kind,
+                     "traffic": traffic, "traffic_note": traffic_note, "peak_kind": peak_kind,
                      "algorithmic_bytes": "224 B per (atom, grid) stencil + 128 B per trajectory-step"},
+        "cupy_reference": cupy_reference(),
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "note": "B200ForceEngine + B200BatchSimulator.run() from host arrays, incl. grid upload"},
         "gpu_launches": 3 * args.steps,
@@ -692,12 +740,23 @@ def main():
         init = aged_poses(aged, cores * 64) if aged is not None else None
         _, info = cpu_baseline(s, cores, n_steps=args.cpu_steps, init=init)
         line["cpu_baseline"] = info
+        if aged is not None and args.workload != "two-spheres":
+            line["force_error"] = force_error_check(s, *aged_poses(aged, 256, seed=11))
     print(json.dumps(line))
     import shutil
 
     shutil.rmtree(work, ignore_errors=True)
     if dist is not None:
         dist.destroy_process_group()
+
+
+def cupy_reference():
+    """The reference's own CuPy path (GPUBatchSimulator on the GPU) can only run where CuPy imports."""
+    try:
+        import cupy  # noqa: F401
+    except Exception as e:  # ImportError, or a CuPy without a usable CUDA runtime
+        return f"unavailable (CuPy not installed: import cupy fails with {type(e).__name__})"
+    return "unavailable (CuPy imports, but the reference source is not shipped to the GPU box)"
 
 
 def _has_cuda():

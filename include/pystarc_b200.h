@@ -69,7 +69,23 @@ typedef struct {
   int32_t stats;             /* 1: collect the per-step statistics read by bd_sim_stats */
   double min_core_rxn_dt;    /* state-machine mode: floor of the reaction-surface dt refinement
                               * (params.minimum_core_reaction_dt, gpu_batch_simulator.py:636) */
+  int32_t save_interval;     /* with stats: record a path and an energy row of every running trajectory
+                              * whose step index is a multiple of this (output_cfg.save_interval, 10) */
+  int64_t trace_capacity;    /* with stats: rows kept on the device for bd_sim_traces (0: no traces) */
+  int32_t hi_mode;           /* with use_hi: BD_HI_REFERENCE_GPU or BD_HI_ZUK */
+  double hi_kT_eta;          /* BD_HI_ZUK: kBT/eta = sqrt(D_t1 6 pi a1 D_t2 6 pi a2), A^3/ps
+                              * (hydrodynamics/rotne_prager.py:121-122) */
 } BdSimParams;
+
+/* Relative translational diffusion D(r) of the stepper when use_hi is set.
+ * BD_HI_REFERENCE_GPU: the reference GPU stepper's line-of-centres formula
+ *   D = Df ainv - 2 Df (2/r - (4/3) a2/r^3) / (8 pi), Df = 1/0.243, clamped at 1e-6
+ *   (gpu_batch_simulator.py:741-751, :1074-1084).
+ * BD_HI_ZUK: the Rotne-Prager-Yamakawa coupling of MobilityTensor.relative_translational_diffusion,
+ *   D = D_t - (2/3) tr M12(r), M12 by the three regimes of Zuk et al. (2014): far field, partial
+ *   overlap, one sphere inside the other; clamped at 1e-12 (hydrodynamics/rotne_prager.py:67-124,
+ *   :177-200). */
+enum { BD_HI_REFERENCE_GPU = 0, BD_HI_ZUK = 1 };
 
 /* Host arrays filled by bd_sim_stats (NULL members are skipped).  Per trajectory
  * (n_traj entries, x3 / x4 for poses): start pose, closest approach |c| with its
@@ -164,6 +180,16 @@ int bd_sim_counters(BdHandle* h, uint64_t* out, int n, void* stream);
 /* Host copies of the per-trajectory outcome (0 running/unstarted, 1 reacted, 2 escaped,
  * 3 max-steps, 5 non-finite pose), step counts and return counts (n_traj each). */
 int bd_sim_outcomes(BdHandle* h, int8_t* status, int32_t* steps, int32_t* returns);
+/* Path and energy traces (gpu_batch_simulator.py:1319-1340): every step whose index s is a
+ * multiple of save_interval adds, per running trajectory, a path row [traj_id, s, x, y, z, q0, q1,
+ * q2] (pose after the step) and an energy row [traj_id, s, fx, fy, fz, dt] (force of the step).
+ * Rows land in device order; up to `cap` of them are copied to path (cap x 8) and energy (cap x 6)
+ * host arrays (either may be NULL).  n_rows receives the rows copied, n_dropped the rows that did
+ * not fit the trace_capacity of the configuration. */
+int bd_sim_traces(BdHandle* h, double* path, double* energy, int64_t cap, int64_t* n_rows, int64_t* n_dropped);
+/* No counterpart in the reference: D(r) of the configured stepper (its HI mode and
+ * precision, BdSimParams) at n centroid distances r.  Host arrays; for parity tests. */
+int bd_sim_hi_diffusion(BdHandle* h, int n, const double* r, double* D);
 /* Per-step statistics (BdSimParams.stats = 1) to host arrays.  Replaces the host-side
  * statistics loops of GPUBatchSimulator.run (gpu_batch_simulator.py:1255-1317). */
 int bd_sim_stats(BdHandle* h, const BdStatsOut* out);
@@ -215,8 +241,8 @@ int bd_get_layout(BdHandle* h, int* flags);
 /* No counterpart in the reference.  Runs p->n_traj trajectories to completion (or for
  * max_launches launches of steps_per_launch steps) on the handle's system WITHOUT
  * allocating device memory, for callers that cannot call cudaMalloc at that point: an
- * application whose allocator already holds the GPU's memory, a process under a memory
- * quota, or code running while another library captures a CUDA graph.  The live-slot
+ * application whose allocator already holds the GPU's memory, or a process under a
+ * device-memory quota.  The live-slot
  * pool, live counts and counters use a fixed file-scope device array of 9.2 MB, enough for
  * BD_NOALLOC_MAX_SLOTS live slots; p->slots above that is rejected with BD_ERR_ARG
  * (0 = use the maximum).  Outputs are DEVICE arrays the caller owns: out_status,
@@ -224,7 +250,12 @@ int bd_get_layout(BdHandle* h, int* flags);
  * The system must already be on the device (its upload allocates): call bd_sim_configure
  * or an evaluation once before.  The first call on a device looks up the array's device
  * address; make that first call before any stream capture.  Every call shares the array
- * and clears the parts it uses; calls that overlap on the GPU race.  Synchronous. */
+ * and clears the parts it uses; calls that overlap on the GPU race.  The launch shape is
+ * chosen from p (as bd_sim_configure would), not from an earlier configuration.  A handle
+ * with a surrogate installed (bd_sim_set_surrogate) is rejected with BD_ERR_STATE.  The
+ * per-reaction fire counts of state-machine runs are not returned (bd_sim_reaction_fires
+ * reads the regular stepper's counters).  Synchronous: it copies a few words between host
+ * and device and waits on `stream`. */
 enum { BD_NOALLOC_MAX_SLOTS = 65536 };
 int bd_sim_run_noalloc(BdHandle* h, const BdSimParams* p, int8_t* out_status, int32_t* out_steps,
                        int32_t* out_returns, uint64_t* counters, int steps_per_launch, int max_launches,

@@ -60,6 +60,8 @@ class StepSystem:
     sm_before: np.ndarray | None = None
     sm_after: np.ndarray | None = None
     sm_terminal: np.ndarray | None = None
+    # kBT/eta of the RPY coupling, sqrt(D_t1 6 pi a1 D_t2 6 pi a2) (rotne_prager.py:121-122); hi_mode "zuk"
+    hi_kT_eta: float | None = None
 
 
 @dataclass
@@ -77,6 +79,10 @@ class StepParams:
     return_prob: float | None = None
     k_b: float | None = None
     min_core_rxn_dt: float = 0.0  # params.minimum_core_reaction_dt (:636)
+    # with use_hi: "reference_gpu" (the reference stepper's D(r), :741-751) or "zuk"
+    # (MobilityTensor.relative_translational_diffusion, rotne_prager.py:177-200)
+    hi_mode: str = "reference_gpu"
+    save_interval: int = 10  # path / energy rows every save_interval steps (:579-581)
 
 
 @dataclass
@@ -96,6 +102,8 @@ class StepResult:
     state: np.ndarray = field(default=None)  # state-machine state of every trajectory at the end
     sm_fires_discrete: np.ndarray = field(default=None)  # per reaction
     sm_fires_bridge: np.ndarray = field(default=None)
+    pos: np.ndarray = field(default=None)  # (N, 3) centroids at the end (the pose where each trajectory stopped)
+    q: np.ndarray = field(default=None)  # (N, 4) quaternions at the end
 
 
 def sm_tables(state_before, state_after, first_state=None):
@@ -239,7 +247,31 @@ def adaptive_dt(r_sr, sys: StepSystem, prm: StepParams, rxn_coord=None):
     return dt_arr
 
 
+def zuk_diffusion(r, a, b, kT_eta, D0):
+    """D0 - (2/3) tr M12(r) with the three-regime RPY tensor of rotne_prager.py:67-124 (whose
+    trace is kBT/eta (3 tt_I + tt_uu)), clamped at 1e-12 (:177-200); vectorised over r."""
+    r = np.asarray(r, dtype=np.float64)
+    PI = math.pi
+    r2 = r * r
+    r3 = r2 * r
+    s2 = a * a + b * b
+    with np.errstate(divide="ignore", invalid="ignore"):
+        far_I = (1.0 + s2 / (3.0 * r2)) / (8.0 * PI * r)
+        far_uu = (1.0 - s2 / r2) / (8.0 * PI * r)
+        am2 = (a - b) ** 2
+        den = 6.0 * 32.0 * PI * a * b * r3
+        mid_I = (16.0 * r3 * (a + b) - (am2 + 3.0 * r2) ** 2) / den
+        mid_uu = 3.0 * (am2 - r2) ** 2 / den
+    in_I = 1.0 / (6.0 * PI * max(a, b))
+    tI = np.where(r > a + b, far_I, np.where(r > abs(a - b), mid_I, in_I))
+    tuu = np.where(r > a + b, far_uu, np.where(r > abs(a - b), mid_uu, 0.0))
+    tr = np.where(r < 1e-10, 0.0, kT_eta * (3.0 * tI + tuu))
+    return np.maximum(D0 - (2.0 / 3.0) * tr, 1e-12)
+
+
 def hi_diffusion(r_sr, sys: StepSystem, prm: StepParams):
+    if prm.use_hi and prm.hi_mode == "zuk":
+        return zuk_diffusion(r_sr, float(sys.r_h_rec), float(sys.r_h_lig), float(sys.hi_kT_eta), sys.D_t)
     if prm.use_hi:
         Df, pi8, a2, ainv = hi_constants(sys.r_h_rec, sys.r_h_lig)
         rm1 = 1.0 / np.maximum(r_sr, np.full_like(r_sr, 0.01))
@@ -281,6 +313,19 @@ class StepStats:
         self.contact_total = 0
         self.trans_bins = np.linspace(0, float(r_esc * 1.2), 51)
         self.trans = np.zeros((50, 50), dtype=np.int64)
+        self.path_steps = []  # (n, 8) per recorded step: traj, step, x, y, z, q0, q1, q2
+        self.energy_steps = []  # (n, 6) per recorded step: traj, step, fx, fy, fz, dt
+
+    def trace(self, sr_idx, pos, q, steps, forces, dt_arr, save_interval):
+        """Path and energy rows of the trajectories that stepped at a step index that is a multiple of
+        save_interval (gpu_batch_simulator.py:1319-1340): pose after the step, force and dt of it."""
+        on = steps[sr_idx] % save_interval == 0
+        if not np.any(on):
+            return
+        i = sr_idx[on]
+        st = steps[i].astype(np.float64)
+        self.path_steps.append(np.column_stack([i.astype(np.float64), st, pos[i], q[i][:, :3]]))
+        self.energy_steps.append(np.column_stack([i.astype(np.float64), st, forces[on], dt_arr[on]]))
 
     def encounter(self, idx, pos, q, steps, bridge):
         self.enc_pos[idx] = pos[idx]
@@ -571,6 +616,7 @@ def run(sys: StepSystem, prm: StepParams, noise: str = "pcg64", termination: str
                         status[g] = 1
                         stats.encounter(g, pos, q, n_steps, bridge=True)
         stats.step(sr_idx, pos, q, n_steps, dt_arr, old_d, cutoffs)
+        stats.trace(sr_idx, pos, q, n_steps, forces, dt_arr, prm.save_interval)
         n_steps[sr_idx] += 1
         total_steps += int(sr_mask.sum())
         done = int((status != 0).sum())
@@ -590,4 +636,4 @@ def run(sys: StepSystem, prm: StepParams, noise: str = "pcg64", termination: str
                       n_escaped=int((status == 2).sum()), n_max_steps=n_max, total_steps=total_steps,
                       loop_steps=loop_steps, return_prob=rp, k_b=kb, n_returns=n_returns,
                       n_overlap_rejected=n_overlap, stats=stats, state=state, sm_fires_discrete=fires_d,
-                      sm_fires_bridge=fires_b)
+                      sm_fires_bridge=fires_b, pos=pos, q=q)

@@ -40,7 +40,12 @@ class BdSimParams(C.Structure):
                 ("D_r", C.c_double), ("q_rec_total", C.c_double), ("q_lig_total", C.c_double),
                 ("adt_debye", C.c_double), ("r_hydro_rec", C.c_double), ("r_hydro_lig", C.c_double),
                 ("precision", C.c_int32), ("torque_mode", C.c_int32), ("slots", C.c_int32),
-                ("id_offset", C.c_int64), ("stats", C.c_int32), ("min_core_rxn_dt", C.c_double)]
+                ("id_offset", C.c_int64), ("stats", C.c_int32), ("min_core_rxn_dt", C.c_double),
+                ("save_interval", C.c_int32), ("trace_capacity", C.c_int64), ("hi_mode", C.c_int32),
+                ("hi_kT_eta", C.c_double)]
+
+
+HI_REFERENCE_GPU, HI_ZUK = 0, 1
 
 
 _D = C.POINTER(C.c_double)
@@ -100,6 +105,8 @@ SIGNATURES = {
     "bd_sim_outcomes": (C.c_int, [P, i8p, i32p, i32p]),
     "bd_sim_stats": (C.c_int, [P, C.POINTER(BdStatsOut)]),
     "bd_sim_live": (C.c_int, [P, i32p]),
+    "bd_sim_hi_diffusion": (C.c_int, [P, C.c_int, dp, dp]),
+    "bd_sim_traces": (C.c_int, [P, dp, dp, C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "bd_sim_capacity": (C.c_int, [P, i32p]),
     "bd_set_reaction_states": (C.c_int, [P, C.c_int, i32p, i32p, C.c_int, C.POINTER(C.c_uint8)]),
     "bd_sim_reaction_fires": (C.c_int, [P, u64p, u64p, C.c_int]),

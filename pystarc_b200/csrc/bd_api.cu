@@ -464,11 +464,52 @@ int n_charged(const BdHandle* h) {
   return n;
 }
 
-int launch_group(const BdHandle* h) {
+// Run constants of the stepper from the caller's parameters (pointers left null).
+void sim_constants(const BdSimParams* p, const DevSystem& S, DevSim& P) {
+  P = DevSim{};
+  P.n_traj = p->n_traj;
+  P.id_offset = p->id_offset;
+  P.k0 = (uint32_t)(p->seed & 0xffffffffull);
+  P.k1 = (uint32_t)(p->seed >> 32);
+  P.r_b = p->r_start;
+  P.r_esc = p->r_escape;
+  P.return_prob = p->return_prob;
+  P.max_steps = p->max_steps;
+  P.max_dt = p->max_dt;
+  P.min_core_dt = p->min_core_dt;
+  P.min_core_rxn_dt = p->min_core_rxn_dt;
+  P.use_hi = p->use_hi;
+  P.overlap = p->overlap && S.n_chunks > 0;
+  P.D_t = p->D_t;
+  P.D_r = p->D_r;
+  // adaptive dt force criterion: dielectric hard-coded to 78 (gpu_batch_simulator.py:622-629)
+  P.adt_V0 = p->q_rec_total * p->q_lig_total / (4.0 * kPi * (78.0 * kEps0));
+  P.adt_has_force = std::fabs(P.adt_V0) > 1e-9;
+  P.adt_debye = p->adt_debye;
+  P.adt_inv_debye = 1.0 / p->adt_debye;
+  // HI constants, mu = 0.243 hard-coded (gpu_batch_simulator.py:741-751)
+  P.hi_Df = 1.0 / 0.243;
+  if (p->use_hi) {
+    const double a0 = p->r_hydro_rec, a1 = p->r_hydro_lig;
+    P.hi_a2 = 0.5 * (a0 * a0 + a1 * a1);
+    P.hi_ainv = (P.hi_Df / (6.0 * kPi * a0) + P.hi_Df / (6.0 * kPi * a1)) / P.hi_Df;
+  }
+  // Zuk RPY coupling (hydrodynamics/rotne_prager.py:67-124)
+  P.hi_mode = p->hi_mode;
+  P.zuk_a = p->r_hydro_rec;
+  P.zuk_b = p->r_hydro_lig;
+  P.zuk_kTeta = p->hi_kT_eta;
+}
+
+// Launch group for a run with overlap rejection on or off: the autotuned or user
+// choice, else the default for this system.
+int launch_group_for(const BdHandle* h, int overlap) {
   if (h->launch_user) return h->group;
-  const bool sweeps = h->S.born_rev || (h->sp.overlap && !h->rec.empty());
+  const bool sweeps = h->S.born_rev || (overlap && !h->rec.empty());
   return default_group(n_charged(h), sweeps);
 }
+
+int launch_group(const BdHandle* h) { return launch_group_for(h, h->sp.overlap); }
 
 int eval_grid_blocks(BdHandle* h, long long n, int G, int block) {
   const long long groups = (n + 0);
@@ -813,6 +854,11 @@ int bd_sim_configure(BdHandle* h, const BdSimParams* p) {
   if (p->precision != BD_PREC_FP64 && p->precision != BD_PREC_MIXED) return fail(h, BD_ERR_ARG, "bad precision");
   if (p->torque_mode != BD_TORQUE_ZERO && p->torque_mode != BD_TORQUE_CENTROID) return fail(h, BD_ERR_ARG, "bad torque");
   if (p->use_hi && !(p->r_hydro_rec > 0 && p->r_hydro_lig > 0)) return fail(h, BD_ERR_ARG, "HI needs hydro radii");
+  if (p->hi_mode != BD_HI_REFERENCE_GPU && p->hi_mode != BD_HI_ZUK) return fail(h, BD_ERR_ARG, "bad hi_mode");
+  if (p->use_hi && p->hi_mode == BD_HI_ZUK && !(p->hi_kT_eta > 0))
+    return fail(h, BD_ERR_ARG, "BD_HI_ZUK needs hi_kT_eta > 0");
+  if (p->trace_capacity < 0 || (p->stats && p->trace_capacity > 0 && p->save_interval <= 0))
+    return fail(h, BD_ERR_ARG, "traces need trace_capacity >= 0 and save_interval > 0");
   int rc = finalize(h);
   if (rc) return rc;
   CK(h, cudaSetDevice(h->device));
@@ -857,34 +903,7 @@ int bd_sim_configure(BdHandle* h, const BdSimParams* p) {
   if ((rc = dev_alloc(h, h->sim_allocs, &q, C_NUM * sizeof(unsigned long long)))) return rc;
   h->d_ctr = (unsigned long long*)q;
   DevSim& P = h->P;
-  P = DevSim{};
-  P.n_traj = p->n_traj;
-  P.id_offset = p->id_offset;
-  P.k0 = (uint32_t)(p->seed & 0xffffffffull);
-  P.k1 = (uint32_t)(p->seed >> 32);
-  P.r_b = p->r_start;
-  P.r_esc = p->r_escape;
-  P.return_prob = p->return_prob;
-  P.max_steps = p->max_steps;
-  P.max_dt = p->max_dt;
-  P.min_core_dt = p->min_core_dt;
-  P.min_core_rxn_dt = p->min_core_rxn_dt;
-  P.use_hi = p->use_hi;
-  P.overlap = p->overlap && h->S.n_chunks > 0;
-  P.D_t = p->D_t;
-  P.D_r = p->D_r;
-  // adaptive dt force criterion: dielectric hard-coded to 78 (gpu_batch_simulator.py:622-629)
-  P.adt_V0 = p->q_rec_total * p->q_lig_total / (4.0 * kPi * (78.0 * kEps0));
-  P.adt_has_force = std::fabs(P.adt_V0) > 1e-9;
-  P.adt_debye = p->adt_debye;
-  P.adt_inv_debye = 1.0 / p->adt_debye;
-  // HI constants, mu = 0.243 hard-coded (gpu_batch_simulator.py:741-751)
-  P.hi_Df = 1.0 / 0.243;
-  if (p->use_hi) {
-    const double a0 = p->r_hydro_rec, a1 = p->r_hydro_lig;
-    P.hi_a2 = 0.5 * (a0 * a0 + a1 * a1);
-    P.hi_ainv = (P.hi_Df / (6.0 * kPi * a0) + P.hi_Df / (6.0 * kPi * a1)) / P.hi_Df;
-  }
+  sim_constants(p, h->S, P);
   P.ctr = h->d_ctr;
   if ((rc = dev_alloc(h, h->sim_allocs, &q, (size_t)p->n_traj))) return rc;
   P.out_status = (int8_t*)q;
@@ -931,6 +950,14 @@ int bd_sim_configure(BdHandle* h, const BdSimParams* p) {
     st.trans_edges = st.rad_edges + ST_RAD_BINS + 1;
     st.ms_radii = st.trans_edges + ST_TRANS + 1;
     P.stats = 1;
+    if (p->trace_capacity > 0) {
+      if ((rc = dev_alloc(h, h->sim_allocs, &q, (size_t)p->trace_capacity * 8 * sizeof(double)))) return rc;
+      P.trace_path = (double*)q;
+      if ((rc = dev_alloc(h, h->sim_allocs, &q, (size_t)p->trace_capacity * 6 * sizeof(double)))) return rc;
+      P.trace_energy = (double*)q;
+      P.trace_cap = p->trace_capacity;
+      P.save_interval = p->save_interval;
+    }
   }
   h->sim_ready = true;
   h->graph_K = -1;
@@ -1190,6 +1217,52 @@ int bd_sim_live(BdHandle* h, int32_t* n_live) {
   return BD_OK;
 }
 
+int bd_sim_traces(BdHandle* h, double* path, double* energy, int64_t cap, int64_t* n_rows, int64_t* n_dropped) {
+  if (!h || !n_rows || !n_dropped || cap < 0) return fail(h, BD_ERR_ARG, "bd_sim_traces: bad arguments");
+  if (!h->sim_ready) return fail(h, BD_ERR_STATE, "no simulation configured");
+  *n_rows = 0;
+  *n_dropped = 0;
+  if (!h->P.stats || h->P.trace_cap <= 0) return BD_OK;
+  CK(h, cudaSetDevice(h->device));
+  CK(h, cudaDeviceSynchronize());
+  unsigned long long claimed = 0;
+  CK(h, cudaMemcpy(&claimed, h->d_ctr + C_TRACE, sizeof claimed, cudaMemcpyDeviceToHost));
+  const long long kept = std::min<long long>((long long)claimed, h->P.trace_cap);
+  const long long n = std::min<long long>(kept, cap);
+  if (path && n > 0) CK(h, cudaMemcpy(path, h->P.trace_path, (size_t)n * 8 * sizeof(double), cudaMemcpyDeviceToHost));
+  if (energy && n > 0)
+    CK(h, cudaMemcpy(energy, h->P.trace_energy, (size_t)n * 6 * sizeof(double), cudaMemcpyDeviceToHost));
+  *n_rows = n;
+  *n_dropped = (long long)claimed - kept;
+  return BD_OK;
+}
+
+int bd_sim_hi_diffusion(BdHandle* h, int n, const double* r, double* D) {
+  if (!h || (n > 0 && (!r || !D)) || n < 0) return fail(h, BD_ERR_ARG, "bd_sim_hi_diffusion: bad arguments");
+  if (!h->sim_ready) return fail(h, BD_ERR_STATE, "no simulation configured");
+  if (n == 0) return BD_OK;
+  CK(h, cudaSetDevice(h->device));
+  std::vector<void*> tmp;
+  void *dr, *dD;
+  int rc;
+  if ((rc = dev_alloc(h, tmp, &dr, (size_t)n * sizeof(double))) || (rc = dev_alloc(h, tmp, &dD, (size_t)n * sizeof(double)))) {
+    free_list(tmp);
+    return rc;
+  }
+  cudaError_t e = cudaMemcpy(dr, r, (size_t)n * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    if (h->sp.precision == BD_PREC_FP64)
+      hi_diffusion_kernel<double><<<(n + 255) / 256, 256>>>(h->P, n, (const double*)dr, (double*)dD);
+    else
+      hi_diffusion_kernel<float><<<(n + 255) / 256, 256>>>(h->P, n, (const double*)dr, (double*)dD);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(D, dD, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost);
+  free_list(tmp);
+  CK(h, e);
+  return BD_OK;
+}
+
 int bd_sim_capacity(BdHandle* h, int32_t* cap) {
   if (!h || !cap) return BD_ERR_ARG;
   if (!h->sim_ready) return fail(h, BD_ERR_STATE, "no simulation configured");
@@ -1318,6 +1391,9 @@ int bd_internal_run_noalloc(BdHandle* h, const BdSimParams* p, unsigned char* sc
   if (p->precision != BD_PREC_FP64 && p->precision != BD_PREC_MIXED) return fail(h, BD_ERR_ARG, "bad precision");
   if (p->torque_mode != BD_TORQUE_ZERO && p->torque_mode != BD_TORQUE_CENTROID) return fail(h, BD_ERR_ARG, "bad torque");
   if (p->use_hi && !(p->r_hydro_rec > 0 && p->r_hydro_lig > 0)) return fail(h, BD_ERR_ARG, "HI needs hydro radii");
+  if (p->hi_mode != BD_HI_REFERENCE_GPU && p->hi_mode != BD_HI_ZUK) return fail(h, BD_ERR_ARG, "bad hi_mode");
+  if (p->use_hi && p->hi_mode == BD_HI_ZUK && !(p->hi_kT_eta > 0))
+    return fail(h, BD_ERR_ARG, "BD_HI_ZUK needs hi_kT_eta > 0");
   if (K <= 0 || max_launches <= 0) return fail(h, BD_ERR_ARG, "steps_per_launch and max_launches must be > 0");
   if (p->slots > max_slots)
     return fail(h, BD_ERR_ARG, "bd_sim_run_noalloc: %d slots requested, the static scratch holds at most %d",
@@ -1326,6 +1402,10 @@ int bd_internal_run_noalloc(BdHandle* h, const BdSimParams* p, unsigned char* sc
     return fail(h, BD_ERR_STATE,
                 "bd_sim_run_noalloc: the system is not on the device yet; its upload allocates, so call "
                 "bd_sim_configure or an evaluation once before");
+  if (h->sur)
+    return fail(h, BD_ERR_STATE,
+                "bd_sim_run_noalloc runs the exact-force stepper only; remove the surrogate "
+                "(bd_sim_set_surrogate with NULL) first");
   CK(h, cudaSetDevice(h->device));
   const int C = (int)std::min<long long>(p->slots > 0 ? p->slots : max_slots, p->n_traj);
   // scratch layout: two slot buffers, two live counts, the counters
@@ -1345,31 +1425,7 @@ int bd_internal_run_noalloc(BdHandle* h, const BdSimParams* p, unsigned char* sc
   unsigned long long* ctr = (unsigned long long*)carve(cur_p, C_NUM * sizeof(unsigned long long));
   if ((size_t)(cur_p - scratch) > scratch_bytes) return fail(h, BD_ERR_ARG, "scratch layout exceeds the array");
   DevSim P{};
-  P.n_traj = p->n_traj;
-  P.id_offset = p->id_offset;
-  P.k0 = (uint32_t)(p->seed & 0xffffffffull);
-  P.k1 = (uint32_t)(p->seed >> 32);
-  P.r_b = p->r_start;
-  P.r_esc = p->r_escape;
-  P.return_prob = p->return_prob;
-  P.max_steps = p->max_steps;
-  P.max_dt = p->max_dt;
-  P.min_core_dt = p->min_core_dt;
-  P.min_core_rxn_dt = p->min_core_rxn_dt;
-  P.use_hi = p->use_hi;
-  P.overlap = p->overlap && h->S.n_chunks > 0;
-  P.D_t = p->D_t;
-  P.D_r = p->D_r;
-  P.adt_V0 = p->q_rec_total * p->q_lig_total / (4.0 * kPi * (78.0 * kEps0));
-  P.adt_has_force = std::fabs(P.adt_V0) > 1e-9;
-  P.adt_debye = p->adt_debye;
-  P.adt_inv_debye = 1.0 / p->adt_debye;
-  P.hi_Df = 1.0 / 0.243;
-  if (p->use_hi) {
-    const double a0 = p->r_hydro_rec, a1 = p->r_hydro_lig;
-    P.hi_a2 = 0.5 * (a0 * a0 + a1 * a1);
-    P.hi_ainv = (P.hi_Df / (6.0 * kPi * a0) + P.hi_Df / (6.0 * kPi * a1)) / P.hi_Df;
-  }
+  sim_constants(p, h->S, P);
   P.ctr = ctr;
   P.out_status = out_status;
   P.out_steps = out_steps;
@@ -1386,7 +1442,7 @@ int bd_internal_run_noalloc(BdHandle* h, const BdSimParams* p, unsigned char* sc
   CK(h, cudaMemcpyAsync(ctr + C_PENDING, &started, sizeof started, cudaMemcpyHostToDevice, s));
   CK(h, cudaMemcpyAsync(live, &c_live, sizeof c_live, cudaMemcpyHostToDevice, s));
   CK(h, cudaStreamSynchronize(s));
-  const int G = launch_group(h);
+  const int G = launch_group_for(h, p->overlap);
   void* fn = kernel_for(p->precision, G, p->torque_mode, 2);
   const size_t smem = stepper_smem(h->S, P, fn);
   const int blocks = persistent_blocks(h, fn, h->block, smem);

@@ -35,6 +35,7 @@ enum : int {
   C_NONFINITE,      // steps that produced a non-finite pose (trajectory stopped)
   C_SLOT_CURSOR,    // dynamic slot cursor of the current launch
   C_LIVE_NEXT,      // live-slot count being built by the compaction
+  C_TRACE,          // path/energy trace rows claimed (may exceed the capacity)
   C_SM_DISCRETE,    // BD_MAX_PAIRS counters: state-machine reactions fired by the discrete test
   C_SM_BRIDGE = C_SM_DISCRETE + BD_MAX_PAIRS,  // BD_MAX_PAIRS counters: fired by the Brownian bridge
   C_NUM = C_SM_BRIDGE + BD_MAX_PAIRS
@@ -140,12 +141,19 @@ struct DevSim {
   double adt_V0, adt_inv_debye, adt_debye;
   int adt_has_force;
   double hi_Df, hi_ainv, hi_a2;
+  int hi_mode;                 // BD_HI_REFERENCE_GPU or BD_HI_ZUK
+  double zuk_a, zuk_b, zuk_kTeta;  // hydrodynamic radii and kBT/eta of the Zuk coupling
   unsigned long long* ctr;
   int8_t* out_status;
   int* out_steps;
   int* out_returns;
   DevStats st;
   int stats;  // collect DevStats (needs SH_NUM * 4 B of dynamic shared memory per block)
+  // path / energy traces (with stats): rows of 8 and 6 doubles every save_interval steps
+  int save_interval;
+  long long trace_cap;
+  double* trace_path;
+  double* trace_energy;
 };
 
 struct SlotBuf {

@@ -661,11 +661,39 @@ __device__ __forceinline__ double adaptive_dt(const DevSim& P, double r, double 
   return dt;
 }
 
-// Relative translational diffusion with HI (far-field RPY along the line of
-// centres, mu = 0.243, clamp 1e-6; gpu_batch_simulator.py:741-751, :1074-1084).
+// Relative translational diffusion D_t - (2/3) tr M12(r) with the Zuk et al. (2014)
+// three-regime RPY coupling M12 = kBT/eta (tt_I I + tt_uu r^ r^T), whose trace is
+// kBT/eta (3 tt_I + tt_uu), clamped at 1e-12 (hydrodynamics/rotne_prager.py:67-124, :177-200).
+template <typename FT>
+__device__ __forceinline__ double zuk_diffusion(const DevSim& P, double rd) {
+  if (rd < 1e-10) return fmax(P.D_t, 1e-12);  // M12 = 0 at coincident centres
+  const FT pi = (FT)3.14159265358979323846;
+  const FT r = (FT)rd, a = (FT)P.zuk_a, b = (FT)P.zuk_b;
+  const FT r2 = r * r, r3 = r2 * r;
+  FT tI, tuu;
+  if (r > a + b) {  // far field
+    const FT den = (FT)8 * pi * r, s2 = a * a + b * b;
+    tI = ((FT)1 + s2 / ((FT)3 * r2)) / den;
+    tuu = ((FT)1 - s2 / r2) / den;
+  } else if (r > fabs(a - b)) {  // partial overlap
+    const FT am2 = (a - b) * (a - b), den = (FT)192 * pi * a * b * r3, w = am2 + (FT)3 * r2;
+    tI = ((FT)16 * r3 * (a + b) - w * w) / den;
+    tuu = (FT)3 * (am2 - r2) * (am2 - r2) / den;
+  } else {  // one sphere inside the other: self-mobility of the larger
+    tI = (FT)1 / ((FT)6 * pi * fmax(a, b));
+    tuu = 0;
+  }
+  const FT tr = (FT)P.zuk_kTeta * ((FT)3 * tI + tuu);
+  return fmax(P.D_t - (2.0 / 3.0) * (double)tr, 1e-12);
+}
+
+// Relative translational diffusion with HI.  Reference GPU mode: far-field RPY along
+// the line of centres, mu = 0.243, clamp 1e-6 (gpu_batch_simulator.py:741-751,
+// :1074-1084); Zuk mode: zuk_diffusion.
 template <typename FT>
 __device__ __forceinline__ double hi_diffusion(const DevSim& P, double r) {
   if (!P.use_hi) return P.D_t;
+  if (P.hi_mode == 1) return zuk_diffusion<FT>(P, r);
   const FT rm1 = (FT)1 / (FT)fmax(r, 0.01);
   const FT rm3 = rm1 * rm1 * rm1;
   const FT Df = (FT)P.hi_Df;
@@ -912,6 +940,31 @@ __device__ __forceinline__ void stats_step(const DevSystem& S, const DevSim& P, 
     if (pair_distance(S, c0, R, p) < S.rx_cut[p]) atomicAdd(sh + SH_CONTACT + p, 1u);
 }
 
+// Path and energy rows of one completed step s (gpu_batch_simulator.py:1319-1340):
+// [id, s, x, y, z, q0, q1, q2] after the step and [id, s, fx, fy, fz, dt] of the step.
+__device__ __forceinline__ void trace_step(const DevSim& P, const Traj& tr, uint32_t s, const double F[3],
+                                           double dt) {
+  if (P.trace_cap <= 0 || (s % (uint32_t)P.save_interval) != 0u) return;
+  const unsigned long long i = atomicAdd(P.ctr + C_TRACE, 1ull);
+  if (i >= (unsigned long long)P.trace_cap) return;
+  double* p = P.trace_path + 8 * i;
+  p[0] = (double)tr.id;
+  p[1] = (double)s;
+  p[2] = tr.c[0];
+  p[3] = tr.c[1];
+  p[4] = tr.c[2];
+  p[5] = tr.q[0];
+  p[6] = tr.q[1];
+  p[7] = tr.q[2];
+  double* e = P.trace_energy + 6 * i;
+  e[0] = (double)tr.id;
+  e[1] = (double)s;
+  e[2] = F[0];
+  e[3] = F[1];
+  e[4] = F[2];
+  e[5] = dt;
+}
+
 // Pose at reaction; `bridge` marks a reaction found by the Brownian bridge.
 __device__ __forceinline__ void stats_encounter(const DevSim& P, const Traj& tr, uint32_t s, bool bridge) {
   const DevStats& st = P.st;
@@ -987,6 +1040,7 @@ __device__ __forceinline__ int bd_step(const DevSystem& S, const DevSim& P, Traj
   const int st = step_end(S, P, key, s, tr, R, cn, qn, moved, dt, tl);
   if (P.stats && lane == 0) {
     stats_step(S, P, tr, s, r_prev, dt, c0, R, sh);
+    trace_step(P, tr, s, F, dt);
     if (st == ST_REACTED) stats_encounter(P, tr, s, true);
   }
   return st;
@@ -1039,6 +1093,13 @@ __global__ void window_kernel(const float* __restrict__ d, float4* __restrict__ 
     }
     w[n] = make_float4(v[0], v[1], v[2], v[3]);
   }
+}
+
+// D(r) of the stepper at n distances (parity entry point bd_sim_hi_diffusion).
+template <typename FT>
+__global__ void hi_diffusion_kernel(DevSim P, int n, const double* __restrict__ r, double* __restrict__ D) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) D[i] = hi_diffusion<FT>(P, r[i]);
 }
 
 // Fill `n_slots` slots with the first trajectories of the pending pool.
@@ -1233,6 +1294,7 @@ __global__ void __launch_bounds__(256, MINB) step_kernel_warp(DevSystem S, DevSi
         st = step_end(S, P, key, s, tr, R, cn, qn, !ovl, dt, tl);
         if (P.stats) {
           stats_step(S, P, tr, s, r_prev, dt, c0, R, sh.stats);
+          trace_step(P, tr, s, F, dt);
           if (st == ST_REACTED) stats_encounter(P, tr, s, true);
         }
       }

@@ -2,12 +2,12 @@
 //
 // Some host applications cannot call cudaMalloc when they want to run trajectories:
 // an application whose own allocator has already reserved the GPU's memory (a
-// framework's caching pool), a process under a device-memory quota, or code that
-// runs while another library is capturing a CUDA graph (cudaMalloc is not allowed
-// during global-mode capture).  For them this entry point runs a whole batch of
-// trajectories without allocating: the live-slot pool (two slot buffers), the live
-// counts and the counters live in the file-scope device array below, and the
-// per-trajectory outputs and final counters go to arrays the caller owns.
+// framework's caching pool), or a process under a device-memory quota.  For them this
+// entry point runs a whole batch of trajectories without allocating: the live-slot
+// pool (two slot buffers), the live counts and the counters live in the file-scope
+// device array below, and the per-trajectory outputs and final counters go to arrays
+// the caller owns.  The call copies a few words between host and device and waits on
+// its stream, so it returns only when the batch is done.
 //
 // The array is a fixed 9.2 MB (room for BD_NOALLOC_MAX_SLOTS = 65536 live slots);
 // every GPU that loads the library keeps it until the process exits.  All calls

@@ -21,15 +21,14 @@ It does steps 5-6 with ``B200ForceEngine`` and ``B200BatchSimulator``:
 * ``reaction_pathway``   -- auto_detect_reactions and the state-machine parser
                             (geometry.py:321-621, pipeline.py:225-291)
 * ``build`` / ``run``    -- the GPU branch of step 6 (pipeline.py:292-351) and the
-                            results.json record of output_writer.write_all (:76-116)
+                            output files of output_writer.write_all (:15-304),
+                            written by ``pystarc_b200.output``
 
 Usage: ``python -m pystarc_b200.pipeline input.xml``.
 """
 
 from __future__ import annotations
 
-import json
-import math
 import re
 import shutil
 import sys
@@ -469,34 +468,18 @@ def build(xml_path, *, precision="fp64", torque_mode="zero", device=0, **sim_opt
     return Prepared(cfg, engine, sim, mob, float(mob.relative_translational_diffusion()))
 
 
-def results_record(result, sim_data, k_b, D_rel, confidence):
-    """The results.json record of output_writer.write_all (:76-116)."""
-    k_on = result.rate_constant(D_rel, k_b)
-    k_lo, k_hi = result.rate_constant_ci(D_rel, k_b, confidence)
-    p_lo, p_hi = result.reaction_probability_ci(confidence)
-    data = {"k_on": k_on, "k_on_low": k_lo, "k_on_high": k_hi, "k_on_units": "M-1 s-1",
-            "P_rxn": result.reaction_probability, "P_rxn_low": p_lo, "P_rxn_high": p_hi, "k_b": k_b,
-            "k_b_units": "A3/ps", "D_rel": D_rel, "D_rel_units": "A2/ps", "n_trajectories": result.n_trajectories,
-            "n_reacted": result.n_reacted, "n_escaped": result.n_escaped, "n_max_steps": result.n_max_steps,
-            "r_start": result.r_start, "r_escape": result.r_escape, "wall_time_sec": result.elapsed_sec,
-            "steps_per_sec": result.steps_per_sec, "confidence_level": confidence}
-    if k_on > 0:
-        data["log10_k_on"] = math.log10(k_on)
-    if "completed_reactions" in sim_data:
-        data["completed_reactions"] = sim_data["completed_reactions"]
-    return data
-
-
 def run(xml_path, **options):
-    """Build, run every trajectory and write results.json and sim_data.npz (the per-trajectory and
-    histogram arrays under the reference's sim_data keys) into the work directory."""
+    """Build, run every trajectory and write the reference's output files (results.json,
+    trajectories.csv, ... energetics.npz) plus sim_data.npz (the per-trajectory and histogram
+    arrays under the reference's sim_data keys) into the work directory."""
+    from .output import write_all
+
     prep = build(xml_path, **options)
     result = prep.simulator.run()
     sd = result.sim_data
     W = prep.cfg.work_path
-    if prep.cfg.outputs.results_json:
-        rec = results_record(result, sd, prep.simulator._k_b, prep.D_rel, prep.cfg.confidence_interval)
-        (W / "results.json").write_text(json.dumps(rec, indent=2))
+    write_all(W, result, sd, prep.cfg.outputs, prep.simulator._k_b, prep.D_rel, prep.cfg.confidence_interval,
+              verbose=False)
     arrays = {k: np.asarray(v) for k, v in sd.items() if k != "completed_reactions" and not isinstance(v, list)}
     np.savez_compressed(W / "sim_data.npz", **arrays)
     return prep, result

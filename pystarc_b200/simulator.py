@@ -156,6 +156,13 @@ def state_machine(pathway_set):
             "states": list(labels), "terminal": terminal, "first_state": first}
 
 
+def zuk_kT_eta(mob):
+    """kBT/eta of the RPY coupling: the geometric mean sqrt(D_t1 6 pi a1 D_t2 6 pi a2)
+    (pystarc/hydrodynamics/rotne_prager.py:121-122)."""
+    a, b = float(mob.radius1), float(mob.radius2)
+    return math.sqrt(float(mob.D_trans1) * 6.0 * math.pi * a * float(mob.D_trans2) * 6.0 * math.pi * b)
+
+
 class B200BatchSimulator:
     """Batched BD of all trajectories on one GPU.
 
@@ -163,12 +170,18 @@ class B200BatchSimulator:
     "mixed"), ``torque_mode`` ("zero" or "centroid"), ``termination``
     ("reference": stop once 99.5 % are done, as the reference loop does;
     "complete": run every trajectory to an outcome or to ``max_steps``),
-    ``steps_per_launch`` (K) and ``launches_per_poll``.
+    ``steps_per_launch`` (K), ``launches_per_poll`` and ``hi_mode`` (with
+    hydrodynamic interactions: "reference_gpu", the reference GPU stepper's
+    line-of-centres D(r), or "zuk", D_t - (2/3) tr M12(r) with the three-regime
+    RPY tensor of MobilityTensor, pystarc/hydrodynamics/rotne_prager.py:67-124, :177-200).
     """
 
     def __init__(self, mol1, mol2, mob, pathway_set, params, batch_engine, *, precision=None, torque_mode=None,
                  termination="reference", steps_per_launch=64, launches_per_poll=8, slots=0, id_offset=0,
-                 stats=None, surrogate=None, verbose=False):
+                 stats=None, surrogate=None, hi_mode="reference_gpu", trace_capacity=None, verbose=False):
+        if hi_mode not in ("reference_gpu", "zuk"):
+            raise ValueError("hi_mode must be 'reference_gpu' or 'zuk'")
+        self.hi_mode = hi_mode
         if not hasattr(batch_engine, "handle"):
             raise TypeError("batch_engine must be a B200ForceEngine")
         self.mol1, self.mol2, self.mob = mol1, mol2, mob
@@ -184,6 +197,15 @@ class B200BatchSimulator:
         self.id_offset = int(id_offset)
         # per-step statistics for write_all: on when the pipeline attached an output config
         self.stats = bool(getattr(params, "_output_cfg", None) is not None) if stats is None else bool(stats)
+        # path / energy traces every save_interval steps (gpu_batch_simulator.py:579-581, :1319-1340): rows
+        # kept on the device up to trace_capacity (default 4M rows, 448 MB); the rest are counted as dropped
+        cfg = getattr(params, "_output_cfg", None)
+        self._save_interval = max(int(getattr(cfg, "save_interval", 10) or 10), 1) if cfg is not None else 10
+        self._want_paths = bool(getattr(cfg, "full_paths", True)) if cfg is not None else True
+        self._want_energy = bool(getattr(cfg, "energetics", True)) if cfg is not None else True
+        if trace_capacity is None:
+            trace_capacity = 4_000_000 if (self._want_paths or self._want_energy) else 0
+        self.trace_capacity = int(trace_capacity) if self.stats else 0
         self.verbose = verbose
         # (MLPEnsemble, SurrogateSpec): far-field + reverse Born from the learned surrogate inside its trust region
         self.surrogate = surrogate
@@ -269,6 +291,10 @@ class B200BatchSimulator:
         sp.slots = self.slots
         sp.id_offset = self.id_offset
         sp.stats = int(self.stats)
+        sp.save_interval = self._save_interval
+        sp.trace_capacity = self.trace_capacity
+        sp.hi_mode = _lib.HI_ZUK if self.hi_mode == "zuk" else _lib.HI_REFERENCE_GPU
+        sp.hi_kT_eta = zuk_kT_eta(self.mob) if self.hi_mode == "zuk" else 0.0
         h.call("bd_sim_configure", _lib.C.byref(sp))
         if self.surrogate is not None:
             ens, spec = self.surrogate
@@ -311,13 +337,43 @@ class B200BatchSimulator:
         a["contact"] = a["contact"][:P]
         return a
 
+    def read_traces(self):
+        """Path rows [traj_id, step, x, y, z, q0, q1, q2] and energy rows [traj_id, step, fx, fy, fz, dt]
+        recorded every save_interval steps, sorted by (step, traj_id) as the reference appends them,
+        and the number of rows that did not fit the trace capacity."""
+        n = max(self.trace_capacity, 0)
+        path = np.zeros((n, 8))
+        energy = np.zeros((n, 6))
+        rows, dropped = _lib.C.c_int64(), _lib.C.c_int64()
+        self.engine.handle.call("bd_sim_traces", _lib.ptr(path), _lib.ptr(energy), n, _lib.C.byref(rows),
+                                _lib.C.byref(dropped))
+        k = rows.value
+        path, energy = path[:k], energy[:k]
+        order = np.lexsort((path[:, 0], path[:, 1]))
+        eorder = np.lexsort((energy[:, 0], energy[:, 1]))
+        return path[order], energy[eorder], int(dropped.value)
+
+    @staticmethod
+    def _per_step(rows):
+        """Rows sorted by step as a list with one array per recorded step (the reference's list)."""
+        if len(rows) == 0:
+            return []
+        cut = np.nonzero(np.diff(rows[:, 1]))[0] + 1
+        return np.split(rows, cut)
+
     def sim_data(self, status, steps, rets, total_steps):
         """The reference's ``sim_data`` dict (gpu_batch_simulator.py:1511-1557) from the device statistics.
 
-        Per-step path and energy snapshots are not recorded (``path_steps`` and
-        ``energy_steps`` are empty lists).
+        ``path_steps`` / ``energy_steps`` hold one array per recorded step (every
+        save_interval steps, as the reference records them); rows beyond the trace
+        capacity are dropped and counted in ``counters["trace_dropped"]``.
         """
         a = self.read_stats()
+        path, energy, dropped = self.read_traces() if self.trace_capacity > 0 else (np.zeros((0, 8)),
+                                                                                       np.zeros((0, 6)), 0)
+        self.counters["trace_dropped"] = dropped
+        if dropped:
+            print(f" [b200] {dropped} path/energy rows beyond the trace capacity of {self.trace_capacity} were dropped")
         outcome = status.astype(np.int32)
         outcome[(outcome != 1) & (outcome != 2)] = 0
         rx = np.where(outcome == 1)[0]
@@ -332,7 +388,8 @@ class B200BatchSimulator:
             "encounter_n_pairs": np.full(len(rx), self._rxn_n_needed, dtype=np.int64),
             "near_miss_pos": a["near_miss_pos"][esc], "near_miss_q": a["near_miss_q"][esc],
             "near_miss_traj": esc.astype(np.int64), "near_miss_dist": a["min_dist"][esc],
-            "path_steps": [], "energy_steps": [],
+            "path_steps": self._per_step(path) if self._want_paths else [],
+            "energy_steps": self._per_step(energy) if self._want_energy else [],
             "radial_bins": a["radial_edges"], "radial_counts": a["radial"].astype(np.int64),
             "angular_theta": np.linspace(0, np.pi, _lib.ST_THETA), "angular_phi": np.linspace(0, 2 * np.pi, _lib.ST_PHI),
             "angular_counts": a["angular"].astype(np.int64), "milestone_radii": a["milestone_radii"],

@@ -1,8 +1,9 @@
 """Generate golden vectors by running the UNMODIFIED reference on seeded synthetic inputs.
 
-Run in a container that has the reference checkout (default /root/reference):
+Run where a checkout of the reference exists, naming its path with ``--reference``
+or the ``PYSTARC_REFERENCE`` environment variable:
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <path to the PySTARC checkout>
 
 The reference's batched engine and stepper import ``cupy``; this script puts
 ``oracle/cupy_standin`` first on ``sys.path`` so they run on NumPy, with the
@@ -23,6 +24,7 @@ import hashlib
 import io
 import json
 import math
+import os
 import sys
 import tempfile
 from pathlib import Path
@@ -223,12 +225,19 @@ def build_sim(s, n_traj, seed, max_steps, work, sm=None, use_lj=False):
     return sim, mob
 
 
-def gen_run(out, name, s, n_traj, seed, max_steps, use_lj=False):
+def gen_run(out, name, s, n_traj, seed, max_steps, use_lj=False, trace_steps=None):
+    """A reference run: tallies, per-trajectory outcomes and statistics; with ``trace_steps`` also the
+    path and energy rows the reference records every save_interval steps, for steps below it."""
     with tempfile.TemporaryDirectory() as work:
         sim, mob = build_sim(s, n_traj, seed, max_steps, work, use_lj=use_lj)
         with quiet():
             res = sim.run()
     sd = res.sim_data
+    traces = {}
+    if trace_steps is not None:
+        for key, ncol in (("path_steps", 8), ("energy_steps", 6)):
+            rows = np.vstack(sd[key]) if len(sd[key]) else np.zeros((0, ncol))
+            traces[f"sd_{key}"] = rows[rows[:, 1] < trace_steps]
     out[name] = dict(digest=system_digest(s), n_traj=n_traj, seed=seed, max_steps=max_steps,
                      n_reacted=res.n_reacted, n_escaped=res.n_escaped, n_max_steps=res.n_max_steps,
                      total_steps=int(round(res.steps_per_sec * res.elapsed_sec)), outcome=sd["outcome"],
@@ -239,7 +248,46 @@ def gen_run(out, name, s, n_traj, seed, max_steps, use_lj=False):
                          "start_pos", "start_q", "min_dist", "step_at_min", "total_time_ps", "bb_triggered",
                          "encounter_traj", "encounter_step", "encounter_pos", "encounter_q", "near_miss_traj",
                          "near_miss_pos", "near_miss_dist", "radial_counts", "angular_counts", "milestone_flux_out",
-                         "milestone_flux_in", "contact_pair_counts", "contact_total_steps", "trans_matrix")})
+                         "milestone_flux_in", "contact_pair_counts", "contact_total_steps", "trans_matrix")},
+                     **traces)
+
+
+WRITER_FILES = ("results.json", "trajectories.csv", "encounters.csv", "near_misses.csv", "paths.npz",
+                "radial_density.csv", "angular_map.npz", "fpt_distribution.csv", "contact_frequency.csv",
+                "milestone_flux.csv", "p_commit.npz", "transition_matrix.npz", "energetics.npz", "pose_clusters.csv")
+
+
+def gen_writer(out, name, s, n_traj, seed, max_steps, save_interval):
+    """The reference's output files (pipeline/output_writer.py:15-304) for one reference run: the run's
+    sim_data and result fields (the writer's inputs) and the content of every file written."""
+    from pystarc.pipeline.input_parser import OutputConfig
+    from pystarc.pipeline.output_writer import write_all
+
+    with tempfile.TemporaryDirectory() as work:
+        sim, mob = build_sim(s, n_traj, seed, max_steps, work)
+        cfg = OutputConfig(save_interval=save_interval)
+        sim.params._output_cfg = cfg
+        with quiet():
+            res = sim.run()
+            sd = res.sim_data
+            D_rel = mob.relative_translational_diffusion()
+            written = write_all(Path(work) / "out", res, sd, cfg, sim._k_b, D_rel, 0.95)
+        rec = {}
+        for fname, path in written:
+            if fname.endswith(".npz"):
+                with np.load(path) as z:
+                    for k in z.files:
+                        rec[f"file:{fname}:{k}"] = z[k]
+            else:
+                rec[f"file:{fname}"] = np.array(Path(path).read_text())
+    arrays = {f"sd:{k}": (np.vstack(v) if len(v) else np.zeros((0, 8 if k == "path_steps" else 6)))
+              if isinstance(v, list) else np.asarray(v) for k, v in sd.items() if k != "completed_reactions"}
+    fields = {f"res:{k}": np.asarray(getattr(res, k)) for k in (
+        "n_trajectories", "n_reacted", "n_escaped", "n_max_steps", "r_start", "r_escape", "elapsed_sec",
+        "steps_per_sec", "dt")}
+    out[name] = dict(digest=system_digest(s), n_traj=n_traj, seed=seed, max_steps=max_steps,
+                     save_interval=save_interval, k_b=sim._k_b, D_rel=D_rel,
+                     written=np.array([f for f, _ in written]), **arrays, **fields, **rec)
 
 
 # State-machine reaction sets: (name, state_before, state_after, (receptor atom, ligand atom, cutoff)).
@@ -441,9 +489,12 @@ def two_sphere_example():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("PYSTARC_REFERENCE"),
+                    help="path of the PySTARC checkout (default: $PYSTARC_REFERENCE)")
     ap.add_argument("--only", nargs="*", help="regenerate only these fixtures (the manifest keeps the others)")
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("name the reference checkout with --reference or PYSTARC_REFERENCE")
     sys.path.insert(0, str(REPO / "oracle" / "cupy_standin"))
     sys.path.insert(0, str(REPO))
     sys.path.insert(1, args.reference)
@@ -460,9 +511,11 @@ def main():
         "engine_wca_c2": lambda: gen_engine_wca(out, "engine_wca_c2", c2, 64, 5.0, 11.0, 23),
         "engine_wca_c3": lambda: gen_engine_wca(out, "engine_wca_c3", c3, 48, 5.0, 11.0, 24),
         "run_two_sphere": lambda: gen_run(out, "run_two_sphere", two_sphere_example(), 2000, 11111113, 1_000_000),
-        "run_c2": lambda: gen_run(out, "run_c2", c2, 160, 424242, 400),
-        "run_c3": lambda: gen_run(out, "run_c3", c3, 64, 515151, 150),
+        "run_c2": lambda: gen_run(out, "run_c2", c2, 160, 424242, 400, trace_steps=100),
+        "run_c3": lambda: gen_run(out, "run_c3", c3, 64, 515151, 150, trace_steps=150),
         "run_lj_c2": lambda: gen_run(out, "run_lj_c2", c2, 160, 424242, 400, use_lj=True),
+        "writer_two_sphere": lambda: gen_writer(out, "writer_two_sphere", two_sphere_example(), 300, 20261205,
+                                                1_000_000, 100),
         "run_sm_two_sphere": lambda: gen_run_sm(out, "run_sm_two_sphere", two_sphere_example(), SM_TWO_SPHERE, 1000,
                                                 31337, 1_000_000),
         "run_sm_c2": lambda: gen_run_sm(out, "run_sm_c2", c2, SM_C2, 160, 434343, 600),

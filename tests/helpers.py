@@ -10,6 +10,7 @@ import numpy as np
 from oracle.forces import FarField, OracleForceEngine, OracleGrid, multipole_moments
 from oracle.stepper import StepParams, StepSystem, n_needed_of
 from pystarc_b200 import synth
+from pystarc_b200.simulator import zuk_kT_eta
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
 
@@ -82,7 +83,7 @@ def step_system(s, engine=None):
                       D_r=mob.relative_rotational_diffusion(), r_h_rec=s.r_hydro_rec, r_h_lig=s.r_hydro_lig,
                       # Molecule.total_charge sums atom by atom (pystarc/structures/molecules.py:69-70)
                       q_rec_total=sum(float(v) for v in s.rec_q), q_lig_total=sum(float(v) for v in s.lig_q),
-                      debye=s.debye)
+                      debye=s.debye, hi_kT_eta=zuk_kT_eta(mob))
 
 
 def sm_spec(g):
@@ -119,6 +120,7 @@ def sm_pathway(g):
     return st.PathwaySet(rx, first_state=first)
 
 
-def step_params(s, n_traj, seed, max_steps):
+def step_params(s, n_traj, seed, max_steps, hi_mode="reference_gpu"):
     return StepParams(n_traj=n_traj, seed=seed, r_b=s.r_start, r_esc=s.r_escape, max_steps=max_steps,
-                      max_dt=s.max_dt, use_hi=s.hi, overlap=s.overlap, kT_scale=s.temperature / 298.15)
+                      max_dt=s.max_dt, use_hi=s.hi, overlap=s.overlap, kT_scale=s.temperature / 298.15,
+                      hi_mode=hi_mode)

@@ -80,6 +80,15 @@ def test_input_xml_run_matches_the_directly_built_system(tmp_path, sm):
     assert ("completed_reactions" in rec) == sm
     sd = np.load(W / "sim_data.npz")
     assert sd["outcome"].shape == (3000,) and "radial_counts" in sd.files
+    # the reference's output files (pipeline/output_writer.py:15-304); pose clusters need > 5 reactions
+    for name in ("results.json", "trajectories.csv", "encounters.csv", "near_misses.csv", "paths.npz",
+                 "radial_density.csv", "angular_map.npz", "fpt_distribution.csv", "contact_frequency.csv",
+                 "milestone_flux.csv", "p_commit.npz", "transition_matrix.npz", "energetics.npz",
+                 "pose_clusters.csv"):
+        assert (W / name).exists(), name
+    assert len((W / "trajectories.csv").read_text().splitlines()) == 3001
+    paths = np.load(W / "paths.npz")["data"]
+    assert paths.shape[1] == 8 and np.all(paths[:, 1] % 10 == 0)
     st_a, steps_a, rets_a = prep.simulator.outcomes()
     # the same system built directly from the synthetic arrays
     eng = B200ForceEngine(**s.engine_kwargs())

@@ -309,3 +309,33 @@ def test_statistics_match_oracle(sysname, n, max_steps, group):
     np.testing.assert_allclose(sd["encounter_pos"], st.enc_pos[rx], rtol=1e-10, atol=1e-10)
     esc = sd["near_miss_traj"]
     np.testing.assert_allclose(sd["near_miss_pos"], st.nm_pos[esc], rtol=1e-10, atol=1e-10)
+
+
+@pytest.mark.parametrize("sysname,n,max_steps,group", [("c2", 96, 300, 64), ("c2", 96, 300, 8)])
+def test_path_and_energy_traces_match_oracle(sysname, n, max_steps, group):
+    """Path and energy rows every save_interval steps (gpu_batch_simulator.py:1319-1340), sorted by
+    (step, trajectory) as the reference appends them, against the oracle with the same draws."""
+    s = system(sysname)
+    sim = make_sim(s, n, max_steps, "fp64", stats=True, steps_per_launch=16, trace_capacity=100_000)
+    sim.engine.handle.call("bd_set_launch", group, 128)
+    res = sim.run()
+    sd = res.sim_data
+    st = oracle_keyed(s, n, max_steps).stats
+    assert res.counters["trace_dropped"] == 0
+    for key, mine in (("path_steps", st.path_steps), ("energy_steps", st.energy_steps)):
+        rows = np.vstack(sd[key])
+        ref = np.vstack(mine)
+        assert rows.shape == ref.shape, (key, rows.shape, ref.shape)
+        np.testing.assert_array_equal(rows[:, :2], ref[:, :2])
+        np.testing.assert_allclose(rows[:, 2:], ref[:, 2:], rtol=1e-9, atol=1e-10, err_msg=key)
+        assert all(len(np.unique(a[:, 1])) == 1 for a in sd[key])  # one array per recorded step
+    assert np.all(np.vstack(sd["path_steps"])[:, 1] % 10 == 0)
+
+
+def test_trace_capacity_drops_and_counts_extra_rows():
+    s = system("c2")
+    sim = make_sim(s, 96, 300, "fp64", stats=True, steps_per_launch=16, trace_capacity=500)
+    res = sim.run()
+    rows = np.vstack(res.sim_data["path_steps"])
+    assert len(rows) == 500
+    assert res.counters["trace_dropped"] > 0

@@ -117,6 +117,24 @@ def test_physics_constants():
                                    atol=1e-18)
 
 
+def test_zuk_relative_diffusion_is_the_rpy_trace_form():
+    """The oracle stepper's Zuk D(r) equals D_t1 + D_t2 - (2/3) tr M12(r) of the RPY tensor pinned
+    above (MobilityTensor.relative_translational_diffusion, rotne_prager.py:177-200) in all three
+    regimes: far field (r > a + b), partial overlap (|a - b| < r <= a + b), one sphere inside the
+    other (r <= |a - b|)."""
+    a, b = 17.5, 16.5
+    Da, Db = oph.stokes_translational(a, eta=0.89e-3), oph.stokes_translational(b, eta=0.89e-3)
+    kT_eta = math.sqrt(Da * 6 * math.pi * a * Db * 6 * math.pi * b)
+    rs = np.array([0.2, 0.7, 1.0, 1.5, 5.0, 20.0, 33.9, 34.0, 34.1, 40.0, 80.0, 200.0])
+    D = ost.zuk_diffusion(rs, a, b, kT_eta, Da + Db)
+    for r, d in zip(rs, D):
+        v = np.array([r, 0.3 * r, -0.2 * r]) / math.sqrt(1 + 0.09 + 0.04)
+        ref = max(Da + Db - (2.0 / 3.0) * np.trace(oph.rpy_offdiagonal(v, a, b, Da, Db)), 1e-12)
+        assert math.isclose(d, ref, rel_tol=1e-13), (r, d, ref)
+    assert np.all(np.diff(D[rs > 34.0]) > 0)  # the coupling fades with distance
+    assert ost.zuk_diffusion(np.array([0.0]), a, b, kT_eta, Da + Db)[0] == Da + Db
+
+
 def test_quaternion_conventions():
     g = golden("quat")
     np.testing.assert_array_equal(ost.rotmats(g["q"]), g["R"])
@@ -302,3 +320,19 @@ def test_stepper_statistics_match_reference(name, sysname):
     nt = g["sd_near_miss_traj"]
     np.testing.assert_array_equal(st.nm_pos[nt], g["sd_near_miss_pos"])
     np.testing.assert_array_equal(st.min_dist[nt], g["sd_near_miss_dist"])
+
+
+@pytest.mark.parametrize("name,sysname", [("run_c2", "c2"), ("run_c3", "c3")])
+def test_stepper_path_and_energy_traces_match_reference(name, sysname):
+    """Path rows [traj, step, x, y, z, q0, q1, q2] and energy rows [traj, step, fx, fy, fz, dt] recorded
+    every save_interval (10) steps, as the reference run recorded them (gpu_batch_simulator.py:1319-1340)."""
+    g = golden(name)
+    s = system(sysname)
+    res = ost.run(step_system(s), step_params(s, int(g["n_traj"]), int(g["seed"]), int(g["max_steps"])), noise="pcg64")
+    for key, mine in (("path_steps", res.stats.path_steps), ("energy_steps", res.stats.energy_steps)):
+        ref = g[f"sd_{key}"]
+        rows = np.vstack(mine)
+        rows = rows[rows[:, 1] <= ref[:, 1].max()]
+        assert rows.shape == ref.shape, (key, rows.shape, ref.shape)
+        np.testing.assert_array_equal(rows[:, :2], ref[:, :2])
+        np.testing.assert_allclose(rows[:, 2:], ref[:, 2:], rtol=1e-13, atol=1e-13, err_msg=key)

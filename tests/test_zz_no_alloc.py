@@ -1,8 +1,8 @@
 """bd_sim_run_noalloc, the stepper entry point that allocates no device memory.
 
 It is for callers that cannot call cudaMalloc when they run trajectories (an
-application whose allocator already holds the GPU memory, a process under a memory
-quota, code running during another library's CUDA graph capture).  Through the C
+application whose allocator already holds the GPU memory, or a process under a
+device-memory quota).  Through the C
 ABI it must give every trajectory the same outcome, step count and return count as
 the regular stepper, and the same counters, on two calls in a row: the calls share
 one static scratch array, so the second call also shows that each call clears what
@@ -98,3 +98,28 @@ def test_noalloc_rejects_more_slots_than_the_array_holds():
     with pytest.raises(_lib.BdError, match="at most 65536"):
         h.call("bd_sim_run_noalloc", C.byref(sp), _lib.P(out.data_ptr()), _lib.P(out.data_ptr()),
                _lib.P(out.data_ptr()), _lib.P(out.data_ptr()), 16, 10, None)
+
+
+def test_noalloc_rejects_a_handle_with_a_surrogate():
+    """The entry point runs only the exact-force stepper; a handle carrying a surrogate is refused
+    instead of silently ignoring it."""
+    import torch
+
+    from pystarc_b200 import _lib
+    from pystarc_b200.surrogate import MLPEnsemble, SurrogateSpec
+    from tests.test_gpu_stepper import make_sim
+
+    s = system("c2")
+    sim = make_sim(s, 200, 50, "mixed", steps_per_launch=16)
+    sim.run()
+    ens = MLPEnsemble(n_members=2, seed=3)
+    spec = SurrogateSpec(r_min=0.0, r_max=1e9, threshold=0.0, force_floor=1.0)
+    h = sim.engine.handle
+    h.call("bd_sim_set_surrogate", ens.h, C.byref(spec.c_params()))
+    sp = _params(sim, 256)
+    out = torch.empty(1024, dtype=torch.int32, device="cuda")
+    with pytest.raises(_lib.BdError, match="exact-force stepper only"):
+        h.call("bd_sim_run_noalloc", C.byref(sp), _lib.P(out.data_ptr()), _lib.P(out.data_ptr()),
+               _lib.P(out.data_ptr()), _lib.P(out.data_ptr()), 16, 10, None)
+    h.call("bd_sim_set_surrogate", None, None)
+    ens.close()
