@@ -215,9 +215,11 @@ int bd_sim_restore(BdHandle* h, const double* c, const double* q, const int32_t*
 /* Launch shape: lanes per trajectory (1, 4, 8, 16 or 32: the lanes of a group share one
  * trajectory's whole step) or BD_GROUP_WARP (each lane owns one trajectory's step logic and
  * the warp sweeps each trajectory's atoms together; BD_GROUP_WARP_CAPPED is the same with
- * registers capped at 128 per thread), and threads per block (multiple of 32, <= 256).
+ * registers capped at 128 per thread), or BD_GROUP_SPLIT (each BD step as three kernels: the
+ * ligand-atom forces, Born direction 2 in a kernel capped at 64 registers, then the rest of the
+ * step; the same trajectories as BD_GROUP_WARP), and threads per block (multiple of 32, <= 256).
  * Set by the autotuner; 0 keeps the current value. */
-enum { BD_GROUP_WARP = 64, BD_GROUP_WARP_CAPPED = 65 };
+enum { BD_GROUP_WARP = 64, BD_GROUP_WARP_CAPPED = 65, BD_GROUP_SPLIT = 66 };
 int bd_set_launch(BdHandle* h, int group, int block_threads);
 int bd_get_launch(BdHandle* h, int* group, int* block_threads, int* grid_blocks);
 
@@ -231,8 +233,12 @@ int bd_get_launch(BdHandle* h, int* group, int* block_threads, int* grid_blocks)
  *   stencil is 8 vector loads instead of 20 scalar ones (4x the grid's memory).
  * BD_LAYOUT_WINDOWS_2: the interleaved elec+Born grid gets a float4 copy whose entry n holds
  *   both channels of nodes n and n+1: 12 loads per stencil instead of 20 (2x its memory).
+ * BD_LAYOUT_CUBES_1: the ligand Born grid gets a copy whose entry n holds the 2x2x2 block of
+ *   nodes at node n (32 bytes, one sector; 8x the grid's memory, made only up to
+ *   BD_CUBE_MAX_BYTES), so a reverse-Born stencil is three 32-byte loads and one 16-byte load.
  * The same values enter the same arithmetic in every layout: results are identical. */
-enum { BD_LAYOUT_STAGE_RECEPTOR = 1, BD_LAYOUT_WINDOWS_1 = 2, BD_LAYOUT_WINDOWS_2 = 4 };
+enum { BD_LAYOUT_STAGE_RECEPTOR = 1, BD_LAYOUT_WINDOWS_1 = 2, BD_LAYOUT_WINDOWS_2 = 4, BD_LAYOUT_CUBES_1 = 8 };
+#define BD_CUBE_MAX_BYTES (48ll * 1024 * 1024)
 #define BD_LAYOUT_DEFAULT BD_LAYOUT_WINDOWS_1
 #define BD_STAGE_MAX_BYTES (64 * 1024)
 int bd_set_layout(BdHandle* h, int flags);

@@ -19,7 +19,7 @@ TORQUE_ZERO, TORQUE_CENTROID = 0, 1
 CTR_NAMES = ("started", "reacted", "escaped", "max_steps", "steps", "returns", "overlap", "bridge", "grid_evals",
              "rev_evals", "ff_evals", "nonfinite")
 N_CTR = len(CTR_NAMES)
-LAYOUT_STAGE_RECEPTOR, LAYOUT_WINDOWS_1, LAYOUT_WINDOWS_2 = 1, 2, 4
+LAYOUT_STAGE_RECEPTOR, LAYOUT_WINDOWS_1, LAYOUT_WINDOWS_2, LAYOUT_CUBES_1 = 1, 2, 4, 8
 LAYOUT_DEFAULT = LAYOUT_WINDOWS_1
 TERM_GRID, TERM_FARFIELD, TERM_REV_BORN, TERM_CONTACT, TERM_ALL = 1, 2, 4, 8, 15
 

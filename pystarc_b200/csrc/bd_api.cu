@@ -11,6 +11,7 @@
 #include "bd_kernels.cuh"
 #include "bd_multi.cuh"
 #include "bd_surrogate.cuh"
+#include "bd_split.cuh"
 #include "pystarc_b200.h"
 
 // surrogate MLP (bd_mlp.cu)
@@ -77,6 +78,9 @@ struct BdHandle {
   DevSurrogate sur_q{};
   SurBuf sur_buf{};
   int sur_cap = 0;
+  // split stepper (BD_GROUP_SPLIT): per-slot scratch of one step
+  SplitBuf split_buf{};
+  int split_cap = 0;
   unsigned long long* sur_ctr_host_base = nullptr;
   // graphs: [cur][steps] cache
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -185,6 +189,18 @@ int add_window(BdHandle* h, DevGrid& g) {
   window_kernel<<<h->n_sm * 8, 256>>>(g.data, (float4*)p, n, g.nz, g.ch);
   CK(h, cudaGetLastError());
   g.win = (const float4*)p;
+  return BD_OK;
+}
+
+// Cube copy of an uploaded one-channel grid for the four-load stencil (DevGrid::cube).
+int add_cube(BdHandle* h, DevGrid& g) {
+  const long n = (long)g.nx * g.ny * g.nz;
+  void* p = nullptr;
+  int rc = dev_alloc(h, h->sys_allocs, &p, (size_t)n * 8 * sizeof(float));
+  if (rc) return rc;
+  cube_kernel<<<h->n_sm * 8, 256>>>(g.data, (float*)p, g.nx, g.ny, g.nz);
+  CK(h, cudaGetLastError());
+  g.cube = (const float*)p;
   return BD_OK;
 }
 
@@ -365,6 +381,9 @@ int finalize(BdHandle* h) {
     grid_to_dev(lb[0], p, 1, S.lig_born);
     if (h->layout & BD_LAYOUT_WINDOWS_1)
       if ((rc = add_window(h, S.lig_born))) return rc;
+    if ((h->layout & BD_LAYOUT_CUBES_1) &&
+        (double)S.lig_born.nx * S.lig_born.ny * S.lig_born.nz * 32.0 <= (double)BD_CUBE_MAX_BYTES)
+      if ((rc = add_cube(h, S.lig_born))) return rc;
     S.born_rev = 1;
     const DevGrid& g = S.lig_born;
     const double mx = std::max(std::fabs(g.lox), std::fabs(g.hix)), my = std::max(std::fabs(g.loy), std::fabs(g.hiy)),
@@ -418,6 +437,11 @@ struct K {
 
 template <typename FT, bool TQ>
 void* pick_g(int G, int which) {
+  if (G == BD_GROUP_SPLIT) {
+    // the stepper's last phase sizes the slot pool; the parity kernels use a full-warp group
+    if (which == 2) return (void*)&split_end_kernel<FT, TQ>;
+    G = 32;
+  }
   if (G == BD_GROUP_WARP || G == BD_GROUP_WARP_CAPPED) {
     // warp-cooperative stepper; the parity kernels use a full-warp group (same sweep code)
     if (which == 2)
@@ -445,11 +469,14 @@ void* kernel_for(int prec, int G, int torque, int which) {
 }
 
 bool valid_group(int g) {
-  return g == 1 || g == 4 || g == 8 || g == 16 || g == 32 || g == BD_GROUP_WARP || g == BD_GROUP_WARP_CAPPED;
+  return g == 1 || g == 4 || g == 8 || g == 16 || g == 32 || g == BD_GROUP_WARP || g == BD_GROUP_WARP_CAPPED ||
+         g == BD_GROUP_SPLIT;
 }
 
 // Lanes that hold one trajectory's state (the warp-cooperative modes keep one per lane).
-int lanes_per_traj(int g) { return (g == BD_GROUP_WARP || g == BD_GROUP_WARP_CAPPED) ? 1 : g; }
+int lanes_per_traj(int g) {
+  return (g == BD_GROUP_WARP || g == BD_GROUP_WARP_CAPPED || g == BD_GROUP_SPLIT) ? 1 : g;
+}
 
 // Tiny ligands with nothing to sweep: one lane per trajectory does everything.
 // Otherwise the warp-cooperative mode.  The autotuner can override either.
@@ -711,7 +738,7 @@ int bd_eval_forces_atoms(BdHandle* h, int64_t n, const double* pos, const double
 
 int bd_set_launch(BdHandle* h, int group, int block) {
   if (!h) return BD_ERR_ARG;
-  if (group && !valid_group(group)) return fail(h, BD_ERR_ARG, "group must be 1, 4, 8, 16, 32, 64 or 65 (warp-cooperative)");
+  if (group && !valid_group(group)) return fail(h, BD_ERR_ARG, "group must be 1, 4, 8, 16, 32, 64 or 65 (warp-cooperative) or 66 (split)");
   if (block && (block % 32 || block < 32 || block > 256)) return fail(h, BD_ERR_ARG, "block must be 32..256, x32");
   if (group) h->group = group;
   if (block) h->block = block;
@@ -722,7 +749,7 @@ int bd_set_launch(BdHandle* h, int group, int block) {
 
 int bd_set_layout(BdHandle* h, int flags) {
   if (!h) return BD_ERR_ARG;
-  const int all = BD_LAYOUT_STAGE_RECEPTOR | BD_LAYOUT_WINDOWS_1 | BD_LAYOUT_WINDOWS_2;
+  const int all = BD_LAYOUT_STAGE_RECEPTOR | BD_LAYOUT_WINDOWS_1 | BD_LAYOUT_WINDOWS_2 | BD_LAYOUT_CUBES_1;
   if (flags & ~all) return fail(h, BD_ERR_ARG, "unknown layout flags 0x%x", flags & ~all);
   if (flags != h->layout) {
     h->layout = flags;
@@ -867,6 +894,8 @@ int bd_sim_configure(BdHandle* h, const BdSimParams* p) {
   h->sim_ready = false;
   h->sur_cap = 0;
   h->sur_buf = SurBuf{};
+  h->split_cap = 0;
+  h->split_buf = SplitBuf{};
   h->sp = *p;
   // live-slot capacity
   const int G = launch_group(h);
@@ -1031,6 +1060,8 @@ int ensure_surrogate_buffers(BdHandle* h) {
   U.T = (double*)q;
   if ((rc = dev_alloc(h, h->sim_allocs, &q, (size_t)C))) return rc;
   U.mode = (int8_t*)q;
+  if ((rc = dev_alloc(h, h->sim_allocs, &q, (size_t)C))) return rc;
+  U.fresh = (int8_t*)q;
   if ((rc = dev_alloc(h, h->sim_allocs, &q, (size_t)C * sizeof(int)))) return rc;
   U.row = (int*)q;
   if ((rc = dev_alloc(h, h->sim_allocs, &q, (size_t)C * kSurInPad * 2))) return rc;
@@ -1070,6 +1101,8 @@ int enqueue_surrogate_step(BdHandle* h, cudaStream_t s, int cur, int blocks) {
 // K surrogate BD steps on buffer `cur`, then the compaction into the other buffer.
 int enqueue_surrogate_launch(BdHandle* h, int K, cudaStream_t s, int cur, int blocks) {
   const bool tq = h->sp.torque_mode == BD_TORQUE_CENTROID, f64 = h->sp.precision == BD_PREC_FP64;
+  // forces kept over rejected steps are per slot: the compaction between launches moves slots
+  CK(h, cudaMemsetAsync(h->sur_buf.fresh, 0, (size_t)h->sur_cap, s));
   for (int k = 0; k < K; ++k) {
     int rc = f64 ? (tq ? enqueue_surrogate_step<double, true>(h, s, cur, blocks)
                        : enqueue_surrogate_step<double, false>(h, s, cur, blocks))
@@ -1092,6 +1125,78 @@ int surrogate_blocks(BdHandle* h) {
   return persistent_blocks(h, fa, 256);
 }
 
+// Scratch of the split stepper for the configured capacity (outside any capture).
+int ensure_split_buffers(BdHandle* h) {
+  const int C = h->buf[0].cap;
+  if (h->split_cap == C) return BD_OK;
+  SplitBuf& U = h->split_buf;
+  void* q;
+  int rc;
+  if ((rc = dev_alloc(h, h->sim_allocs, &q, 3 * (size_t)C * sizeof(double)))) return rc;
+  U.F = (double*)q;
+  if ((rc = dev_alloc(h, h->sim_allocs, &q, 3 * (size_t)C * sizeof(double)))) return rc;
+  U.T = (double*)q;
+  if ((rc = dev_alloc(h, h->sim_allocs, &q, 6 * (size_t)C * sizeof(double)))) return rc;
+  U.rv = (double*)q;
+  if ((rc = dev_alloc(h, h->sim_allocs, &q, (size_t)C * sizeof(double)))) return rc;
+  U.rprev = (double*)q;
+  if ((rc = dev_alloc(h, h->sim_allocs, &q, (size_t)C))) return rc;
+  U.mode = (int8_t*)q;
+  if ((rc = dev_alloc(h, h->sim_allocs, &q, (size_t)C))) return rc;
+  U.fresh = (int8_t*)q;
+  if ((rc = dev_alloc(h, h->sim_allocs, &q, (size_t)C * sizeof(int)))) return rc;
+  U.list = (int*)q;
+  if ((rc = dev_alloc(h, h->sim_allocs, &q, 2 * sizeof(int)))) return rc;
+  U.cnt = (int*)q;
+  h->split_cap = C;
+  return BD_OK;
+}
+
+struct SplitKernels {
+  void *begin, *rev, *end;
+};
+
+extern "C++" {
+template <typename FT, bool TQ>
+SplitKernels split_kernels_t() {
+  return {(void*)&split_begin_kernel<FT, TQ>, (void*)&split_rev_kernel<FT, TQ>, (void*)&split_end_kernel<FT, TQ>};
+}
+}  // extern "C++"
+
+SplitKernels split_kernels(int prec, int torque) {
+  const bool tq = torque == BD_TORQUE_CENTROID;
+  if (prec == BD_PREC_FP64) return tq ? split_kernels_t<double, true>() : split_kernels_t<double, false>();
+  return tq ? split_kernels_t<float, true>() : split_kernels_t<float, false>();
+}
+
+// K split steps on buffer `cur` (three kernels each), then the compaction into the other buffer.
+int enqueue_split_launch(BdHandle* h, int K, cudaStream_t s, int cur) {
+  const SplitKernels kn = split_kernels(h->sp.precision, h->sp.torque_mode);
+  const size_t smem = stepper_smem(h->S, h->P, kn.end);
+  const int b_begin = persistent_blocks(h, kn.begin, 256), b_rev = persistent_blocks(h, kn.rev, 256),
+            b_end = persistent_blocks(h, kn.end, 256, smem);
+  SlotBuf src = h->buf[cur], dst = h->buf[1 - cur];
+  const int* live = h->d_live + cur;
+  SplitBuf U = h->split_buf;
+  unsigned long long* ctr = h->d_ctr;
+  // forces kept over rejected steps are per slot: the compaction between launches moves slots
+  CK(h, cudaMemsetAsync(U.fresh, 0, (size_t)h->split_cap, s));
+  for (int k = 0; k < K; ++k) {
+    CK(h, cudaMemsetAsync(U.cnt, 0, 2 * sizeof(int), s));
+    void* a_args[] = {&h->S, &h->P, &src, &live, &U};
+    CK(h, cudaLaunchKernel(kn.begin, dim3(b_begin), dim3(256), a_args, 0, s));
+    void* r_args[] = {&h->S, &src, &U, &ctr};
+    CK(h, cudaLaunchKernel(kn.rev, dim3(b_rev), dim3(256), r_args, 0, s));
+    void* e_args[] = {&h->S, &h->P, &src, &live, &U};
+    CK(h, cudaLaunchKernel(kn.end, dim3(b_end), dim3(256), e_args, smem, s));
+  }
+  compact_kernel<<<h->n_sm * 4, 256, 0, s>>>(src, dst, live, h->d_ctr);
+  CK(h, cudaGetLastError());
+  finish_compact_kernel<<<1, 1, 0, s>>>(h->d_live + (1 - cur), h->d_ctr);
+  CK(h, cudaGetLastError());
+  return BD_OK;
+}
+
 int build_graphs(BdHandle* h, int K) {
   const int G = launch_group(h);
   if (h->graph_K == K && h->graph_G == G && h->graph_B == h->block && h->graph_prec == h->sp.precision &&
@@ -1110,10 +1215,17 @@ int build_graphs(BdHandle* h, int K) {
     int rc = ensure_surrogate_buffers(h);
     if (rc) return rc;
   }
+  const bool split = !h->sur && G == BD_GROUP_SPLIT;
+  if (split) {
+    int rc = ensure_split_buffers(h);
+    if (rc) return rc;
+  }
   for (int c = 0; c < 2; ++c) {
     cudaGraph_t graph;
     CK(h, cudaStreamBeginCapture(h->own, cudaStreamCaptureModeThreadLocal));
-    int rc = h->sur ? enqueue_surrogate_launch(h, K, h->own, c, sblocks) : enqueue_launch(h, K, h->own, c, fn, smem, blocks);
+    int rc = h->sur ? enqueue_surrogate_launch(h, K, h->own, c, sblocks)
+             : split ? enqueue_split_launch(h, K, h->own, c)
+                     : enqueue_launch(h, K, h->own, c, fn, smem, blocks);
     cudaError_t e = cudaStreamEndCapture(h->own, &graph);
     if (rc) return rc;
     CK(h, e);
@@ -1442,7 +1554,8 @@ int bd_internal_run_noalloc(BdHandle* h, const BdSimParams* p, unsigned char* sc
   CK(h, cudaMemcpyAsync(ctr + C_PENDING, &started, sizeof started, cudaMemcpyHostToDevice, s));
   CK(h, cudaMemcpyAsync(live, &c_live, sizeof c_live, cudaMemcpyHostToDevice, s));
   CK(h, cudaStreamSynchronize(s));
-  const int G = launch_group_for(h, p->overlap);
+  int G = launch_group_for(h, p->overlap);
+  if (G == BD_GROUP_SPLIT) G = BD_GROUP_WARP_CAPPED;  // the split stepper's scratch would need allocating
   void* fn = kernel_for(p->precision, G, p->torque_mode, 2);
   const size_t smem = stepper_smem(h->S, P, fn);
   const int blocks = persistent_blocks(h, fn, h->block, smem);

@@ -44,6 +44,8 @@ enum : int {
 struct DevGrid {
   const float* data;  // FP32 values; `ch` interleaved channels per node
   const float4* win;  // optional: entry n = nodes n .. n + 4/ch - 1 of node n's z row, all channels
+  const float* cube;  // optional (ch = 1): 8 floats per node n = (x, y, z), the 2x2x2 block
+                      // v(x + i, y + j, z + k) at 4i + 2j + k, 32-byte aligned (one sector)
   int nx, ny, nz, ch;
   double ox, oy, oz;
   double isx, isy, isz;  // 1/spacing
@@ -299,6 +301,13 @@ __device__ __forceinline__ void ld(const float* p, float v[CH]) {
   }
 }
 
+// One 32-byte read-only load (a whole sector) of eight floats; p is 32-byte aligned.
+__device__ __forceinline__ void ld8(const float* p, float v[8]) {
+  asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
+      : "l"(p));
+}
+
 // floor(u) as a value and as an int, for 0 <= u < 2^23 (float) or 2^52 (double):
 // adding 2^23 (2^52) with round-down leaves exactly floor(u) in the low mantissa
 // bits, so the cell index needs no float-to-int conversion.  Every stencil
@@ -358,7 +367,32 @@ __device__ __forceinline__ StencilOut<FT, CH> stencil(const DevGrid& g, PT x, PT
   const int zc = lz ? 1 : 0;  // position of node cz inside the three-node run
   const int ze = lz ? 0 : 2;  // position of the extra z node
   float r[2][2][3][CH], xe[2][2][CH], ye[2][2][CH];
-  if (g.win) {
+  if (CH == 1 && g.cube) {
+    // cube copy: the centre block, the x-extra face, the y-extra and z-extra edges in four loads
+    const float* cb = g.cube;
+    float c8[8], y8[8], z8[8];
+    ld8(cb + 8 * (long)((cx * g.ny + cy) * nz + cz), c8);
+    const float4 xf = __ldg(reinterpret_cast<const float4*>(cb + 8 * (long)((ex * g.ny + cy) * nz + cz)));
+    ld8(cb + 8 * (long)((cx * g.ny + ey) * nz + cz), y8);
+    ld8(cb + 8 * (long)((cx * g.ny + cy) * nz + (lz ? cz - 1 : cz + 2)), z8);
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        r[i][j][zc][0] = c8[4 * i + 2 * j];
+        r[i][j][zc + 1][0] = c8[4 * i + 2 * j + 1];
+        r[i][j][ze][0] = z8[4 * i + 2 * j];
+      }
+    xe[0][0][0] = xf.x;
+    xe[0][1][0] = xf.y;
+    xe[1][0][0] = xf.z;
+    xe[1][1][0] = xf.w;
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      ye[i][0][0] = y8[4 * i];
+      ye[i][1][0] = y8[4 * i + 1];
+    }
+  } else if (g.win) {
     // window copy: one 16-byte load per z run (two for a 3-node run of two channels)
     const float4* w = g.win;
 #pragma unroll

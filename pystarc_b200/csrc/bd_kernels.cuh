@@ -335,7 +335,9 @@ __device__ void group_contact(const DevSystem& S, const double c[3], int lane, u
 // direction 1 on the receptor Born grid, Born direction 2 on the ligand Born
 // grid at the receptor atoms with the force negated, and the WCA contact forces
 // when they are on.  Every lane returns the same totals.
-template <typename FT, int G, bool TORQUE, bool ENERGY, class PosFn>
+// REV = false compiles the function without Born direction 2 (the split stepper sweeps it in a
+// kernel of its own).
+template <typename FT, int G, bool TORQUE, bool ENERGY, class PosFn, bool REV = true>
 __device__ void group_forces(const DevSystem& S, const double c[3], const double R[9], int lane, unsigned gm,
                              const PosFn& pos, double F[3], double T[3], double& E, Counts& cnt,
                              const RecView& v = RecView{nullptr, nullptr}, unsigned terms = 15u) {
@@ -419,7 +421,8 @@ __device__ void group_forces(const DevSystem& S, const double c[3], const double
   // Lanes test G receptor chunks at a time against the box's circumsphere, then
   // sweep the hit chunks' atoms together.
   double r0 = 0, r1 = 0, r2 = 0, u0 = 0, u1 = 0, u2 = 0;
-  if constexpr (G == 32) {
+  if constexpr (!REV) {
+  } else if constexpr (G == 32) {
     if (t_rev && S.born_rev && norm3(c[0], c[1], c[2]) - S.rec_max_r < S.lig_born_rho) {
       double rr[3] = {0, 0, 0}, uu[3] = {0, 0, 0};
       warp_reverse_born<FT, TORQUE>(S, c, R, lane, rr, uu, nr);
@@ -483,7 +486,7 @@ __device__ void group_forces(const DevSystem& S, const double c[3], const double
       t1 = gsum<G>(t1, gm);
       t2 = gsum<G>(t2, gm);
     }
-    if (S.born_rev) {
+    if (REV && S.born_rev) {
       r0 = gsum<G>(r0, gm);
       r1 = gsum<G>(r1, gm);
       r2 = gsum<G>(r2, gm);
@@ -1092,6 +1095,27 @@ __global__ void window_kernel(const float* __restrict__ d, float4* __restrict__ 
       v[k] = z + node < nz ? d[(n + node) * ch + c] : 0.f;
     }
     w[n] = make_float4(v[0], v[1], v[2], v[3]);
+  }
+}
+
+// Cube copy of a one-channel grid (DevGrid::cube): entry n = (x, y, z) holds the 2x2x2 block
+// v(x + i, y + j, z + k) at 4i + 2j + k, zero past the grid's faces.
+__global__ void cube_kernel(const float* __restrict__ d, float* __restrict__ cube, int nx, int ny, int nz) {
+  const long n_nodes = (long)nx * ny * nz;
+  for (long n = blockIdx.x * (long)blockDim.x + threadIdx.x; n < n_nodes; n += (long)gridDim.x * blockDim.x) {
+    const int z = (int)(n % nz), y = (int)((n / nz) % ny), x = (int)(n / ((long)ny * nz));
+    float v[8];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int k = 0; k < 2; ++k)
+          v[4 * i + 2 * j + k] =
+              (x + i < nx && y + j < ny && z + k < nz) ? d[((long)(x + i) * ny + (y + j)) * nz + (z + k)] : 0.f;
+    float4* o = reinterpret_cast<float4*>(cube + 8 * n);
+    o[0] = make_float4(v[0], v[1], v[2], v[3]);
+    o[1] = make_float4(v[4], v[5], v[6], v[7]);
   }
 }
 

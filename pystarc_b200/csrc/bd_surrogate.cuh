@@ -53,7 +53,10 @@ __device__ __forceinline__ double sur_envelope(const DevSurrogate& Q, double r) 
 struct SurBuf {
   double* F;       // 3 * cap
   double* T;       // 3 * cap
-  int8_t* mode;    // 0: no step this time, 1: exact forces complete, 2: trusted (surrogate pending)
+  int8_t* mode;    // 0: no step this time, 1: exact forces complete, 2: trusted (surrogate pending),
+                   // 3: the pose did not move since the last step, F and T are its complete forces
+  int8_t* fresh;   // per slot: F and T hold the complete forces of the slot's current pose (cleared
+                   // at the start of every launch, whose compaction moves slots)
   int* row;        // trusted: row of the MLP input
   __nv_bfloat16* X;  // cap x kSurInPad packed features
   const float* mean;    // cap x kSurOut (ensemble mean, scaled outputs)
@@ -117,11 +120,14 @@ __global__ void __launch_bounds__(256, 2) sur_begin_kernel(DevSystem S, DevSim P
     const bool run = own && tr.status == ST_RUNNING;
     double R[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, r = 0;
     int st = ST_EMPTY;
+    const int rets0 = tr.rets;
     if (run) st = step_begin(S, P, traj_key(P, tr.id), (uint32_t)tr.steps, tr, R, r, tl);
     const bool need = run && st == ST_RUNNING;
-    const bool trusted = need && r >= Q.r_min && r <= Q.r_max;
+    // a step rejected by the overlap test left the pose unchanged: its forces are reused
+    const bool reuse = need && tr.rets == rets0 && U.fresh[slot];
+    const bool trusted = need && !reuse && r >= Q.r_min && r <= Q.r_max;
     double F[3] = {0, 0, 0}, T[3] = {0, 0, 0};
-    warp_forces_terms<FT, TORQUE>(S, tr.c, R, need, trusted ? 9u : 15u, F, T, lane, tl.cnt);
+    warp_forces_terms<FT, TORQUE>(S, tr.c, R, need && !reuse, trusted ? 9u : 15u, F, T, lane, tl.cnt);
     if (run && st != ST_RUNNING) {
       tr.status = st;
       record_end(P, tr, st, tl);
@@ -156,12 +162,14 @@ __global__ void __launch_bounds__(256, 2) sur_begin_kernel(DevSystem S, DevSim P
     }
     if (own) {
       store_slot(B, slot, tr);
+      if (!reuse) {
 #pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        U.F[3 * slot + k] = F[k];
-        U.T[3 * slot + k] = T[k];
+        for (int k = 0; k < 3; ++k) {
+          U.F[3 * slot + k] = F[k];
+          U.T[3 * slot + k] = T[k];
+        }
       }
-      U.mode[slot] = (int8_t)(need ? (trusted ? 2 : 1) : 0);
+      U.mode[slot] = (int8_t)(need ? (reuse ? 3 : trusted ? 2 : 1) : 0);
     }
   }
   flush_tally(P, tl, true);
@@ -250,7 +258,19 @@ __global__ void __launch_bounds__(256, 2) sur_end_kernel(DevSystem S, DevSim P, 
     }
     bool dead = !own;
     warp_refill(P, tr, dead, lane);
-    if (own) store_slot(B, slot, tr);
+    if (own) {
+      store_slot(B, slot, tr);
+      // rejected and still running: the next step starts from the same pose with these forces
+      const bool keep = need && ok && ovl && st == ST_RUNNING;
+      if (keep && mode != 3) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          U.F[3 * slot + k] = F[k];
+          U.T[3 * slot + k] = T[k];
+        }
+      }
+      U.fresh[slot] = (int8_t)keep;
+    }
   }
   flush_tally(P, tl, true);
   n_fb = gsumu<32>(n_fb, FULL);

@@ -219,11 +219,13 @@ def identity_run(name, n=32, launches=6, K=16, torque=None, s=None, hi_mode="ref
     o = ost.run(step_system(s, fn), step_params(s, n, s.seed, M, hi_mode=hi_mode), noise="philox",
                 termination="complete", init=(c0, q0))
     run = gst == 3
-    dpos = float(np.max(np.abs(gpos[run] - o.pos[run]))) if run.any() else 0.0
+    per = np.where(run, np.max(np.abs(np.nan_to_num(gpos) - o.pos), axis=1), 0.0)
+    dpos = float(np.max(per)) if run.any() else 0.0
     dq = float(np.max(np.abs(gq[run] - o.q[run]))) if run.any() else 0.0
     return {"gpu": (gst, gsteps, grets), "oracle": (o.status, o.n_steps, o.n_returns), "running": int(run.sum()),
             "max_pose_diff_A": dpos, "max_quat_diff": dq, "steps": int(o.total_steps),
-            "overlap_rejections": int(o.n_overlap_rejected)}
+            "overlap_rejections": int(o.n_overlap_rejected), "pose_diff_per_trajectory": per,
+            "start": (c0, q0)}
 
 
 def analytic_p_rxn(s, return_prob):

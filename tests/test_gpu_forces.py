@@ -81,13 +81,15 @@ def test_random_poses_against_oracle(sysname, precision, tol):
 @pytest.mark.parametrize("sysname", ["c2", "c3"])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_grid_windows_give_identical_forces(sysname, precision):
-    """Window copies (vector loads) and plain scalar loads feed the same values to the same arithmetic."""
+    """Window copies, cube copies (vector loads) and plain scalar loads feed the same values to the same
+    arithmetic."""
     from pystarc_b200 import _lib
 
     s = system(sysname)
     c, q = random_poses(2000, 0.5, 35.0, 5)
     out = []
-    for layout in (0, _lib.LAYOUT_WINDOWS_1, _lib.LAYOUT_WINDOWS_2, _lib.LAYOUT_DEFAULT):
+    for layout in (0, _lib.LAYOUT_WINDOWS_1, _lib.LAYOUT_WINDOWS_2, _lib.LAYOUT_DEFAULT, _lib.LAYOUT_CUBES_1,
+                   _lib.LAYOUT_CUBES_1 | _lib.LAYOUT_WINDOWS_1):
         eng = make_engine(s, precision, "centroid", layout=layout)
         out.append(eng.eval_poses(c, q))
         eng.close()

@@ -39,10 +39,13 @@ def oracle_keyed(s, n_traj, max_steps, torque="zero", seed=None, use_lj=False):
 CASES = [("two_sphere", 400, 100000, "zero"), ("c2", 96, 300, "zero"), ("c3", 32, 80, "centroid")]
 
 
+@pytest.mark.parametrize("group", [None, 66])
 @pytest.mark.parametrize("sysname,n,max_steps,torque", CASES)
-def test_fp64_trajectories_match_oracle_exactly(sysname, n, max_steps, torque):
+def test_fp64_trajectories_match_oracle_exactly(sysname, n, max_steps, torque, group):
     s = system(sysname)
     sim = make_sim(s, n, max_steps, "fp64", torque, steps_per_launch=16, launches_per_poll=4)
+    if group:
+        sim.engine.handle.call("bd_set_launch", group, 0)
     res = sim.run()
     st, steps, rets = sim.outcomes()
     o = oracle_keyed(s, n, max_steps, torque)
@@ -241,8 +244,8 @@ def test_checkpoint_resume_replays_exactly(tmp_path):
 def test_launch_shape_does_not_change_fates():
     s = system("c2")
     outs = []
-    for group, slots in [(4, 300), (16, 2000), (64, 500), (65, 150)]:
-        sim = make_sim(s, 600, 250, "fp64", slots=slots, steps_per_launch=4 if group in (4, 65) else 32)
+    for group, slots in [(4, 300), (16, 2000), (64, 500), (65, 150), (66, 400), (66, 150)]:
+        sim = make_sim(s, 600, 250, "fp64", slots=slots, steps_per_launch=4 if group in (4, 65) or slots == 150 else 32)
         sim.engine.handle.call("bd_set_launch", group, 128)
         sim.run()
         outs.append(sim.outcomes())
@@ -251,14 +254,15 @@ def test_launch_shape_does_not_change_fates():
             np.testing.assert_array_equal(x, y)
 
 
-@pytest.mark.parametrize("precision,group", [("fp64", 64), ("mixed", 65), ("mixed", 8)])
+@pytest.mark.parametrize("precision,group", [("fp64", 64), ("mixed", 65), ("mixed", 8), ("mixed", 66)])
 def test_data_layouts_do_not_change_fates(precision, group):
     """Grid windows and the shared-memory receptor table change loads, not values: same fates and counters."""
     from pystarc_b200 import _lib
 
     s = system("c2")
     outs = []
-    for layout in (0, _lib.LAYOUT_DEFAULT, _lib.LAYOUT_WINDOWS_1 | _lib.LAYOUT_WINDOWS_2 | _lib.LAYOUT_STAGE_RECEPTOR):
+    for layout in (0, _lib.LAYOUT_DEFAULT, _lib.LAYOUT_WINDOWS_1 | _lib.LAYOUT_WINDOWS_2 | _lib.LAYOUT_STAGE_RECEPTOR,
+                   _lib.LAYOUT_CUBES_1 | _lib.LAYOUT_WINDOWS_1):
         sim = make_sim(s, 800, 250, precision, slots=400, steps_per_launch=16, layout=layout)
         sim.engine.handle.call("bd_set_launch", group, 128)
         res = sim.run()
@@ -270,7 +274,7 @@ def test_data_layouts_do_not_change_fates(precision, group):
 
 
 @pytest.mark.parametrize("sysname,n,max_steps,group", [("c2", 96, 300, 64), ("two_sphere", 300, 100000, 1),
-                                                       ("c2", 96, 300, 8)])
+                                                       ("c2", 96, 300, 8), ("c2", 96, 300, 66)])
 def test_statistics_match_oracle(sysname, n, max_steps, group):
     """Device statistics (the reference's output-file data) against the oracle with the same draws."""
     s = system(sysname)
@@ -311,7 +315,7 @@ def test_statistics_match_oracle(sysname, n, max_steps, group):
     np.testing.assert_allclose(sd["near_miss_pos"], st.nm_pos[esc], rtol=1e-10, atol=1e-10)
 
 
-@pytest.mark.parametrize("sysname,n,max_steps,group", [("c2", 96, 300, 64), ("c2", 96, 300, 8)])
+@pytest.mark.parametrize("sysname,n,max_steps,group", [("c2", 96, 300, 64), ("c2", 96, 300, 8), ("c2", 96, 300, 66)])
 def test_path_and_energy_traces_match_oracle(sysname, n, max_steps, group):
     """Path and energy rows every save_interval steps (gpu_batch_simulator.py:1319-1340), sorted by
     (step, trajectory) as the reference appends them, against the oracle with the same draws."""
@@ -339,3 +343,21 @@ def test_trace_capacity_drops_and_counts_extra_rows():
     rows = np.vstack(res.sim_data["path_steps"])
     assert len(rows) == 500
     assert res.counters["trace_dropped"] > 0
+
+
+@pytest.mark.parametrize("precision,torque", [("fp64", "zero"), ("mixed", "zero"), ("mixed", "centroid")])
+def test_split_stepper_matches_the_fused_stepper(precision, torque):
+    """The three-kernel step (ligand forces, Born direction 2 in its own kernel, the rest) sums the same
+    terms in the same order as the fused kernel: the same fates, steps, returns and counters."""
+    s = system("c2")
+    outs = []
+    for group in (65, 66):
+        sim = make_sim(s, 1500, 400, precision, torque, slots=700, steps_per_launch=16)
+        sim.engine.handle.call("bd_set_launch", group, 256)
+        res = sim.run()
+        outs.append((sim.outcomes(), res.counters))
+    for x, y in zip(outs[0][0], outs[1][0]):
+        np.testing.assert_array_equal(x, y)
+    for k in ("steps", "reacted", "escaped", "returns", "overlap", "bridge", "grid_evals", "rev_evals", "ff_evals"):
+        assert outs[0][1][k] == outs[1][1][k], k
+    assert outs[0][1]["rev_evals"] > 0
