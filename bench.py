@@ -679,7 +679,13 @@ def main():
         st = torch.tensor([steps_all], device="cuda", dtype=torch.int64)
         dist.all_reduce(st)
         steps_all = int(st.item())
+        # the outcome tallies of the timed window, summed over the ranks (the one data collective)
+        from pystarc_b200.shard import allreduce_tallies
+
+        pooled_tallies = allreduce_tallies(d_mixed, device=torch.device("cuda", local))
     value = steps_all / t_max
+    if dist is None:
+        pooled_tallies = None
     peak, peak_kind = peaks()
     gathers = d_mixed["grid_evals"] + d_mixed["rev_evals"]
     algo_bytes = gathers * ALGO_BYTES_PER_GATHER + d_mixed["steps"] * STATE_BYTES_PER_STEP
@@ -722,6 +728,7 @@ def main():
             "mixed_over_fp64": (d_mixed["steps"] / t_mixed) / (d_fp64["steps"] / t_fp64),
         },
         "counters": {k: int(v) for k, v in d_mixed.items()},
+        "counters_all_ranks": pooled_tallies,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "traffic_note": traffic_note, "peak_kind": peak_kind,
                      "algorithmic_bytes": "224 B per (atom, grid) stencil + 128 B per trajectory-step"},

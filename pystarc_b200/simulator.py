@@ -195,6 +195,7 @@ class B200BatchSimulator:
         self.M = int(launches_per_poll)
         self.slots = int(slots)
         self.id_offset = int(id_offset)
+        self._shard = None  # (rank, world, first global id, local count) of a sharded run
         # per-step statistics for write_all: on when the pipeline attached an output config
         self.stats = bool(getattr(params, "_output_cfg", None) is not None) if stats is None else bool(stats)
         # path / energy traces every save_interval steps (gpu_batch_simulator.py:579-581, :1319-1340): rows
@@ -227,6 +228,15 @@ class B200BatchSimulator:
         self._k_b = 0.0
         self._qb_factor = 1.1
         self.counters = {}
+
+    @property
+    def _n_run(self):
+        """Trajectories this process runs: all of them, or its shard of a sharded run."""
+        return int(self.params.n_trajectories) if self._shard is None else self._shard[3]
+
+    @property
+    def _offset(self):
+        return self.id_offset + (0 if self._shard is None else self._shard[2])
 
     # ------------------------------------------------------------------
     def _setup(self):
@@ -268,7 +278,7 @@ class B200BatchSimulator:
         else:
             h.call("bd_set_reaction_states", 0, None, None, 0, None)
         sp = _lib.BdSimParams()
-        sp.n_traj = int(p.n_trajectories)
+        sp.n_traj = self._n_run
         sp.seed = int(p.seed if p.seed is not None else 0) & 0xFFFFFFFFFFFFFFFF
         sp.r_start = float(p.r_start)
         sp.r_escape = float(p.r_escape)
@@ -289,7 +299,7 @@ class B200BatchSimulator:
         sp.precision = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}[self.precision]
         sp.torque_mode = {"zero": _lib.TORQUE_ZERO, "centroid": _lib.TORQUE_CENTROID}[self.torque_mode]
         sp.slots = self.slots
-        sp.id_offset = self.id_offset
+        sp.id_offset = self._offset
         sp.stats = int(self.stats)
         sp.save_interval = self._save_interval
         sp.trace_capacity = self.trace_capacity
@@ -315,7 +325,7 @@ class B200BatchSimulator:
 
     def read_stats(self):
         """Per-step statistics as host arrays (requires ``stats=True``)."""
-        N = int(self.params.n_trajectories)
+        N = self._n_run
         P = len(self._rxn_cutoffs)
         L = _lib
         a = {"start_pos": np.zeros((N, 3)), "start_q": np.zeros((N, 4)), "min_dist": np.zeros(N),
@@ -401,7 +411,7 @@ class B200BatchSimulator:
         }
 
     def outcomes(self):
-        N = int(self.params.n_trajectories)
+        N = self._n_run
         st = np.zeros(N, dtype=np.int8)
         steps = np.zeros(N, dtype=np.int32)
         rets = np.zeros(N, dtype=np.int32)
@@ -410,7 +420,8 @@ class B200BatchSimulator:
         return st, steps, rets
 
     def _checkpoint_path(self):
-        return Path(getattr(self.params, "_work_dir", "bd_sims")) / "checkpoint_b200.npz"
+        name = "checkpoint_b200.npz" if self._shard is None else f"checkpoint_b200_rank{self._shard[0]}.npz"
+        return Path(getattr(self.params, "_work_dir", "bd_sims")) / name
 
     def reaction_fires(self):
         """State-machine mode: per-reaction fire counts (discrete test, Brownian bridge) since the reset."""
@@ -443,13 +454,13 @@ class B200BatchSimulator:
         np.savez_compressed(path, c=c, q=q, traj=traj, steps=steps, rets=rets, status=status, state=state,
                             n_live=live.value,
                             counters=ctr, out_status=o_st, out_steps=o_steps, out_returns=o_rets,
-                            n_traj=int(self.params.n_trajectories), seed=int(self.params.seed or 0), cap=C)
+                            n_traj=self._n_run, seed=int(self.params.seed or 0), cap=C)
         return path
 
     def load_checkpoint(self, path):
         """Restore a checkpoint written by ``save_checkpoint`` (same system, seed and n_trajectories)."""
         d = np.load(path)
-        if int(d["n_traj"]) != int(self.params.n_trajectories) or int(d["seed"]) != int(self.params.seed or 0):
+        if int(d["n_traj"]) != self._n_run or int(d["seed"]) != int(self.params.seed or 0):
             raise ValueError(f"{path}: checkpoint is for another run (n_trajectories/seed differ)")
         h = self.engine.handle
         cap = _lib.C.c_int32()
@@ -466,9 +477,87 @@ class B200BatchSimulator:
         h.call("bd_sim_set_states", _lib.ptr(state, _lib.C.c_int8))
 
     # ------------------------------------------------------------------
-    def run(self, max_launches=None) -> B200BatchResult:
+    def run(self, max_launches=None, dist=None) -> B200BatchResult:
+        """Run every trajectory; see the class docstring.
+
+        ``dist``: None for one process, or ``True`` (the default process group) or a
+        ``torch.distributed`` process group for one process per GPU.  Rank r of W then
+        runs the contiguous global-id shard ``shard.shard_range(n, r, W)`` (its ids key
+        the noise, so a trajectory's fate does not depend on W), and the tallies, the
+        per-reaction fire counts and the wall time (max) are pooled over the ranks once
+        at the end, as pystarc/multi_GPU/combine_data.py:66-87 pools separate runs.  The
+        result's counts are the pooled ones; ``sim_data`` holds this rank's trajectories
+        (local ids, global id = local id + ``sim_data["shard"]["id_offset"]``).
+        """
+        group = None
+        if dist is not None:
+            import torch.distributed as td
+
+            from .shard import shard_range
+
+            group = None if dist is True else dist
+            rank, world = td.get_rank(group), td.get_world_size(group)
+            off, n_local = shard_range(int(self.params.n_trajectories), rank, world)
+            self._shard = (rank, world, off, n_local)
         t0 = time.perf_counter()
+        if self._n_run == 0:
+            result = self._empty_result()
+        else:
+            result = self._run_local(t0, max_launches)
+        if dist is not None:
+            result = self._pool(result, group)
+        return result
+
+    def _empty_result(self):
+        """A shard without trajectories (more ranks than trajectories)."""
+        self.counters = {k: 0 for k in _lib.CTR_NAMES}
+        sd = {"outcome": np.zeros(0, np.int32), "n_steps": np.zeros(0, np.int64), "n_returns": np.zeros(0, np.int64)}
+        return B200BatchResult(n_trajectories=0, n_reacted=0, n_escaped=0, n_max_steps=0, reaction_counts={},
+                               r_start=float(self.params.r_start), r_escape=float(self.params.r_escape),
+                               dt=float(getattr(self.params, "dt", 0.2)), elapsed_sec=0.0, steps_per_sec=0.0,
+                               sim_data=sd, total_steps=0, counters=dict(self.counters))
+
+    def _pool(self, res, group):
+        """Sum the shards' tallies and fire counts, take the longest wall time (every rank makes the same
+        collective calls in the same order)."""
+        import torch
+        import torch.distributed as td
+
+        from .shard import allreduce_reaction_fires, allreduce_tallies
+
+        device = torch.device("cuda", self.engine.handle.device) if td.get_backend(group) == "nccl" else None
+        c = res.counters
+        local = {"started": c.get("started", 0), "reacted": res.n_reacted, "escaped": res.n_escaped,
+                 "max_steps": res.n_max_steps, "steps": res.total_steps, "returns": c.get("returns", 0),
+                 "overlap": c.get("overlap", 0), "bridge": c.get("bridge", 0)}
+        pooled = allreduce_tallies(local, group, device)
+        t = torch.tensor([res.elapsed_sec], dtype=torch.float64, device=device)
+        td.all_reduce(t, op=td.ReduceOp.MAX, group=group)
+        elapsed = float(t.item())
+        sd = res.sim_data
+        rank, world, off, n_local = self._shard
+        sd["shard"] = {"rank": rank, "world": world, "id_offset": self.id_offset + off, "n_local": n_local}
+        if self._sm_active:
+            n = len(self._sm["names"])
+            d, b = self.reaction_fires() if n_local else (np.zeros(n, np.int64), np.zeros(n, np.int64))
+            d, b = allreduce_reaction_fires(d, b, group, device)
+            sd["completed_reactions"] = [
+                {"name": self._sm["names"][i], "n_fired": int(d[i] + b[i]),
+                 "state_before": self._sm["state_before"][i], "state_after": self._sm["state_after"][i]}
+                for i in range(n)]
+        counters = dict(res.counters)
+        counters.update(pooled)
+        self.counters = counters
         N = int(self.params.n_trajectories)
+        return B200BatchResult(n_trajectories=N, n_reacted=pooled["reacted"], n_escaped=pooled["escaped"],
+                               n_max_steps=N - pooled["reacted"] - pooled["escaped"],
+                               reaction_counts={"stage_0": pooled["reacted"]}, r_start=res.r_start,
+                               r_escape=res.r_escape, dt=res.dt, elapsed_sec=elapsed,
+                               steps_per_sec=pooled["steps"] / elapsed if elapsed > 0 else 0.0, sim_data=sd,
+                               total_steps=pooled["steps"], counters=counters)
+
+    def _run_local(self, t0, max_launches):
+        N = self._n_run
         self._setup()
         h = self.engine.handle
         h.call("bd_sim_reset", None)

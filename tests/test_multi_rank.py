@@ -125,3 +125,98 @@ def test_two_rank_state_machine_fire_counts_pool():
     assert results[0] == results[1]
     assert results[0] == (single.sm_fires_discrete.tolist(), single.sm_fires_bridge.tolist())
     assert sum(results[0][0]) + sum(results[0][1]) > 0
+
+
+class _FakeHandle:
+    """The engine's C entry points as the stepper drives them, answered by the oracle stepper with
+    the engine's keyed draws: bd_sim_configure runs the configured shard (n_traj trajectories from
+    global id id_offset), the counter and outcome calls copy its results out."""
+
+    def __init__(self, s):
+        self.s = s
+        self.device = 0
+        self.res = None
+        self.configured = None
+
+    def call(self, name, *args):
+        from oracle import stepper as ost
+        from tests.helpers import step_params, step_system
+
+        if name == "bd_sim_configure":
+            sp = args[0]._obj
+            self.configured = (int(sp.n_traj), int(sp.id_offset))
+            prm = step_params(self.s, int(sp.n_traj), int(sp.seed), int(sp.max_steps))
+            self.res = ost.run(step_system(self.s), prm, noise="philox", termination="complete",
+                               id_offset=int(sp.id_offset))
+        elif name == "bd_sim_counters":
+            r = self.res
+            vals = {"started": len(r.status), "reacted": r.n_reacted, "escaped": r.n_escaped,
+                    "max_steps": r.n_max_steps, "steps": r.total_steps, "returns": int(r.n_returns.sum()),
+                    "overlap": r.n_overlap_rejected}
+            from pystarc_b200 import _lib
+
+            for i, k in enumerate(_lib.CTR_NAMES):
+                args[0][i] = int(vals.get(k, 0))
+        elif name == "bd_sim_live":
+            args[0]._obj.value = 0
+        elif name == "bd_sim_outcomes":
+            for i in range(len(self.res.status)):
+                args[0][i] = int(self.res.status[i])
+                args[1][i] = int(self.res.n_steps[i])
+                args[2][i] = int(self.res.n_returns[i])
+        return 0
+
+
+class _FakeEngine:
+    def __init__(self, s):
+        self.handle = _FakeHandle(s)
+        self.precision, self.torque_mode, self._debye = "fp64", "zero", s.debye
+
+    def set_ligand(self, body, q):
+        pass
+
+
+def _sim_worker(rank, world, port, n_total, out):
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from pystarc_b200.simulator import B200BatchSimulator
+        from tests.helpers import system
+
+        s = system("two_sphere")
+        mol1, mol2 = s.molecules()
+        eng = _FakeEngine(s)
+        sim = B200BatchSimulator(mol1, mol2, s.mobility(), s.pathway_set(), s.params(n_traj=n_total, max_steps=5000),
+                                 eng, termination="complete")
+        res = sim.run(dist=True)
+        out[rank] = (res.n_trajectories, res.n_reacted, res.n_escaped, res.n_max_steps, res.total_steps,
+                     eng.handle.configured, res.sim_data["shard"], res.sim_data["outcome"].tolist(),
+                     res.sim_data["n_steps"].tolist())
+    finally:
+        dist.destroy_process_group()
+
+
+def test_simulator_run_shards_and_pools_over_two_ranks():
+    """B200BatchSimulator.run(dist=True): each rank configures its contiguous id shard, runs it, and
+    the result carries the pooled tallies; fates per global id equal one process running everything."""
+    n_total = 101
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as mgr:
+        out = mgr.dict()
+        port = _free_port()
+        mp.start_processes(_sim_worker, args=(2, port, n_total, out), nprocs=2, join=True, start_method="spawn")
+        results = dict(out)
+    single = _run_shard(n_total, 0, 1)
+    for r in (0, 1):
+        n, nr, ne, nm, steps, cfg, shard, _, _ = results[r]
+        assert (n, nr, ne, nm, steps) == (n_total, single.n_reacted, single.n_escaped, single.n_max_steps,
+                                          single.total_steps)
+        assert cfg == (shard["n_local"], shard["id_offset"]) == shard_range(n_total, r, 2)[::-1]
+    outcome = np.array(results[0][7] + results[1][7])
+    expect = single.status.copy()
+    expect[(expect != 1) & (expect != 2)] = 0
+    np.testing.assert_array_equal(outcome, expect)
+    np.testing.assert_array_equal(np.array(results[0][8] + results[1][8]), single.n_steps)
