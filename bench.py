@@ -151,7 +151,7 @@ _OPTS = {"layout": None}
 
 
 def make_sim(s, precision, n_traj, K, id_offset=0, torque="zero", surrogate=None, termination="complete", seed=None,
-             slots=0):
+             slots=0, hi_mode="reference_gpu"):
     from pystarc_b200.engine import B200ForceEngine
     from pystarc_b200.simulator import B200BatchSimulator
 
@@ -160,7 +160,7 @@ def make_sim(s, precision, n_traj, K, id_offset=0, torque="zero", surrogate=None
     mol1, mol2 = s.molecules()
     sim = B200BatchSimulator(mol1, mol2, s.mobility(), s.pathway_set(), s.params(n_traj=n_traj, seed=seed), eng,
                              termination=termination, steps_per_launch=K, id_offset=id_offset, surrogate=surrogate,
-                             slots=slots)
+                             slots=slots, hi_mode=hi_mode)
     return sim
 
 
@@ -185,19 +185,22 @@ def age_pool(sim, K, age, path):
 
 
 def time_device_arm(s, precision, steps, warmup, K, n_traj, id_offset, dist, fixed_launch=None, aged=None,
-                    surrogate=None):
+                    surrogate=None, candidates=None, hi_mode="reference_gpu"):
     """Per-launch CUDA-event times (graph launches) with L2 flushes in between, from the aged pool."""
     import torch
 
     from pystarc_b200 import _lib
-    from pystarc_b200.autotune import autotune
+    from pystarc_b200.autotune import DEFAULT_LAYOUTS, autotune
 
-    sim = make_sim(s, precision, n_traj, K, id_offset, surrogate=surrogate, slots=pool_slots(n_traj))
+    sim = make_sim(s, precision, n_traj, K, id_offset, surrogate=surrogate, slots=pool_slots(n_traj), hi_mode=hi_mode)
     table = {}
     if fixed_launch:
         sim.engine.handle.call("bd_set_launch", fixed_launch[0], fixed_launch[1])
     elif surrogate is None:
-        best, table = autotune(sim)  # untimed; the run below starts from the restored pool
+        # untimed, on the aged pool that is timed below; the run then starts again from it
+        layouts = DEFAULT_LAYOUTS if _OPTS["layout"] is None else (_OPTS["layout"],)
+        kw = {} if candidates is None else {"candidates": candidates}
+        best, table = autotune(sim, layouts=layouts, aged=aged, **kw)
     sim._setup()
     h = sim.engine.handle
     h.call("bd_sim_reset", None)
@@ -234,7 +237,7 @@ def time_device_arm(s, precision, steps, warmup, K, n_traj, id_offset, dist, fix
     h.call("bd_get_layout", _lib.ptr(lay, _lib.C.c_int32))
     sim.engine.close()
     launch = {"group": int(g[0]), "block": int(g[1]), "grid": int(g[2]), "layout_flags": int(lay[0]),
-              "autotune_steps_per_s": {f"{a}x{b}": round(v) for (a, b), v in table.items()}}
+              "autotune_steps_per_s": {f"{a}x{b}/layout{c}": round(v) for (a, b, c), v in table.items()}}
     return sum(times), times, d, launch
 
 
@@ -273,10 +276,11 @@ def e2e_arm(s, precision, steps, K, n_traj, id_offset, launch):
     return res.total_steps / el, h2d / launches, d2h / launches, res
 
 
-def surrogate_arm(s, steps, warmup, K, n_traj, n_poses, train_steps, members, kon_traj, kon_launches=300, log=None,
-                  aged=None):
+def surrogate_arm(s, steps, warmup, K, n_traj, n_poses, train_steps, members, kon_traj, kon_launches=4000, log=None,
+                  aged=None, n_held=100_000, hi_mode="reference_gpu"):
     """Config 4: train the surrogate on exact-kernel BD poses, evaluate it on held-out poses, time the
-    surrogate stepper like the exact one, and compare k_on of exact and surrogate runs."""
+    surrogate stepper like the exact one, and compare k_on of exact and surrogate runs (each run to the
+    reference's stopping rule, 99.5 % of the trajectories ended)."""
     import torch
 
     from pystarc_b200 import surrogate as sg
@@ -285,8 +289,7 @@ def surrogate_arm(s, steps, warmup, K, n_traj, n_poses, train_steps, members, ko
     t0 = time.perf_counter()
     say = log or (lambda m: None)
     r_lo, r_hi = 25.0, min(80.0, float(s.r_escape))
-    sampler = make_sim(s, "mixed", n_traj, 16)
-    n_held = max(n_poses // 10, 1024)
+    sampler = make_sim(s, "mixed", n_traj, 16, hi_mode=hi_mode)
     c, q = sg.sample_poses(sampler, n_poses + n_held, r_lo=r_lo, r_hi=r_hi)
     eng = sampler.engine
     eng.set_ligand(s.lig_pos - s.lig_pos.mean(axis=0), s.lig_q)
@@ -304,10 +307,14 @@ def surrogate_arm(s, steps, warmup, K, n_traj, n_poses, train_steps, members, ko
                        "tflops": round(members * train_steps * rep.batch * 3 * 2 *
                                        sum(i * o for i, o in ens.dims) / rep.seconds / 1e12, 1)}
     out["heldout"] = sg.heldout_error(ens, spec, c[n_poses:], q[n_poses:], T[n_poses:])
+    trusted = spec.trusted(c[n_poses:])
+    if trusted.any():
+        ch, qh, Th = c[n_poses:][trusted], q[n_poses:][trusted], T[n_poses:][trusted]
+        out["heldout_trust_region"] = sg.heldout_error(ens, spec, ch, qh, Th)
     say(f"surrogate: trained in {rep.seconds:.1f} s, held-out {out['heldout']}")
     out["trust_region_A"] = [round(spec.r_min, 2), round(spec.r_max, 2)]
     # timed like the exact arm: graph launches of K steps, L2 flushed in between
-    sim = make_sim(s, "mixed", n_traj, K, surrogate=(ens, spec), slots=pool_slots(n_traj))
+    sim = make_sim(s, "mixed", n_traj, K, surrogate=(ens, spec), slots=pool_slots(n_traj), hi_mode=hi_mode)
     sim._setup()
     h = sim.engine.handle
     h.call("bd_sim_reset", None)
@@ -336,11 +343,12 @@ def surrogate_arm(s, steps, warmup, K, n_traj, n_poses, train_steps, members, ko
     out["fallback_fraction"] = d["surrogate_fallbacks"] / max(d["surrogate_evals"], 1)
     out["counters"] = {k: int(v) for k, v in d.items()}
     say(f"surrogate: stepper {out['bd_steps_per_s']:.3e} steps/s, fallback {out['fallback_fraction']:.3f}")
-    # k_on: the same trajectories (seed, keyed noise) with and without the surrogate, each given the same
-    # budget of kon_launches x K steps per slot; trajectories unfinished by then are left out of both
+    # k_on: the same trajectories (seed, keyed noise) with and without the surrogate, each run until the
+    # reference's stopping rule (99.5 % ended) or kon_launches launches, whichever comes first; the
+    # trajectories still running then count as max-steps in both
     kon = {}
     D_rel = s.mobility().relative_translational_diffusion()
-    for name, sur in (("plain", None), ("surrogate", (ens, spec))):
+    for name, sur in (() if kon_traj <= 0 else (("plain", None), ("surrogate", (ens, spec)))):
         sm = make_sim(s, "mixed", kon_traj, K, surrogate=sur, termination="reference", seed=4242)
         t1 = time.perf_counter()
         res = sm.run(max_launches=kon_launches)
@@ -352,10 +360,51 @@ def surrogate_arm(s, steps, warmup, K, n_traj, n_poses, train_steps, members, ko
                      "wall_s": round(time.perf_counter() - t1, 1)}
         say(f"surrogate: k_on run {name}: {kon[name]}")
         sm.engine.close()
-    a, b = kon["plain"]["wilson95"], kon["surrogate"]["wilson95"]
-    kon["cis_overlap"] = bool(a[0] <= b[1] and b[0] <= a[1])
-    out["k_on"] = kon
+    if kon:
+        a, b = kon["plain"]["wilson95"], kon["surrogate"]["wilson95"]
+        kon["cis_overlap"] = bool(a[0] <= b[1] and b[0] <= a[1])
+        out["k_on"] = kon
     ens.close()
+    return out
+
+
+PP_CANDIDATES = ((65, 256), (66, 256))
+
+
+def protein_protein_section(args, log):
+    """Config 3 beside the headline: plain FP64, mixed precision, and mixed + surrogate, each timed
+    like the headline arms on an aged protein-protein pool (Zuk RPY mobility).  The pool is a
+    sample of the 1e7-trajectory workload (``--pp-traj`` trajectories, all live at once, aged
+    ``--pp-age`` launches) so that the section takes about a minute."""
+    from pystarc_b200 import synth
+
+    t0 = time.perf_counter()
+    s = synth.config3(scale=1.0, device="cuda")
+    n = args.pp_traj
+    work = tempfile.mkdtemp(prefix="bench_pp_")
+    ager = make_sim(s, "mixed", n, args.inner, slots=pool_slots(n), hi_mode="zuk")
+    aged = age_pool(ager, args.inner, args.pp_age, os.path.join(work, "aged.npz"))
+    ager.engine.close()
+    log(f"protein-protein: system and {args.pp_age}-launch aging in {time.perf_counter() - t0:.1f} s")
+    out = {"workload": WORKLOADS["protein-protein"][0].replace("HI", "Zuk RPY HI"),
+           "timed_pool": f"{n} trajectories aged {args.pp_age} launches of {args.inner} BD steps"}
+    for prec in ("mixed", "fp64"):
+        t, _, d, launch = time_device_arm(s, prec, args.pp_steps, args.warmup, args.inner, n, 0, None, aged=aged,
+                                          candidates=PP_CANDIDATES, hi_mode="zuk")
+        out[prec] = {"bd_steps_per_s": d["steps"] / t, "steps": int(d["steps"]), "launch": launch,
+                     "rev_stencils_per_step": d["rev_evals"] / max(d["steps"], 1),
+                     "grid_stencils_per_step": d["grid_evals"] / max(d["steps"], 1)}
+        log(f"protein-protein {prec}: {d['steps'] / t:.3e} steps/s")
+    out["mixed_over_fp64"] = out["mixed"]["bd_steps_per_s"] / out["fp64"]["bd_steps_per_s"]
+    if not args.no_surrogate:
+        sur = surrogate_arm(s, args.pp_steps, args.warmup, args.inner, n, args.pp_sur_poses, args.pp_sur_train_steps,
+                            args.sur_members, kon_traj=0, log=log, aged=aged, n_held=20_000, hi_mode="zuk")
+        out["surrogate"] = sur
+        out["surrogate_over_fp64"] = sur["bd_steps_per_s"] / out["fp64"]["bd_steps_per_s"]
+    import shutil
+
+    shutil.rmtree(work, ignore_errors=True)
+    out["seconds"] = round(time.perf_counter() - t0, 1)
     return out
 
 
@@ -365,8 +414,11 @@ def hetero_arm(systems, precision, steps, warmup, K):
 
     from pystarc_b200.multi import B200MultiBatch
 
+    from pystarc_b200.autotune import autotune_multi
+
     sims = [make_sim(s, precision, s.n_traj, K) for s in systems]
     batch = B200MultiBatch(sims, steps_per_launch=K)
+    best_layout, tune = autotune_multi(batch)  # untimed; the timed run below starts fresh
     batch.setup()
     batch._call("bd_multi_reset", None)
     stream = torch.cuda.current_stream()
@@ -388,7 +440,9 @@ def hetero_arm(systems, precision, steps, warmup, K):
     batch.close()
     for sm in sims:
         sm.engine.close()
-    return t, {k: c1[k] - c0[k] for k in c1}
+    d = {k: c1[k] - c0[k] for k in c1}
+    d["autotune"] = {"layout": best_layout, "steps_per_s": {f"layout{k}": round(v) for k, v in tune.items()}}
+    return t, d
 
 
 def hetero_main(args):
@@ -409,6 +463,7 @@ def hetero_main(args):
     from pystarc_b200.multi import B200MultiBatch
 
     torch.cuda.synchronize()
+    _OPTS["layout"] = d_mixed["autotune"]["layout"]  # the tuned layout, through the public API
     te = time.perf_counter()
     sims = [make_sim(s, "mixed", s.n_traj, args.inner) for s in systems]
     batch = B200MultiBatch(sims, steps_per_launch=args.inner, launches_per_poll=1)
@@ -429,7 +484,8 @@ def hetero_main(args):
                    "systems": [s.meta | {"n_traj": s.n_traj} for s in systems],
                    "l2": "flushed (256 MiB write) between launches", "parallelism": "one persistent launch"},
         "variants": {"fp64": {"bd_steps_per_s": d_fp64["steps"] / t_fp64, "steps": d_fp64["steps"]}},
-        "counters": {k: int(v) for k, v in d_mixed.items()},
+        "counters": {k: int(v) for k, v in d_mixed.items() if k != "autotune"},
+        "autotune": d_mixed["autotune"],
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "peak_kind": peak_kind,
                      "algorithmic_bytes": "224 B per (atom, grid) stencil + 128 B per trajectory-step"},
@@ -583,15 +639,22 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--layout", type=int, default=-1,
                     help="device data layout flags (1 stage receptor, 2 windows for 1-channel grids, "
-                         "4 windows for the paired grid; -1: library default)")
+                         "4 windows for the paired grid, 8 cubes for the ligand Born grid; -1: autotuned)")
     ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate arm (config 4)")
     ap.add_argument("--age", type=int, default=64,
                     help="untimed launches that age the pool before every timed arm (0: time from the b-sphere)")
-    ap.add_argument("--sur-poses", type=int, default=200_000)
-    ap.add_argument("--sur-train-steps", type=int, default=8000)
+    ap.add_argument("--sur-poses", type=int, default=2_000_000)
+    ap.add_argument("--sur-train-steps", type=int, default=20_000)
     ap.add_argument("--sur-members", type=int, default=5)
     ap.add_argument("--sur-kon-traj", type=int, default=20_000)
+    ap.add_argument("--no-protein-protein", action="store_true",
+                    help="skip the protein-protein variants (config 3) of the default run")
+    ap.add_argument("--pp-traj", type=int, default=200_000)
+    ap.add_argument("--pp-age", type=int, default=16)
+    ap.add_argument("--pp-steps", type=int, default=3)
+    ap.add_argument("--pp-sur-poses", type=int, default=500_000)
+    ap.add_argument("--pp-sur-train-steps", type=int, default=8000)
     args = ap.parse_args()
     _OPTS["layout"] = None if args.layout < 0 else args.layout
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -667,8 +730,11 @@ def main():
     t_fp64, tl_fp64, d_fp64, launch64 = time_device_arm(s, "fp64", args.steps, args.warmup, args.inner, n_traj,
                                                         id_offset, dist, fixed, aged=aged)
     _progress(f"exact arms: mixed {d_mixed['steps'] / t_mixed:.3e}, fp64 {d_fp64['steps'] / t_fp64:.3e} steps/s")
+    layout_cli = _OPTS["layout"]
+    _OPTS["layout"] = launch["layout_flags"]  # the tuned shape and layout, through the public API
     e2e_val, h2d, d2h, e2e_res = e2e_arm(s, "mixed", args.age + max(args.steps, 20), args.inner, n_traj, id_offset,
                                          (launch["group"], launch["block"]))
+    _OPTS["layout"] = layout_cli
     _progress(f"e2e arm: {e2e_val:.3e} steps/s")
     t_max = t_mixed
     steps_all = d_mixed["steps"]
@@ -691,7 +757,7 @@ def main():
     algo_bytes = gathers * ALGO_BYTES_PER_GATHER + d_mixed["steps"] * STATE_BYTES_PER_STEP
     achieved = algo_bytes / t_mixed / 1e9
     traffic, traffic_note = None, None
-    tf = ROOT / "profiles" / "step_kernel_warp_traffic.json"
+    tf = ROOT / "profiles" / "stepper_traffic.json"
     if args.workload == "protein-ligand" and tf.exists():
         # DRAM bytes (read + write) of one stepper launch, from the ncu capture of a small case scaled by the
         # trajectory-steps of this launch (the figure and its scaling are stated in the file)
@@ -742,6 +808,8 @@ def main():
         line["variants"]["surrogate"] = surrogate_arm(s, args.steps, args.warmup, args.inner, n_traj, args.sur_poses,
                                                       args.sur_train_steps, args.sur_members, args.sur_kon_traj,
                                                       log=_progress, aged=aged)
+    if world == 1 and args.workload == "protein-ligand" and not args.no_protein_protein:
+        line["variants"]["protein_protein"] = protein_protein_section(args, _progress)
     if world == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
         init = aged_poses(aged, cores * 64) if aged is not None else None

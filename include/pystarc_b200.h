@@ -239,7 +239,7 @@ int bd_get_launch(BdHandle* h, int* group, int* block_threads, int* grid_blocks)
  * The same values enter the same arithmetic in every layout: results are identical. */
 enum { BD_LAYOUT_STAGE_RECEPTOR = 1, BD_LAYOUT_WINDOWS_1 = 2, BD_LAYOUT_WINDOWS_2 = 4, BD_LAYOUT_CUBES_1 = 8 };
 #define BD_CUBE_MAX_BYTES (48ll * 1024 * 1024)
-#define BD_LAYOUT_DEFAULT BD_LAYOUT_WINDOWS_1
+#define BD_LAYOUT_DEFAULT (BD_LAYOUT_WINDOWS_1 | BD_LAYOUT_CUBES_1)
 #define BD_STAGE_MAX_BYTES (64 * 1024)
 int bd_set_layout(BdHandle* h, int flags);
 int bd_get_layout(BdHandle* h, int* flags);
