@@ -316,6 +316,10 @@ int bd_mlp_train_step(BdMlp* m, int member, int n, const float* X, const float* 
  * (hidden <= 256, in_dim <= 32, out_dim <= 32; other shapes use 0); 0 = the mma.sync GEMM chain
  * the training kernels use.  Both give the same values up to FP32 summation order. */
 int bd_mlp_set_inference(BdMlp* m, int mode);
+/* No reference counterpart.  GEMMs of training (forward, weight and activation gradients) and of
+ * the GEMM-chain inference: 1 (default) on tcgen05 with TMEM accumulators, 0 on mma.sync.  Both
+ * accumulate BF16 products in FP32 with the same fused epilogues. */
+int bd_mlp_set_gemm(BdMlp* m, int mode);
 /* `steps` Adam steps of one member on random batches (rows drawn with replacement by a
  * counter-based hash of seed, member and step) of device-resident data X (n_data x in_dim),
  * T (n_data x out_dim).  The step is captured once as a CUDA graph and replayed; loss_trace

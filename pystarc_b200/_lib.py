@@ -141,6 +141,7 @@ SIGNATURES = {
     "bd_mlp_ensemble": (C.c_int, [P, C.c_int64, P, P, P, P]),
     "bd_mlp_train": (C.c_int, [P, C.c_int, C.c_int64, P, P, C.c_int, C.c_int, C.c_float, C.c_uint64, P, P]),
     "bd_mlp_set_inference": (C.c_int, [P, C.c_int]),
+    "bd_mlp_set_gemm": (C.c_int, [P, C.c_int]),
 }
 
 _LIB = None

@@ -529,6 +529,176 @@ __global__ void __launch_bounds__(512, 1) mlp_forward_tc_kernel(TcArgs a) {
 }
 
 
+// ---------------------------------------------------------------------------
+// The training GEMMs on tcgen05: C[M][N] = A[M][K] B[N][K]^T with the fused epilogues of gemm_nt.
+// One CTA of 128 threads per 128-row tile (looping over its share of the tiles) and N columns
+// (N <= 256, a multiple of 16): K is staged 64 at a time into two shared-memory buffers in the
+// canonical K-major no-swizzle layout by cp.async (rows past M read as zero), one elected thread
+// issues the 128 x N x 16 MMAs into a TMEM accumulator and commits them to the buffer's mbarrier,
+// and the next chunk loads while they run.  The four warps read their 32 TMEM lanes (rows) back
+// with tcgen05.ld for the epilogue.  Split-K (gridDim.z) writes partials for a fixed-order
+// reduction, as gemm_nt does.
+// ---------------------------------------------------------------------------
+constexpr int kGtKc = 64;                                  // K per staged chunk
+constexpr int kGtSbo = kGtKc / 8 * 128;                    // bytes between 8-row groups of a chunk
+constexpr int kGtBytesA = 128 * kGtKc * 2;                 // 16 KB
+constexpr int kGtBytesB = 256 * kGtKc * 2;                 // 32 KB
+constexpr int kGtSmem = 2 * (kGtBytesA + kGtBytesB) + 64;  // two stages + two mbarriers + TMEM address
+
+template <int EPI>
+__global__ void __launch_bounds__(128, 1) gemm_nt_tc(GemmArgs g, int BN) {
+  extern __shared__ __align__(1024) unsigned char gt_smem[];
+  // stage st: A tile at st * (A + B) bytes, B tile right after it
+  auto As = [&](int st) { return gt_smem + st * (kGtBytesA + kGtBytesB); };
+  auto Bs = [&](int st) { return gt_smem + st * (kGtBytesA + kGtBytesB) + kGtBytesA; };
+  uint64_t* bar = reinterpret_cast<uint64_t*>(gt_smem + 2 * (kGtBytesA + kGtBytesB));
+  uint32_t* taddr_slot = reinterpret_cast<uint32_t*>(gt_smem + 2 * (kGtBytesA + kGtBytesB) + 16);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int n0 = blockIdx.x * BN;
+  const int M = g.m_dev ? min(g.M, *g.m_dev) : g.M;
+  const int kb = blockIdx.z * g.k_per_split, ke = min(g.K, kb + g.k_per_split);
+  if (blockIdx.y * 128 >= M || kb >= ke) return;  // whole block, before any allocation
+  const int nb = min(BN, g.N - n0);  // columns of this block (a multiple of 16)
+  const uint32_t ncols = nb <= 32 ? 32 : nb <= 64 ? 64 : nb <= 128 ? 128 : 256;
+  const uint32_t bar0 = smem_u32(bar), bar1 = smem_u32(bar + 1);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(taddr_slot)),
+                 "r"(ncols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar0), "r"(1));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar1), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *taddr_slot;
+  const uint32_t idesc = umma_idesc_bf16(128, nb);
+  uint32_t phase[2] = {0u, 0u};
+  bool pending[2] = {false, false};
+  bool ok = true;
+  auto wait_stage = [&](int st) {
+    if (pending[st]) {
+      ok = mbar_wait(st ? bar1 : bar0, phase[st]) && ok;
+      phase[st] ^= 1u;
+      pending[st] = false;
+    }
+  };
+  for (int m0 = blockIdx.y * 128; m0 < M; m0 += gridDim.y * 128) {
+    int kc = 0;
+    for (int k = kb; k < ke; k += kGtKc, ++kc) {
+      const int st = kc & 1, klen = min(kGtKc, ke - k), nch = klen / 8;
+      wait_stage(st);  // the MMAs that read this buffer two chunks ago are done
+      for (int c = tid; c < 128 * nch; c += 128) {
+        const int r = c / nch, kk = (c % nch) * 8;
+        const bool in = m0 + r < M;
+        cp_async16(As(st) + kmajor_off(r, kk, kGtSbo), g.A + (size_t)(in ? m0 + r : 0) * g.lda + k + kk, in ? 16 : 0);
+      }
+      for (int c = tid; c < nb * nch; c += 128) {
+        const int r = c / nch, kk = (c % nch) * 8;
+        cp_async16(Bs(st) + kmajor_off(r, kk, kGtSbo), g.B + (size_t)(n0 + r) * g.ldb + k + kk, 16);
+      }
+      cp_async_commit();
+      cp_async_wait<0>();
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncthreads();
+      if (tid == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        for (int j = 0; j < klen / 16; ++j) {
+          const uint64_t ad = umma_desc(smem_u32(As(st)) + j * 256, 128, kGtSbo);
+          const uint64_t bd = umma_desc(smem_u32(Bs(st)) + j * 256, 128, kGtSbo);
+          const uint32_t acc = (k > kb || j > 0) ? 1u : 0u;
+          asm volatile(
+              "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+              "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         st ? bar1 : bar0)
+                     : "memory");
+      }
+      pending[st] = true;
+    }
+    wait_stage(0);
+    wait_stage(1);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // epilogue: thread = row m0 + 32 warp + lane, 32 columns per TMEM load
+    const int r = m0 + warp * 32 + lane;
+    for (int c0 = 0; c0 < nb; c0 += 32) {
+      uint32_t v[32];
+      const uint32_t addr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+          "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+            "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+            "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+          : "r"(addr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (r >= M) continue;
+      const int cw = min(32, nb - c0);  // columns of this load that exist (32 or 16)
+      const int cb = n0 + c0;           // first column
+      float f[32];
+#pragma unroll
+      for (int e = 0; e < 32; ++e) f[e] = ok ? __uint_as_float(v[e]) : __int_as_float(0x7fc00000);
+      if constexpr (EPI == EPI_PARTIAL) {
+        float* p = g.C + blockIdx.z * g.split_stride + (size_t)r * g.ldc + cb;
+#pragma unroll
+        for (int e = 0; e < 32; e += 4)
+          if (e < cw) *reinterpret_cast<float4*>(p + e) = make_float4(f[e], f[e + 1], f[e + 2], f[e + 3]);
+      } else if constexpr (EPI == EPI_OUT_FWD) {
+#pragma unroll
+        for (int e = 0; e < 32; ++e)
+          if (e < cw && cb + e < g.n_real) g.C[(size_t)r * g.ldc + cb + e] = f[e] + g.bias[cb + e];
+      } else {
+        uint32_t pk[16];
+#pragma unroll
+        for (int e = 0; e < 32; e += 2) {
+          float o0, o1;
+          if constexpr (EPI == EPI_HIDDEN_FWD) {
+            f[e] += g.bias[cb + e];
+            f[e + 1] += g.bias[cb + e + 1];
+            o0 = silu(f[e]);
+            o1 = silu(f[e + 1]);
+          } else {  // EPI_HIDDEN_BWD: f = dA, output dZ
+            o0 = e < cw ? f[e] * silu_grad(g.Zin[(size_t)r * g.ldz + cb + e]) : 0.f;
+            o1 = e < cw ? f[e + 1] * silu_grad(g.Zin[(size_t)r * g.ldz + cb + e + 1]) : 0.f;
+          }
+          __nv_bfloat162 h2 = __floats2bfloat162_rn(o0, o1);
+          pk[e / 2] = *reinterpret_cast<uint32_t*>(&h2);
+        }
+        if (EPI == EPI_HIDDEN_FWD && g.C) {
+          float* z = g.C + (size_t)r * g.ldc + cb;
+#pragma unroll
+          for (int e = 0; e < 32; e += 4)
+            if (e < cw) *reinterpret_cast<float4*>(z + e) = make_float4(f[e], f[e + 1], f[e + 2], f[e + 3]);
+        }
+        if (g.O) {
+          bf16* o = g.O + (size_t)r * g.ldo + cb;
+#pragma unroll
+          for (int e = 0; e < 32; e += 8)
+            if (e < cw) *reinterpret_cast<uint4*>(o + e) = make_uint4(pk[e / 2], pk[e / 2 + 1], pk[e / 2 + 2], pk[e / 2 + 3]);
+        }
+        if (g.Ot) {
+#pragma unroll
+          for (int e = 0; e < 32; ++e) {
+            if (e >= cw) break;
+            const uint32_t w = pk[e / 2];
+            const unsigned short h = (e & 1) ? (unsigned short)(w >> 16) : (unsigned short)(w & 0xffffu);
+            g.Ot[(size_t)(cb + e) * g.ldot + r] = __ushort_as_bfloat16(h);
+          }
+        }
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();  // every lane is read before the next tile's MMAs overwrite the accumulator
+  }
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
+}
+
 // Adam on the FP32 parameters, then the padded BF16 copies W [out_pad][in_pad] and W^T [in_pad][out_pad].
 __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ grad, float* __restrict__ m1,
                             float* __restrict__ m2, long long n_params, float lr, float b1, float b2, float eps,
@@ -634,6 +804,8 @@ struct BdMlp {
   float *Y = nullptr, *part = nullptr, *loss_part = nullptr, *loss_tmp = nullptr;
   long long part_stride = 0;
   int inference = 1;  // 1: tcgen05 kernel when the shape allows, 0: mma.sync GEMM chain
+  int gemm_tc = 1;    // GEMMs of training and of the GEMM chain: 1 tcgen05 (gemm_nt_tc), 0 mma.sync
+  bool gt_attr = false;
   bool tc_attr = false;
   // inference scratch (infer_cap rows)
   int infer_cap = 0;
@@ -689,9 +861,31 @@ int launch_gemm(BdMlp* m, const GemmArgs& g, int splits, cudaStream_t s) {
   return BD_OK;
 }
 
-// C = A B^T with the tile picked from N (hidden widths use 128-wide tiles).
+template <int EPI>
+int launch_gemm_tc(BdMlp* m, const GemmArgs& g, int splits, cudaStream_t s) {
+  if (!m->gt_attr) {
+    MCK(m, cudaFuncSetAttribute(gemm_nt_tc<EPI_HIDDEN_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGtSmem));
+    MCK(m, cudaFuncSetAttribute(gemm_nt_tc<EPI_OUT_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGtSmem));
+    MCK(m, cudaFuncSetAttribute(gemm_nt_tc<EPI_HIDDEN_BWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGtSmem));
+    MCK(m, cudaFuncSetAttribute(gemm_nt_tc<EPI_PARTIAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGtSmem));
+    m->gt_attr = true;
+  }
+  const int BN = std::min(g.N, 256);
+  const int nx = (g.N + BN - 1) / BN, tiles = (g.M + 127) / 128;
+  // one CTA per SM at most (TMEM and shared memory); each loops over its share of the row tiles
+  const int ny = std::max(1, std::min(tiles, (m->n_sm + nx * splits - 1) / (nx * splits)));
+  dim3 grid(nx, ny, splits);
+  gemm_nt_tc<EPI><<<grid, 128, kGtSmem, s>>>(g, BN);
+  MCK(m, cudaGetLastError());
+  return BD_OK;
+}
+
+// C = A B^T: tcgen05 (N a multiple of 16, K of 32), else mma.sync with the tile picked from N
+// (hidden widths use 128-wide tiles).
 template <int EPI>
 int gemm(BdMlp* m, const GemmArgs& g, int splits, cudaStream_t s) {
+  if (m->gemm_tc && g.N % 16 == 0 && g.K % 32 == 0 && g.k_per_split % 32 == 0)
+    return launch_gemm_tc<EPI>(m, g, splits, s);
   if (g.N >= 128) return launch_gemm<128, 128, 2, 4, EPI>(m, g, splits, s);
   return launch_gemm<128, 32, 4, 2, EPI>(m, g, splits, s);
 }
@@ -1254,6 +1448,18 @@ int bd_mlp_set_inference(BdMlp* m, int mode) {
   if (!m) return BD_ERR_ARG;
   if (mode != 0 && mode != 1) return mfail(m, BD_ERR_ARG, "inference mode must be 0 (mma.sync) or 1 (tcgen05)");
   m->inference = mode;
+  return BD_OK;
+}
+
+int bd_mlp_set_gemm(BdMlp* m, int mode) {
+  if (!m) return BD_ERR_ARG;
+  if (mode != 0 && mode != 1) return mfail(m, BD_ERR_ARG, "GEMM mode must be 0 (mma.sync) or 1 (tcgen05)");
+  if (mode != m->gemm_tc && m->train_graph) {  // the captured training step holds the old kernels
+    cudaGraphExecDestroy(m->train_graph);
+    m->train_graph = nullptr;
+    m->tg_member = -1;
+  }
+  m->gemm_tc = mode;
   return BD_OK;
 }
 

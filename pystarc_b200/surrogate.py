@@ -184,6 +184,10 @@ class MLPEnsemble:
         """1: tcgen05 inference kernel (default), 0: the mma.sync GEMM chain."""
         self._call("bd_mlp_set_inference", int(mode))
 
+    def set_gemm(self, mode):
+        """GEMMs of training and of the GEMM chain: 1 tcgen05 (default), 0 mma.sync."""
+        self._call("bd_mlp_set_gemm", int(mode))
+
     def train(self, member, X, T, batch, steps, lr, seed=0, trace=True):
         """``steps`` Adam steps on random batches of device-resident (X, T); returns the loss trace."""
         import torch

@@ -135,3 +135,29 @@ def test_tcgen05_inference_matches_mma_sync_and_oracle(shape, n):
     Yo, _ = om.forward(e.get_params(1).astype(np.float64), e.dims, X[:k], rounding=True)
     assert np.max(np.abs(Y_tc[:k] - Yo)) <= 2e-2 * np.max(np.abs(Yo)) + 1e-4
     e.close()
+
+
+@pytest.mark.parametrize("shape,n", [((13, 256, 4, 6), 4096), ((7, 128, 2, 3), 2080)])
+def test_tcgen05_training_gemms_match_mma_sync(shape, n):
+    """The training GEMMs on tcgen05 (forward, weight and activation gradients, split-K partials) give
+    the loss and the per-layer gradients of the mma.sync GEMMs to BF16-rounding accuracy."""
+    in_dim, hidden, n_hidden, out_dim = shape
+    e = _ens(1, in_dim, hidden, n_hidden, out_dim, seed=11)
+    X, T = _data(n, in_dim, out_dim, seed=6)
+    e.set_gemm(1)
+    l_tc, g_tc = e.grad(0, X, T)
+    Y_tc = e.forward(0, X).cpu().numpy()
+    e.set_gemm(0)
+    l_mma, g_mma = e.grad(0, X, T)
+    Y_mma = e.forward(0, X).cpu().numpy()
+    e.set_gemm(1)
+    assert abs(l_tc - l_mma) <= 1e-3 * l_mma
+    assert np.max(np.abs(Y_tc - Y_mma)) <= 1e-2 * np.max(np.abs(Y_mma))
+    g_tc, g_mma = g_tc.cpu().numpy().astype(np.float64), g_mma.cpu().numpy().astype(np.float64)
+    k = 0
+    for i, o in e.dims:
+        for size in (o * i, o):
+            a, b = g_tc[k:k + size], g_mma[k:k + size]
+            assert np.linalg.norm(a - b) <= 1e-2 * np.linalg.norm(b) + 1e-9, (i, o, size)
+            k += size
+    e.close()
