@@ -254,14 +254,32 @@ def aged_poses(path, n, seed=7):
     return c, q
 
 
-def e2e_arm(s, precision, steps, K, n_traj, id_offset, launch):
-    """Through the public API from host arrays: engine construction (grid uploads), run() of the
-    first ``steps`` launches from the b-sphere (the aging and the timed window together), outcomes."""
+def e2e_arm(s, precision, steps, K, n_traj, id_offset, launch, aged=None):
+    """Through the public API with host buffers: the engine is built from host arrays (grid and atom
+    uploads); ``run()`` resumes the saved aged pool through its checkpoint mechanism (the slots and
+    per-trajectory outcomes are copied to the device), advances ``steps`` launches in the regime the
+    device arms time, polling the counters after every launch, and copies the outcomes back.
+    Without an aged pool it starts from the b-sphere."""
+    import shutil
+
     import torch
 
+    from pystarc_b200 import _lib
+
+    work = tempfile.mkdtemp(prefix="bench_e2e_")
+    steps0, h2d_pool = 0, 0
+    if aged is not None:
+        shutil.copy(aged, os.path.join(work, "checkpoint_b200.npz"))
+        with np.load(aged) as d:
+            steps0 = int(d["counters"][_lib.CTR_NAMES.index("steps")])
+            h2d_pool = sum(d[k].nbytes for k in ("c", "q", "traj", "steps", "rets", "status", "state", "counters",
+                                                  "out_status", "out_steps", "out_returns"))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     sim = make_sim(s, precision, n_traj, K, id_offset, slots=pool_slots(n_traj))
+    if aged is not None:
+        sim.params.checkpoint_interval = 1 << 60  # resume the saved pool; never write a new checkpoint
+        sim.params._work_dir = work
     sim.engine.handle.call("bd_set_launch", launch[0], launch[1])
     sim.M = 1
     res = sim.run(max_launches=steps)
@@ -269,14 +287,15 @@ def e2e_arm(s, precision, steps, K, n_traj, id_offset, launch):
     el = time.perf_counter() - t0
     h2d = sum(np.asarray(g.data).nbytes for g in s.elec_grids[:1] + s.born_grids[:1] + s.lig_born_grids)
     h2d += np.asarray(s.elec_grids[0].data).nbytes * 2  # interleaved elec+Born copy of the shared lattice
-    h2d += (len(s.rec_q) + len(s.lig_q)) * 32
-    d2h = n_traj * 9 + steps * 12 * 8 * 2
-    launches = max(1, steps)
+    h2d += (len(s.rec_q) + len(s.lig_q)) * 32 + h2d_pool
+    d2h = n_traj * 9 + steps * (_lib.N_CTR * 8 + 4)  # outcomes, and the counters and live count of every poll
     sim.engine.close()
-    return res.total_steps / el, h2d / launches, d2h / launches, res
+    shutil.rmtree(work, ignore_errors=True)
+    launches = max(1, steps)
+    return (res.total_steps - steps0) / el, h2d / launches, d2h / launches, res
 
 
-def surrogate_arm(s, steps, warmup, K, n_traj, n_poses, train_steps, members, kon_traj, kon_launches=4000, log=None,
+def surrogate_arm(s, steps, warmup, K, n_traj, n_poses, train_steps, members, kon_traj, kon_launches=1500, log=None,
                   aged=None, n_held=100_000, hi_mode="reference_gpu"):
     """Config 4: train the surrogate on exact-kernel BD poses, evaluate it on held-out poses, time the
     surrogate stepper like the exact one, and compare k_on of exact and surrogate runs (each run to the
@@ -293,7 +312,7 @@ def surrogate_arm(s, steps, warmup, K, n_traj, n_poses, train_steps, members, ko
     c, q = sg.sample_poses(sampler, n_poses + n_held, r_lo=r_lo, r_hi=r_hi)
     eng = sampler.engine
     eng.set_ligand(s.lig_pos - s.lig_pos.mean(axis=0), s.lig_q)
-    T = sg.exact_targets(eng, c, q)
+    T = sg.exact_targets(eng, c, q, precision="mixed")
     eng.close()
     out["data_s"] = round(time.perf_counter() - t0, 1)
     say(f"surrogate: {len(c)} poses and exact targets in {out['data_s']} s")
@@ -647,13 +666,13 @@ def main():
     ap.add_argument("--sur-poses", type=int, default=2_000_000)
     ap.add_argument("--sur-train-steps", type=int, default=20_000)
     ap.add_argument("--sur-members", type=int, default=5)
-    ap.add_argument("--sur-kon-traj", type=int, default=20_000)
+    ap.add_argument("--sur-kon-traj", type=int, default=8_000)
     ap.add_argument("--no-protein-protein", action="store_true",
                     help="skip the protein-protein variants (config 3) of the default run")
     ap.add_argument("--pp-traj", type=int, default=200_000)
     ap.add_argument("--pp-age", type=int, default=16)
     ap.add_argument("--pp-steps", type=int, default=3)
-    ap.add_argument("--pp-sur-poses", type=int, default=500_000)
+    ap.add_argument("--pp-sur-poses", type=int, default=200_000)
     ap.add_argument("--pp-sur-train-steps", type=int, default=8000)
     args = ap.parse_args()
     _OPTS["layout"] = None if args.layout < 0 else args.layout
@@ -732,8 +751,8 @@ def main():
     _progress(f"exact arms: mixed {d_mixed['steps'] / t_mixed:.3e}, fp64 {d_fp64['steps'] / t_fp64:.3e} steps/s")
     layout_cli = _OPTS["layout"]
     _OPTS["layout"] = launch["layout_flags"]  # the tuned shape and layout, through the public API
-    e2e_val, h2d, d2h, e2e_res = e2e_arm(s, "mixed", args.age + max(args.steps, 20), args.inner, n_traj, id_offset,
-                                         (launch["group"], launch["block"]))
+    e2e_val, h2d, d2h, e2e_res = e2e_arm(s, "mixed", max(args.steps, 10), args.inner, n_traj, id_offset,
+                                         (launch["group"], launch["block"]), aged=aged)
     _OPTS["layout"] = layout_cli
     _progress(f"e2e arm: {e2e_val:.3e} steps/s")
     t_max = t_mixed
@@ -800,7 +819,9 @@ def main():
                      "algorithmic_bytes": "224 B per (atom, grid) stencil + 128 B per trajectory-step"},
         "cupy_reference": cupy_reference(),
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                "note": "B200ForceEngine + B200BatchSimulator.run() from host arrays, incl. grid upload"},
+                "note": ("B200ForceEngine from host arrays (grid uploads) + B200BatchSimulator.run() resuming the "
+                         "aged pool from its checkpoint file (slots copied host-to-device), "
+                         f"{max(args.steps, 10)} launches with a counter poll after each, outcomes copied back")},
         "gpu_launches": 3 * args.steps,
         "clocks": ck,
     }

@@ -265,11 +265,12 @@ def sample_poses(sim, n_poses, r_lo=25.0, r_hi=80.0, launches_between=2, steps_p
     return c, q
 
 
-def exact_targets(engine, c, q, chunk=200_000):
-    """Exact reverse-Born plus far-field force and torque (n, 6) of the engine's ligand at poses."""
+def exact_targets(engine, c, q, chunk=200_000, precision="fp64"):
+    """Exact reverse-Born plus far-field force and torque (n, 6) of the engine's ligand at poses
+    (``precision="mixed"``: FP32 force arithmetic, ~1e-6 relative, far below the network's error)."""
     out = []
     for i in range(0, len(c), chunk):
-        F, T, _ = engine.eval_poses(c[i:i + chunk], q[i:i + chunk], precision="fp64",
+        F, T, _ = engine.eval_poses(c[i:i + chunk], q[i:i + chunk], precision=precision,
                                     terms=_lib.TERM_FARFIELD | _lib.TERM_REV_BORN)
         out.append(np.concatenate([F, T], axis=1))
     return np.concatenate(out) if out else np.zeros((0, 6))

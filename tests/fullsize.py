@@ -228,6 +228,25 @@ def identity_run(name, n=32, launches=6, K=16, torque=None, s=None, hi_mode="ref
             "start": (c0, q0)}
 
 
+def oracle_sensitivity(name, start, M, torque=None, s=None, hi_mode="reference_gpu", rel=1e-13):
+    """Per-trajectory pose change of the oracle run from ``start`` when every force is scaled by
+    (1 + rel): how strongly the dynamics amplify a rounding-sized force difference in M steps."""
+    s = s or system(name)
+    torque = torque or ("centroid" if len(s.lig_q) > 100 else "zero")
+    c0, q0 = start
+    n = len(c0)
+    eo = oracle_engine(s, born_chunk_skip=False)
+    out = []
+    for eps in (0.0, rel):
+        def fn(*a, _e=eps, **k):
+            F, T, E = eo(*a, torque_mode="centroid", **k) if torque == "centroid" else eo(*a, **k)
+            return F * (1.0 + _e), T, E
+
+        out.append(ost.run(step_system(s, fn), step_params(s, n, s.seed, M, hi_mode=hi_mode), noise="philox",
+                           termination="complete", init=(c0, q0)))
+    return np.max(np.abs(out[0].pos - out[1].pos), axis=1)
+
+
 def analytic_p_rxn(s, return_prob):
     """Exact reaction probability of radial diffusion from b with absorption at the reaction
     distance a and, at r_escape = q, a return to b with probability ``return_prob`` (the
