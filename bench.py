@@ -309,13 +309,14 @@ def surrogate_arm(s, steps, warmup, K, n_traj, n_poses, train_steps, members, ko
     say = log or (lambda m: None)
     r_lo, r_hi = 25.0, min(80.0, float(s.r_escape))
     sampler = make_sim(s, "mixed", n_traj, 16, hi_mode=hi_mode)
-    c, q = sg.sample_poses(sampler, n_poses + n_held, r_lo=r_lo, r_hi=r_hi)
+    c, q = sg.sample_poses(sampler, n_poses + n_held, r_lo=r_lo, r_hi=r_hi, max_seconds=300.0)
+    say(f"surrogate: {len(c)} poses sampled in {time.perf_counter() - t0:.1f} s")
     eng = sampler.engine
     eng.set_ligand(s.lig_pos - s.lig_pos.mean(axis=0), s.lig_q)
     T = sg.exact_targets(eng, c, q, precision="mixed")
     eng.close()
     out["data_s"] = round(time.perf_counter() - t0, 1)
-    say(f"surrogate: {len(c)} poses and exact targets in {out['data_s']} s")
+    say(f"surrogate: exact targets, {out['data_s']} s with the sampling")
     spec = sg.SurrogateSpec(r_scale=80.0)
     spec.r_min = sg.contact_distance(s.rec_pos, s.lig_pos) + 8.0
     spec.r_max = r_hi
@@ -415,7 +416,7 @@ def protein_protein_section(args, log):
                      "grid_stencils_per_step": d["grid_evals"] / max(d["steps"], 1)}
         log(f"protein-protein {prec}: {d['steps'] / t:.3e} steps/s")
     out["mixed_over_fp64"] = out["mixed"]["bd_steps_per_s"] / out["fp64"]["bd_steps_per_s"]
-    if not args.no_surrogate:
+    if args.pp_surrogate and not args.no_surrogate:
         sur = surrogate_arm(s, args.pp_steps, args.warmup, args.inner, n, args.pp_sur_poses, args.pp_sur_train_steps,
                             args.sur_members, kon_traj=0, log=log, aged=aged, n_held=20_000, hi_mode="zuk")
         out["surrogate"] = sur
@@ -672,6 +673,8 @@ def main():
     ap.add_argument("--pp-traj", type=int, default=200_000)
     ap.add_argument("--pp-age", type=int, default=16)
     ap.add_argument("--pp-steps", type=int, default=3)
+    ap.add_argument("--pp-surrogate", action="store_true",
+                    help="also train and time a surrogate on the protein-protein workload (minutes)")
     ap.add_argument("--pp-sur-poses", type=int, default=200_000)
     ap.add_argument("--pp-sur-train-steps", type=int, default=8000)
     args = ap.parse_args()

@@ -531,28 +531,32 @@ __global__ void __launch_bounds__(512, 1) mlp_forward_tc_kernel(TcArgs a) {
 
 // ---------------------------------------------------------------------------
 // The training GEMMs on tcgen05: C[M][N] = A[M][K] B[N][K]^T with the fused epilogues of gemm_nt.
-// One CTA of 128 threads per 128-row tile (looping over its share of the tiles) and N columns
-// (N <= 256, a multiple of 16): K is staged 64 at a time into two shared-memory buffers in the
-// canonical K-major no-swizzle layout by cp.async (rows past M read as zero), one elected thread
-// issues the 128 x N x 16 MMAs into a TMEM accumulator and commits them to the buffer's mbarrier,
-// and the next chunk loads while they run.  The four warps read their 32 TMEM lanes (rows) back
-// with tcgen05.ld for the epilogue.  Split-K (gridDim.z) writes partials for a fixed-order
-// reduction, as gemm_nt does.
+// One CTA of 128 threads per 128-row tile (looping over its share of the tiles) and BN columns
+// (BN <= 256, a multiple of 16): K is staged 64 at a time into kGtStages shared-memory buffers in
+// the canonical K-major no-swizzle layout by cp.async (rows past M read as zero).  The first
+// kGtStages - 1 chunks load up front; one elected thread issues each chunk's 128 x BN x 16 MMAs
+// into a TMEM accumulator as soon as it is in and commits them to the buffer's mbarrier, and the
+// chunk kGtStages - 1 ahead then loads into the buffer the previous chunk's MMAs release.  The four
+// warps read their 32 TMEM lanes (rows) back with tcgen05.ld for the epilogue.  Split-K
+// (gridDim.z) writes partials for a fixed-order reduction, as gemm_nt does.
 // ---------------------------------------------------------------------------
-constexpr int kGtKc = 64;                                  // K per staged chunk
-constexpr int kGtSbo = kGtKc / 8 * 128;                    // bytes between 8-row groups of a chunk
-constexpr int kGtBytesA = 128 * kGtKc * 2;                 // 16 KB
-constexpr int kGtBytesB = 256 * kGtKc * 2;                 // 32 KB
-constexpr int kGtSmem = 2 * (kGtBytesA + kGtBytesB) + 64;  // two stages + two mbarriers + TMEM address
+constexpr int kGtKc = 64;                  // K per staged chunk
+constexpr int kGtStages = 4;               // staged chunks in flight
+constexpr int kGtSbo = kGtKc / 8 * 128;    // bytes between 8-row groups of a chunk
+constexpr int kGtBytesA = 128 * kGtKc * 2;  // 16 KB
+__host__ __device__ constexpr int gt_stage_bytes(int BN) { return kGtBytesA + BN * kGtKc * 2; }
+// stages + kGtStages mbarriers + the TMEM address
+__host__ __device__ constexpr int gt_smem_bytes(int BN) { return kGtStages * gt_stage_bytes(BN) + 8 * kGtStages + 16; }
 
 template <int EPI>
 __global__ void __launch_bounds__(128, 1) gemm_nt_tc(GemmArgs g, int BN) {
   extern __shared__ __align__(1024) unsigned char gt_smem[];
-  // stage st: A tile at st * (A + B) bytes, B tile right after it
-  auto As = [&](int st) { return gt_smem + st * (kGtBytesA + kGtBytesB); };
-  auto Bs = [&](int st) { return gt_smem + st * (kGtBytesA + kGtBytesB) + kGtBytesA; };
-  uint64_t* bar = reinterpret_cast<uint64_t*>(gt_smem + 2 * (kGtBytesA + kGtBytesB));
-  uint32_t* taddr_slot = reinterpret_cast<uint32_t*>(gt_smem + 2 * (kGtBytesA + kGtBytesB) + 16);
+  // stage st: A tile at st * stage bytes, B tile right after it
+  const int sb = gt_stage_bytes(BN);
+  auto As = [&](int st) { return gt_smem + st * sb; };
+  auto Bs = [&](int st) { return gt_smem + st * sb + kGtBytesA; };
+  uint64_t* bar = reinterpret_cast<uint64_t*>(gt_smem + kGtStages * sb);
+  uint32_t* taddr_slot = reinterpret_cast<uint32_t*>(gt_smem + kGtStages * sb + 8 * kGtStages);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int n0 = blockIdx.x * BN;
   const int M = g.m_dev ? min(g.M, *g.m_dev) : g.M;
@@ -560,15 +564,14 @@ __global__ void __launch_bounds__(128, 1) gemm_nt_tc(GemmArgs g, int BN) {
   if (blockIdx.y * 128 >= M || kb >= ke) return;  // whole block, before any allocation
   const int nb = min(BN, g.N - n0);  // columns of this block (a multiple of 16)
   const uint32_t ncols = nb <= 32 ? 32 : nb <= 64 ? 64 : nb <= 128 ? 128 : 256;
-  const uint32_t bar0 = smem_u32(bar), bar1 = smem_u32(bar + 1);
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(taddr_slot)),
                  "r"(ncols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
   }
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar0), "r"(1));
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar1), "r"(1));
+    for (int st = 0; st < kGtStages; ++st)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar + st)), "r"(1));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -576,21 +579,22 @@ __global__ void __launch_bounds__(128, 1) gemm_nt_tc(GemmArgs g, int BN) {
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *taddr_slot;
   const uint32_t idesc = umma_idesc_bf16(128, nb);
-  uint32_t phase[2] = {0u, 0u};
-  bool pending[2] = {false, false};
+  uint32_t phase[kGtStages] = {};
+  bool pending[kGtStages] = {};
   bool ok = true;
   auto wait_stage = [&](int st) {
     if (pending[st]) {
-      ok = mbar_wait(st ? bar1 : bar0, phase[st]) && ok;
+      ok = mbar_wait(smem_u32(bar + st), phase[st]) && ok;
       phase[st] ^= 1u;
       pending[st] = false;
     }
   };
+  const int nk = (ke - kb + kGtKc - 1) / kGtKc;
   for (int m0 = blockIdx.y * 128; m0 < M; m0 += gridDim.y * 128) {
-    int kc = 0;
-    for (int k = kb; k < ke; k += kGtKc, ++kc) {
-      const int st = kc & 1, klen = min(kGtKc, ke - k), nch = klen / 8;
-      wait_stage(st);  // the MMAs that read this buffer two chunks ago are done
+    // chunk kc of this tile into buffer kc % kGtStages (whose MMAs, if any, are waited for first)
+    auto load_chunk = [&](int kc) {
+      const int st = kc % kGtStages, k = kb + kc * kGtKc, nch = min(kGtKc, ke - k) / 8;
+      wait_stage(st);
       for (int c = tid; c < 128 * nch; c += 128) {
         const int r = c / nch, kk = (c % nch) * 8;
         const bool in = m0 + r < M;
@@ -600,8 +604,18 @@ __global__ void __launch_bounds__(128, 1) gemm_nt_tc(GemmArgs g, int BN) {
         const int r = c / nch, kk = (c % nch) * 8;
         cp_async16(Bs(st) + kmajor_off(r, kk, kGtSbo), g.B + (size_t)(n0 + r) * g.ldb + k + kk, 16);
       }
+    };
+    // every thread commits one cp.async group per chunk slot (empty past the last chunk), so
+    // "all but the newest kGtStages - 2 groups done" means "chunk kc is in"
+#pragma unroll 1
+    for (int kc = 0; kc < kGtStages - 1; ++kc) {
+      if (kc < nk) load_chunk(kc);
       cp_async_commit();
-      cp_async_wait<0>();
+    }
+#pragma unroll 1
+    for (int kc = 0; kc < nk; ++kc) {
+      const int st = kc % kGtStages, klen = min(kGtKc, ke - (kb + kc * kGtKc));
+      cp_async_wait<kGtStages - 2>();
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncthreads();
       if (tid == 0) {
@@ -609,20 +623,24 @@ __global__ void __launch_bounds__(128, 1) gemm_nt_tc(GemmArgs g, int BN) {
         for (int j = 0; j < klen / 16; ++j) {
           const uint64_t ad = umma_desc(smem_u32(As(st)) + j * 256, 128, kGtSbo);
           const uint64_t bd = umma_desc(smem_u32(Bs(st)) + j * 256, 128, kGtSbo);
-          const uint32_t acc = (k > kb || j > 0) ? 1u : 0u;
+          const uint32_t acc = (kc > 0 || j > 0) ? 1u : 0u;
           asm volatile(
               "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
               "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
               "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
         }
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                         st ? bar1 : bar0)
+                         smem_u32(bar + st))
                      : "memory");
       }
       pending[st] = true;
+      // the chunk kGtStages - 1 ahead goes into the buffer of chunk kc - 1 once its MMAs are done
+      if (kc + kGtStages - 1 < nk) load_chunk(kc + kGtStages - 1);
+      cp_async_commit();
     }
-    wait_stage(0);
-    wait_stage(1);
+    cp_async_wait<0>();
+#pragma unroll
+    for (int st = 0; st < kGtStages; ++st) wait_stage(st);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     // epilogue: thread = row m0 + 32 warp + lane, 32 columns per TMEM load
     const int r = m0 + warp * 32 + lane;
@@ -864,18 +882,22 @@ int launch_gemm(BdMlp* m, const GemmArgs& g, int splits, cudaStream_t s) {
 template <int EPI>
 int launch_gemm_tc(BdMlp* m, const GemmArgs& g, int splits, cudaStream_t s) {
   if (!m->gt_attr) {
-    MCK(m, cudaFuncSetAttribute(gemm_nt_tc<EPI_HIDDEN_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGtSmem));
-    MCK(m, cudaFuncSetAttribute(gemm_nt_tc<EPI_OUT_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGtSmem));
-    MCK(m, cudaFuncSetAttribute(gemm_nt_tc<EPI_HIDDEN_BWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGtSmem));
-    MCK(m, cudaFuncSetAttribute(gemm_nt_tc<EPI_PARTIAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGtSmem));
+    const int mx = gt_smem_bytes(256);
+    MCK(m, cudaFuncSetAttribute(gemm_nt_tc<EPI_HIDDEN_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    MCK(m, cudaFuncSetAttribute(gemm_nt_tc<EPI_OUT_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    MCK(m, cudaFuncSetAttribute(gemm_nt_tc<EPI_HIDDEN_BWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    MCK(m, cudaFuncSetAttribute(gemm_nt_tc<EPI_PARTIAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
     m->gt_attr = true;
   }
-  const int BN = std::min(g.N, 256);
-  const int nx = (g.N + BN - 1) / BN, tiles = (g.M + 127) / 128;
-  // one CTA per SM at most (TMEM and shared memory); each loops over its share of the row tiles
-  const int ny = std::max(1, std::min(tiles, (m->n_sm + nx * splits - 1) / (nx * splits)));
+  // the widest column tile (256, 128 or 64) whose CTAs still cover every SM; 64-wide tiles fit
+  // two CTAs per SM (96 KB of shared memory, 64 TMEM columns each)
+  const int tiles = (g.M + 127) / 128;
+  int BN = std::min(g.N, 256);
+  while (BN > 64 && ((g.N + BN - 1) / BN) * tiles * splits < m->n_sm) BN = std::max(64, (BN / 2 + 15) / 16 * 16);
+  const int nx = (g.N + BN - 1) / BN, per_sm = BN <= 64 ? 2 : 1;
+  const int ny = std::max(1, std::min(tiles, (per_sm * m->n_sm + nx * splits - 1) / (nx * splits)));
   dim3 grid(nx, ny, splits);
-  gemm_nt_tc<EPI><<<grid, 128, kGtSmem, s>>>(g, BN);
+  gemm_nt_tc<EPI><<<grid, 128, gt_smem_bytes(BN), s>>>(g, BN);
   MCK(m, cudaGetLastError());
   return BD_OK;
 }

@@ -222,12 +222,15 @@ class MLPEnsemble:
 
 
 # ---------------------------------------------------------------------------------------- training
-def sample_poses(sim, n_poses, r_lo=25.0, r_hi=80.0, launches_between=2, steps_per_launch=16, max_rounds=100000):
+def sample_poses(sim, n_poses, r_lo=25.0, r_hi=80.0, launches_between=2, steps_per_launch=16, max_rounds=100000,
+                 max_seconds=None):
     """Poses (c, q) of live trajectories of an exact-kernel BD run, kept where r_lo <= |c| <= r_hi.
 
     ``sim`` is a configured ``B200BatchSimulator`` (any precision); its pool is
-    advanced ``launches_between`` launches between snapshots.
+    advanced ``launches_between`` launches between snapshots.  Raises RuntimeError when
+    ``max_rounds`` snapshots or ``max_seconds`` seconds pass with fewer than ``n_poses`` kept.
     """
+    t_end = None if max_seconds is None else time.perf_counter() + max_seconds
     h = sim.engine.handle
     sim._setup()
     h.call("bd_sim_reset", None)
@@ -260,6 +263,10 @@ def sample_poses(sim, n_poses, r_lo=25.0, r_hi=80.0, launches_between=2, steps_p
         got += int(keep.sum())
         if got >= n_poses:
             break
+        if t_end is not None and time.perf_counter() > t_end:
+            break
+    if got < n_poses:
+        raise RuntimeError(f"sample_poses: {got} of {n_poses} poses in [{r_lo}, {r_hi}] A kept")
     c = np.concatenate(cs)[:n_poses]
     q = np.concatenate(qs)[:n_poses]
     return c, q

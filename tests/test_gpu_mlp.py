@@ -137,7 +137,9 @@ def test_tcgen05_inference_matches_mma_sync_and_oracle(shape, n):
     e.close()
 
 
-@pytest.mark.parametrize("shape,n", [((13, 256, 4, 6), 4096), ((7, 128, 2, 3), 2080)])
+# 4096 rows: 64-column tiles; 12800: 128-column tiles; 40000: 256-column tiles, several row tiles per CTA
+@pytest.mark.parametrize("shape,n", [((13, 256, 4, 6), 4096), ((7, 128, 2, 3), 2080), ((13, 256, 4, 6), 12800),
+                                     ((13, 256, 4, 6), 40000)])
 def test_tcgen05_training_gemms_match_mma_sync(shape, n):
     """The training GEMMs on tcgen05 (forward, weight and activation gradients, split-K partials) give
     the loss and the per-layer gradients of the mma.sync GEMMs to BF16-rounding accuracy."""

@@ -348,16 +348,29 @@ def test_trace_capacity_drops_and_counts_extra_rows():
 @pytest.mark.parametrize("precision,torque", [("fp64", "zero"), ("mixed", "zero"), ("mixed", "centroid")])
 def test_split_stepper_matches_the_fused_stepper(precision, torque):
     """The three-kernel step (ligand forces, Born direction 2 in its own kernel, the rest) sums the same
-    terms in the same order as the fused kernel: the same fates, steps, returns and counters."""
+    terms in the same order as the fused kernel: the same fates, steps, returns and counters.
+
+    With refill (more trajectories than slots) the fused kernel hands pending ids to slots in the order
+    its warps reach them, so a refilled trajectory may start at another global step than in the split
+    stepper.  Its launch boundaries then fall at other steps of its own, and a launch boundary ends the
+    reuse of forces over overlap-rejected steps: the evaluation counters may differ by a few poses while
+    every fate, step count and pose stays the same.  Without refill the counters are exact too."""
     s = system("c2")
-    outs = []
-    for group in (65, 66):
-        sim = make_sim(s, 1500, 400, precision, torque, slots=700, steps_per_launch=16)
-        sim.engine.handle.call("bd_set_launch", group, 256)
-        res = sim.run()
-        outs.append((sim.outcomes(), res.counters))
-    for x, y in zip(outs[0][0], outs[1][0]):
-        np.testing.assert_array_equal(x, y)
-    for k in ("steps", "reacted", "escaped", "returns", "overlap", "bridge", "grid_evals", "rev_evals", "ff_evals"):
-        assert outs[0][1][k] == outs[1][1][k], k
-    assert outs[0][1]["rev_evals"] > 0
+    for n, slots, exact_evals in ((700, 700, True), (1500, 700, False)):
+        outs = []
+        for group in (65, 66):
+            sim = make_sim(s, n, 400, precision, torque, slots=slots, steps_per_launch=16)
+            sim.engine.handle.call("bd_set_launch", group, 256)
+            res = sim.run()
+            outs.append((sim.outcomes(), res.counters))
+        for x, y in zip(outs[0][0], outs[1][0]):
+            np.testing.assert_array_equal(x, y)
+        for k in ("steps", "reacted", "escaped", "returns", "overlap", "bridge"):
+            assert outs[0][1][k] == outs[1][1][k], k
+        for k in ("grid_evals", "rev_evals", "ff_evals"):
+            a, b = outs[0][1][k], outs[1][1][k]
+            if exact_evals:
+                assert a == b, k
+            else:
+                assert abs(a - b) <= 1e-3 * max(a, b), (k, a, b)
+        assert outs[0][1]["rev_evals"] > 0
