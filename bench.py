@@ -296,7 +296,7 @@ def e2e_arm(s, precision, steps, K, n_traj, id_offset, launch, aged=None):
 
 
 def surrogate_arm(s, steps, warmup, K, n_traj, n_poses, train_steps, members, kon_traj, kon_launches=1500, log=None,
-                  aged=None, n_held=100_000, hi_mode="reference_gpu"):
+                  aged=None, n_held=100_000, hi_mode="reference_gpu", r_hi=None, terms=None, sample_traj=None):
     """Config 4: train the surrogate on exact-kernel BD poses, evaluate it on held-out poses, time the
     surrogate stepper like the exact one, and compare k_on of exact and surrogate runs (each run to the
     reference's stopping rule, 99.5 % of the trajectories ended)."""
@@ -307,17 +307,23 @@ def surrogate_arm(s, steps, warmup, K, n_traj, n_poses, train_steps, members, ko
     out = {}
     t0 = time.perf_counter()
     say = log or (lambda m: None)
-    r_lo, r_hi = 25.0, min(80.0, float(s.r_escape))
-    sampler = make_sim(s, "mixed", n_traj, 16, hi_mode=hi_mode)
+    from pystarc_b200 import _lib
+
+    terms = (_lib.TERM_FARFIELD | _lib.TERM_REV_BORN) if terms is None else int(terms)
+    r_lo, r_hi = 25.0, min(80.0, float(s.r_escape)) if r_hi is None else float(r_hi)
+    # the poses come from fresh trajectories (all live at once) in their first few launches
+    n_s = sample_traj or n_traj
+    sampler = make_sim(s, "mixed", n_s, 16, slots=n_s, hi_mode=hi_mode)
     c, q = sg.sample_poses(sampler, n_poses + n_held, r_lo=r_lo, r_hi=r_hi, max_seconds=300.0)
     say(f"surrogate: {len(c)} poses sampled in {time.perf_counter() - t0:.1f} s")
     eng = sampler.engine
     eng.set_ligand(s.lig_pos - s.lig_pos.mean(axis=0), s.lig_q)
-    T = sg.exact_targets(eng, c, q, precision="mixed")
+    T = sg.exact_targets(eng, c, q, precision="mixed", terms=terms)
     eng.close()
     out["data_s"] = round(time.perf_counter() - t0, 1)
     say(f"surrogate: exact targets, {out['data_s']} s with the sampling")
-    spec = sg.SurrogateSpec(r_scale=80.0)
+    centres, width = sg.rbf_default(r_lo, r_hi)
+    spec = sg.SurrogateSpec(r_scale=max(80.0, r_hi), rbf_centres=centres, rbf_width=width, terms=terms)
     spec.r_min = sg.contact_distance(s.rec_pos, s.lig_pos) + 8.0
     spec.r_max = r_hi
     ens = sg.MLPEnsemble(n_members=members, seed=20261203)
@@ -333,6 +339,7 @@ def surrogate_arm(s, steps, warmup, K, n_traj, n_poses, train_steps, members, ko
         out["heldout_trust_region"] = sg.heldout_error(ens, spec, ch, qh, Th)
     say(f"surrogate: trained in {rep.seconds:.1f} s, held-out {out['heldout']}")
     out["trust_region_A"] = [round(spec.r_min, 2), round(spec.r_max, 2)]
+    out["terms"] = {6: "far-field + reverse Born", 7: "grid + far-field + reverse Born (total force)"}.get(terms, terms)
     # timed like the exact arm: graph launches of K steps, L2 flushed in between
     sim = make_sim(s, "mixed", n_traj, K, surrogate=(ens, spec), slots=pool_slots(n_traj), hi_mode=hi_mode)
     sim._setup()
@@ -662,8 +669,10 @@ def main():
                          "4 windows for the paired grid, 8 cubes for the ligand Born grid; -1: autotuned)")
     ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate arm (config 4)")
-    ap.add_argument("--age", type=int, default=64,
-                    help="untimed launches that age the pool before every timed arm (0: time from the b-sphere)")
+    ap.add_argument("--age", type=int, default=-1,
+                    help="untimed launches that age the pool before every timed arm (0: time from the b-sphere; "
+                         "default: 64, 16 for protein-protein, 0 for the two spheres, whose trajectories are all "
+                         "done well before 64 launches)")
     ap.add_argument("--sur-poses", type=int, default=2_000_000)
     ap.add_argument("--sur-train-steps", type=int, default=20_000)
     ap.add_argument("--sur-members", type=int, default=5)
@@ -678,6 +687,8 @@ def main():
     ap.add_argument("--pp-sur-poses", type=int, default=200_000)
     ap.add_argument("--pp-sur-train-steps", type=int, default=8000)
     args = ap.parse_args()
+    if args.age < 0:
+        args.age = {"two-spheres": 0, "protein-protein": 16}.get(args.workload, 64)
     _OPTS["layout"] = None if args.layout < 0 else args.layout
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -273,8 +273,8 @@ int bd_sim_run_noalloc(BdHandle* h, const BdSimParams* p, int8_t* out_status, in
  * BD_TERM_FARFIELD: the Yukawa multipole far-field of atoms outside every electrostatic grid;
  * BD_TERM_REV_BORN: Born direction 2 (ligand Born grid at the receptor atoms);
  * BD_TERM_CONTACT: WCA contact forces (bd_set_contact).  Default: all.
- * The surrogate is trained on BD_TERM_FARFIELD | BD_TERM_REV_BORN.  The stepper always
- * sums every term (or the surrogate's share, see bd_sim_set_surrogate). */
+ * The surrogate is trained on the terms it replaces (BdSurrogateParams.terms).  The stepper
+ * always sums every term (or the surrogate's share, see bd_sim_set_surrogate). */
 enum { BD_TERM_GRID = 1, BD_TERM_FARFIELD = 2, BD_TERM_REV_BORN = 4, BD_TERM_CONTACT = 8, BD_TERM_ALL = 15 };
 int bd_set_terms(BdHandle* h, int terms);
 
@@ -331,13 +331,15 @@ int bd_mlp_train(BdMlp* m, int member, int64_t n_data, const float* X, const flo
 int bd_mlp_ensemble(BdMlp* m, int64_t n, const float* X, float* mean, float* spread, void* stream);
 
 /* Stepper with the surrogate (no reference counterpart).  While set, each BD step of
- * bd_sim_run runs as three phases: the exact grid forces everywhere plus the exact far-field
- * and reverse Born outside the trust region r_min <= |c| <= r_max; the ensemble on the trusted
- * poses' features (c / r_scale, |c| / r_scale, q with w >= 0, five Gaussian radial basis values
- * exp(-((|c| - rbf_centre[k]) / rbf_width)^2 / 2)); then the surrogate's far-field + reverse Born
- * (mean output x out_scale x envelope) where the members agree (spread of the force <=
- * threshold x max(|force|, force_floor x envelope)), the exact kernels elsewhere, and the rest
- * of the step.  envelope(|c|) = exp of env_log interpolated linearly over 32 evenly spaced radii
+ * bd_sim_run runs as three phases: every exact force term outside the trust region
+ * r_min <= |c| <= r_max and the terms the surrogate does not replace inside it; the ensemble on
+ * the trusted poses' features (c / r_scale, |c| / r_scale, q with w >= 0, five Gaussian radial
+ * basis values exp(-((|c| - rbf_centre[k]) / rbf_width)^2 / 2)); then the surrogate's share of
+ * the force and torque (mean output x out_scale x envelope) where the members agree (spread of
+ * the force <= threshold x max(|force|, force_floor x envelope)), the exact kernels for that
+ * share elsewhere, and the rest of the step.  `terms` are the BD_TERM_* flags the surrogate
+ * replaces: a non-empty subset of BD_TERM_GRID | BD_TERM_FARFIELD | BD_TERM_REV_BORN (0 means
+ * BD_TERM_FARFIELD | BD_TERM_REV_BORN); contact forces are always exact.  envelope(|c|) = exp of env_log interpolated linearly over 32 evenly spaced radii
  * from env_r0 to env_r1 (clamped outside), or 1 when env_r1 <= env_r0.  The
  * ensemble needs 13 inputs and 6 outputs (force, torque).  m = NULL returns to the fused
  * exact stepper.  The ensemble must not be used by other calls while the stepper runs, and
@@ -352,6 +354,8 @@ typedef struct {
   double force_floor;
   double env_r0, env_r1;
   double env_log[32];
+  int32_t terms;
+  int32_t reserved;
 } BdSurrogateParams;
 int bd_sim_set_surrogate(BdHandle* h, BdMlp* m, const BdSurrogateParams* p);
 /* Trusted-pose evaluations and exact fallbacks since configure: out[0], out[1]. */

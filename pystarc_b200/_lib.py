@@ -68,7 +68,8 @@ class BdSurrogateParams(C.Structure):
     _fields_ = [("r_scale", C.c_double), ("rbf_centre", C.c_double * 5), ("rbf_width", C.c_double),
                 ("out_scale", C.c_double * 6), ("r_min", C.c_double), ("r_max", C.c_double),
                 ("threshold", C.c_double), ("force_floor", C.c_double), ("env_r0", C.c_double),
-                ("env_r1", C.c_double), ("env_log", C.c_double * 32)]
+                ("env_r1", C.c_double), ("env_log", C.c_double * 32), ("terms", C.c_int32),
+                ("reserved", C.c_int32)]
 
 
 class BdMlpDesc(C.Structure):

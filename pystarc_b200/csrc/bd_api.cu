@@ -777,7 +777,11 @@ int bd_sim_set_surrogate(BdHandle* h, BdMlp* m, const BdSurrogateParams* p) {
                 out_dim);
   if (!(p->r_scale > 0) || !(p->rbf_width > 0) || !(p->threshold >= 0) || !(p->r_max >= p->r_min))
     return fail(h, BD_ERR_ARG, "bd_sim_set_surrogate: bad feature or trust-region constants");
+  const int terms = p->terms ? p->terms : (BD_TERM_FARFIELD | BD_TERM_REV_BORN);
+  if (terms & ~(BD_TERM_GRID | BD_TERM_FARFIELD | BD_TERM_REV_BORN))
+    return fail(h, BD_ERR_ARG, "bd_sim_set_surrogate: terms %d outside grid | far-field | reverse Born", p->terms);
   DevSurrogate& q = h->sur_q;
+  q.terms = (unsigned)terms;
   q.r_scale = p->r_scale;
   for (int k = 0; k < 5; ++k) q.rbf_centre[k] = p->rbf_centre[k];
   q.rbf_width = p->rbf_width;

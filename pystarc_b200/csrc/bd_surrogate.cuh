@@ -2,13 +2,13 @@
 // slots instead of the fused persistent kernel, because the surrogate is a
 // batched tensor-core GEMM chain over every trusted trajectory at once.
 //
-//   sur_begin_kernel  reaction test and escape/return (step_begin); the exact grid
-//                     forces, plus the exact far-field and reverse Born for poses
-//                     outside the trust region; features of the trusted poses,
+//   sur_begin_kernel  reaction test and escape/return (step_begin); every exact force
+//                     term for poses outside the trust region, the terms the surrogate
+//                     does not replace for the others; features of the trusted poses,
 //                     packed as BF16 rows of the MLP's input
 //   MLP ensemble      every member on the trusted rows (bd_mlp.cu)
-//   sur_end_kernel    surrogate far-field + reverse Born for trusted poses whose
-//                     ensemble agrees, exact kernels for the others; then the move,
+//   sur_end_kernel    the surrogate's terms for trusted poses whose ensemble agrees,
+//                     the exact kernels for them elsewhere; then the move,
 //                     overlap test, bridge and step count (step_move, step_end);
 //                     ended trajectories are replaced from the pending pool
 //
@@ -34,6 +34,7 @@ struct DevSurrogate {
   double r_min, r_max, threshold, force_floor;
   double env_r0, env_r1;       // envelope table range (env_r1 <= env_r0: no envelope)
   double env_log[kSurEnv];     // log of the force size at kSurEnv evenly spaced radii
+  unsigned terms;              // force terms (group_forces bits) the surrogate replaces
 };
 
 // Outputs are normalised by out_scale and by a radial envelope: the RMS force
@@ -127,7 +128,7 @@ __global__ void __launch_bounds__(256, 2) sur_begin_kernel(DevSystem S, DevSim P
     const bool reuse = need && tr.rets == rets0 && U.fresh[slot];
     const bool trusted = need && !reuse && r >= Q.r_min && r <= Q.r_max;
     double F[3] = {0, 0, 0}, T[3] = {0, 0, 0};
-    warp_forces_terms<FT, TORQUE>(S, tr.c, R, need && !reuse, trusted ? 9u : 15u, F, T, lane, tl.cnt);
+    warp_forces_terms<FT, TORQUE>(S, tr.c, R, need && !reuse, trusted ? (15u & ~Q.terms) : 15u, F, T, lane, tl.cnt);
     if (run && st != ST_RUNNING) {
       tr.status = st;
       record_end(P, tr, st, tl);
@@ -229,9 +230,9 @@ __global__ void __launch_bounds__(256, 2) sur_end_kernel(DevSystem S, DevSim P, 
         }
       }
     }
-    // exact far-field and reverse Born where the ensemble disagrees
+    // the surrogate's terms, exact, where the ensemble disagrees
     double Fx[3] = {0, 0, 0}, Tx[3] = {0, 0, 0};
-    warp_forces_terms<FT, TORQUE>(S, tr.c, R, fallback, 6u, Fx, Tx, lane, tl.cnt);
+    warp_forces_terms<FT, TORQUE>(S, tr.c, R, fallback, Q.terms, Fx, Tx, lane, tl.cnt);
     if (fallback) {
       n_fb += 1;
 #pragma unroll

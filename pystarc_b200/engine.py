@@ -212,7 +212,7 @@ class B200ForceEngine:
         """Forces for poses (centroid + quaternion (w,x,y,z) or 3x3 matrix) with the ligand from ``set_ligand``.
 
         ``terms`` (``_lib.TERM_*`` bits) restricts the sum to some force terms; the
-        surrogate's training targets are ``TERM_FARFIELD | TERM_REV_BORN``.
+        surrogate's training targets are the terms it replaces (``SurrogateSpec.terms``).
         """
         import torch
 

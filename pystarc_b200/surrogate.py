@@ -14,7 +14,10 @@ the same rotation), and Gaussian radial basis values of ``|c|`` (5 centres on
 from the training set.  The surrogate is trusted only for
 ``contact + margin <= |c| <= r_max`` and while the ensemble agrees (member spread
 of the force within ``threshold`` of its size); elsewhere the exact kernels
-run.
+run.  Which force terms it replaces is ``SurrogateSpec.terms``: the far-field and
+reverse Born by default, or with the grid terms too (the total force, which is
+smooth where a ligand atom leaves the electrostatic grid and the far-field takes
+over, while each term alone jumps there).
 """
 
 from __future__ import annotations
@@ -46,6 +49,7 @@ class SurrogateSpec:
     env_r0: float = 0.0  # radial envelope: log force size at N_ENV radii from env_r0 to env_r1
     env_r1: float = 0.0
     env_log: tuple = (0.0,) * 32
+    terms: int = _lib.TERM_FARFIELD | _lib.TERM_REV_BORN  # force terms the surrogate replaces
 
     def features(self, c, q):
         """(n, 13) float32 features of centroids c (n, 3) and quaternions q (n, 4, w first)."""
@@ -101,6 +105,7 @@ class SurrogateSpec:
         p.env_r0, p.env_r1 = self.env_r0, self.env_r1
         for k in range(32):
             p.env_log[k] = self.env_log[k]
+        p.terms = int(self.terms)
         return p
 
     def trusted(self, c):
@@ -272,13 +277,13 @@ def sample_poses(sim, n_poses, r_lo=25.0, r_hi=80.0, launches_between=2, steps_p
     return c, q
 
 
-def exact_targets(engine, c, q, chunk=200_000, precision="fp64"):
-    """Exact reverse-Born plus far-field force and torque (n, 6) of the engine's ligand at poses
-    (``precision="mixed"``: FP32 force arithmetic, ~1e-6 relative, far below the network's error)."""
+def exact_targets(engine, c, q, chunk=200_000, precision="fp64", terms=_lib.TERM_FARFIELD | _lib.TERM_REV_BORN):
+    """Exact force and torque (n, 6) of the ``terms`` (``_lib.TERM_*`` bits; by default reverse Born
+    plus far-field) of the engine's ligand at poses (``precision="mixed"``: FP32 force arithmetic,
+    ~1e-6 relative, far below the network's error)."""
     out = []
     for i in range(0, len(c), chunk):
-        F, T, _ = engine.eval_poses(c[i:i + chunk], q[i:i + chunk], precision=precision,
-                                    terms=_lib.TERM_FARFIELD | _lib.TERM_REV_BORN)
+        F, T, _ = engine.eval_poses(c[i:i + chunk], q[i:i + chunk], precision=precision, terms=terms)
         out.append(np.concatenate([F, T], axis=1))
     return np.concatenate(out) if out else np.zeros((0, 6))
 

@@ -37,11 +37,13 @@ def _ens(members=2, seed=3):
     return MLPEnsemble(n_members=members, seed=seed)
 
 
-def test_forced_fallback_reproduces_the_exact_stepper():
-    """threshold 0: every trusted pose falls back to the exact far-field + reverse Born."""
+@pytest.mark.parametrize("terms", [6, 7])
+def test_forced_fallback_reproduces_the_exact_stepper(terms):
+    """threshold 0: every trusted pose falls back to the exact terms the surrogate replaces (far-field
+    + reverse Born, or those and the grid terms: the total force)."""
     s = system("c2")
     ens = _ens()
-    spec = _spec(r_min=0.0, r_max=1e9, threshold=0.0, force_floor=1.0)
+    spec = _spec(r_min=0.0, r_max=1e9, threshold=0.0, force_floor=1.0, terms=terms)
     a = make_sim(s, 400, 300, "fp64", steps_per_launch=8, surrogate=(ens, spec))
     ra = a.run()
     b = make_sim(s, 400, 300, "fp64", steps_per_launch=8)
