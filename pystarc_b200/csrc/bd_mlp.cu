@@ -271,13 +271,19 @@ __global__ void loss_kernel(const float* __restrict__ Y, int ldy, const float* _
 }
 
 // loss = sum(partials) / (n out_dim), in a fixed order.
+// One warp: lane l sums partials l, l + 32, ... in order, then a fixed-order butterfly.
 __global__ void loss_finish_kernel(const float* __restrict__ partial, int nb, float denom, float* __restrict__ loss,
                                    float* __restrict__ trace, const long long* __restrict__ step) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int lane = threadIdx.x;
+  if (lane >= 32 || blockIdx.x != 0) return;
   float s = 0.f;
-  for (int i = 0; i < nb; ++i) s += partial[i];
-  if (loss) *loss = s / denom;
-  if (trace) trace[*step] = s / denom;
+  for (int i = lane; i < nb; i += 32) s += partial[i];
+#pragma unroll
+  for (int w = 16; w > 0; w >>= 1) s += __shfl_xor_sync(0xffffffffu, s, w);
+  if (lane == 0) {
+    if (loss) *loss = s / denom;
+    if (trace) trace[*step] = s / denom;
+  }
 }
 
 // Weight gradient of one layer from split partials (summed in split order) and
@@ -293,16 +299,34 @@ __global__ void grad_reduce_kernel(const float* __restrict__ part, int splits, l
   }
 }
 
-// Bias gradient: one warp per output row o sums dZ^T[o][0..n) (lanes stride the
-// row, then a fixed-order butterfly).
-__global__ void bias_grad_kernel(const bf16* __restrict__ dZt, int ldt, int n, int out_real, float* __restrict__ gb) {
-  const int lane = threadIdx.x & 31;
-  for (int o = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; o < out_real; o += (gridDim.x * blockDim.x) >> 5) {
-    float s = 0.f;
-    for (int m = lane; m < n; m += 32) s += __bfloat162float(dZt[(size_t)o * ldt + m]);
+// Bias gradient: one 256-thread block per output row o sums dZ^T[o][0..n) (n and ldt
+// multiples of 8): thread t adds the 8-element vectors t, t + 256, ... in order, then a
+// fixed-order butterfly per warp and the eight warp sums in order.
+__global__ void __launch_bounds__(256) bias_grad_kernel(const bf16* __restrict__ dZt, int ldt, int n, int out_real,
+                                                        float* __restrict__ gb) {
+  __shared__ float ws[8];
+  const int o = blockIdx.x, tid = threadIdx.x, lane = tid & 31;
+  if (o >= out_real) return;
+  const uint4* row = reinterpret_cast<const uint4*>(dZt + (size_t)o * ldt);
+  float s = 0.f;
+  for (int v = tid; v < n / 8; v += 256) {
+    const uint4 u = __ldg(row + v);
+    const uint32_t w[4] = {u.x, u.y, u.z, u.w};
 #pragma unroll
-    for (int w = 16; w > 0; w >>= 1) s += __shfl_xor_sync(0xffffffffu, s, w);
-    if (lane == 0) gb[o] = s;
+    for (int k = 0; k < 4; ++k) {
+      const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&w[k]));
+      s += f.x + f.y;
+    }
+  }
+#pragma unroll
+  for (int w = 16; w > 0; w >>= 1) s += __shfl_xor_sync(0xffffffffu, s, w);
+  if (lane == 0) ws[tid >> 5] = s;
+  __syncthreads();
+  if (tid == 0) {
+    float t = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) t += ws[k];
+    gb[o] = t;
   }
 }
 
@@ -1082,7 +1106,9 @@ int backward(BdMlp* m, int member, int n, const float* X, const float* T, float*
   loss_finish_kernel<<<1, 32, 0, s>>>(m->loss_part, nb, (float)n * (float)m->d.out_dim, loss ? loss : m->loss_tmp,
                                      trace, trace ? m->data_step : nullptr);
   MCK(m, cudaGetLastError());
-  const int splits = std::max(1, std::min(64, n / 256));
+  // split-K of the weight gradients: 512 rows per split (16 at batch 8192) keep every SM busy
+  // while halving the partials that grad_reduce_kernel reads back
+  const int splits = std::max(1, std::min(64, n / 512));
   const int kps = round_up((n + splits - 1) / splits, kBK);
   for (int l = nl - 1; l >= 0; --l) {
     const bf16* dZ = l == nl - 1 ? m->dY : m->dZ[l];
@@ -1107,7 +1133,7 @@ int backward(BdMlp* m, int member, int n, const float* X, const float* T, float*
     grad_reduce_kernel<<<grid_for(m, tot), 256, 0, s>>>(m->part, used, m->part_stride, L.in_pad[l], L.out_real[l],
                                                          L.in_real[l], w.grad + L.w_off[l]);
     MCK(m, cudaGetLastError());
-    bias_grad_kernel<<<(L.out_real[l] * 32 + 255) / 256, 256, 0, s>>>(dZt, n, n, L.out_real[l], w.grad + L.b_off[l]);
+    bias_grad_kernel<<<L.out_real[l], 256, 0, s>>>(dZt, n, n, L.out_real[l], w.grad + L.b_off[l]);
     MCK(m, cudaGetLastError());
     if (l == 0) break;
     // dZ_{l-1} = (dZ_l W_l) * SiLU'(Z_{l-1}): M = n, N = in_pad (hidden), K = out_pad
