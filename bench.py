@@ -277,6 +277,8 @@ def e2e_arm(s, precision, steps, K, n_traj, id_offset, launch, aged=None):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     sim = make_sim(s, precision, n_traj, K, id_offset, slots=pool_slots(n_traj))
+    torch.cuda.synchronize()
+    t_engine = time.perf_counter() - t0
     if aged is not None:
         sim.params.checkpoint_interval = 1 << 60  # resume the saved pool; never write a new checkpoint
         sim.params._work_dir = work
@@ -292,6 +294,7 @@ def e2e_arm(s, precision, steps, K, n_traj, id_offset, launch, aged=None):
     sim.engine.close()
     shutil.rmtree(work, ignore_errors=True)
     launches = max(1, steps)
+    res.e2e_split = {"engine_s": round(t_engine, 3), "run_s": round(el - t_engine, 3)}
     return (res.total_steps - steps0) / el, h2d / launches, d2h / launches, res
 
 
@@ -835,8 +838,11 @@ def main():
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "note": ("B200ForceEngine from host arrays (grid uploads) + B200BatchSimulator.run() resuming the "
                          "aged pool from its checkpoint file (slots copied host-to-device), "
-                         f"{max(args.steps, 10)} launches with a counter poll after each, outcomes copied back")},
-        "gpu_launches": 3 * args.steps,
+                         f"{max(args.steps, 10)} launches with a counter poll after each, outcomes copied back"),
+                "seconds": getattr(e2e_res, "e2e_split", None)},
+        # kernels per timed launch: the split step is three kernels per BD step plus the compaction's two;
+        # the fused stepper is one kernel plus the compaction's two
+        "gpu_launches": ((3 * args.inner + 2) if launch["group"] == 66 else 3) * args.steps,
         "clocks": ck,
     }
     if world == 1 and not args.no_surrogate and args.workload != "two-spheres":

@@ -451,7 +451,8 @@ class B200BatchSimulator:
         o_st, o_steps, o_rets = self.outcomes()
         path = Path(path or self._checkpoint_path())
         path.parent.mkdir(parents=True, exist_ok=True)
-        np.savez_compressed(path, c=c, q=q, traj=traj, steps=steps, rets=rets, status=status, state=state,
+        # uncompressed: the poses are FP64 noise that barely compresses, and a resume should not wait on zlib
+        np.savez(path, c=c, q=q, traj=traj, steps=steps, rets=rets, status=status, state=state,
                             n_live=live.value,
                             counters=ctr, out_status=o_st, out_steps=o_steps, out_returns=o_rets,
                             n_traj=self._n_run, seed=int(self.params.seed or 0), cap=C)
@@ -467,7 +468,10 @@ class B200BatchSimulator:
         h.call("bd_sim_capacity", _lib.C.byref(cap))
         if int(d["cap"]) != cap.value:
             raise ValueError(f"{path}: slot capacity {int(d['cap'])} != {cap.value}")
-        arr = {k: (np.ascontiguousarray(d[k]) if d[k].ndim else d[k][()]) for k in d.files}
+        arr = {}
+        for k in d.files:  # each NpzFile lookup reads the member again: one lookup per key
+            v = d[k]
+            arr[k] = np.ascontiguousarray(v) if v.ndim else v[()]
         h.call("bd_sim_restore", _lib.ptr(arr["c"]), _lib.ptr(arr["q"]), _lib.ptr(arr["traj"], _lib.C.c_int32),
                _lib.ptr(arr["steps"], _lib.C.c_int32), _lib.ptr(arr["rets"], _lib.C.c_int32),
                _lib.ptr(arr["status"], _lib.C.c_int8), int(arr["n_live"]), _lib.ptr(arr["counters"], _lib.C.c_uint64),
