@@ -669,7 +669,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--layout", type=int, default=-1,
                     help="device data layout flags (1 stage receptor, 2 windows for 1-channel grids, "
-                         "4 windows for the paired grid, 8 cubes for the ligand Born grid; -1: autotuned)")
+                         "4 windows for the paired grid, 8 cubes for the ligand Born grid, 16 overlap "
+                         "occupancy grid; -1: autotuned)")
     ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate arm (config 4)")
     ap.add_argument("--age", type=int, default=-1,

@@ -167,6 +167,10 @@ int bd_eval_forces(BdHandle* h, int64_t n, const double* centroids, const double
 int bd_eval_forces_atoms(BdHandle* h, int64_t n, const double* lig_positions, const double* R,
                          const double* centroids, double* F, double* T, double* E, int precision, int torque_mode,
                          void* stream);
+/* The stepper's overlap test for n centroids: out[i] = 1 when some receptor atom lies within
+ * 1.5 A of centroid i (gpu_batch_simulator.py:770-781, 1102-1128), else 0.  DEVICE arrays
+ * centroids (n*3) and out (n); uses the occupancy grid when the layout has it. */
+int bd_eval_overlap(BdHandle* h, int64_t n, const double* centroids, int8_t* out, void* stream);
 
 /* Stepper.  configure allocates the live-slot pool and per-trajectory outputs; reset
  * starts the first `slots` trajectories; run enqueues n_launch launches of
@@ -236,10 +240,22 @@ int bd_get_launch(BdHandle* h, int* group, int* block_threads, int* grid_blocks)
  * BD_LAYOUT_CUBES_1: the ligand Born grid gets a copy whose entry n holds the 2x2x2 block of
  *   nodes at node n (32 bytes, one sector; 8x the grid's memory, made only up to
  *   BD_CUBE_MAX_BYTES), so a reverse-Born stencil is three 32-byte loads and one 16-byte load.
+ * BD_LAYOUT_OVERLAP_GRID: an occupancy grid of 0.5 A cells over the receptor (one 32-bit word
+ *   per cell: no atom within 1.5 A of the cell, every point within 1.5 A of an atom, or a
+ *   short list of atoms to test), so the overlap test of a centroid is one load and a few
+ *   distances in one lane instead of a warp's sweep of the receptor chunks (made only up to
+ *   BD_OVERLAP_MAX_CELLS cells).
  * The same values enter the same arithmetic in every layout: results are identical. */
-enum { BD_LAYOUT_STAGE_RECEPTOR = 1, BD_LAYOUT_WINDOWS_1 = 2, BD_LAYOUT_WINDOWS_2 = 4, BD_LAYOUT_CUBES_1 = 8 };
+enum {
+  BD_LAYOUT_STAGE_RECEPTOR = 1,
+  BD_LAYOUT_WINDOWS_1 = 2,
+  BD_LAYOUT_WINDOWS_2 = 4,
+  BD_LAYOUT_CUBES_1 = 8,
+  BD_LAYOUT_OVERLAP_GRID = 16
+};
 #define BD_CUBE_MAX_BYTES (48ll * 1024 * 1024)
-#define BD_LAYOUT_DEFAULT (BD_LAYOUT_WINDOWS_1 | BD_LAYOUT_CUBES_1)
+#define BD_OVERLAP_MAX_CELLS (32ll * 1024 * 1024)
+#define BD_LAYOUT_DEFAULT (BD_LAYOUT_WINDOWS_1 | BD_LAYOUT_CUBES_1 | BD_LAYOUT_OVERLAP_GRID)
 #define BD_STAGE_MAX_BYTES (64 * 1024)
 int bd_set_layout(BdHandle* h, int flags);
 int bd_get_layout(BdHandle* h, int* flags);

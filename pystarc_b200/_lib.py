@@ -19,8 +19,8 @@ TORQUE_ZERO, TORQUE_CENTROID = 0, 1
 CTR_NAMES = ("started", "reacted", "escaped", "max_steps", "steps", "returns", "overlap", "bridge", "grid_evals",
              "rev_evals", "ff_evals", "nonfinite")
 N_CTR = len(CTR_NAMES)
-LAYOUT_STAGE_RECEPTOR, LAYOUT_WINDOWS_1, LAYOUT_WINDOWS_2, LAYOUT_CUBES_1 = 1, 2, 4, 8
-LAYOUT_DEFAULT = LAYOUT_WINDOWS_1 | LAYOUT_CUBES_1
+LAYOUT_STAGE_RECEPTOR, LAYOUT_WINDOWS_1, LAYOUT_WINDOWS_2, LAYOUT_CUBES_1, LAYOUT_OVERLAP_GRID = 1, 2, 4, 8, 16
+LAYOUT_DEFAULT = LAYOUT_WINDOWS_1 | LAYOUT_CUBES_1 | LAYOUT_OVERLAP_GRID
 TERM_GRID, TERM_FARFIELD, TERM_REV_BORN, TERM_CONTACT, TERM_ALL = 1, 2, 4, 8, 15
 
 _ERR_NAMES = {BD_ERR_ARG: "bad argument", BD_ERR_CUDA: "CUDA error", BD_ERR_OOM: "out of device memory",
@@ -99,6 +99,7 @@ SIGNATURES = {
     "bd_set_reactions": (C.c_int, [P, C.c_int, dp, dp, dp, dp, C.c_int]),
     "bd_eval_forces": (C.c_int, [P, C.c_int64, P, P, C.c_int, P, P, P, C.c_int, C.c_int, P]),
     "bd_eval_forces_atoms": (C.c_int, [P, C.c_int64, P, P, P, P, P, P, C.c_int, C.c_int, P]),
+    "bd_eval_overlap": (C.c_int, [P, C.c_int64, P, P, P]),
     "bd_sim_configure": (C.c_int, [P, C.POINTER(BdSimParams)]),
     "bd_sim_reset": (C.c_int, [P, P]),
     "bd_sim_run": (C.c_int, [P, C.c_int, C.c_int, P]),

@@ -204,6 +204,110 @@ int add_cube(BdHandle* h, DevGrid& g) {
   return BD_OK;
 }
 
+// Overlap occupancy grid over the first nr atoms of the receptor table ra (x, y, z, q per
+// atom, already on the device as S.rec): classified on the device in two passes around a
+// host prefix sum.  Leaves S.ov_cell NULL (the chunk sweep) when the grid would exceed
+// BD_OVERLAP_MAX_CELLS cells or its lists the 24-bit offsets.
+int build_overlap_grid(BdHandle* h, DevSystem& S, const std::vector<double>& ra, int nr) {
+  OvGeom G{};
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (int a = 0; a < nr; ++a)
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = std::min(lo[d], ra[4 * a + d]);
+      hi[d] = std::max(hi[d], ra[4 * a + d]);
+    }
+  long long cells = 1;
+  for (int d = 0; d < 3; ++d) {
+    G.o[d] = lo[d] - (kOvR + kOvCell);
+    G.n[d] = (int)std::ceil((hi[d] + kOvR + kOvCell - G.o[d]) / kOvCell);
+    G.nb[d] = (int)std::ceil(G.n[d] * kOvCell / kOvBin);
+    cells *= G.n[d];
+  }
+  if (cells > BD_OVERLAP_MAX_CELLS) return BD_OK;
+  // atoms binned on the kOvBin lattice (CSR, atoms in table order within a bin)
+  const int nbins = G.nb[0] * G.nb[1] * G.nb[2];
+  std::vector<int> bin_of(nr), start(nbins + 1, 0), atoms(nr);
+  for (int a = 0; a < nr; ++a) {
+    int b[3];
+    for (int d = 0; d < 3; ++d) b[d] = std::min(G.nb[d] - 1, std::max(0, (int)std::floor((ra[4 * a + d] - G.o[d]) / kOvBin)));
+    bin_of[a] = (b[0] * G.nb[1] + b[1]) * G.nb[2] + b[2];
+    ++start[bin_of[a] + 1];
+  }
+  for (int b = 0; b < nbins; ++b) start[b + 1] += start[b];
+  {
+    std::vector<int> fill(start.begin(), start.end() - 1);
+    for (int a = 0; a < nr; ++a) atoms[fill[bin_of[a]]++] = a;
+  }
+  int *d_start = nullptr, *d_atoms = nullptr, *d_cnt = nullptr, *d_list = nullptr;
+  uint8_t* d_cls = nullptr;
+  uint32_t* d_word = nullptr;
+  auto release = [&]() {
+    cudaFree(d_start);
+    cudaFree(d_atoms);
+    cudaFree(d_cnt);
+    cudaFree(d_cls);
+  };
+  if (cudaMalloc(&d_start, start.size() * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&d_atoms, std::max<size_t>(1, atoms.size()) * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&d_cnt, (size_t)cells * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&d_cls, (size_t)cells) != cudaSuccess) {
+    release();
+    cudaGetLastError();
+    return fail(h, BD_ERR_CUDA, "out of device memory for the overlap grid (%lld cells)", cells);
+  }
+  CK(h, cudaMemcpy(d_start, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CK(h, cudaMemcpy(d_atoms, atoms.data(), atoms.size() * sizeof(int), cudaMemcpyHostToDevice));
+  const int blocks = h->n_sm * 8;
+  ov_cells_kernel<<<blocks, 256>>>(S.rec, d_start, d_atoms, G, d_cls, d_cnt, nullptr, nullptr);
+  CK(h, cudaGetLastError());
+  std::vector<uint8_t> cls((size_t)cells);
+  std::vector<int> cnt((size_t)cells);
+  CK(h, cudaMemcpy(cls.data(), d_cls, cls.size(), cudaMemcpyDeviceToHost));
+  CK(h, cudaMemcpy(cnt.data(), d_cnt, cnt.size() * sizeof(int), cudaMemcpyDeviceToHost));
+  std::vector<uint32_t> word((size_t)cells);
+  long long total = 0;
+  for (long long c = 0; c < cells; ++c) {
+    if (cls[c] == 0) {
+      word[c] = 0u;
+    } else if (cls[c] == 1) {
+      word[c] = 0xffffffffu;
+    } else {
+      if (cnt[c] > 255 || total + cnt[c] >= (1ll << 24) - 1) {  // does not fit the encoding: keep the sweep
+        release();
+        return BD_OK;
+      }
+      word[c] = ((uint32_t)total << 8) | (uint32_t)cnt[c];
+      total += cnt[c];
+    }
+  }
+  void* p;
+  int rc = dev_alloc(h, h->sys_allocs, &p, (size_t)cells * sizeof(uint32_t));
+  if (rc) {
+    release();
+    return rc;
+  }
+  d_word = (uint32_t*)p;
+  CK(h, cudaMemcpy(d_word, word.data(), word.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  rc = dev_alloc(h, h->sys_allocs, &p, (size_t)std::max(1ll, total) * sizeof(int));
+  if (rc) {
+    release();
+    return rc;
+  }
+  d_list = (int*)p;
+  ov_cells_kernel<<<blocks, 256>>>(S.rec, d_start, d_atoms, G, nullptr, nullptr, d_word, d_list);
+  CK(h, cudaGetLastError());
+  CK(h, cudaDeviceSynchronize());
+  release();
+  S.ov_cell = d_word;
+  S.ov_list = d_list;
+  for (int d = 0; d < 3; ++d) {
+    S.ov_o[d] = G.o[d];
+    S.ov_n[d] = G.n[d];
+  }
+  S.ov_inv_h = 1.0 / kOvCell;
+  return BD_OK;
+}
+
 bool same_lattice(const GridHost& a, const GridHost& b) {
   for (int i = 0; i < 3; ++i)
     if (a.n[i] != b.n[i] || a.o[i] != b.o[i] || a.sp[i] != b.sp[i]) return false;
@@ -348,6 +452,9 @@ int finalize(BdHandle* h) {
     S.chunks_f = (const float4*)p;
     S.rec_in_smem = (h->layout & BD_LAYOUT_STAGE_RECEPTOR) &&
                     (size_t)(S.n_rec_pad + nc) * sizeof(float4) <= BD_STAGE_MAX_BYTES;
+    if (h->layout & BD_LAYOUT_OVERLAP_GRID) {
+      if ((rc = build_overlap_grid(h, S, ra, nr))) return rc;
+    }
     // WCA radii in the same order; padding entries never come within a cutoff
     if (!h->rec_rad.empty()) {
       if (h->rec_rad.size() != (size_t)nr || h->lig_rad.size() != (size_t)nl)
@@ -740,6 +847,18 @@ int bd_eval_forces_atoms(BdHandle* h, int64_t n, const double* pos, const double
   return BD_OK;
 }
 
+int bd_eval_overlap(BdHandle* h, int64_t n, const double* cen, int8_t* out, void* stream) {
+  if (!h) return BD_ERR_ARG;
+  if (n < 0 || (n > 0 && (!cen || !out))) return fail(h, BD_ERR_ARG, "bd_eval_overlap: bad arguments");
+  int rc = finalize(h);
+  if (rc) return rc;
+  if (n == 0) return BD_OK;
+  const int blocks = (int)std::min<long long>((n + 255) / 256, (long long)h->n_sm * 16);
+  eval_overlap_kernel<<<blocks, 256, 0, pick(h, stream)>>>(h->S, (long long)n, cen, out);
+  CK(h, cudaGetLastError());
+  return BD_OK;
+}
+
 int bd_set_launch(BdHandle* h, int group, int block) {
   if (!h) return BD_ERR_ARG;
   if (group && !valid_group(group)) return fail(h, BD_ERR_ARG, "group must be 1, 4, 8, 16, 32, 64 or 65 (warp-cooperative) or 66 (split)");
@@ -753,7 +872,8 @@ int bd_set_launch(BdHandle* h, int group, int block) {
 
 int bd_set_layout(BdHandle* h, int flags) {
   if (!h) return BD_ERR_ARG;
-  const int all = BD_LAYOUT_STAGE_RECEPTOR | BD_LAYOUT_WINDOWS_1 | BD_LAYOUT_WINDOWS_2 | BD_LAYOUT_CUBES_1;
+  const int all = BD_LAYOUT_STAGE_RECEPTOR | BD_LAYOUT_WINDOWS_1 | BD_LAYOUT_WINDOWS_2 | BD_LAYOUT_CUBES_1 |
+                  BD_LAYOUT_OVERLAP_GRID;
   if (flags & ~all) return fail(h, BD_ERR_ARG, "unknown layout flags 0x%x", flags & ~all);
   if (flags != h->layout) {
     h->layout = flags;

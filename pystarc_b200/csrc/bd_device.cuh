@@ -66,6 +66,13 @@ struct DevSystem {
   int rec_in_smem;        // stepper kernels stage rec_f / chunks_f in shared memory
   unsigned terms;         // BD_TERM_* summed by the evaluation kernels (the stepper sums all)
   double rec_max_r;
+  // overlap occupancy grid (BD_LAYOUT_OVERLAP_GRID; ov_cell = NULL: not built).  Cell words:
+  // 0 no receptor atom within 1.5 A of any point of the cell, 0xffffffff every point within
+  // 1.5 A of some atom, else (offset << 8 | count): the atoms (indices into rec) that may be
+  const uint32_t* ov_cell;
+  const int* ov_list;
+  double ov_o[3], ov_inv_h;
+  int ov_n[3];
   // grids
   int n_elec;
   DevGrid elec[BD_MAX_ELEC];

@@ -707,10 +707,14 @@ __device__ __forceinline__ double hi_diffusion(const DevSim& P, double r) {
 
 // Overlap rejection test: is the new centroid within 1.5 A of any receptor atom
 // (gpu_batch_simulator.py:1106-1128)?  Chunks whose bounding sphere is farther
-// than 1.5 A are skipped; the answer is exact.
+// than 1.5 A are skipped; the answer is exact.  With the occupancy grid built, one lane
+// answers alone from the cell holding c (overlap_cells); the answer is the same.
+__device__ __forceinline__ bool overlap_cells(const DevSystem& S, const double c[3]);
+
 template <int G>
 __device__ __forceinline__ bool overlap_any(const DevSystem& S, const double c[3], int lane, unsigned gm,
                                             const RecView& v = RecView{nullptr, nullptr}) {
+  if (S.ov_cell) return overlap_cells(S, c);
   bool any = false;
   if (norm3(c[0], c[1], c[2]) < S.rec_max_r + 1.5) {
     const float cf0 = (float)c[0], cf1 = (float)c[1], cf2 = (float)c[2];
@@ -735,6 +739,118 @@ __device__ __forceinline__ bool overlap_any(const DevSystem& S, const double c[3
     }
   }
   return any;
+}
+
+// ----------------------------------------------------------------------------
+// Overlap occupancy grid.  The reference rejects a move when the new centroid lies within
+// 1.5 A of any receptor atom (gpu_batch_simulator.py:770-781, 1102-1128).  Cells of
+// kOvCell A over the receptor's box (widened by 1.5 A + one cell) are classified once:
+// EMPTY when every atom is at least 1.5 A + kOvEps from the whole cell, FULL when some atom
+// is within 1.5 A - kOvEps of all of it, MIXED otherwise with the list of atoms that come
+// within 1.5 A + kOvEps of it.  A query reads the cell word and, for a MIXED cell, tests
+// the listed atoms with the reference's distance (the same norm3 < 1.5 as the sweep).  The
+// margins are far above the rounding of the cell index and of the distance, so the answer
+// equals the sweep's for every centroid; outside the box no atom is within 1.5 A.
+// ----------------------------------------------------------------------------
+constexpr double kOvCell = 0.5;   // cell edge (A)
+constexpr double kOvEps = 1e-9;   // classification margin (A)
+constexpr double kOvBin = 2.0;    // atom bins of the build (A)
+constexpr double kOvR = 1.5;      // the reference's overlap distance (A)
+
+__device__ __forceinline__ bool overlap_cells(const DevSystem& S, const double c[3]) {
+  const double u0 = (c[0] - S.ov_o[0]) * S.ov_inv_h, u1 = (c[1] - S.ov_o[1]) * S.ov_inv_h,
+               u2 = (c[2] - S.ov_o[2]) * S.ov_inv_h;
+  // outside the box (or NaN): no atom within 1.5 A
+  if (!(u0 >= 0.0 && u0 < (double)S.ov_n[0] && u1 >= 0.0 && u1 < (double)S.ov_n[1] && u2 >= 0.0 &&
+        u2 < (double)S.ov_n[2]))
+    return false;
+  const long cell = ((long)(int)u0 * S.ov_n[1] + (int)u1) * S.ov_n[2] + (int)u2;
+  const uint32_t w = __ldg(S.ov_cell + cell);
+  if (w == 0u) return false;
+  if (w == 0xffffffffu) return true;
+  const int off = (int)(w >> 8), cnt = (int)(w & 255u);
+  for (int t = 0; t < cnt; ++t) {
+    const double4 a = S.rec[__ldg(S.ov_list + off + t)];
+    if (norm3(c[0] - a.x, c[1] - a.y, c[2] - a.z) < kOvR) return true;
+  }
+  return false;
+}
+
+struct OvGeom {
+  double o[3];   // grid origin (cell and bin lattices share it)
+  int n[3];      // cells per axis
+  int nb[3];     // bins per axis
+};
+
+// Nearest and farthest distance from atom a to cell (i, j, k).
+__device__ __forceinline__ void ov_cell_dist(const OvGeom& G, int i, int j, int k, const double4& a, double& dn,
+                                             double& df) {
+  const int ix[3] = {i, j, k};
+  const double x[3] = {a.x, a.y, a.z};
+  double n2 = 0, f2 = 0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double lo = G.o[d] + ix[d] * kOvCell, hi = lo + kOvCell;
+    const double e = fmax(fmax(lo - x[d], x[d] - hi), 0.0);
+    const double f = fmax(fabs(x[d] - lo), fabs(x[d] - hi));
+    n2 += e * e;
+    f2 += f * f;
+  }
+  dn = sqrt(n2);
+  df = sqrt(f2);
+}
+
+// One thread per cell.  Pass 1 (list == NULL): class (0 empty, 1 full, 2 mixed) and the
+// number of listed atoms.  Pass 2: the atoms of each mixed cell, in bin order, at the offset
+// held in its cell word.
+__global__ void ov_cells_kernel(const double4* __restrict__ rec, const int* __restrict__ bin_start,
+                                const int* __restrict__ bin_atoms, OvGeom G, uint8_t* __restrict__ cls,
+                                int* __restrict__ cnt, const uint32_t* __restrict__ word, int* __restrict__ list) {
+  const long n_cells = (long)G.n[0] * G.n[1] * G.n[2];
+  for (long cell = (long)blockIdx.x * blockDim.x + threadIdx.x; cell < n_cells; cell += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(cell / ((long)G.n[1] * G.n[2])), j = (int)((cell / G.n[2]) % G.n[1]), k = (int)(cell % G.n[2]);
+    if (list && (word[cell] == 0u || word[cell] == 0xffffffffu)) continue;
+    const int ix[3] = {i, j, k};
+    int b0[3], b1[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double lo = ix[d] * kOvCell - (kOvR + kOvEps), hi = (ix[d] + 1) * kOvCell + (kOvR + kOvEps);
+      b0[d] = max(0, (int)floor(lo / kOvBin));
+      b1[d] = min(G.nb[d] - 1, (int)floor(hi / kOvBin));
+    }
+    bool full = false;
+    int m = 0;
+    int at = list ? (int)(word[cell] >> 8) : 0;
+    for (int bx = b0[0]; bx <= b1[0] && !full; ++bx)
+      for (int by = b0[1]; by <= b1[1] && !full; ++by)
+        for (int bz = b0[2]; bz <= b1[2] && !full; ++bz) {
+          const int b = (bx * G.nb[1] + by) * G.nb[2] + bz;
+          for (int t = bin_start[b]; t < bin_start[b + 1]; ++t) {
+            const int a = bin_atoms[t];
+            double dn, df;
+            ov_cell_dist(G, i, j, k, rec[a], dn, df);
+            if (!list && df < kOvR - kOvEps) {
+              full = true;
+              break;
+            }
+            if (dn < kOvR + kOvEps) {
+              if (list) list[at++] = a;
+              ++m;
+            }
+          }
+        }
+    if (!list) {
+      cls[cell] = full ? 1 : (m ? 2 : 0);
+      cnt[cell] = full ? 0 : m;
+    }
+  }
+}
+
+__global__ void eval_overlap_kernel(DevSystem S, long long n, const double* __restrict__ cen, int8_t* __restrict__ out) {
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const double c[3] = {cen[3 * t], cen[3 * t + 1], cen[3 * t + 2]};
+    out[t] = (int8_t)overlap_any<1>(S, c, 0, 1u);
+  }
 }
 
 __device__ __forceinline__ double pair_distance(const DevSystem& S, const double c[3], const double R[9], int p) {
@@ -1220,6 +1336,8 @@ __device__ __forceinline__ void warp_forces(const DevSystem& S, const double c[3
 // Overlap test of every lane with `need`, the warp sweeping the receptor chunks together.
 __device__ __forceinline__ bool warp_overlap(const DevSystem& S, const double cn[3], bool need, int lane,
                                              const RecView& v) {
+  // with the occupancy grid every lane answers for its own centroid
+  if (S.ov_cell) return need && overlap_cells(S, cn);
   const unsigned FULL = 0xffffffffu;
   unsigned m = __ballot_sync(FULL, need);
   bool mine = false;

@@ -680,12 +680,14 @@ __global__ void __launch_bounds__(128, 1) gemm_nt_tc(GemmArgs g, int BN) {
             "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
           : "r"(addr));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (r >= M) continue;
+      // rows past M store nothing, but their lanes stay for the transposed store's shuffles
+      const bool valid = r < M;
       const int cw = min(32, nb - c0);  // columns of this load that exist (32 or 16)
       const int cb = n0 + c0;           // first column
       float f[32];
 #pragma unroll
       for (int e = 0; e < 32; ++e) f[e] = ok ? __uint_as_float(v[e]) : __int_as_float(0x7fc00000);
+      if (!valid && !(EPI == EPI_HIDDEN_FWD || EPI == EPI_HIDDEN_BWD)) continue;
       if constexpr (EPI == EPI_PARTIAL) {
         float* p = g.C + blockIdx.z * g.split_stride + (size_t)r * g.ldc + cb;
 #pragma unroll
@@ -705,32 +707,45 @@ __global__ void __launch_bounds__(128, 1) gemm_nt_tc(GemmArgs g, int BN) {
             f[e + 1] += g.bias[cb + e + 1];
             o0 = silu(f[e]);
             o1 = silu(f[e + 1]);
-          } else {  // EPI_HIDDEN_BWD: f = dA, output dZ
-            o0 = e < cw ? f[e] * silu_grad(g.Zin[(size_t)r * g.ldz + cb + e]) : 0.f;
-            o1 = e < cw ? f[e + 1] * silu_grad(g.Zin[(size_t)r * g.ldz + cb + e + 1]) : 0.f;
+          } else {  // EPI_HIDDEN_BWD: f = dA, output dZ; Z read two columns at a time
+            float z0 = 0.f, z1 = 0.f;
+            if (valid && e < cw) {
+              const float2 z = *reinterpret_cast<const float2*>(g.Zin + (size_t)r * g.ldz + cb + e);
+              z0 = z.x;
+              z1 = z.y;
+            }
+            o0 = e < cw ? f[e] * silu_grad(z0) : 0.f;
+            o1 = e < cw ? f[e + 1] * silu_grad(z1) : 0.f;
           }
           __nv_bfloat162 h2 = __floats2bfloat162_rn(o0, o1);
           pk[e / 2] = *reinterpret_cast<uint32_t*>(&h2);
         }
-        if (EPI == EPI_HIDDEN_FWD && g.C) {
+        if (valid && EPI == EPI_HIDDEN_FWD && g.C) {
           float* z = g.C + (size_t)r * g.ldc + cb;
 #pragma unroll
           for (int e = 0; e < 32; e += 4)
             if (e < cw) *reinterpret_cast<float4*>(z + e) = make_float4(f[e], f[e + 1], f[e + 2], f[e + 3]);
         }
-        if (g.O) {
+        if (valid && g.O) {
           bf16* o = g.O + (size_t)r * g.ldo + cb;
 #pragma unroll
           for (int e = 0; e < 32; e += 8)
             if (e < cw) *reinterpret_cast<uint4*>(o + e) = make_uint4(pk[e / 2], pk[e / 2 + 1], pk[e / 2 + 2], pk[e / 2 + 3]);
         }
         if (g.Ot) {
+          // transposed copy, two rows per 4-byte store: the lane pair (2k, 2k+1) holds rows r, r + 1;
+          // for columns (e, e + 1) the even lane stores column e of both rows, the odd lane column e + 1
+          // (M is even wherever a transposed copy is kept, so both rows of a pair are valid or neither)
+          const bool odd = lane & 1;
+          const int r0 = r & ~1;
 #pragma unroll
-          for (int e = 0; e < 32; ++e) {
-            if (e >= cw) break;
-            const uint32_t w = pk[e / 2];
-            const unsigned short h = (e & 1) ? (unsigned short)(w >> 16) : (unsigned short)(w & 0xffffu);
-            g.Ot[(size_t)(cb + e) * g.ldot + r] = __ushort_as_bfloat16(h);
+          for (int e = 0; e < 32; e += 2) {
+            const uint32_t w = pk[e / 2];  // columns e (low half) and e + 1 (high half) of this row
+            const uint32_t send = odd ? (w & 0xffffu) : (w >> 16);
+            const uint32_t recv = __shfl_xor_sync(0xffffffffu, send, 1);
+            const uint32_t out = odd ? (recv | (w & 0xffff0000u)) : ((w & 0xffffu) | (recv << 16));
+            if (valid && e < cw)
+              *reinterpret_cast<uint32_t*>(g.Ot + (size_t)(cb + e + (odd ? 1 : 0)) * g.ldot + r0) = out;
           }
         }
       }

@@ -208,6 +208,18 @@ class B200ForceEngine:
             return F, T, E
         return F.cpu().numpy(), T.cpu().numpy(), E.cpu().numpy()
 
+    def eval_overlap(self, centroids):
+        """The stepper's overlap test (gpu_batch_simulator.py:770-781, 1102-1128): a bool per centroid,
+        True when some receptor atom lies within 1.5 A of it."""
+        import torch
+
+        dev = torch.device("cuda", self.handle.device)
+        c = torch.as_tensor(centroids, dtype=torch.float64, device=dev).reshape(-1, 3).contiguous()
+        out = torch.empty(c.shape[0], dtype=torch.int8, device=dev)
+        self.handle.call("bd_eval_overlap", c.shape[0], _lib.P(c.data_ptr()), _lib.P(out.data_ptr()),
+                         _lib.P(torch.cuda.current_stream(dev).cuda_stream))
+        return out.cpu().numpy().astype(bool)
+
     def eval_poses(self, centroids, rotations, precision=None, torque_mode=None, terms=None):
         """Forces for poses (centroid + quaternion (w,x,y,z) or 3x3 matrix) with the ligand from ``set_ligand``.
 
