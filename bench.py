@@ -496,10 +496,12 @@ def hetero_main(args):
     _OPTS["layout"] = d_mixed["autotune"]["layout"]  # the tuned layout, through the public API
     te = time.perf_counter()
     sims = [make_sim(s, "mixed", s.n_traj, args.inner) for s in systems]
+    t_eng = time.perf_counter() - te
     batch = B200MultiBatch(sims, steps_per_launch=args.inner, launches_per_poll=1)
     res = batch.run(max_launches=max(args.steps, 20))
     torch.cuda.synchronize()
-    e2e = sum(r.total_steps for r in res) / (time.perf_counter() - te)
+    t_all = time.perf_counter() - te
+    e2e = sum(r.total_steps for r in res) / t_all
     batch.close()
     h2d = sum(np.asarray(g.data).nbytes for s in systems for g in s.elec_grids + s.born_grids + s.lig_born_grids)
     d2h = sum(s.n_traj * 9 for s in systems)
@@ -521,7 +523,9 @@ def hetero_main(args):
                      "algorithmic_bytes": "224 B per (atom, grid) stencil + 128 B per trajectory-step"},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d / max(args.steps, 20)),
                 "d2h_bytes_per_step": int(d2h / max(args.steps, 20)),
-                "note": "B200ForceEngine x16 + B200MultiBatch.run() from host arrays, incl. grid upload"},
+                "note": "B200ForceEngine x16 + B200MultiBatch.run() from host arrays, incl. grid upload",
+                "seconds": {"engines_s": round(t_eng, 3), "run_s": round(t_all - t_eng, 3),
+                            "launches": max(args.steps, 20)}},
         "gpu_launches": 3 * args.steps,
         "clocks": ck,
     }

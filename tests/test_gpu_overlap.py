@@ -88,15 +88,15 @@ def test_overlap_grid_keeps_fp64_trajectories():
     from pystarc_b200.engine import B200ForceEngine
     from pystarc_b200.simulator import B200BatchSimulator
 
-    s = system("c3")
+    s = system("c2")
     outs = []
     for layout in (_lib.LAYOUT_DEFAULT, _lib.LAYOUT_DEFAULT & ~_lib.LAYOUT_OVERLAP_GRID):
         for group in (65, 66):
             eng = B200ForceEngine(**s.engine_kwargs(), multipole_expansion=_MP(s) if s.multipole else None,
                                   precision="fp64", layout=layout)
             mol1, mol2 = s.molecules()
-            sim = B200BatchSimulator(mol1, mol2, s.mobility(), s.pathway_set(), s.params(n_traj=600, max_steps=300),
-                                     eng, termination="complete", steps_per_launch=16)
+            sim = B200BatchSimulator(mol1, mol2, s.mobility(), s.pathway_set(), s.params(n_traj=700, max_steps=400),
+                                     eng, termination="complete", steps_per_launch=16, slots=700)
             eng.handle.call("bd_set_launch", group, 256)
             res = sim.run()
             outs.append((sim.outcomes(), res.counters))
