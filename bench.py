@@ -547,8 +547,8 @@ def _lib_P(v):
 
 
 # --------------------------------------------------------------------------- CPU baseline
-def _cpu_worker(args):
-    grid_file, n_traj, seed, n_steps, init = args
+def oracle_system(grid_file, n_traj, seed, n_steps):
+    """The oracle's (StepSystem, StepParams) of a system saved by ``save_cpu_inputs``."""
     from oracle import stepper as ost
     from oracle.forces import FarField, OracleForceEngine, OracleGrid
 
@@ -566,6 +566,14 @@ def _cpu_worker(args):
                         q_lig_total=float(d["q_lig"]), debye=float(d["debye"]))
     prm = ost.StepParams(n_traj=n_traj, seed=seed, r_b=float(d["r_b"]), r_esc=float(d["r_esc"]), max_steps=n_steps,
                          max_dt=float(d["max_dt"]), use_hi=bool(d["hi"]), overlap=bool(d["overlap"]))
+    return ss, prm
+
+
+def _cpu_worker(args):
+    grid_file, n_traj, seed, n_steps, init = args
+    from oracle import stepper as ost
+
+    ss, prm = oracle_system(grid_file, n_traj, seed, n_steps)
     t0 = time.perf_counter()
     res = ost.run(ss, prm, noise="pcg64", termination="reference", init=init)
     return res.total_steps, time.perf_counter() - t0
@@ -674,7 +682,7 @@ def main():
     ap.add_argument("--layout", type=int, default=-1,
                     help="device data layout flags (1 stage receptor, 2 windows for 1-channel grids, "
                          "4 windows for the paired grid, 8 cubes for the ligand Born grid, 16 overlap "
-                         "occupancy grid; -1: autotuned)")
+                         "occupancy grid, 32 xy records with the cubes; -1: autotuned)")
     ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate arm (config 4)")
     ap.add_argument("--age", type=int, default=-1,

@@ -245,16 +245,22 @@ int bd_get_launch(BdHandle* h, int* group, int* block_threads, int* grid_blocks)
  *   short list of atoms to test), so the overlap test of a centroid is one load and a few
  *   distances in one lane instead of a warp's sweep of the receptor chunks (made only up to
  *   BD_OVERLAP_MAX_CELLS cells).
+ * BD_LAYOUT_XY_1 (with BD_LAYOUT_CUBES_1): the ligand Born grid also gets, per node, four
+ *   32-byte records holding the extra x plane and extra y row of a stencil for each cell half
+ *   (16x the grid's memory, made only up to BD_XY_MAX_BYTES), so a reverse-Born stencil is three
+ *   32-byte loads.
  * The same values enter the same arithmetic in every layout: results are identical. */
 enum {
   BD_LAYOUT_STAGE_RECEPTOR = 1,
   BD_LAYOUT_WINDOWS_1 = 2,
   BD_LAYOUT_WINDOWS_2 = 4,
   BD_LAYOUT_CUBES_1 = 8,
-  BD_LAYOUT_OVERLAP_GRID = 16
+  BD_LAYOUT_OVERLAP_GRID = 16,
+  BD_LAYOUT_XY_1 = 32
 };
 #define BD_CUBE_MAX_BYTES (48ll * 1024 * 1024)
 #define BD_OVERLAP_MAX_CELLS (32ll * 1024 * 1024)
+#define BD_XY_MAX_BYTES (64ll * 1024 * 1024)
 #define BD_LAYOUT_DEFAULT (BD_LAYOUT_WINDOWS_1 | BD_LAYOUT_CUBES_1 | BD_LAYOUT_OVERLAP_GRID)
 #define BD_STAGE_MAX_BYTES (64 * 1024)
 int bd_set_layout(BdHandle* h, int flags);

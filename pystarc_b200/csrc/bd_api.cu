@@ -308,6 +308,18 @@ int build_overlap_grid(BdHandle* h, DevSystem& S, const std::vector<double>& ra,
   return BD_OK;
 }
 
+// xy records of a grid that has its cube copy (DevGrid::xy).
+int add_xy(BdHandle* h, DevGrid& g) {
+  const long n = (long)g.nx * g.ny * g.nz;
+  void* p = nullptr;
+  int rc = dev_alloc(h, h->sys_allocs, &p, (size_t)n * 32 * sizeof(float));
+  if (rc) return rc;
+  xy_kernel<<<h->n_sm * 8, 256>>>(g.data, (float*)p, g.nx, g.ny, g.nz);
+  CK(h, cudaGetLastError());
+  g.xy = (const float*)p;
+  return BD_OK;
+}
+
 bool same_lattice(const GridHost& a, const GridHost& b) {
   for (int i = 0; i < 3; ++i)
     if (a.n[i] != b.n[i] || a.o[i] != b.o[i] || a.sp[i] != b.sp[i]) return false;
@@ -491,6 +503,9 @@ int finalize(BdHandle* h) {
     if ((h->layout & BD_LAYOUT_CUBES_1) &&
         (double)S.lig_born.nx * S.lig_born.ny * S.lig_born.nz * 32.0 <= (double)BD_CUBE_MAX_BYTES)
       if ((rc = add_cube(h, S.lig_born))) return rc;
+    if ((h->layout & BD_LAYOUT_XY_1) && S.lig_born.cube &&
+        (double)S.lig_born.nx * S.lig_born.ny * S.lig_born.nz * 128.0 <= (double)BD_XY_MAX_BYTES)
+      if ((rc = add_xy(h, S.lig_born))) return rc;
     S.born_rev = 1;
     const DevGrid& g = S.lig_born;
     const double mx = std::max(std::fabs(g.lox), std::fabs(g.hix)), my = std::max(std::fabs(g.loy), std::fabs(g.hiy)),
@@ -873,7 +888,7 @@ int bd_set_launch(BdHandle* h, int group, int block) {
 int bd_set_layout(BdHandle* h, int flags) {
   if (!h) return BD_ERR_ARG;
   const int all = BD_LAYOUT_STAGE_RECEPTOR | BD_LAYOUT_WINDOWS_1 | BD_LAYOUT_WINDOWS_2 | BD_LAYOUT_CUBES_1 |
-                  BD_LAYOUT_OVERLAP_GRID;
+                  BD_LAYOUT_OVERLAP_GRID | BD_LAYOUT_XY_1;
   if (flags & ~all) return fail(h, BD_ERR_ARG, "unknown layout flags 0x%x", flags & ~all);
   if (flags != h->layout) {
     h->layout = flags;

@@ -46,6 +46,10 @@ struct DevGrid {
   const float4* win;  // optional: entry n = nodes n .. n + 4/ch - 1 of node n's z row, all channels
   const float* cube;  // optional (ch = 1): 8 floats per node n = (x, y, z), the 2x2x2 block
                       // v(x + i, y + j, z + k) at 4i + 2j + k, 32-byte aligned (one sector)
+  const float* xy;    // optional (with cube): per node n = (x, y, z), four 8-float records, record
+                      // 2a + b for the extra x plane ex = (a ? x + 2 : x - 1) and the extra y row
+                      // ey = (b ? y + 2 : y - 1): v(ex, y + j, z + k) at 2j + k, v(x + i, ey, z + k)
+                      // at 4 + 2i + k
   int nx, ny, nz, ch;
   double ox, oy, oz;
   double isx, isy, isz;  // 1/spacing
@@ -376,12 +380,12 @@ __device__ __forceinline__ StencilOut<FT, CH> stencil(const DevGrid& g, PT x, PT
   float r[2][2][3][CH], xe[2][2][CH], ye[2][2][CH];
   if (CH == 1 && g.cube) {
     // cube copy: the centre block, the x-extra face, the y-extra and z-extra edges in four loads
+    // (three with the xy records: the x face and the y edge of this cell half come in one)
     const float* cb = g.cube;
-    float c8[8], y8[8], z8[8];
-    ld8(cb + 8 * (long)((cx * g.ny + cy) * nz + cz), c8);
-    const float4 xf = __ldg(reinterpret_cast<const float4*>(cb + 8 * (long)((ex * g.ny + cy) * nz + cz)));
-    ld8(cb + 8 * (long)((cx * g.ny + ey) * nz + cz), y8);
-    ld8(cb + 8 * (long)((cx * g.ny + cy) * nz + (lz ? cz - 1 : cz + 2)), z8);
+    const long node = (long)(cx * g.ny + cy) * nz + cz;
+    float c8[8], z8[8];
+    ld8(cb + 8 * node, c8);
+    ld8(cb + 8 * ((long)(cx * g.ny + cy) * nz + (lz ? cz - 1 : cz + 2)), z8);
 #pragma unroll
     for (int i = 0; i < 2; ++i)
 #pragma unroll
@@ -390,14 +394,29 @@ __device__ __forceinline__ StencilOut<FT, CH> stencil(const DevGrid& g, PT x, PT
         r[i][j][zc + 1][0] = c8[4 * i + 2 * j + 1];
         r[i][j][ze][0] = z8[4 * i + 2 * j];
       }
-    xe[0][0][0] = xf.x;
-    xe[0][1][0] = xf.y;
-    xe[1][0][0] = xf.z;
-    xe[1][1][0] = xf.w;
+    if (g.xy) {
+      float e8[8];
+      ld8(g.xy + 8 * (4 * node + 2 * (lx ? 0 : 1) + (ly ? 0 : 1)), e8);
 #pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      ye[i][0][0] = y8[4 * i];
-      ye[i][1][0] = y8[4 * i + 1];
+      for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          xe[j][k][0] = e8[2 * j + k];
+          ye[j][k][0] = e8[4 + 2 * j + k];
+        }
+    } else {
+      float y8[8];
+      const float4 xf = __ldg(reinterpret_cast<const float4*>(cb + 8 * (long)((ex * g.ny + cy) * nz + cz)));
+      ld8(cb + 8 * (long)((cx * g.ny + ey) * nz + cz), y8);
+      xe[0][0][0] = xf.x;
+      xe[0][1][0] = xf.y;
+      xe[1][0][0] = xf.z;
+      xe[1][1][0] = xf.w;
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        ye[i][0][0] = y8[4 * i];
+        ye[i][1][0] = y8[4 * i + 1];
+      }
     }
   } else if (g.win) {
     // window copy: one 16-byte load per z run (two for a 3-node run of two channels)

@@ -1235,6 +1235,36 @@ __global__ void cube_kernel(const float* __restrict__ d, float* __restrict__ cub
   }
 }
 
+// The xy records of a one-channel grid (DevGrid::xy): per node, for each cell half in x and y,
+// the extra x plane's four nodes and the extra y row's four nodes of the stencil (nodes off the
+// grid read as 0; stencils never reach them, every stencil position lies in the margin box).
+__global__ void xy_kernel(const float* __restrict__ d, float* __restrict__ xy, int nx, int ny, int nz) {
+  const long n_nodes = (long)nx * ny * nz;
+  auto at = [&](int x, int y, int z) -> float {
+    return (x >= 0 && x < nx && y >= 0 && y < ny && z >= 0 && z < nz) ? d[((long)x * ny + y) * nz + z] : 0.f;
+  };
+  for (long n = blockIdx.x * (long)blockDim.x + threadIdx.x; n < n_nodes; n += (long)gridDim.x * blockDim.x) {
+    const int z = (int)(n % nz), y = (int)((n / nz) % ny), x = (int)(n / ((long)ny * nz));
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        const int ex = a ? x + 2 : x - 1, ey = b ? y + 2 : y - 1;
+        float v[8];
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+          for (int k = 0; k < 2; ++k) {
+            v[2 * j + k] = at(ex, y + j, z + k);
+            v[4 + 2 * j + k] = at(x + j, ey, z + k);
+          }
+        float4* o = reinterpret_cast<float4*>(xy + 8 * (4 * n + 2 * a + b));
+        o[0] = make_float4(v[0], v[1], v[2], v[3]);
+        o[1] = make_float4(v[4], v[5], v[6], v[7]);
+      }
+  }
+}
+
 // D(r) of the stepper at n distances (parity entry point bd_sim_hi_diffusion).
 template <typename FT>
 __global__ void hi_diffusion_kernel(DevSim P, int n, const double* __restrict__ r, double* __restrict__ D) {
