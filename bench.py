@@ -525,7 +525,7 @@ def hetero_main(args):
                 "d2h_bytes_per_step": int(d2h / max(args.steps, 20)),
                 "note": "B200ForceEngine x16 + B200MultiBatch.run() from host arrays, incl. grid upload",
                 "seconds": {"engines_s": round(t_eng, 3), "run_s": round(t_all - t_eng, 3),
-                            "launches": max(args.steps, 20)}},
+                            **getattr(batch, "last_timing", {})}},
         "gpu_launches": 3 * args.steps,
         "clocks": ck,
     }

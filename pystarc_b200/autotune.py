@@ -30,8 +30,8 @@ from . import _lib
 
 DEFAULT_CANDIDATES = ((1, 128), (8, 128), (16, 128), (32, 128), (64, 128), (64, 256), (65, 128), (65, 256),
                       (66, 256))
-DEFAULT_LAYOUTS = (_lib.LAYOUT_WINDOWS_1 | _lib.LAYOUT_OVERLAP_GRID, _lib.LAYOUT_DEFAULT,
-                   _lib.LAYOUT_DEFAULT | _lib.LAYOUT_XY_1)
+DEFAULT_LAYOUTS = (_lib.LAYOUT_WINDOWS_1 | _lib.LAYOUT_OVERLAP_GRID, _lib.LAYOUT_DEFAULT & ~_lib.LAYOUT_XY_1,
+                   _lib.LAYOUT_DEFAULT)
 
 
 def measure(sim, group, block, K=16, launches=4, aged=None):

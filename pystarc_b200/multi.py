@@ -58,6 +58,7 @@ class B200MultiBatch:
         t0 = time.perf_counter()
         self.setup()
         self._call("bd_multi_reset", None)
+        t_setup = time.perf_counter() - t0
         N = sum(int(s.params.n_trajectories) for s in self.sims)
         stop_at = int(N * 0.995) if self.termination == "reference" else N
         launches, stalled, last = 0, 0, -1
@@ -84,6 +85,9 @@ class B200MultiBatch:
                 break
         c = self.counters()
         elapsed = time.perf_counter() - t0
+        # wall seconds of this run: device builds and configuration, then the launches
+        self.last_timing = {"setup_s": round(t_setup, 3), "launches_s": round(elapsed - t_setup, 3),
+                            "launches": launches}
         results = []
         for s in self.sims:
             st, steps, rets = s.outcomes()
