@@ -501,7 +501,9 @@ def hetero_main(args):
     res = batch.run(max_launches=max(args.steps, 20))
     torch.cuda.synchronize()
     t_all = time.perf_counter() - te
-    e2e = sum(r.total_steps for r in res) / t_all
+    # every BD step of the run, from the batch's counters (a system's result counts only the steps of
+    # its trajectories that ended)
+    e2e = batch.last_counters["steps"] / t_all
     batch.close()
     h2d = sum(np.asarray(g.data).nbytes for s in systems for g in s.elec_grids + s.born_grids + s.lig_born_grids)
     d2h = sum(s.n_traj * 9 for s in systems)

@@ -54,7 +54,10 @@ class B200MultiBatch:
         return dict(zip(_lib.CTR_NAMES, (int(v) for v in out)))
 
     def run(self, max_launches=None):
-        """Run every system to completion; one B200BatchResult per system (counters are the batch's)."""
+        """Run every system to completion; one B200BatchResult per system (counters are the batch's).
+
+        A system's ``total_steps`` sums the steps of its trajectories that ended; the batch's own
+        step count over all systems, running trajectories included, is ``last_counters["steps"]``."""
         t0 = time.perf_counter()
         self.setup()
         self._call("bd_multi_reset", None)
