@@ -715,7 +715,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        s = build_system(None if not _has_cuda() else "cuda", args.workload)
+        s = build_system("cuda" if _has_cuda() else "cpu", args.workload)
         cores = os.cpu_count() or 1
         init, where = None, "the b-sphere"
         sample = ROOT / "oracle" / "samples" / "aged_protein_ligand.npz"
