@@ -238,23 +238,26 @@ int build_overlap_grid(BdHandle* h, DevSystem& S, const std::vector<double>& ra,
     std::vector<int> fill(start.begin(), start.end() - 1);
     for (int a = 0; a < nr; ++a) atoms[fill[bin_of[a]]++] = a;
   }
-  int *d_start = nullptr, *d_atoms = nullptr, *d_cnt = nullptr, *d_list = nullptr;
-  uint8_t* d_cls = nullptr;
-  uint32_t* d_word = nullptr;
-  auto release = [&]() {
-    cudaFree(d_start);
-    cudaFree(d_atoms);
-    cudaFree(d_cnt);
-    cudaFree(d_cls);
-  };
-  if (cudaMalloc(&d_start, start.size() * sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&d_atoms, std::max<size_t>(1, atoms.size()) * sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&d_cnt, (size_t)cells * sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&d_cls, (size_t)cells) != cudaSuccess) {
-    release();
+  // build-only buffers, freed on every way out
+  struct Tmp {
+    void* p = nullptr;
+    ~Tmp() {
+      if (p) cudaFree(p);
+    }
+  } t_start, t_atoms, t_cnt, t_cls;
+  if (cudaMalloc(&t_start.p, start.size() * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&t_atoms.p, std::max<size_t>(1, atoms.size()) * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&t_cnt.p, (size_t)cells * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&t_cls.p, (size_t)cells) != cudaSuccess) {
     cudaGetLastError();
     return fail(h, BD_ERR_CUDA, "out of device memory for the overlap grid (%lld cells)", cells);
   }
+  int* d_start = (int*)t_start.p;
+  int* d_atoms = (int*)t_atoms.p;
+  int* d_cnt = (int*)t_cnt.p;
+  uint8_t* d_cls = (uint8_t*)t_cls.p;
+  int* d_list = nullptr;
+  uint32_t* d_word = nullptr;
   CK(h, cudaMemcpy(d_start, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice));
   CK(h, cudaMemcpy(d_atoms, atoms.data(), atoms.size() * sizeof(int), cudaMemcpyHostToDevice));
   const int blocks = h->n_sm * 8;
@@ -272,32 +275,22 @@ int build_overlap_grid(BdHandle* h, DevSystem& S, const std::vector<double>& ra,
     } else if (cls[c] == 1) {
       word[c] = 0xffffffffu;
     } else {
-      if (cnt[c] > 255 || total + cnt[c] >= (1ll << 24) - 1) {  // does not fit the encoding: keep the sweep
-        release();
-        return BD_OK;
-      }
+      if (cnt[c] > 255 || total + cnt[c] >= (1ll << 24) - 1) return BD_OK;  // does not fit the encoding: keep the sweep
       word[c] = ((uint32_t)total << 8) | (uint32_t)cnt[c];
       total += cnt[c];
     }
   }
   void* p;
   int rc = dev_alloc(h, h->sys_allocs, &p, (size_t)cells * sizeof(uint32_t));
-  if (rc) {
-    release();
-    return rc;
-  }
+  if (rc) return rc;
   d_word = (uint32_t*)p;
   CK(h, cudaMemcpy(d_word, word.data(), word.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
   rc = dev_alloc(h, h->sys_allocs, &p, (size_t)std::max(1ll, total) * sizeof(int));
-  if (rc) {
-    release();
-    return rc;
-  }
+  if (rc) return rc;
   d_list = (int*)p;
   ov_cells_kernel<<<blocks, 256>>>(S.rec, d_start, d_atoms, G, nullptr, nullptr, d_word, d_list);
   CK(h, cudaGetLastError());
   CK(h, cudaDeviceSynchronize());
-  release();
   S.ov_cell = d_word;
   S.ov_list = d_list;
   for (int d = 0; d < 3; ++d) {
