@@ -726,7 +726,7 @@ def main():
                      f"b-sphere by the oracle alone ({sample.name})")
         vals = []
         for i in range(args.warmup + args.steps):
-            v, info = cpu_baseline(s, cores, traj_per_proc=64, n_steps=max(4, args.cpu_steps // 4), init=init,
+            v, info = cpu_baseline(s, cores, traj_per_proc=64, n_steps=args.cpu_steps, init=init,
                                    where=where)
             if i >= args.warmup:
                 vals.append(v)

@@ -249,6 +249,11 @@ int bd_get_launch(BdHandle* h, int* group, int* block_threads, int* grid_blocks)
  *   32-byte records holding the extra x plane and extra y row of a stencil for each cell half
  *   (16x the grid's memory, made only up to BD_XY_MAX_BYTES), so a reverse-Born stencil is three
  *   32-byte loads.
+ * BD_LAYOUT_ZTEX_1 (with BD_LAYOUT_CUBES_1): the stencil's extra z nodes come from 16-byte
+ *   records read through the texture path instead of a third 32-byte global load (2x the
+ *   grid's memory in float4 records).
+ * BD_LAYOUT_XYTEX_1 (with BD_LAYOUT_XY_1): the xy records are read through the texture path as
+ *   two 16-byte fetches instead of one 32-byte global load.
  * The same values enter the same arithmetic in every layout: results are identical. */
 enum {
   BD_LAYOUT_STAGE_RECEPTOR = 1,
@@ -256,7 +261,9 @@ enum {
   BD_LAYOUT_WINDOWS_2 = 4,
   BD_LAYOUT_CUBES_1 = 8,
   BD_LAYOUT_OVERLAP_GRID = 16,
-  BD_LAYOUT_XY_1 = 32
+  BD_LAYOUT_XY_1 = 32,
+  BD_LAYOUT_ZTEX_1 = 64,
+  BD_LAYOUT_XYTEX_1 = 128
 };
 #define BD_CUBE_MAX_BYTES (48ll * 1024 * 1024)
 #define BD_OVERLAP_MAX_CELLS (32ll * 1024 * 1024)

@@ -60,6 +60,7 @@ struct BdHandle {
   // device system
   DevSystem S{};
   std::vector<void*> sys_allocs;
+  std::vector<cudaTextureObject_t> sys_tex;  // texture views of system buffers
   // stepper
   bool sim_ready = false;
   BdSimParams sp{};
@@ -116,6 +117,11 @@ int dev_alloc(BdHandle* h, std::vector<void*>& list, void** p, size_t bytes) {
 
 void free_list(std::vector<void*>& list) {
   for (void* p : list) cudaFree(p);
+  list.clear();
+}
+
+void free_tex(std::vector<cudaTextureObject_t>& list) {
+  for (cudaTextureObject_t t : list) cudaDestroyTextureObject(t);
   list.clear();
 }
 
@@ -301,8 +307,26 @@ int build_overlap_grid(BdHandle* h, DevSystem& S, const std::vector<double>& ra,
   return BD_OK;
 }
 
-// xy records of a grid that has its cube copy (DevGrid::xy).
-int add_xy(BdHandle* h, DevGrid& g) {
+// A float4 texture view of n float4 elements at p (linear memory, point sampling).
+int float4_texture(BdHandle* h, void* p, size_t n, cudaTextureObject_t* out) {
+  cudaResourceDesc res{};
+  res.resType = cudaResourceTypeLinear;
+  res.res.linear.devPtr = p;
+  res.res.linear.desc = cudaCreateChannelDesc<float4>();
+  res.res.linear.sizeInBytes = n * sizeof(float4);
+  cudaTextureDesc td{};
+  td.readMode = cudaReadModeElementType;
+  td.filterMode = cudaFilterModePoint;
+  td.addressMode[0] = cudaAddressModeClamp;
+  cudaTextureObject_t t = 0;
+  CK(h, cudaCreateTextureObject(&t, &res, &td, nullptr));
+  h->sys_tex.push_back(t);
+  *out = t;
+  return BD_OK;
+}
+
+// xy records of a grid that has its cube copy (DevGrid::xy), and their texture view when asked.
+int add_xy(BdHandle* h, DevGrid& g, bool tex) {
   const long n = (long)g.nx * g.ny * g.nz;
   void* p = nullptr;
   int rc = dev_alloc(h, h->sys_allocs, &p, (size_t)n * 32 * sizeof(float));
@@ -310,7 +334,20 @@ int add_xy(BdHandle* h, DevGrid& g) {
   xy_kernel<<<h->n_sm * 8, 256>>>(g.data, (float*)p, g.nx, g.ny, g.nz);
   CK(h, cudaGetLastError());
   g.xy = (const float*)p;
+  // linear textures address at most 2^27 elements
+  if (tex && (double)n * 8.0 <= (double)(1 << 27)) return float4_texture(h, p, (size_t)n * 8, &g.xytex);
   return BD_OK;
+}
+
+// z-edge records of a grid that has its cube copy, read through the texture path (DevGrid::ztex).
+int add_ztex(BdHandle* h, DevGrid& g) {
+  const long n = (long)g.nx * g.ny * g.nz;
+  void* p = nullptr;
+  int rc = dev_alloc(h, h->sys_allocs, &p, (size_t)n * 2 * sizeof(float4));
+  if (rc) return rc;
+  zedge_kernel<<<h->n_sm * 8, 256>>>(g.data, (float4*)p, g.nx, g.ny, g.nz);
+  CK(h, cudaGetLastError());
+  return float4_texture(h, p, (size_t)n * 2, &g.ztex);
 }
 
 bool same_lattice(const GridHost& a, const GridHost& b) {
@@ -324,6 +361,7 @@ int finalize(BdHandle* h) {
   if (!h->dirty) return BD_OK;
   CK(h, cudaSetDevice(h->device));
   CK(h, cudaDeviceSynchronize());
+  free_tex(h->sys_tex);
   free_list(h->sys_allocs);
   DevSystem S{};
   if (h->lig.empty()) return fail(h, BD_ERR_STATE, "ligand not set");
@@ -498,7 +536,11 @@ int finalize(BdHandle* h) {
       if ((rc = add_cube(h, S.lig_born))) return rc;
     if ((h->layout & BD_LAYOUT_XY_1) && S.lig_born.cube &&
         (double)S.lig_born.nx * S.lig_born.ny * S.lig_born.nz * 128.0 <= (double)BD_XY_MAX_BYTES)
-      if ((rc = add_xy(h, S.lig_born))) return rc;
+      if ((rc = add_xy(h, S.lig_born, h->layout & BD_LAYOUT_XYTEX_1))) return rc;
+    // linear textures address at most 2^27 elements
+    if ((h->layout & BD_LAYOUT_ZTEX_1) && S.lig_born.cube &&
+        (double)S.lig_born.nx * S.lig_born.ny * S.lig_born.nz * 2.0 <= (double)(1 << 27))
+      if ((rc = add_ztex(h, S.lig_born))) return rc;
     S.born_rev = 1;
     const DevGrid& g = S.lig_born;
     const double mx = std::max(std::fabs(g.lox), std::fabs(g.hix)), my = std::max(std::fabs(g.loy), std::fabs(g.hiy)),
@@ -717,6 +759,7 @@ int bd_destroy(BdHandle* h) {
   cudaDeviceSynchronize();
   for (auto& g : h->graph)
     if (g) cudaGraphExecDestroy(g);
+  free_tex(h->sys_tex);
   free_list(h->sys_allocs);
   free_list(h->sim_allocs);
   if (h->own) cudaStreamDestroy(h->own);
@@ -881,7 +924,7 @@ int bd_set_launch(BdHandle* h, int group, int block) {
 int bd_set_layout(BdHandle* h, int flags) {
   if (!h) return BD_ERR_ARG;
   const int all = BD_LAYOUT_STAGE_RECEPTOR | BD_LAYOUT_WINDOWS_1 | BD_LAYOUT_WINDOWS_2 | BD_LAYOUT_CUBES_1 |
-                  BD_LAYOUT_OVERLAP_GRID | BD_LAYOUT_XY_1;
+                  BD_LAYOUT_OVERLAP_GRID | BD_LAYOUT_XY_1 | BD_LAYOUT_ZTEX_1 | BD_LAYOUT_XYTEX_1;
   if (flags & ~all) return fail(h, BD_ERR_ARG, "unknown layout flags 0x%x", flags & ~all);
   if (flags != h->layout) {
     h->layout = flags;

@@ -50,6 +50,11 @@ struct DevGrid {
                       // 2a + b for the extra x plane ex = (a ? x + 2 : x - 1) and the extra y row
                       // ey = (b ? y + 2 : y - 1): v(ex, y + j, z + k) at 2j + k, v(x + i, ey, z + k)
                       // at 4 + 2i + k
+  cudaTextureObject_t xytex;  // optional: a float4 texture view of xy (record r = elements 2r, 2r + 1)
+  cudaTextureObject_t ztex;  // optional (with cube): per node n = (x, y, z), two float4 records
+                             // read through the texture path, record 2n + c for the extra z node
+                             // ez = (c ? z + 2 : z - 1): v(x, y, ez), v(x, y + 1, ez),
+                             // v(x + 1, y, ez), v(x + 1, y + 1, ez)
   int nx, ny, nz, ch;
   double ox, oy, oz;
   double isx, isy, isz;  // 1/spacing
@@ -385,7 +390,15 @@ __device__ __forceinline__ StencilOut<FT, CH> stencil(const DevGrid& g, PT x, PT
     const long node = (long)(cx * g.ny + cy) * nz + cz;
     float c8[8], z8[8];
     ld8(cb + 8 * node, c8);
-    ld8(cb + 8 * ((long)(cx * g.ny + cy) * nz + (lz ? cz - 1 : cz + 2)), z8);
+    if (g.ztex) {
+      const float4 zr = tex1Dfetch<float4>(g.ztex, (int)(2 * node + (lz ? 0 : 1)));
+      z8[0] = zr.x;
+      z8[2] = zr.y;
+      z8[4] = zr.z;
+      z8[6] = zr.w;
+    } else {
+      ld8(cb + 8 * ((long)(cx * g.ny + cy) * nz + (lz ? cz - 1 : cz + 2)), z8);
+    }
 #pragma unroll
     for (int i = 0; i < 2; ++i)
 #pragma unroll
@@ -396,7 +409,20 @@ __device__ __forceinline__ StencilOut<FT, CH> stencil(const DevGrid& g, PT x, PT
       }
     if (g.xy) {
       float e8[8];
-      ld8(g.xy + 8 * (4 * node + 2 * (lx ? 0 : 1) + (ly ? 0 : 1)), e8);
+      const long rec = 4 * node + 2 * (lx ? 0 : 1) + (ly ? 0 : 1);
+      if (g.xytex) {
+        const float4 a = tex1Dfetch<float4>(g.xytex, (int)(2 * rec)), b = tex1Dfetch<float4>(g.xytex, (int)(2 * rec + 1));
+        e8[0] = a.x;
+        e8[1] = a.y;
+        e8[2] = a.z;
+        e8[3] = a.w;
+        e8[4] = b.x;
+        e8[5] = b.y;
+        e8[6] = b.z;
+        e8[7] = b.w;
+      } else {
+        ld8(g.xy + 8 * rec, e8);
+      }
 #pragma unroll
       for (int j = 0; j < 2; ++j)
 #pragma unroll

@@ -1265,6 +1265,22 @@ __global__ void xy_kernel(const float* __restrict__ d, float* __restrict__ xy, i
   }
 }
 
+// z-edge records of a one-channel grid (DevGrid::ztex); nodes off the grid read as 0.
+__global__ void zedge_kernel(const float* __restrict__ d, float4* __restrict__ out, int nx, int ny, int nz) {
+  const long n_nodes = (long)nx * ny * nz;
+  auto at = [&](int x, int y, int z) -> float {
+    return (x >= 0 && x < nx && y >= 0 && y < ny && z >= 0 && z < nz) ? d[((long)x * ny + y) * nz + z] : 0.f;
+  };
+  for (long n = blockIdx.x * (long)blockDim.x + threadIdx.x; n < n_nodes; n += (long)gridDim.x * blockDim.x) {
+    const int z = (int)(n % nz), y = (int)((n / nz) % ny), x = (int)(n / ((long)ny * nz));
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const int ez = c ? z + 2 : z - 1;
+      out[2 * n + c] = make_float4(at(x, y, ez), at(x, y + 1, ez), at(x + 1, y, ez), at(x + 1, y + 1, ez));
+    }
+  }
+}
+
 // D(r) of the stepper at n distances (parity entry point bd_sim_hi_diffusion).
 template <typename FT>
 __global__ void hi_diffusion_kernel(DevSim P, int n, const double* __restrict__ r, double* __restrict__ D) {
