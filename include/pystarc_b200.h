@@ -268,7 +268,8 @@ enum {
 #define BD_CUBE_MAX_BYTES (48ll * 1024 * 1024)
 #define BD_OVERLAP_MAX_CELLS (32ll * 1024 * 1024)
 #define BD_XY_MAX_BYTES (64ll * 1024 * 1024)
-#define BD_LAYOUT_DEFAULT (BD_LAYOUT_WINDOWS_1 | BD_LAYOUT_CUBES_1 | BD_LAYOUT_OVERLAP_GRID | BD_LAYOUT_XY_1)
+#define BD_LAYOUT_DEFAULT \
+  (BD_LAYOUT_WINDOWS_1 | BD_LAYOUT_CUBES_1 | BD_LAYOUT_OVERLAP_GRID | BD_LAYOUT_XY_1 | BD_LAYOUT_ZTEX_1)
 #define BD_STAGE_MAX_BYTES (64 * 1024)
 int bd_set_layout(BdHandle* h, int flags);
 int bd_get_layout(BdHandle* h, int* flags);

@@ -13,9 +13,10 @@ The tuned "tile shapes" of the stepper:
 * trajectories per CTA -- threads per block (128 or 256) divided by the lanes per trajectory;
 * the receptor tile of Born direction 2 -- how the ligand Born grid is read: float4 windows of
   4 z-nodes (8 loads per stencil) or 2x2x2 node cubes (4 loads, 8x the grid's memory).
-  A third candidate adds the xy records (x face and y edge of a cell half in one 32-byte record:
-  3 loads per stencil, 16x the grid's memory).  Every candidate keeps the overlap occupancy grid
-  (one lane per overlap test).
+  A third candidate, the default layout, adds the xy records (x face and y edge of a cell half
+  in one 32-byte record) and reads the z edge through the texture path: two global loads and
+  one texture fetch per stencil.  Every candidate keeps the overlap occupancy grid (one lane per
+  overlap test).
 
 Which is fastest depends on the ligand and receptor sizes, on how often trajectories are near
 the receptor and on precision, so the tuner times short bursts of the real stepper on the
@@ -30,8 +31,8 @@ from . import _lib
 
 DEFAULT_CANDIDATES = ((1, 128), (8, 128), (16, 128), (32, 128), (64, 128), (64, 256), (65, 128), (65, 256),
                       (66, 256))
-DEFAULT_LAYOUTS = (_lib.LAYOUT_WINDOWS_1 | _lib.LAYOUT_OVERLAP_GRID, _lib.LAYOUT_DEFAULT & ~_lib.LAYOUT_XY_1,
-                   _lib.LAYOUT_DEFAULT)
+DEFAULT_LAYOUTS = (_lib.LAYOUT_WINDOWS_1 | _lib.LAYOUT_OVERLAP_GRID,
+                   _lib.LAYOUT_DEFAULT & ~(_lib.LAYOUT_XY_1 | _lib.LAYOUT_ZTEX_1), _lib.LAYOUT_DEFAULT)
 
 
 def measure(sim, group, block, K=16, launches=4, aged=None):
