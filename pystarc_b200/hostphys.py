@@ -4,6 +4,8 @@
 * ``return_prob_and_kb`` -- GPUBatchSimulator._compute_return_prob
                             (pystarc/simulation/gpu_batch_simulator.py:320-404): Yukawa U with
                             the dielectric hard-coded to 78 * 0.000142, optional HI D_parallel
+* ``bradius_cover``      -- the cover-zone boundary b + x0 (:406-460); the stepper does not
+                            use it, the simulator keeps it as ``_bradius_cover`` as the reference does
 * ``bridge_d_eff``       -- per-pair D_eff of the Brownian bridge (:637-660)
 * ``multipole``          -- MultipoleExpansion moments (pystarc/forces/multipole_farfield.py:86-110)
 * ``wilson_ci`` / ``rate_constant`` -- GPUBatchResult (:61-113)
@@ -63,6 +65,59 @@ def return_prob_and_kb(r_start, r_escape, q_rec, q_lig, debye, D_t, use_hi=False
         return float(max(0.0, min(1.0, rp))), k_b
     except (OverflowError, ZeroDivisionError, ValueError):
         return b / q_out, 4.0 * math.pi * D_t * b
+
+
+def bradius_cover(b, q_rec, q_lig, debye, eps=78.0 * EPS0):
+    """b + x0: the radius beyond the b-sphere where the Yukawa force stops being linear enough.
+
+    Two bisections, as the reference takes them:
+      1. the linear-region width L: the first r > b where the force's relative curvature
+         (2 l^2 + 2 r l + r^2) |r - b| / (r l (l + r)) reaches 0.05 (l = Debye length), found by
+         doubling from 2b and halving to 1e-6 b, capped at 0.1 b;
+      2. x0 in (0, L) where the probability of a step leaving the linear region,
+         erfc((L - x0^2 F(b) - x0) / (2 x0)) / (erf((x0 F(b) + 1) / 2) + 1), falls to 0.01
+         (F = the Yukawa force, in kT/A), to 1e-6 L or 100 halvings.
+    """
+    from scipy.special import erf, erfc  # the reference's error functions
+
+    v_factor = q_rec * q_lig / (4.0 * math.pi * eps)
+    lam = debye
+
+    def excess_curvature(r):
+        return (2 * lam ** 2 + 2 * r * lam + r ** 2) * abs(r - b) / (r * lam * (lam + r)) - 0.05
+
+    hi = 2.0 * b
+    while excess_curvature(hi) < 0.0:
+        hi *= 2.0
+    lo = b
+    while hi - lo > 1e-6 * b:
+        mid = 0.5 * (lo + hi)
+        if excess_curvature(mid) * excess_curvature(hi) < 0.0:
+            lo = mid
+        else:
+            hi = mid
+    width = min(0.5 * (lo + hi) - b, 0.1 * b)
+    rm1 = 1.0 / b
+    f_b = v_factor * math.exp(-b / lam) * rm1 * (rm1 + 1.0 / lam)
+
+    def p_leave(x0):
+        if x0 <= 1e-10:
+            return 1.0
+        try:
+            return erfc((width - x0 ** 2 * f_b - x0) / (2.0 * x0)) / (erf((x0 * f_b + 1.0) / 2.0) + 1.0 + 1e-30)
+        except (OverflowError, ValueError, ZeroDivisionError):
+            return 0.0
+
+    lo, hi = 0.0, width
+    for _ in range(100):
+        if hi - lo < 1e-6 * max(width, 1e-10):
+            break
+        mid = 0.5 * (lo + hi)
+        if p_leave(mid) > 0.01:
+            hi = mid
+        else:
+            lo = mid
+    return float(b + 0.5 * (lo + hi))
 
 
 def bridge_d_eff(D_t, r_h_rec, r_h_lig, rec_pair_xyz, lig_pair_body):

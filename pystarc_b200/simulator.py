@@ -28,7 +28,7 @@ from typing import Dict
 import numpy as np
 
 from . import _lib
-from .hostphys import bridge_d_eff, rate_constant, return_prob_and_kb, wilson_ci
+from .hostphys import bradius_cover, bridge_d_eff, rate_constant, return_prob_and_kb, wilson_ci
 
 
 @dataclass
@@ -251,6 +251,14 @@ class B200BatchSimulator:
         kT = float(getattr(p, "_kT_scale", 1.0))
         self._return_prob, self._k_b = return_prob_and_kb(p.r_start, p.r_escape, q_rec, q_lig, debye, D_t,
                                                           self._use_hi, r_h_rec, r_h_lig, kT)
+        # cover-zone boundary (unused by the stepper): 0 for uncharged pairs, 1.05 b when it fails
+        # (gpu_batch_simulator.py:183, 394-403)
+        self._bradius_cover = 0.0
+        if abs(q_rec * q_lig) >= 1e-9:
+            try:
+                self._bradius_cover = bradius_cover(float(p.r_start), q_rec, q_lig, debye)
+            except (OverflowError, ValueError, ZeroDivisionError):
+                self._bradius_cover = float(p.r_start) * 1.05
         h = self.engine.handle
         self.engine.set_ligand(self._mol2_pos0, self._charges)
         P = len(self._rxn_cutoffs)

@@ -190,6 +190,21 @@ def gen_physics(out):
                             pts=pts, V=np.array([mp.potential(p) for p in pts]))
 
 
+def gen_bradius(out):
+    """GPUBatchSimulator._compute_bradius_cover (it reads no instance state) on a grid of b-sphere
+    radii, charge pairs and Debye lengths, with the reference's dielectric 78 * 0.000142."""
+    from pystarc.simulation.gpu_batch_simulator import GPUBatchSimulator
+
+    rows, vals = [], []
+    for b in (10.0, 26.0, 50.0, 60.0, 80.0, 120.0):
+        for q_rec, q_lig in ((8.0, 1.0), (8.0, -1.0), (2.0, -6.0), (5.0, -5.0), (1.0, -1.0), (-3.0, -2.0), (0.5, 0.1)):
+            for debye in (3.0, 7.828, 7.858, 15.0):
+                rows.append((b, q_rec, q_lig, debye))
+                vals.append(GPUBatchSimulator._compute_bradius_cover(None, b, q_rec, q_lig, 78.0 * 0.000142, debye,
+                                                                     0.05))
+    out["bradius"] = dict(inputs=np.array(rows), cover=np.array(vals))
+
+
 def build_sim(s, n_traj, seed, max_steps, work, sm=None, use_lj=False):
     from pystarc.simulation.gpu_batch_simulator import GPUBatchSimulator
     from pystarc.simulation.nam_simulator import NAMParameters
@@ -506,6 +521,7 @@ def main():
     jobs = {
         "k1": lambda: gen_k1(out),
         "physics": lambda: gen_physics(out),
+        "bradius": lambda: gen_bradius(out),
         "engine_c2": lambda: gen_engine(out, "engine_c2", c2, 96, 3.0, 40.0, 21),
         "engine_c3": lambda: gen_engine(out, "engine_c3", c3, 64, 4.0, 40.0, 22),
         "engine_wca_c2": lambda: gen_engine_wca(out, "engine_wca_c2", c2, 64, 5.0, 11.0, 23),

@@ -22,6 +22,13 @@ def test_return_prob_matches_reference_runs():
         assert rp == float(g["return_prob"]) and kb == float(g["k_b"])
 
 
+def test_bradius_cover_matches_reference():
+    """The cover-zone boundary (gpu_batch_simulator.py:406-460), bit for bit on the reference's fixture."""
+    g = golden("bradius")
+    for (b, q_rec, q_lig, debye), want in zip(g["inputs"], g["cover"]):
+        assert hostphys.bradius_cover(float(b), float(q_rec), float(q_lig), float(debye)) == float(want)
+
+
 def test_mobility_mirror_matches_reference():
     g = golden("stokes")
     for i, r in enumerate(g["radii"]):
