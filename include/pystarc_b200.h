@@ -254,6 +254,9 @@ int bd_get_launch(BdHandle* h, int* group, int* block_threads, int* grid_blocks)
  *   grid's memory in float4 records).
  * BD_LAYOUT_XYTEX_1 (with BD_LAYOUT_XY_1): the xy records are read through the texture path as
  *   two 16-byte fetches instead of one 32-byte global load.
+ * BD_LAYOUT_PTEX_2: the interleaved elec+Born grid gets a float2 texture view, and a forward
+ *   stencil reads its eight extra nodes through the texture path (its twelve centre-row nodes
+ *   stay global loads).
  * The same values enter the same arithmetic in every layout: results are identical. */
 enum {
   BD_LAYOUT_STAGE_RECEPTOR = 1,
@@ -263,7 +266,8 @@ enum {
   BD_LAYOUT_OVERLAP_GRID = 16,
   BD_LAYOUT_XY_1 = 32,
   BD_LAYOUT_ZTEX_1 = 64,
-  BD_LAYOUT_XYTEX_1 = 128
+  BD_LAYOUT_XYTEX_1 = 128,
+  BD_LAYOUT_PTEX_2 = 256
 };
 #define BD_CUBE_MAX_BYTES (48ll * 1024 * 1024)
 #define BD_OVERLAP_MAX_CELLS (32ll * 1024 * 1024)

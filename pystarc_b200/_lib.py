@@ -20,7 +20,7 @@ CTR_NAMES = ("started", "reacted", "escaped", "max_steps", "steps", "returns", "
              "rev_evals", "ff_evals", "nonfinite")
 N_CTR = len(CTR_NAMES)
 LAYOUT_STAGE_RECEPTOR, LAYOUT_WINDOWS_1, LAYOUT_WINDOWS_2, LAYOUT_CUBES_1, LAYOUT_OVERLAP_GRID = 1, 2, 4, 8, 16
-LAYOUT_XY_1, LAYOUT_ZTEX_1, LAYOUT_XYTEX_1 = 32, 64, 128
+LAYOUT_XY_1, LAYOUT_ZTEX_1, LAYOUT_XYTEX_1, LAYOUT_PTEX_2 = 32, 64, 128, 256
 LAYOUT_DEFAULT = LAYOUT_WINDOWS_1 | LAYOUT_CUBES_1 | LAYOUT_OVERLAP_GRID | LAYOUT_XY_1 | LAYOUT_ZTEX_1
 TERM_GRID, TERM_FARFIELD, TERM_REV_BORN, TERM_CONTACT, TERM_ALL = 1, 2, 4, 8, 15
 

@@ -325,6 +325,24 @@ int float4_texture(BdHandle* h, void* p, size_t n, cudaTextureObject_t* out) {
   return BD_OK;
 }
 
+// A float2 texture view of n float2 elements at p (linear memory, point sampling).
+int float2_texture(BdHandle* h, void* p, size_t n, cudaTextureObject_t* out) {
+  cudaResourceDesc res{};
+  res.resType = cudaResourceTypeLinear;
+  res.res.linear.devPtr = p;
+  res.res.linear.desc = cudaCreateChannelDesc<float2>();
+  res.res.linear.sizeInBytes = n * sizeof(float2);
+  cudaTextureDesc td{};
+  td.readMode = cudaReadModeElementType;
+  td.filterMode = cudaFilterModePoint;
+  td.addressMode[0] = cudaAddressModeClamp;
+  cudaTextureObject_t t = 0;
+  CK(h, cudaCreateTextureObject(&t, &res, &td, nullptr));
+  h->sys_tex.push_back(t);
+  *out = t;
+  return BD_OK;
+}
+
 // xy records of a grid that has its cube copy (DevGrid::xy), and their texture view when asked.
 int add_xy(BdHandle* h, DevGrid& g, bool tex) {
   const long n = (long)g.nx * g.ny * g.nz;
@@ -415,6 +433,9 @@ int finalize(BdHandle* h) {
       if (rc) return rc;
       grid_to_dev(el[0], p, 2, S.pair);
       S.paired = 1;
+      // linear textures address at most 2^27 elements
+      if ((h->layout & BD_LAYOUT_PTEX_2) && el[0].data.size() <= (size_t)(1 << 27))
+        if ((rc = float2_texture(h, (void*)p, el[0].data.size(), &S.pair.ptex))) return rc;
     }
   }
   if (h->layout & BD_LAYOUT_WINDOWS_1) {
@@ -924,7 +945,7 @@ int bd_set_launch(BdHandle* h, int group, int block) {
 int bd_set_layout(BdHandle* h, int flags) {
   if (!h) return BD_ERR_ARG;
   const int all = BD_LAYOUT_STAGE_RECEPTOR | BD_LAYOUT_WINDOWS_1 | BD_LAYOUT_WINDOWS_2 | BD_LAYOUT_CUBES_1 |
-                  BD_LAYOUT_OVERLAP_GRID | BD_LAYOUT_XY_1 | BD_LAYOUT_ZTEX_1 | BD_LAYOUT_XYTEX_1;
+                  BD_LAYOUT_OVERLAP_GRID | BD_LAYOUT_XY_1 | BD_LAYOUT_ZTEX_1 | BD_LAYOUT_XYTEX_1 | BD_LAYOUT_PTEX_2;
   if (flags & ~all) return fail(h, BD_ERR_ARG, "unknown layout flags 0x%x", flags & ~all);
   if (flags != h->layout) {
     h->layout = flags;

@@ -51,6 +51,7 @@ struct DevGrid {
                       // ey = (b ? y + 2 : y - 1): v(ex, y + j, z + k) at 2j + k, v(x + i, ey, z + k)
                       // at 4 + 2i + k
   cudaTextureObject_t xytex;  // optional: a float4 texture view of xy (record r = elements 2r, 2r + 1)
+  cudaTextureObject_t ptex;   // optional (ch = 2): a float2 texture view of data (element = node)
   cudaTextureObject_t ztex;  // optional (with cube): per node n = (x, y, z), two float4 records
                              // read through the texture path, record 2n + c for the extra z node
                              // ez = (c ? z + 2 : z - 1): v(x, y, ez), v(x, y + 1, ez),
@@ -499,17 +500,38 @@ __device__ __forceinline__ StencilOut<FT, CH> stencil(const DevGrid& g, PT x, PT
 #pragma unroll
         for (int k = 0; k < 3; ++k) ld<CH>(d + base + k * CH, r[i][j][k]);
       }
+    if (CH == 2 && g.ptex) {
+      // the eight extra nodes through the texture path, the twelve centre-row nodes above through LSU
+      auto tx = [&](int node, float v[CH]) {
+        const float2 t = tex1Dfetch<float2>(g.ptex, node);
+        v[0] = t.x;
+        v[CH - 1] = t.y;
+      };
 #pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      const int base = (ex * syz + (cy + j) * nz + cz) * CH;
-      ld<CH>(d + base, xe[j][0]);
-      ld<CH>(d + base + CH, xe[j][1]);
-    }
+      for (int j = 0; j < 2; ++j) {
+        const int n = ex * syz + (cy + j) * nz + cz;
+        tx(n, xe[j][0]);
+        tx(n + 1, xe[j][1]);
+      }
 #pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      const int base = ((cx + i) * syz + ey * nz + cz) * CH;
-      ld<CH>(d + base, ye[i][0]);
-      ld<CH>(d + base + CH, ye[i][1]);
+      for (int i = 0; i < 2; ++i) {
+        const int n = (cx + i) * syz + ey * nz + cz;
+        tx(n, ye[i][0]);
+        tx(n + 1, ye[i][1]);
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int base = (ex * syz + (cy + j) * nz + cz) * CH;
+        ld<CH>(d + base, xe[j][0]);
+        ld<CH>(d + base + CH, xe[j][1]);
+      }
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int base = ((cx + i) * syz + ey * nz + cz) * CH;
+        ld<CH>(d + base, ye[i][0]);
+        ld<CH>(d + base + CH, ye[i][1]);
+      }
     }
   }
   const FT wx[2] = {(FT)1 - sx, sx}, wy[2] = {(FT)1 - sy, sy}, wz[2] = {(FT)1 - sz, sz};

@@ -90,7 +90,8 @@ def test_grid_windows_give_identical_forces(sysname, precision):
     out = []
     for layout in (0, _lib.LAYOUT_WINDOWS_1, _lib.LAYOUT_WINDOWS_2, _lib.LAYOUT_DEFAULT, _lib.LAYOUT_CUBES_1,
                    _lib.LAYOUT_CUBES_1 | _lib.LAYOUT_WINDOWS_1, _lib.LAYOUT_DEFAULT & ~_lib.LAYOUT_XY_1,
-                   _lib.LAYOUT_DEFAULT & ~_lib.LAYOUT_ZTEX_1, _lib.LAYOUT_DEFAULT | _lib.LAYOUT_XYTEX_1):
+                   _lib.LAYOUT_DEFAULT & ~_lib.LAYOUT_ZTEX_1, _lib.LAYOUT_DEFAULT | _lib.LAYOUT_XYTEX_1,
+                   _lib.LAYOUT_DEFAULT | _lib.LAYOUT_PTEX_2):
         eng = make_engine(s, precision, "centroid", layout=layout)
         out.append(eng.eval_poses(c, q))
         eng.close()

@@ -263,7 +263,8 @@ def test_data_layouts_do_not_change_fates(precision, group):
     outs = []
     for layout in (0, _lib.LAYOUT_DEFAULT, _lib.LAYOUT_WINDOWS_1 | _lib.LAYOUT_WINDOWS_2 | _lib.LAYOUT_STAGE_RECEPTOR,
                    _lib.LAYOUT_CUBES_1 | _lib.LAYOUT_WINDOWS_1, _lib.LAYOUT_DEFAULT & ~_lib.LAYOUT_XY_1,
-                   _lib.LAYOUT_DEFAULT & ~_lib.LAYOUT_ZTEX_1, _lib.LAYOUT_DEFAULT | _lib.LAYOUT_XYTEX_1):
+                   _lib.LAYOUT_DEFAULT & ~_lib.LAYOUT_ZTEX_1, _lib.LAYOUT_DEFAULT | _lib.LAYOUT_XYTEX_1,
+                   _lib.LAYOUT_DEFAULT | _lib.LAYOUT_PTEX_2):
         sim = make_sim(s, 800, 250, precision, slots=400, steps_per_launch=16, layout=layout)
         sim.engine.handle.call("bd_set_launch", group, 128)
         res = sim.run()
