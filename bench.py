@@ -661,11 +661,14 @@ def cpu_baseline(s, cores, traj_per_proc=256, n_steps=40, init=None, where=None)
         wall = time.perf_counter() - t0
     steps = sum(o[0] for o in out)
     busy = max(o[1] for o in out)
+    # one single-threaded process's own rate (median over the processes, all running at once)
+    per_proc = float(np.median([o[0] / o[1] for o in out if o[1] > 0])) if any(o[1] > 0 for o in out) else 0.0
     if where is None:
         where = "poses sampled from the GPU arm's aged pool" if init is not None else "the b-sphere"
     return steps / busy, {"value": steps / busy, "unit": UNIT, "cores": cores, "kind": "port",
                           "sample": f"{cores} processes x {traj_per_proc} trajectories x <= {n_steps} steps of the "
                                     f"same system from {where} ({steps} trajectory-steps, {busy:.1f} s)",
+                          "one_process_value": per_proc,
                           "wall_s": round(wall, 1)}
 
 
@@ -684,7 +687,9 @@ def main():
     ap.add_argument("--layout", type=int, default=-1,
                     help="device data layout flags (1 stage receptor, 2 windows for 1-channel grids, "
                          "4 windows for the paired grid, 8 cubes for the ligand Born grid, 16 overlap "
-                         "occupancy grid, 32 xy records with the cubes; -1: autotuned)")
+                         "occupancy grid, 32 xy records with the cubes, 64 z-edge texture records with the cubes, "
+                         "128 xy records read through the texture path, 256 a texture view of the paired grid; "
+                         "-1: autotuned)")
     ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate arm (config 4)")
     ap.add_argument("--age", type=int, default=-1,
