@@ -183,6 +183,40 @@ def test_reference_known_answers():
     assert 0 <= lo < 0.05 < hi <= 1
 
 
+def test_reference_known_answers_grid_and_farfield():
+    """The reference suite's known answers for trilinear grids and the multipole far-field
+    (tests/test_pystarc.py:935-960, :4505-4566), applied to the oracle's K1 and far-field."""
+    data = np.zeros((5, 5, 5))
+    for i in range(5):
+        data[i] = float(i)  # potential rises along x
+    o, sp = np.zeros(3), np.ones(3)
+    pts = np.array([[2.0, 2.0, 2.0], [1.5, 1.0, 1.0], [100.0, 0.0, 0.0]])
+    f, e = k1_batch_force(pts, np.ones(3), data, o, sp, 0.0, False)  # q = 1: E = phi, F = -grad phi
+    assert abs(e[0] - 2.0) < 1e-12 and abs(e[1] - 1.5) < 1e-12 and e[2] == 0.0  # :941-954
+    assert abs(-f[0, 0] - 1.0) < 1e-12 and abs(f[0, 1]) < 1e-12 and abs(f[0, 2]) < 1e-12  # :956-960
+    assert np.all(f[2] == 0.0)
+    # monopole of +3 e at the origin, lambda = 7.86, eps = 78 * 0.000142 (:4511-4520)
+    ff = FarField(3.0, 7.86, 78.0)
+    r = 20.0
+    V_exact = 3.0 / (4 * math.pi * 78.0 * 0.000142 * r) * math.exp(-r / 7.86)
+    _, V = yukawa_forces(np.array([[r, 0.0, 0.0]]), np.ones(1), ff)
+    assert abs(V[0] - V_exact) / abs(V_exact) < 1e-12
+    # F = -grad V by central differences (:4552-4566)
+    rv = np.array([15.0, 3.0, -2.0])
+    F, _ = yukawa_forces(rv[None], np.ones(1), ff)
+    h = 1e-4
+    for i in range(3):
+        d = np.zeros(3)
+        d[i] = h
+        _, vp = yukawa_forces((rv + d)[None], np.ones(1), ff)
+        _, vm = yukawa_forces((rv - d)[None], np.ones(1), ff)
+        F_num = -(vp[0] - vm[0]) / (2 * h)
+        assert abs(F[0, i] - F_num) < 1e-6 * max(abs(F_num), 1e-10)
+    # two opposite charges: no monopole, dipole magnitude 10 (:4522-4531)
+    dip, quad = multipole_moments(np.array([[5.0, 0, 0], [-5.0, 0, 0]]), np.array([1.0, -1.0]))
+    assert abs(np.linalg.norm(dip) - 10.0) < 1e-12
+
+
 def test_philox_known_answers():
     """Random123 known-answer vectors for philox4x32-10."""
     out = philox4x32_10(0, 0, 0, 0, 0, 0)
