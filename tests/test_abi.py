@@ -45,6 +45,24 @@ def test_errors_are_codes_not_crashes():
     assert lib.bd_sim_set_states(None, None) == _lib.BD_ERR_ARG
 
 
+_NO_HANDLE = {"bd_version", "bd_create", "bd_destroy", "bd_last_error", "bd_mlp_last_error", "bd_mlp_destroy",
+              "bd_multi_destroy"}
+
+
+def test_every_entry_point_rejects_a_null_handle():
+    """Each entry point that takes a handle returns BD_ERR_ARG for NULL (zero sizes, NULL arrays)
+    before it touches the GPU; destroying NULL is a no-op."""
+    lib = _lib.load()
+    ints = (ctypes.c_int, ctypes.c_int8, ctypes.c_int32, ctypes.c_int64, ctypes.c_uint32, ctypes.c_uint64,
+            ctypes.c_long, ctypes.c_longlong, ctypes.c_size_t)
+    for name, (_, args) in _lib.SIGNATURES.items():
+        if name in _NO_HANDLE:
+            continue
+        vals = [0 if a in ints else 0.0 if a in (ctypes.c_double, ctypes.c_float) else None for a in args]
+        assert getattr(lib, name)(*vals) == _lib.BD_ERR_ARG, name
+    assert lib.bd_multi_destroy(None) == 0
+
+
 def test_create_without_gpu_reports_cuda_error():
     import torch
 
