@@ -295,6 +295,7 @@ def e2e_arm(s, precision, steps, K, n_traj, id_offset, launch, aged=None):
     shutil.rmtree(work, ignore_errors=True)
     launches = max(1, steps)
     res.e2e_split = {"engine_s": round(t_engine, 3), "run_s": round(el - t_engine, 3)}
+    res.e2e_steps, res.e2e_seconds = res.total_steps - steps0, el
     return (res.total_steps - steps0) / el, h2d / launches, d2h / launches, res
 
 
@@ -805,6 +806,13 @@ def main():
         from pystarc_b200.shard import allreduce_tallies
 
         pooled_tallies = allreduce_tallies(d_mixed, device=torch.device("cuda", local))
+        # the end-to-end arm for the whole job: steps and copied bytes summed, time the slowest rank's
+        et = torch.tensor([e2e_res.e2e_seconds], device="cuda", dtype=torch.float64)
+        dist.all_reduce(et, op=dist.ReduceOp.MAX)
+        eb = torch.tensor([e2e_res.e2e_steps, int(h2d), int(d2h)], device="cuda", dtype=torch.int64)
+        dist.all_reduce(eb)
+        e2e_val = int(eb[0].item()) / float(et.item())
+        h2d, d2h = int(eb[1].item()), int(eb[2].item())
     value = steps_all / t_max
     if dist is None:
         pooled_tallies = None
