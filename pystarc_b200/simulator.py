@@ -578,7 +578,7 @@ class B200BatchSimulator:
         if ckpt_interval > 0 and ckpt.exists():
             try:
                 self.load_checkpoint(ckpt)
-            except (ValueError, OSError, KeyError) as e:
+            except Exception as e:  # unreadable, truncated or another run's file (gpu_batch_simulator.py:574-575)
                 print(f" Checkpoint load failed: {e}. Starting fresh.")
                 h.call("bd_sim_reset", None)
         last_ckpt_done = 0
