@@ -490,7 +490,7 @@ def main(argv=None):
     if not argv or argv[0] in ("-h", "--help"):
         print(__doc__)
         return 0
-    prep, result = run(argv[0])
+    prep, result = run(argv[0], verbose=True)  # the reference's console reports while the BD stage runs
     print(result.summary(prep.D_rel, prep.simulator._k_b, prep.cfg.confidence_interval))
     return 0
 

@@ -91,6 +91,63 @@ class B200BatchResult:
         return "\n".join(lines)
 
 
+class ProgressLog:
+    """The reference loop's console reports (gpu_batch_simulator.py:753-761, 1357-1399, 1491-1510).
+
+    ``poll`` prints a "converged" line when the trajectories done pass a milestone (every
+    ``conv_interval`` percent of n; the reference tests for equality at each step, this engine
+    polls between launches, so the line comes at the first poll at or past the milestone) and
+    a progress line every ``every_s`` seconds.  ``final`` prints the closing totals.  The live
+    k_on is the reference's CONV * k_b * P, without the return-probability correction of the
+    final result.
+    """
+
+    CONV = 6.022e23 * 1e-30 / 1e-12 / 1e-3  # A^3/ps -> M^-1 s^-1
+
+    def __init__(self, n, k_b, conv_interval, t0, every_s=10.0, out=print):
+        self.n, self.k_b, self.t0, self.every, self.out = int(n), float(k_b), t0, float(every_s), out
+        ci = int(conv_interval or 0)
+        self.marks = sorted({int(self.n * p / 100) for p in range(ci, 100, ci)}) if ci > 0 else []
+        self.last_mark = 0
+        self.last_t = t0
+
+    def _k(self, p):
+        return self.CONV * self.k_b * p if self.k_b > 0 else 0
+
+    def poll(self, done, reacted, escaped, now=None):
+        now = time.perf_counter() if now is None else now
+        crossed = [m for m in self.marks if self.last_mark < m <= done]
+        n_comp = reacted + escaped
+        if crossed:
+            self.last_mark = crossed[-1]
+            if n_comp > 0:
+                p = reacted / n_comp
+                self.out(f"  -- {done / self.n * 100:.0f}% converged --  P_rxn={p:.5f}  k_on={self._k(p):.3e}  "
+                         f"({reacted:,} react / {escaped:,} esc)  [{now - self.t0:.0f}s]")
+        if now - self.last_t >= self.every:
+            self.last_t = now
+            head = (f"  [T] {now - self.t0:6.0f}s  done={done:,}/{self.n:,} ({done / self.n * 100:.1f}%)  "
+                    f"reacted={reacted:,}  escaped={escaped:,}")
+            k = self._k(reacted / n_comp) if n_comp > 0 else 0
+            if k > 0:
+                e = int(math.floor(math.log10(k)))
+                self.out(f"{head}  P_rxn={reacted / n_comp:.5f}  k_on={k / 10 ** e:.2f}e{e}")
+            else:
+                self.out(head)
+
+    def final(self, reacted, escaped, max_steps, total_steps, elapsed, overlap, removed_checkpoint):
+        sps = total_steps / elapsed if elapsed > 0 else 0
+        self.out(f"  BD complete: {reacted} reacted, {escaped} escaped, {max_steps} max-steps")
+        self.out(f"  Total steps: {total_steps:,}  ({sps:,.0f} steps/sec)")
+        if overlap > 0:
+            self.out(f"  Overlap rejections: {overlap:,}")
+        if reacted + escaped > 0 and self.k_b > 0:
+            p = reacted / (reacted + escaped)
+            self.out(f"  Final: P_rxn={p:.6f}  k_on={self._k(p):.4e} M-1 s-1")
+        if removed_checkpoint:
+            self.out("  Checkpoint removed (run completed successfully)")
+
+
 def flatten_pairs(pathway_set):
     """All pairs of all reactions; n_needed of the first reaction (gpu_batch_simulator.py:186-205)."""
     rec_idx, lig_idx, cut = [], [], []
@@ -174,6 +231,9 @@ class B200BatchSimulator:
     hydrodynamic interactions: "reference_gpu", the reference GPU stepper's
     line-of-centres D(r), or "zuk", D_t - (2/3) tr M12(r) with the three-regime
     RPY tensor of MobilityTensor, pystarc/hydrodynamics/rotne_prager.py:67-124, :177-200).
+    ``verbose`` prints the reference loop's console reports while it runs: convergence
+    milestones every ``params.convergence_interval`` percent, progress every 10 s and the
+    closing totals (``ProgressLog``).
     """
 
     def __init__(self, mol1, mol2, mob, pathway_set, params, batch_engine, *, precision=None, torque_mode=None,
@@ -585,6 +645,7 @@ class B200BatchSimulator:
         launches = 0
         stalled, last_steps = 0, -1
         stop_at = int(N * 0.995) if self.termination == "reference" else N
+        log = ProgressLog(N, self._k_b, getattr(self.params, "convergence_interval", 10), t0) if self.verbose else None
         while True:
             h.call("bd_sim_run", self.M, self.K, None)
             launches += self.M
@@ -592,8 +653,8 @@ class B200BatchSimulator:
             if c["nonfinite"]:
                 raise _lib.BdError(_lib.BD_ERR_NAN, f"{c['nonfinite']} trajectories produced a non-finite pose")
             done = c["reacted"] + c["escaped"] + c["max_steps"]
-            if self.verbose:
-                print(f"  [b200] launches={launches} done={done}/{N} steps={c['steps']:,}")
+            if log is not None:
+                log.poll(done, c["reacted"], c["escaped"])
             if ckpt_interval > 0 and done - last_ckpt_done >= ckpt_interval:
                 last_ckpt_done = done
                 self.save_checkpoint(ckpt)
@@ -619,8 +680,11 @@ class B200BatchSimulator:
         n_reacted = int(np.sum(status == 1))
         n_escaped = int(np.sum(status == 2))
         n_max = N - n_reacted - n_escaped
-        if ckpt_interval > 0 and ckpt.exists():
+        removed = ckpt_interval > 0 and ckpt.exists()
+        if removed:
             ckpt.unlink()
+        if log is not None:
+            log.final(n_reacted, n_escaped, n_max, int(c["steps"]), elapsed, int(c["overlap"]), removed)
         self.counters = c
         total = int(c["steps"])
         if self.stats:
