@@ -135,6 +135,9 @@ class ProgressLog:
             else:
                 self.out(head)
 
+    def stall(self, trapped, recent):
+        self.out(f"  Stall detected: {trapped} trajectories trapped (+{recent} in last 10k steps). Stopping.")
+
     def final(self, reacted, escaped, max_steps, total_steps, elapsed, overlap, removed_checkpoint):
         sps = total_steps / elapsed if elapsed > 0 else 0
         self.out(f"  BD complete: {reacted} reacted, {escaped} escaped, {max_steps} max-steps")
@@ -234,7 +237,14 @@ class B200BatchSimulator:
     ``verbose`` prints the reference loop's console reports while it runs: convergence
     milestones every ``params.convergence_interval`` percent, progress every 10 s and the
     closing totals (``ProgressLog``).
+
+    With ``termination="reference"`` the run also stops on the reference's stall rule: at
+    every STALL_STEPS BD steps of the pool (the reference's loop counter when every
+    trajectory starts at once), once more than 95 % are done and fewer than max(2, N/1000)
+    finished since the last check; ``stall_stopped`` records it.
     """
+
+    STALL_STEPS = 10000
 
     def __init__(self, mol1, mol2, mob, pathway_set, params, batch_engine, *, precision=None, torque_mode=None,
                  termination="reference", steps_per_launch=64, launches_per_poll=8, slots=0, id_offset=0,
@@ -268,6 +278,7 @@ class B200BatchSimulator:
             trace_capacity = 4_000_000 if (self._want_paths or self._want_energy) else 0
         self.trace_capacity = int(trace_capacity) if self.stats else 0
         self.verbose = verbose
+        self.stall_stopped = False
         # (MLPEnsemble, SurrogateSpec): far-field + reverse Born from the learned surrogate inside its trust region
         self.surrogate = surrogate
         c0 = np.asarray(mol2.centroid(), dtype=float)
@@ -645,6 +656,10 @@ class B200BatchSimulator:
         launches = 0
         stalled, last_steps = 0, -1
         stop_at = int(N * 0.995) if self.termination == "reference" else N
+        # the reference's stall stop (gpu_batch_simulator.py:1349-1356): every STALL_STEPS BD steps of the
+        # pool, stop once more than 95 % are done and fewer than max(2, 0.1 % of N) finished since the last check
+        next_stall, stall_done = self.STALL_STEPS, 0
+        self.stall_stopped = False
         log = ProgressLog(N, self._k_b, getattr(self.params, "convergence_interval", 10), t0) if self.verbose else None
         while True:
             h.call("bd_sim_run", self.M, self.K, None)
@@ -660,6 +675,14 @@ class B200BatchSimulator:
                 self.save_checkpoint(ckpt)
             if done >= stop_at:
                 break
+            if self.termination == "reference" and launches * self.K >= next_stall:
+                next_stall = (launches * self.K // self.STALL_STEPS + 1) * self.STALL_STEPS
+                if done > int(N * 0.95) and done - stall_done < max(2, int(N * 0.001)):
+                    self.stall_stopped = True
+                    if log is not None:
+                        log.stall(N - done, done - stall_done)
+                    break
+                stall_done = done
             live = _lib.C.c_int32()
             h.call("bd_sim_live", _lib.C.byref(live))
             if live.value == 0 and c["started"] >= N:
