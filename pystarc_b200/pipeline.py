@@ -367,6 +367,22 @@ def flattened_pairs(path):
     return pairs, n_needed
 
 
+def check_reaction_indices(pathway, n_rec, n_lig, where):
+    """Reaction atom indices (0-based) must name atoms of the prepared molecules (GHO atom
+    included).  The reference indexes its position arrays with them, so an index past the end
+    raises IndexError when its simulator is built; this raises the same error, naming the
+    reaction source, before any grid is uploaded.  Negative indices keep NumPy's meaning (from
+    the end), as in the reference."""
+    k = 0
+    for rxn in pathway.reactions:
+        for p in rxn.criteria.pairs:
+            k += 1
+            for idx, n, mol in ((p.mol1_atom_index, n_rec, "receptor"), (p.mol2_atom_index, n_lig, "ligand")):
+                if not -n <= int(idx) < n:
+                    raise IndexError(f"{where}: reaction pair {k} names {mol} atom {int(idx) + 1} (1-based), "
+                                     f"but the {mol} has {n} atoms")
+
+
 def reaction_pathway(cfg: RunConfig, rec_atoms, lig_atoms) -> st.PathwaySet:
     """The PathwaySet of step 6 (pipeline.py:225-291 with auto_detect_reactions, geometry.py:391-482)."""
     rxns = _resolve(cfg.rxns_xml, cfg.xml_dir, Path.cwd()) if cfg.rxns_xml and cfg.rxns_xml.strip() else None
@@ -443,6 +459,7 @@ def build(xml_path, *, precision="fp64", torque_mode="zero", device=0, **sim_opt
     lig_born = load_grids(W, "ligand", "_born.dx")
     mob = st.MobilityTensor.from_radii(r_rec, r_lig, use_rpy=True, T=cfg.temperature)
     pathway = reaction_pathway(cfg, rec_atoms, lig_atoms)
+    check_reaction_indices(pathway, len(rec_atoms), len(lig_atoms), cfg.rxns_xml or "ghost_atoms")
     r_start = cfg.bd_milestone_radius
     params = st.NAMParameters(n_trajectories=cfg.n_trajectories, dt=cfg.dt, dt_rxn=cfg.minimum_core_reaction_dt,
                               max_steps=cfg.max_steps, r_start=r_start, r_escape=2.0 * r_start, seed=cfg.seed,

@@ -120,6 +120,28 @@ def test_reaction_pathway_state_machine_flattened_and_gho():
         pl.reaction_pathway(_cfg(state_machine_reactions=False, rxns_xml=""), rec, lig)
 
 
+def test_reaction_index_past_the_molecule_is_an_index_error(tmp_path):
+    """A reaction atom that the prepared molecule does not have stops the run before any grid is
+    uploaded, with the IndexError the reference raises when it builds its simulator."""
+    rec, _ = pl.centre_and_inject_gho(pl.read_pqr(PIPE / "rec.pqr"))
+    lig, _ = pl.centre_and_inject_gho(pl.read_pqr(PIPE / "lig.pqr"))
+    for sm in (True, False):  # both reaction files' pairs are in range once the GHO atoms are there
+        pl.check_reaction_indices(pl.reaction_pathway(_cfg(state_machine_reactions=sm), rec, lig), len(rec),
+                                  len(lig), "rxns")
+    bad = tmp_path / "rxns_bad.xml"
+    bad.write_text((PIPE / "rxns_flat.xml").read_text().replace("<atom1>5</atom1>", f"<atom1>{len(rec) + 1}</atom1>"))
+    pw = pl.reaction_pathway(_cfg(state_machine_reactions=False, rxns_xml=str(bad)), rec, lig)
+    with pytest.raises(IndexError, match="reaction pair 3 names receptor atom"):
+        pl.check_reaction_indices(pw, len(rec), len(lig), bad.name)
+    pw = pl.reaction_pathway(_cfg(state_machine_reactions=False, rxns_xml="", ghost_atoms=f"0,{len(lig)},4"), rec, lig)
+    with pytest.raises(IndexError, match="ligand atom"):
+        pl.check_reaction_indices(pw, len(rec), len(lig), "ghost_atoms")
+    # the last atom, and NumPy's -1 as the reference reads it
+    pw = pl.reaction_pathway(_cfg(state_machine_reactions=False, rxns_xml="", ghost_atoms=f"{len(rec) - 1},-1,4"),
+                             rec, lig)
+    pl.check_reaction_indices(pw, len(rec), len(lig), "ghost_atoms")
+
+
 def test_prepare_molecules_copies_centres_and_reads_back(ref, tmp_path):
     for f in ("rec.pqr", "lig.pqr", "input.xml"):
         shutil.copy(PIPE / f, tmp_path / f)
