@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "bd_kernels.cuh"
+#include "bd_nvtx.cuh"
 #include "bd_multi.cuh"
 #include "bd_surrogate.cuh"
 #include "bd_split.cuh"
@@ -882,6 +883,7 @@ int bd_set_reactions(BdHandle* h, int n_pairs, const double* rec_xyz, const doub
 
 int bd_eval_forces(BdHandle* h, int64_t n, const double* cen, const double* rot, int rot_is_matrix, double* F,
                    double* T, double* E, int prec, int torque, void* stream) {
+  bd::NvtxRange nvtx("bd_eval_forces");
   if (!h) return BD_ERR_ARG;
   if (n < 0 || (n > 0 && (!cen || !rot || !F || !T || !E))) return fail(h, BD_ERR_ARG, "bd_eval_forces: bad arguments");
   if (prec != BD_PREC_FP64 && prec != BD_PREC_MIXED) return fail(h, BD_ERR_ARG, "bad precision %d", prec);
@@ -902,6 +904,7 @@ int bd_eval_forces(BdHandle* h, int64_t n, const double* cen, const double* rot,
 
 int bd_eval_forces_atoms(BdHandle* h, int64_t n, const double* pos, const double* R, const double* cen, double* F,
                          double* T, double* E, int prec, int torque, void* stream) {
+  bd::NvtxRange nvtx("bd_eval_forces_atoms");
   if (!h) return BD_ERR_ARG;
   if (n < 0 || (n > 0 && (!pos || !R || !cen || !F || !T || !E)))
     return fail(h, BD_ERR_ARG, "bd_eval_forces_atoms: bad arguments");
@@ -920,6 +923,7 @@ int bd_eval_forces_atoms(BdHandle* h, int64_t n, const double* pos, const double
 }
 
 int bd_eval_overlap(BdHandle* h, int64_t n, const double* cen, int8_t* out, void* stream) {
+  bd::NvtxRange nvtx("bd_eval_overlap");
   if (!h) return BD_ERR_ARG;
   if (n < 0 || (n > 0 && (!cen || !out))) return fail(h, BD_ERR_ARG, "bd_eval_overlap: bad arguments");
   int rc = finalize(h);
@@ -1072,6 +1076,7 @@ int bd_get_launch(BdHandle* h, int* group, int* block, int* grid) {
 }
 
 int bd_sim_configure(BdHandle* h, const BdSimParams* p) {
+  bd::NvtxRange nvtx("bd_sim_configure");
   if (!h || !p) return fail(h, BD_ERR_ARG, "bd_sim_configure: NULL");
   if (p->n_traj <= 0 || p->n_traj > 0x7ffffff0ll) return fail(h, BD_ERR_ARG, "n_traj out of range");
   if (p->id_offset < 0) return fail(h, BD_ERR_ARG, "id_offset must be >= 0");
@@ -1194,6 +1199,7 @@ int bd_sim_configure(BdHandle* h, const BdSimParams* p) {
 }
 
 int bd_sim_reset(BdHandle* h, void* stream) {
+  bd::NvtxRange nvtx("bd_sim_reset");
   if (!h) return BD_ERR_ARG;
   if (!h->sim_ready) return fail(h, BD_ERR_STATE, "bd_sim_reset before bd_sim_configure");
   int rc = finalize(h);
@@ -1444,6 +1450,7 @@ int build_graphs(BdHandle* h, int K) {
 }  // namespace
 
 int bd_sim_run(BdHandle* h, int n_launch, int K, void* stream) {
+  bd::NvtxRange nvtx("bd_sim_run");
   if (!h) return BD_ERR_ARG;
   if (!h->sim_ready) return fail(h, BD_ERR_STATE, "bd_sim_run before bd_sim_configure");
   if (n_launch < 0 || K <= 0) return fail(h, BD_ERR_ARG, "bd_sim_run: n_launch >= 0 and steps > 0 needed");
@@ -1987,6 +1994,7 @@ int bd_multi_last_error(const BdMulti* m, char* buf, int len) {
 }
 
 int bd_multi_reset(BdMulti* m, void* stream) {
+  bd::NvtxRange nvtx("bd_multi_reset");
   if (!m) return BD_ERR_ARG;
   MCK(m, cudaSetDevice(m->device));
   cudaStream_t s = (cudaStream_t)stream;
@@ -2009,6 +2017,7 @@ int bd_multi_reset(BdMulti* m, void* stream) {
 }
 
 int bd_multi_run(BdMulti* m, int n_launch, int K, void* stream) {
+  bd::NvtxRange nvtx("bd_multi_run");
   if (!m) return BD_ERR_ARG;
   if (n_launch < 0 || K <= 0) return mfail(m, BD_ERR_ARG, "bd_multi_run: n_launch >= 0 and steps > 0 needed");
   MCK(m, cudaSetDevice(m->device));

@@ -28,6 +28,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include "bd_nvtx.cuh"
 #include "pystarc_b200.h"
 
 typedef __nv_bfloat16 bf16;
@@ -1403,6 +1404,7 @@ int bd_mlp_set_params(BdMlp* m, int member, const float* params) {
 }
 
 int bd_mlp_forward(BdMlp* m, int member, int64_t n, const float* X, float* Y, void* stream) {
+  bd::NvtxRange nvtx("bd_mlp_forward");
   int rc = check_member(m, member);
   if (rc) return rc;
   if (n < 0 || (n > 0 && (!X || !Y))) return mfail(m, BD_ERR_ARG, "bd_mlp_forward: bad arguments");
@@ -1445,6 +1447,7 @@ int bd_mlp_train_step(BdMlp* m, int member, int n, const float* X, const float* 
 
 int bd_mlp_train(BdMlp* m, int member, int64_t n_data, const float* X, const float* T, int batch, int steps,
                  float lr, uint64_t seed, float* loss_trace, void* stream) {
+  bd::NvtxRange nvtx("bd_mlp_train");
   int rc = check_member(m, member);
   if (rc) return rc;
   if (n_data <= 0 || !X || !T || batch <= 0 || batch % 32 || steps < 0 || !(lr > 0))
@@ -1527,6 +1530,7 @@ int bd_mlp_set_gemm(BdMlp* m, int mode) {
 }
 
 int bd_mlp_ensemble(BdMlp* m, int64_t n, const float* X, float* mean, float* spread, void* stream) {
+  bd::NvtxRange nvtx("bd_mlp_ensemble");
   if (!m) return BD_ERR_ARG;
   MCK(m, cudaSetDevice(m->device));
   if (n < 0 || (n > 0 && (!X || !mean))) return mfail(m, BD_ERR_ARG, "bd_mlp_ensemble: bad arguments");
