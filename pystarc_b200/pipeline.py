@@ -24,6 +24,12 @@ It does steps 5-6 with ``B200ForceEngine`` and ``B200BatchSimulator``:
                             output files of output_writer.write_all (:15-304),
                             written by ``pystarc_b200.output``
 
+Engine-only options may sit in a ``<b200>`` block of the same file, which the
+reference's parser ignores: ``precision`` (fp64 | mixed), ``torque_mode`` (zero |
+centroid), ``hi_mode`` (reference_gpu | zuk), ``termination`` (reference |
+complete), ``steps_per_launch``, ``launches_per_poll``, ``slots``, ``device``,
+``layout`` and ``verbose``.  An unknown key or value is an error.
+
 Usage: ``python -m pystarc_b200.pipeline input.xml``.
 """
 
@@ -65,6 +71,14 @@ _FIELDS = [
 _OUTPUT_FLAGS = ["results_json", "trajectories_csv", "encounters_csv", "near_misses_csv", "full_paths",
                  "radial_density", "angular_map", "fpt_distribution", "contact_frequency", "milestone_flux",
                  "p_commit", "transition_matrix", "energetics", "pose_clusters"]
+# engine-only keys of an optional <b200> block (no reference counterpart; the reference's tags stay as
+# they are): tag -> (cast, allowed values or None)
+_B200_KEYS = {
+    "precision": (str, ("fp64", "mixed")), "torque_mode": (str, ("zero", "centroid")),
+    "hi_mode": (str, ("reference_gpu", "zuk")), "termination": (str, ("reference", "complete")),
+    "steps_per_launch": (int, None), "launches_per_poll": (int, None), "slots": (int, None),
+    "device": (int, None), "layout": (int, None), "verbose": (bool, None),
+}
 
 
 @dataclass
@@ -95,6 +109,7 @@ class RunConfig:
     values: dict
     outputs: OutputConfig = field(default_factory=OutputConfig)
     xml_dir: Path = Path(".")
+    b200: dict = field(default_factory=dict)  # the keys the <b200> block sets
 
     def __getattr__(self, name):
         try:
@@ -134,12 +149,27 @@ def parse_input(xml_path) -> RunConfig:
             setattr(outputs, flag, _cast(None if el is None else el.text, True, bool))
         el = out_el.find("save_interval")
         outputs.save_interval = _cast(None if el is None else el.text, 10, int)
+    b200 = {}
+    b_el = root.find("b200")
+    if b_el is not None:
+        for child in b_el:
+            if child.tag not in _B200_KEYS:
+                raise ValueError(f"<b200>: unknown key <{child.tag}>; known: {', '.join(sorted(_B200_KEYS))}")
+            cast, allowed = _B200_KEYS[child.tag]
+            try:
+                v = _cast(child.text, None, cast)
+            except ValueError:
+                raise ValueError(f"<b200><{child.tag}>: {child.text!r} is not an integer") from None
+            if v is None or (allowed is not None and v not in allowed):
+                raise ValueError(f"<b200><{child.tag}>: {child.text!r} is not one of {allowed}" if allowed else
+                                 f"<b200><{child.tag}>: no value")
+            b200[child.tag] = v
     has_pqrs = bool(vals["receptor_pqr"] and vals["ligand_pqr"])
     if not has_pqrs and vals["pdb"] is None:
         raise ValueError("Either <pdb> or both <receptor_pqr> and <ligand_pqr> must be specified")
     if vals["n_trajectories"] < 1:
         raise ValueError("n_trajectories must be >= 1")
-    return RunConfig(vals, outputs, xml_path.resolve().parent)
+    return RunConfig(vals, outputs, xml_path.resolve().parent, b200)
 
 
 # ----------------------------------------------------------------------------
@@ -440,12 +470,26 @@ class Prepared:
     D_rel: float
 
 
-def build(xml_path, *, precision="fp64", torque_mode="zero", device=0, **sim_options) -> Prepared:
-    """Engine and stepper for ``input.xml`` from its prepared work directory (pipeline.py:292-351)."""
+def engine_options(cfg: RunConfig, **explicit) -> dict:
+    """Engine and stepper options of a run: keyword arguments given (not None) first, then the
+    input file's <b200> block, then the defaults (FP64, zero torque, device 0)."""
+    opts = {"precision": "fp64", "torque_mode": "zero", "device": 0}
+    opts.update(cfg.b200)
+    opts.update({k: v for k, v in explicit.items() if v is not None})
+    return opts
+
+
+def build(xml_path, *, precision=None, torque_mode=None, device=None, **sim_options) -> Prepared:
+    """Engine and stepper for ``input.xml`` from its prepared work directory (pipeline.py:292-351).
+    Options come from the keyword arguments, else from the file's <b200> block (``engine_options``)."""
     from .engine import B200ForceEngine
     from .simulator import B200BatchSimulator
 
     cfg = parse_input(xml_path)
+    opts = engine_options(cfg, precision=precision, torque_mode=torque_mode, device=device, **sim_options)
+    precision, torque_mode, device = opts.pop("precision"), opts.pop("torque_mode"), opts.pop("device")
+    layout = opts.pop("layout", None)
+    sim_options = opts
     W = cfg.work_path
     mol_rec, mol_lig = prepare_molecules(cfg)
     rec_atoms, lig_atoms = read_pqr(W / "receptor.pqr"), read_pqr(W / "ligand.pqr")
@@ -473,7 +517,7 @@ def build(xml_path, *, precision="fp64", torque_mode="zero", device=0, **sim_opt
                              rec_charges=mol_rec.charges_array(), multipole_expansion=mp,
                              rec_radii=mol_rec.radii_array() if cfg.lj_forces else None,
                              lig_radii=mol_lig.radii_array() if cfg.lj_forces else None, use_lj=cfg.lj_forces,
-                             precision=precision, torque_mode=torque_mode, device=device)
+                             precision=precision, torque_mode=torque_mode, device=device, layout=layout)
     params._output_cfg = cfg.outputs
     params.max_dt = cfg.max_dt
     params.checkpoint_interval = cfg.checkpoint_interval
@@ -507,7 +551,9 @@ def main(argv=None):
     if not argv or argv[0] in ("-h", "--help"):
         print(__doc__)
         return 0
-    prep, result = run(argv[0], verbose=True)  # the reference's console reports while the BD stage runs
+    # the reference's console reports while the BD stage runs, unless the <b200> block says otherwise
+    extra = {} if "verbose" in parse_input(argv[0]).b200 else {"verbose": True}
+    prep, result = run(argv[0], **extra)
     print(result.summary(prep.D_rel, prep.simulator._k_b, prep.cfg.confidence_interval))
     return 0
 

@@ -170,3 +170,29 @@ def test_missing_grids_or_radii_name_the_missing_step(tmp_path):
 def test_main_prints_usage(capsys):
     assert pl.main(["--help"]) == 0
     assert "input.xml" in capsys.readouterr().out
+
+
+def test_b200_block_sets_engine_options(tmp_path):
+    """Engine-only keys in a <b200> block; keyword arguments override them, unknown keys and values fail."""
+    xml = (PIPE / "input.xml").read_text()
+    close = xml.rstrip().rsplit("</", 1)
+    block = ("<b200><precision>mixed</precision><hi_mode>zuk</hi_mode><steps_per_launch>32</steps_per_launch>"
+             "<verbose>false</verbose><layout>58</layout></b200>")
+    p = tmp_path / "input.xml"
+    p.write_text(close[0] + block + "</" + close[1])
+    cfg = pl.parse_input(p)
+    assert cfg.b200 == {"precision": "mixed", "hi_mode": "zuk", "steps_per_launch": 32, "verbose": False,
+                        "layout": 58}
+    assert cfg.n_trajectories == pl.parse_input(PIPE / "input.xml").n_trajectories  # reference tags unchanged
+    opts = pl.engine_options(cfg, precision=None, termination="complete")
+    assert opts == {"precision": "mixed", "torque_mode": "zero", "device": 0, "hi_mode": "zuk",
+                    "steps_per_launch": 32, "verbose": False, "layout": 58, "termination": "complete"}
+    assert pl.engine_options(cfg, precision="fp64")["precision"] == "fp64"
+    assert pl.engine_options(pl.parse_input(PIPE / "input.xml")) == {"precision": "fp64", "torque_mode": "zero",
+                                                                    "device": 0}
+    for bad, msg in (("<b200><precision>half</precision></b200>", "not one of"),
+                     ("<b200><warp_size>64</warp_size></b200>", "unknown key"),
+                     ("<b200><slots>many</slots></b200>", "not an integer")):
+        p.write_text(close[0] + bad + "</" + close[1])
+        with pytest.raises(ValueError, match=msg):
+            pl.parse_input(p)
