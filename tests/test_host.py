@@ -135,3 +135,24 @@ def test_nan_grid_rejected(tmp_path):
     g.write(tmp_path / "n.dx")
     with pytest.raises(ValueError):
         DXGrid.from_file(tmp_path / "n.dx")
+
+
+def test_reference_known_answers_on_the_host_physics():
+    """The reference suite's known answers (tests/test_pystarc.py) on this package's host physics:
+    Romberg integrals (:4290-4307), CONV (:4322-4325), Wilson bounds at small P (:5318-5330)."""
+    for n in range(6):
+        assert abs(hostphys.romberg(lambda x, n=n: x ** n, 0.0, 1.0) - 1.0 / (n + 1)) < 1e-8
+    assert abs(hostphys.romberg(math.sin, 0.0, math.pi) - 2.0) < 1e-8
+    assert abs(hostphys.CONV - 6.022e8) / 6.022e8 < 1e-12
+    for nr, ne in ((50, 950), (2, 998), (0, 1000), (1000, 0)):
+        r = B200BatchResult(nr + ne, nr, ne, 0, {}, 50.0, 100.0, 0.2, 1.0, 1.0)
+        lo, hi = r.reaction_probability_ci()
+        assert 0.0 <= lo and hi <= 1.0 + 1e-15  # the bounds the reference tests
+        if 0 < nr < nr + ne:
+            assert lo < r.reaction_probability < hi
+    # k_b of two +-1 e spheres at b = 10 A (:4246-4249) and its k_on(P) table (:4333-4341) without the
+    # return-probability correction
+    _, kb = hostphys.return_prob_and_kb(10.0, 20.1, 1.0, -1.0, 7.828, 0.43371)
+    assert abs(kb - 57.5) < 1.0
+    for P, k in ((0.1, 3.46e9), (0.2, 6.93e9), (0.3, 1.04e10), (0.4, 1.39e10), (0.5, 1.73e10)):
+        assert abs(hostphys.CONV * 57.5 * P - k) / k < 0.02
