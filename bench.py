@@ -793,29 +793,11 @@ def main():
                                          (launch["group"], launch["block"]), aged=aged)
     _OPTS["layout"] = layout_cli
     _progress(f"e2e arm: {e2e_val:.3e} steps/s")
-    t_max = t_mixed
-    steps_all = d_mixed["steps"]
+    t_max, steps_all, pooled_tallies = t_mixed, d_mixed["steps"], None
     if dist is not None:
-        tt = torch.tensor([t_mixed], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
-        st = torch.tensor([steps_all], device="cuda", dtype=torch.int64)
-        dist.all_reduce(st)
-        steps_all = int(st.item())
-        # the outcome tallies of the timed window, summed over the ranks (the one data collective)
-        from pystarc_b200.shard import allreduce_tallies
-
-        pooled_tallies = allreduce_tallies(d_mixed, device=torch.device("cuda", local))
-        # the end-to-end arm for the whole job: steps and copied bytes summed, time the slowest rank's
-        et = torch.tensor([e2e_res.e2e_seconds], device="cuda", dtype=torch.float64)
-        dist.all_reduce(et, op=dist.ReduceOp.MAX)
-        eb = torch.tensor([e2e_res.e2e_steps, int(h2d), int(d2h)], device="cuda", dtype=torch.int64)
-        dist.all_reduce(eb)
-        e2e_val = int(eb[0].item()) / float(et.item())
-        h2d, d2h = int(eb[1].item()), int(eb[2].item())
+        t_max, steps_all, pooled_tallies, e2e_val, h2d, d2h = pool_over_ranks(
+            dist, torch.device("cuda", local), t_mixed, d_mixed, e2e_res.e2e_seconds, e2e_res.e2e_steps, h2d, d2h)
     value = steps_all / t_max
-    if dist is None:
-        pooled_tallies = None
     peak, peak_kind = peaks()
     gathers = d_mixed["grid_evals"] + d_mixed["rev_evals"]
     algo_bytes = gathers * ALGO_BYTES_PER_GATHER + d_mixed["steps"] * STATE_BYTES_PER_STEP
@@ -892,6 +874,25 @@ def main():
     shutil.rmtree(work, ignore_errors=True)
     if dist is not None:
         dist.destroy_process_group()
+
+
+def pool_over_ranks(dist, device, t_local, counters, e2e_seconds, e2e_steps, h2d, d2h):
+    """The whole job's figures under torchrun, the same collectives in the same order on every rank:
+    the timed window's time (max over ranks) and BD steps (sum), the outcome tallies (sum, the one
+    data collective), and the end-to-end arm's steps and copied bytes (sum) over its slowest rank's
+    time.  Returns (t_max, steps, tallies, e2e_value, h2d_bytes, d2h_bytes)."""
+    import torch
+
+    from pystarc_b200.shard import allreduce_tallies
+
+    tt = torch.tensor([t_local, e2e_seconds], device=device, dtype=torch.float64)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    st = torch.tensor([counters["steps"], e2e_steps, int(h2d), int(d2h)], device=device, dtype=torch.int64)
+    dist.all_reduce(st)
+    tallies = allreduce_tallies(counters, device=device)
+    t_max, e2e_t = float(tt[0].item()), float(tt[1].item())
+    steps, e2e_steps_all, h2d_all, d2h_all = (int(v) for v in st.cpu())
+    return t_max, steps, tallies, e2e_steps_all / e2e_t, h2d_all, d2h_all
 
 
 def cupy_reference():

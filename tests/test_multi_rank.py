@@ -220,3 +220,36 @@ def test_simulator_run_shards_and_pools_over_two_ranks():
     expect[(expect != 1) & (expect != 2)] = 0
     np.testing.assert_array_equal(outcome, expect)
     np.testing.assert_array_equal(np.array(results[0][8] + results[1][8]), single.n_steps)
+
+
+def _bench_pool_worker(rank, world, port, out):
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        import bench
+
+        counters = {k: 10 * (rank + 1) + i for i, k in enumerate(TALLY_KEYS)}
+        counters["steps"] = 1000 * (rank + 1)
+        out[rank] = bench.pool_over_ranks(dist, None, 2.0 + rank, counters, e2e_seconds=5.0 - rank,
+                                          e2e_steps=300 * (rank + 1), h2d=7 + rank, d2h=11 + rank)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_bench_pools_time_steps_tallies_and_e2e_over_two_ranks():
+    """bench.py under torchrun: time is the slowest rank's, steps, tallies and copied bytes are summed,
+    and the end-to-end rate is the summed steps over the slowest rank's end-to-end time."""
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as mgr:
+        out = mgr.dict()
+        mp.start_processes(_bench_pool_worker, args=(2, _free_port(), out), nprocs=2, join=True,
+                           start_method="spawn")
+        res = dict(out)
+    t_max, steps, tallies, e2e, h2d, d2h = res[0]
+    assert res[0] == res[1]
+    assert t_max == 3.0 and steps == 3000
+    assert tallies["steps"] == 3000 and tallies["reacted"] == (10 + 1) + (20 + 1)
+    assert e2e == 900 / 5.0 and (h2d, d2h) == (15, 23)
