@@ -114,6 +114,13 @@ class ProgressLog:
     def _k(self, p):
         return self.CONV * self.k_b * p if self.k_b > 0 else 0
 
+    def start(self, max_steps, D_t, dt, dt_rxn, return_prob, r_escape):
+        """The run's opening lines (gpu_batch_simulator.py:486-505)."""
+        self.out(f"  B200 batch BD: {self.n:,} trajectories x up to {int(max_steps):,} steps")
+        self.out(f"  D_rel={D_t:.5f} A2/ps  dt={dt}ps  dt_rxn={dt_rxn}ps")
+        self.out(f"  Outer propagator (LMZ): return_prob={return_prob:.4f}  (applied at r_esc={r_escape:.1f}Å)  "
+                 f"k_b={self.k_b:.4f} Å³/ps")
+
     def poll(self, done, reacted, escaped, now=None):
         now = time.perf_counter() if now is None else now
         crossed = [m for m in self.marks if self.last_mark < m <= done]
@@ -661,6 +668,10 @@ class B200BatchSimulator:
         next_stall, stall_done = self.STALL_STEPS, 0
         self.stall_stopped = False
         log = ProgressLog(N, self._k_b, getattr(self.params, "convergence_interval", 10), t0) if self.verbose else None
+        if log is not None:
+            p = self.params
+            log.start(p.max_steps, float(self.mob.relative_translational_diffusion()), getattr(p, "dt", None),
+                      getattr(p, "dt_rxn", None), self._return_prob, float(p.r_escape))
         while True:
             h.call("bd_sim_run", self.M, self.K, None)
             launches += self.M

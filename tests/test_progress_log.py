@@ -48,6 +48,8 @@ def test_verbose_run_prints_the_reports(capsys):
                              _FakeEngine(s), termination="complete", verbose=True)
     res = sim.run()
     out = capsys.readouterr().out
+    assert out.startswith("  B200 batch BD: 64 trajectories x up to 5,000 steps\n  D_rel=")
+    assert f"return_prob={sim._return_prob:.4f}" in out and f"k_b={sim._k_b:.4f}" in out
     assert f"  BD complete: {res.n_reacted} reacted, {res.n_escaped} escaped, {res.n_max_steps} max-steps" in out
     assert f"  Total steps: {res.total_steps:,}" in out
     assert f"  Final: P_rxn={res.reaction_probability:.6f}" in out
